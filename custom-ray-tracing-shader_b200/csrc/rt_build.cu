@@ -1,0 +1,556 @@
+// GPU BVH construction.
+//
+// Stage 1, binned SAH (level-synchronous, all nodes of one depth per pass).
+// The split rules are the reference's (Native/bvh.cuh:35-105), evaluated with
+// the same floating-point expressions so every decision matches:
+//   - primitive box padded by 1e-5 + 1e-6 * max|coord| per axis, centroid
+//     (a + b + c) / 3 of the unpadded corners (bvh.cuh:38-48);
+//   - leaf when count <= 4 or depth == 32 (bvh.cuh:64);
+//   - 12 centroid bins per axis, axes with centroid extent <= 1e-12 skipped,
+//     bin = min(11, max(0, int((c - min) * (12 / extent)))) (bvh.cuh:53-76);
+//   - split cost A(node) + A(L) nL + A(R) nR against leaf cost A(node) n,
+//     strict "<" so the first minimum in (axis, bin) order wins (bvh.cuh:66-91);
+//   - partition by bin <= best (bvh.cuh:94-98).
+// Binning and box unions are min/max/counts, which are order independent, so
+// the tree (node boxes, ranges, counts, depth) equals the reference's. The
+// partition here is stable (prefix sums) where the reference uses
+// std::partition, so only the order of triangles inside a leaf can differ.
+// A final pass renumbers nodes into the reference's depth-first numbering
+// (children allocated in pairs when their parent splits), so the node array
+// is the reference's node array.
+//
+// Stage 2, collapse into 8-wide compressed nodes: each wide node greedily
+// opens its largest-area interior descendant while the children still fit in
+// eight slots; leaves become groups of up to three triangles. Children are
+// assigned to slots by ray octant and quantised outward to 8 bits per plane.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "rt_build.cuh"
+#include "rt_collapse.cuh"
+
+namespace rt {
+namespace {
+
+constexpr int kBins = 12;          // bvh.cuh:29
+constexpr int kLeafSize = 4;       // bvh.cuh:64
+constexpr int kScanBlock = 1024;   // elements per scan block
+constexpr int kBinBlock = 256;
+constexpr int kBinPer = 8;         // positions per thread in the binning pass
+
+struct Task {
+    int node, first, count, depth;
+    float lo[3], hi[3], clo[3], chi[3];
+};
+struct BinAcc { unsigned count; float lo[3], hi[3], clo[3], chi[3]; };
+struct Split { int axis, bin, leftCount, childTask[2]; };
+
+__device__ __forceinline__ void atomicMinFloat(float* a, float v) {
+    if (v >= 0.0f) atomicMin(reinterpret_cast<int*>(a), __float_as_int(v));
+    else atomicMax(reinterpret_cast<unsigned*>(a), __float_as_uint(v));
+}
+__device__ __forceinline__ void atomicMaxFloat(float* a, float v) {
+    if (v >= 0.0f) atomicMax(reinterpret_cast<int*>(a), __float_as_int(v));
+    else atomicMin(reinterpret_cast<unsigned*>(a), __float_as_uint(v));
+}
+RT_HD int binOf(float c, float lo, float s) {
+    int b = (int)((c - lo) * s);
+    return b < 0 ? 0 : (b > kBins - 1 ? kBins - 1 : b);
+}
+// Half surface area with the reference's expression (bvh.cuh:20-23).
+RT_HD float halfArea(const float lo[3], const float hi[3]) {
+    float x = fmaxf(0.0f, hi[0] - lo[0]), y = fmaxf(0.0f, hi[1] - lo[1]), z = fmaxf(0.0f, hi[2] - lo[2]);
+    return x * y + x * z + y * z;
+}
+__device__ __forceinline__ void growBox(float lo[3], float hi[3], const float olo[3], const float ohi[3]) {
+    for (int a = 0; a < 3; a++) { lo[a] = fminf(lo[a], olo[a]); hi[a] = fmaxf(hi[a], ohi[a]); }
+}
+
+// ---- primitive boxes and root bounds ----
+__global__ void primBoxesKernel(const SceneTri* tris, int n, float4* plo, float4* phi, float4* cent, Task* root) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    float v[12];
+    for (int k = 0; k < 3; k++) { v[k] = FLT_MAX; v[3 + k] = -FLT_MAX; v[6 + k] = FLT_MAX; v[9 + k] = -FLT_MAX; }
+    if (i < n) {
+        const SceneTri& t = tris[i];
+        float3 o = t.origin;
+        float3 b = v3(o.x + t.edge1.x, o.y + t.edge1.y, o.z + t.edge1.z);
+        float3 c = v3(o.x + t.edge2.x, o.y + t.edge2.y, o.z + t.edge2.z);
+        float lo[3], hi[3], ce[3];
+        for (int a = 0; a < 3; a++) {
+            float oa = comp(o, a), ba = comp(b, a), ca = comp(c, a);
+            lo[a] = fminf(fminf(fminf(FLT_MAX, oa), ba), ca);
+            hi[a] = fmaxf(fmaxf(fmaxf(-FLT_MAX, oa), ba), ca);
+            ce[a] = (oa + ba + ca) / 3.0f;
+            float pad = 1e-5f + 1e-6f * fmaxf(fabsf(lo[a]), fabsf(hi[a]));
+            lo[a] -= pad; hi[a] += pad;
+        }
+        plo[i] = make_float4(lo[0], lo[1], lo[2], 0.0f);
+        phi[i] = make_float4(hi[0], hi[1], hi[2], 0.0f);
+        cent[i] = make_float4(ce[0], ce[1], ce[2], 0.0f);
+        for (int k = 0; k < 3; k++) { v[k] = lo[k]; v[3 + k] = hi[k]; v[6 + k] = ce[k]; v[9 + k] = ce[k]; }
+    }
+    for (int off = 16; off > 0; off >>= 1)
+        for (int k = 0; k < 12; k++) {
+            float o = __shfl_xor_sync(0xFFFFFFFFu, v[k], off);
+            v[k] = ((k / 3) & 1) ? fmaxf(v[k], o) : fminf(v[k], o);
+        }
+    if ((threadIdx.x & 31) == 0) {
+        for (int k = 0; k < 3; k++) {
+            atomicMinFloat(&root->lo[k], v[k]); atomicMaxFloat(&root->hi[k], v[3 + k]);
+            atomicMinFloat(&root->clo[k], v[6 + k]); atomicMaxFloat(&root->chi[k], v[9 + k]);
+        }
+    }
+}
+
+__global__ void iotaKernel(int* a, int n, int value0, int* b, int bValue) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) { a[i] = i + value0; if (b) b[i] = bValue; }
+}
+
+__global__ void clearBinsKernel(BinAcc* bins, int count) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    BinAcc& b = bins[i];
+    b.count = 0;
+    for (int a = 0; a < 3; a++) { b.lo[a] = FLT_MAX; b.hi[a] = -FLT_MAX; b.clo[a] = FLT_MAX; b.chi[a] = -FLT_MAX; }
+}
+
+__device__ __forceinline__ void accumulateBin(BinAcc* dst, float4 lo, float4 hi, float4 c) {
+    atomicAdd(&dst->count, 1u);
+    atomicMinFloat(&dst->lo[0], lo.x); atomicMinFloat(&dst->lo[1], lo.y); atomicMinFloat(&dst->lo[2], lo.z);
+    atomicMaxFloat(&dst->hi[0], hi.x); atomicMaxFloat(&dst->hi[1], hi.y); atomicMaxFloat(&dst->hi[2], hi.z);
+    atomicMinFloat(&dst->clo[0], c.x); atomicMinFloat(&dst->clo[1], c.y); atomicMinFloat(&dst->clo[2], c.z);
+    atomicMaxFloat(&dst->chi[0], c.x); atomicMaxFloat(&dst->chi[1], c.y); atomicMaxFloat(&dst->chi[2], c.z);
+}
+
+// Bins every primitive of every open task. The task owning the first position
+// of a block's chunk is aggregated in shared memory; others go to global bins.
+__global__ void __launch_bounds__(kBinBlock) binKernel(const int* order, const int* posTask, const float4* cent,
+                                                       const float4* plo, const float4* phi, const Task* tasks,
+                                                       int nPos, BinAcc* bins) {
+    __shared__ BinAcc sb[3 * kBins];
+    __shared__ int sTask;
+    int base = blockIdx.x * kBinBlock * kBinPer;
+    if (threadIdx.x == 0) sTask = base < nPos ? posTask[base] : -1;
+    if (threadIdx.x < 3 * kBins) {
+        BinAcc& b = sb[threadIdx.x];
+        b.count = 0;
+        for (int a = 0; a < 3; a++) { b.lo[a] = FLT_MAX; b.hi[a] = -FLT_MAX; b.clo[a] = FLT_MAX; b.chi[a] = -FLT_MAX; }
+    }
+    __syncthreads();
+    int st = sTask;
+    for (int k = 0; k < kBinPer; k++) {
+        int j = base + k * kBinBlock + threadIdx.x;
+        if (j >= nPos) break;
+        int t = posTask[j];
+        if (t < 0) continue;
+        int prim = order[j];
+        float4 c = cent[prim], lo = plo[prim], hi = phi[prim];
+        const Task& T = tasks[t];
+        for (int a = 0; a < 3; a++) {
+            float extent = T.chi[a] - T.clo[a];
+            if (extent <= 1e-12f) continue;
+            float s = kBins / extent;
+            float ca = a == 0 ? c.x : (a == 1 ? c.y : c.z);
+            int b = binOf(ca, T.clo[a], s);
+            BinAcc* dst = t == st ? &sb[a * kBins + b] : &bins[((size_t)t * 3 + a) * kBins + b];
+            accumulateBin(dst, lo, hi, c);
+        }
+    }
+    __syncthreads();
+    if (st >= 0 && threadIdx.x < 3 * kBins) {
+        const BinAcc& s = sb[threadIdx.x];
+        if (s.count) {
+            BinAcc* d = &bins[(size_t)st * 3 * kBins + threadIdx.x];
+            atomicAdd(&d->count, s.count);
+            for (int a = 0; a < 3; a++) {
+                atomicMinFloat(&d->lo[a], s.lo[a]); atomicMaxFloat(&d->hi[a], s.hi[a]);
+                atomicMinFloat(&d->clo[a], s.clo[a]); atomicMaxFloat(&d->chi[a], s.chi[a]);
+            }
+        }
+    }
+}
+
+// One thread per open task: the reference's SAH sweep, then node records.
+__global__ void splitKernel(const Task* tasks, int nTasks, const BinAcc* bins, Split* splits, BinNode* nodes,
+                            int* counters /*0 nodes,1 next tasks,2 max depth,3 error*/, Task* nextTasks,
+                            int nodeCapacity, int taskCapacity) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nTasks) return;
+    const Task T = tasks[t];
+    atomicMax(&counters[2], T.depth);
+    int bestAxis = -1, bestBin = -1;
+    float nodeArea = halfArea(T.lo, T.hi);
+    float bestCost = nodeArea * T.count;
+    if (T.count > kLeafSize && T.depth != kBinaryMaxDepth) {
+        for (int a = 0; a < 3; a++) {
+            float extent = T.chi[a] - T.clo[a];
+            if (extent <= 1e-12f) continue;
+            const BinAcc* B = &bins[((size_t)t * 3 + a) * kBins];
+            float sufLo[kBins][3], sufHi[kBins][3];
+            int sufN[kBins];
+            float accLo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, accHi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+            int accN = 0;
+            for (int b = kBins - 1; b >= 0; b--) {
+                if (B[b].count) growBox(accLo, accHi, B[b].lo, B[b].hi);
+                accN += (int)B[b].count;
+                for (int k = 0; k < 3; k++) { sufLo[b][k] = accLo[k]; sufHi[b][k] = accHi[k]; }
+                sufN[b] = accN;
+            }
+            float preLo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, preHi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+            int preN = 0;
+            for (int b = 0; b < kBins - 1; b++) {
+                if (B[b].count) growBox(preLo, preHi, B[b].lo, B[b].hi);
+                preN += (int)B[b].count;
+                if (!preN || !sufN[b + 1]) continue;
+                float cost = nodeArea + halfArea(preLo, preHi) * preN + halfArea(sufLo[b + 1], sufHi[b + 1]) * sufN[b + 1];
+                if (cost < bestCost) { bestCost = cost; bestAxis = a; bestBin = b; }
+            }
+        }
+    }
+    Split S;
+    S.axis = bestAxis; S.bin = bestBin; S.leftCount = 0; S.childTask[0] = S.childTask[1] = -1;
+    if (bestAxis < 0) {
+        nodes[T.node] = BinNode{v3(T.lo[0], T.lo[1], T.lo[2]), T.first, v3(T.hi[0], T.hi[1], T.hi[2]), T.count};
+        splits[t] = S;
+        return;
+    }
+    // Children's boxes, centroid boxes and counts are unions over the bins.
+    Task C[2];
+    for (int side = 0; side < 2; side++) {
+        for (int k = 0; k < 3; k++) { C[side].lo[k] = C[side].clo[k] = FLT_MAX; C[side].hi[k] = C[side].chi[k] = -FLT_MAX; }
+        C[side].count = 0;
+    }
+    const BinAcc* B = &bins[((size_t)t * 3 + bestAxis) * kBins];
+    for (int b = 0; b < kBins; b++) {
+        if (!B[b].count) continue;
+        Task& c = C[b <= bestBin ? 0 : 1];
+        growBox(c.lo, c.hi, B[b].lo, B[b].hi);
+        growBox(c.clo, c.chi, B[b].clo, B[b].chi);
+        c.count += (int)B[b].count;
+    }
+    int child = atomicAdd(&counters[0], 2);
+    if (child + 2 > nodeCapacity) { atomicExch(&counters[3], 1); splits[t] = Split{-1, -1, 0, {-1, -1}}; return; }
+    nodes[T.node] = BinNode{v3(T.lo[0], T.lo[1], T.lo[2]), child, v3(T.hi[0], T.hi[1], T.hi[2]), 0};
+    C[0].first = T.first;
+    C[1].first = T.first + C[0].count;
+    S.leftCount = C[0].count;
+    for (int side = 0; side < 2; side++) {
+        Task& c = C[side];
+        c.node = child + side;
+        c.depth = T.depth + 1;
+        atomicMax(&counters[2], c.depth);
+        if (c.count <= kLeafSize || c.depth == kBinaryMaxDepth) {
+            nodes[c.node] = BinNode{v3(c.lo[0], c.lo[1], c.lo[2]), c.first, v3(c.hi[0], c.hi[1], c.hi[2]), c.count};
+        } else {
+            int k = atomicAdd(&counters[1], 1);
+            if (k >= taskCapacity) { atomicExch(&counters[3], 2); continue; }
+            nextTasks[k] = c;
+            S.childTask[side] = k;
+        }
+    }
+    splits[t] = S;
+}
+
+__global__ void flagKernel(const int* order, const int* posTask, const float4* cent, const Task* tasks,
+                           const Split* splits, int nPos, unsigned* flags) {
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= nPos) return;
+    int t = posTask[j];
+    unsigned f = 0;
+    if (t >= 0) {
+        Split S = splits[t];
+        if (S.axis >= 0) {
+            const Task& T = tasks[t];
+            float lo = T.clo[S.axis];
+            float s = kBins / (T.chi[S.axis] - lo);
+            float4 c = cent[order[j]];
+            float ca = S.axis == 0 ? c.x : (S.axis == 1 ? c.y : c.z);
+            f = binOf(ca, lo, s) <= S.bin ? 1u : 0u;
+        }
+    }
+    flags[j] = f;
+}
+
+// Exclusive scan, phase 1: per-block scan in place, block totals out.
+__global__ void __launch_bounds__(256) scanBlocksKernel(unsigned* data, int n, unsigned* blockSums) {
+    __shared__ unsigned warpSums[8];
+    int base = blockIdx.x * kScanBlock;
+    unsigned v[4], local = 0;
+    for (int k = 0; k < 4; k++) {
+        int j = base + threadIdx.x * 4 + k;
+        v[k] = j < n ? data[j] : 0u;
+        local += v[k];
+    }
+    unsigned incl = local;
+    for (int off = 1; off < 32; off <<= 1) {
+        unsigned o = __shfl_up_sync(0xFFFFFFFFu, incl, off);
+        if ((threadIdx.x & 31) >= off) incl += o;
+    }
+    if ((threadIdx.x & 31) == 31) warpSums[threadIdx.x >> 5] = incl;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        unsigned w = threadIdx.x < 8 ? warpSums[threadIdx.x] : 0u, wi = w;
+        for (int off = 1; off < 8; off <<= 1) {
+            unsigned o = __shfl_up_sync(0xFFFFFFFFu, wi, off);
+            if (threadIdx.x >= off) wi += o;
+        }
+        if (threadIdx.x < 8) warpSums[threadIdx.x] = wi - w;
+        if (threadIdx.x == 7) blockSums[blockIdx.x] = wi;
+    }
+    __syncthreads();
+    unsigned run = warpSums[threadIdx.x >> 5] + incl - local;
+    for (int k = 0; k < 4; k++) {
+        int j = base + threadIdx.x * 4 + k;
+        if (j < n) data[j] = run;
+        run += v[k];
+    }
+}
+// Phase 2: one block scans the block totals (exclusive, in place).
+__global__ void __launch_bounds__(1024) scanTotalsKernel(unsigned* sums, int count) {
+    __shared__ unsigned carry;
+    __shared__ unsigned warpSums[32];
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < count; base += 1024) {
+        int j = base + threadIdx.x;
+        unsigned v = j < count ? sums[j] : 0u, incl = v;
+        for (int off = 1; off < 32; off <<= 1) {
+            unsigned o = __shfl_up_sync(0xFFFFFFFFu, incl, off);
+            if ((threadIdx.x & 31) >= off) incl += o;
+        }
+        if ((threadIdx.x & 31) == 31) warpSums[threadIdx.x >> 5] = incl;
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            unsigned w = warpSums[threadIdx.x], wi = w;
+            for (int off = 1; off < 32; off <<= 1) {
+                unsigned o = __shfl_up_sync(0xFFFFFFFFu, wi, off);
+                if (threadIdx.x >= off) wi += o;
+            }
+            warpSums[threadIdx.x] = wi - w;
+        }
+        __syncthreads();
+        unsigned excl = carry + warpSums[threadIdx.x >> 5] + incl - v;
+        if (j < count) sums[j] = excl;
+        __syncthreads();
+        if (threadIdx.x == 1023) carry = excl + v;
+        __syncthreads();
+    }
+}
+// Phase 3 is folded into the consumer: prefix(j) = data[j] + sums[j / kScanBlock].
+
+__global__ void scatterKernel(const int* order, const int* posTask, const Task* tasks, const Split* splits,
+                              const unsigned* flags, const unsigned* prefix, const unsigned* blockSums, int nPos,
+                              int* orderNext, int* posTaskNext, int* error) {
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= nPos) return;
+    int t = posTask[j];
+    int prim = order[j];
+    if (t < 0 || splits[t].axis < 0) { orderNext[j] = prim; posTaskNext[j] = -1; return; }
+    const Task& T = tasks[t];
+    Split S = splits[t];
+    unsigned pj = prefix[j] + blockSums[j / kScanBlock];
+    unsigned p0 = prefix[T.first] + blockSums[T.first / kScanBlock];
+    int leftRank = (int)(pj - p0);
+    bool left = flags[j] != 0u;
+    int dst = left ? T.first + leftRank : T.first + S.leftCount + ((j - T.first) - leftRank);
+    if (dst < T.first || dst >= T.first + T.count) { atomicExch(error, 5); return; }
+    orderNext[dst] = prim;
+    posTaskNext[dst] = S.childTask[left ? 0 : 1];
+}
+
+// ---- renumbering into the reference's depth-first numbering ----
+__global__ void subtreeInteriorKernel(const BinNode* nodes, int begin, int end, int* interior) {
+    int i = begin + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= end) return;
+    const BinNode& n = nodes[i];
+    interior[i] = n.count > 0 ? 0 : 1 + interior[n.first] + interior[n.first + 1];
+}
+__global__ void preorderKernel(const BinNode* nodes, int begin, int end, int count, const int* interior, int* rank,
+                               int* newIndex, int* error) {
+    int i = begin + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= end) return;
+    const BinNode& n = nodes[i];
+    if (n.count > 0) return;
+    int c = n.first, r = rank[i];
+    if (c < 1 || c + 1 >= count || r < 0 || 2 + 2 * r >= count) { atomicExch(error, 6); return; }
+    newIndex[c] = 1 + 2 * r;
+    newIndex[c + 1] = 2 + 2 * r;
+    rank[c] = r + 1;
+    rank[c + 1] = r + 1 + interior[c];
+}
+__global__ void renumberKernel(const BinNode* nodes, int count, const int* newIndex, BinNode* out, int* error) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    BinNode n = nodes[i];
+    if (n.count == 0) n.first = newIndex[n.first];
+    int dst = newIndex[i];
+    if (dst < 0 || dst >= count || (n.count == 0 && (n.first < 1 || n.first + 1 >= count))) { atomicExch(error, 7); return; }
+    out[dst] = n;
+}
+
+// ---- collapse into wide nodes (logic in rt_collapse.cuh) ----
+__global__ void collapseKernel(const BinNode* bn, const int* order, const float4* plo, const float4* phi,
+                               const SceneTri* tris, const Job* jobs, int nJobs, Job* nextJobs, WideNode* wide,
+                               float4* packed, int* counters, int wideCapacity, int jobCapacity, int triCapacity) {
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= nJobs) return;
+    collapseJob(jobs[j], bn, order, plo, phi, tris, nextJobs, wide, packed, counters, wideCapacity, jobCapacity,
+                triCapacity);
+}
+
+inline int blocksFor(long long n, int block) { return (int)((n + block - 1) / block); }
+
+template <class T>
+cudaError_t alloc(T*& p, size_t count) { return cudaMalloc(reinterpret_cast<void**>(&p), sizeof(T) * (count ? count : 1)); }
+
+}  // namespace
+
+void freeBvh(BuiltBvh& b) {
+    void* owned[] = {b.binNodes, b.order, b.wideNodes, b.packedTris, b.primLo, b.primHi};
+    for (void* p : owned)
+        if (p) cudaFree(p);
+    b = BuiltBvh{};
+}
+
+cudaError_t buildBvh(const SceneTri* tris, int n, cudaStream_t stream, BuiltBvh& out, BuildResult& result,
+                     const char** failure) {
+    *failure = nullptr;
+    cudaError_t err = cudaSuccess;
+    const int nodeCapacity = 2 * n + 2;
+    const int taskCapacity = n / (kLeafSize + 1) + 2;
+    // Temporaries.
+    float4* cent = nullptr; int* orderB = nullptr; int* posTask = nullptr; int* posTaskB = nullptr;
+    Task* tasks = nullptr; Task* tasksB = nullptr; BinAcc* bins = nullptr; Split* splits = nullptr;
+    unsigned* flags = nullptr; unsigned* prefix = nullptr; unsigned* blockSums = nullptr; int* counters = nullptr;
+    BinNode* rawNodes = nullptr; int* interior = nullptr; int* rank = nullptr; int* newIndex = nullptr;
+    Job* jobs = nullptr; Job* jobsB = nullptr;
+    int* hostCounters = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
+    std::vector<int> levelStart;
+    int nScanBlocks = blocksFor(n, kScanBlock);
+
+#define RT_TRY(x) do { err = (x); if (err != cudaSuccess) goto done; } while (0)
+    RT_TRY(alloc(out.primLo, n)); RT_TRY(alloc(out.primHi, n)); RT_TRY(alloc(cent, n));
+    RT_TRY(alloc(out.order, n)); RT_TRY(alloc(orderB, n)); RT_TRY(alloc(posTask, n)); RT_TRY(alloc(posTaskB, n));
+    RT_TRY(alloc(tasks, taskCapacity)); RT_TRY(alloc(tasksB, taskCapacity));
+    RT_TRY(alloc(bins, (size_t)taskCapacity * 3 * kBins)); RT_TRY(alloc(splits, taskCapacity));
+    RT_TRY(alloc(flags, n)); RT_TRY(alloc(prefix, n)); RT_TRY(alloc(blockSums, nScanBlocks));
+    RT_TRY(alloc(counters, 8)); RT_TRY(alloc(rawNodes, nodeCapacity));
+    RT_TRY(cudaMallocHost(reinterpret_cast<void**>(&hostCounters), 8 * sizeof(int)));
+    RT_TRY(cudaEventCreate(&e0)); RT_TRY(cudaEventCreate(&e1)); RT_TRY(cudaEventCreate(&e2));
+    RT_TRY(cudaEventRecord(e0, stream));
+    {
+        Task root{};
+        root.node = 0; root.first = 0; root.count = n; root.depth = 0;
+        for (int a = 0; a < 3; a++) { root.lo[a] = root.clo[a] = FLT_MAX; root.hi[a] = root.chi[a] = -FLT_MAX; }
+        RT_TRY(cudaMemcpyAsync(tasks, &root, sizeof(Task), cudaMemcpyHostToDevice, stream));
+        int init[8] = {1, 0, 0, 0, 0, 0, 0, 0};
+        RT_TRY(cudaMemcpyAsync(counters, init, sizeof(init), cudaMemcpyHostToDevice, stream));
+        primBoxesKernel<<<blocksFor(n, 256), 256, 0, stream>>>(tris, n, out.primLo, out.primHi, cent, tasks);
+        iotaKernel<<<blocksFor(n, 256), 256, 0, stream>>>(out.order, n, 0, posTask, 0);
+        RT_TRY(cudaGetLastError());
+        int nTasks = 1;
+        levelStart.push_back(0);  // depth 0 holds node 0
+        levelStart.push_back(1);
+        while (nTasks > 0) {
+            clearBinsKernel<<<blocksFor((long long)nTasks * 3 * kBins, 256), 256, 0, stream>>>(bins, nTasks * 3 * kBins);
+            binKernel<<<blocksFor(n, kBinBlock * kBinPer), kBinBlock, 0, stream>>>(out.order, posTask, cent, out.primLo,
+                                                                                    out.primHi, tasks, n, bins);
+            RT_TRY(cudaMemsetAsync(counters + 1, 0, sizeof(int), stream));
+            splitKernel<<<blocksFor(nTasks, 128), 128, 0, stream>>>(tasks, nTasks, bins, splits, rawNodes, counters,
+                                                                    tasksB, nodeCapacity, taskCapacity);
+            flagKernel<<<blocksFor(n, 256), 256, 0, stream>>>(out.order, posTask, cent, tasks, splits, n, flags);
+            RT_TRY(cudaMemcpyAsync(prefix, flags, sizeof(unsigned) * n, cudaMemcpyDeviceToDevice, stream));
+            scanBlocksKernel<<<nScanBlocks, 256, 0, stream>>>(prefix, n, blockSums);
+            scanTotalsKernel<<<1, 1024, 0, stream>>>(blockSums, nScanBlocks);
+            scatterKernel<<<blocksFor(n, 256), 256, 0, stream>>>(out.order, posTask, tasks, splits, flags, prefix,
+                                                                 blockSums, n, orderB, posTaskB, counters + 3);
+            RT_TRY(cudaGetLastError());
+            RT_TRY(cudaMemcpyAsync(hostCounters, counters, 8 * sizeof(int), cudaMemcpyDeviceToHost, stream));
+            RT_TRY(cudaStreamSynchronize(stream));
+            if (hostCounters[3]) { *failure = "BVH build ran out of node or task capacity"; err = cudaErrorMemoryAllocation; goto done; }
+            std::swap(out.order, orderB); std::swap(posTask, posTaskB); std::swap(tasks, tasksB);
+            levelStart.push_back(hostCounters[0]);
+            nTasks = hostCounters[1];
+            if ((int)levelStart.size() > kBinaryMaxDepth + 3) { *failure = "BVH build exceeded the depth limit"; err = cudaErrorUnknown; goto done; }
+        }
+        int nodeCount = hostCounters[0];
+        result.binaryNodes = nodeCount;
+        result.binaryDepth = hostCounters[2];
+        // levelStart[d] .. levelStart[d+1] are the nodes of depth d.
+        while (levelStart.size() > 2 && levelStart.back() == levelStart[levelStart.size() - 2]) levelStart.pop_back();
+        int depths = (int)levelStart.size() - 1;
+        RT_TRY(alloc(interior, nodeCount)); RT_TRY(alloc(rank, nodeCount)); RT_TRY(alloc(newIndex, nodeCount));
+        RT_TRY(alloc(out.binNodes, nodeCount));
+        for (int d = depths - 1; d >= 0; d--) {
+            int b = levelStart[d], e = levelStart[d + 1];
+            subtreeInteriorKernel<<<blocksFor(e - b, 256), 256, 0, stream>>>(rawNodes, b, e, interior);
+        }
+        RT_TRY(cudaMemsetAsync(rank, 0xFF, sizeof(int) * nodeCount, stream));
+        RT_TRY(cudaMemsetAsync(newIndex, 0xFF, sizeof(int) * nodeCount, stream));
+        RT_TRY(cudaMemsetAsync(rank, 0, sizeof(int), stream));
+        RT_TRY(cudaMemsetAsync(newIndex, 0, sizeof(int), stream));
+        for (int d = 0; d < depths; d++) {
+            int b = levelStart[d], e = levelStart[d + 1];
+            preorderKernel<<<blocksFor(e - b, 256), 256, 0, stream>>>(rawNodes, b, e, nodeCount, interior, rank,
+                                                                      newIndex, counters + 3);
+        }
+        renumberKernel<<<blocksFor(nodeCount, 256), 256, 0, stream>>>(rawNodes, nodeCount, newIndex, out.binNodes,
+                                                                      counters + 3);
+        RT_TRY(cudaGetLastError());
+        RT_TRY(cudaMemcpyAsync(hostCounters, counters, 8 * sizeof(int), cudaMemcpyDeviceToHost, stream));
+        RT_TRY(cudaStreamSynchronize(stream));
+        if (hostCounters[3]) { *failure = "BVH renumbering found an inconsistent tree"; err = cudaErrorUnknown; goto done; }
+        RT_TRY(cudaEventRecord(e1, stream));
+
+        // Collapse.
+        int wideCapacity = 2 * n + 8, jobCapacity = 2 * n + 8;
+        RT_TRY(alloc(out.wideNodes, (size_t)wideCapacity * 5));
+        RT_TRY(alloc(out.packedTris, (size_t)n * 3));
+        RT_TRY(alloc(jobs, jobCapacity)); RT_TRY(alloc(jobsB, jobCapacity));
+        Job rootJob{0, 0, 0, 0, 0};
+        RT_TRY(cudaMemcpyAsync(jobs, &rootJob, sizeof(Job), cudaMemcpyHostToDevice, stream));
+        int cinit[8] = {1, 0, 0, 0, 0, 0, 0, 0};
+        RT_TRY(cudaMemcpyAsync(counters, cinit, sizeof(cinit), cudaMemcpyHostToDevice, stream));
+        int nJobs = 1, wideDepth = 0;
+        while (nJobs > 0) {
+            wideDepth++;
+            if (wideDepth > kStackCapacity) { *failure = "wide BVH deeper than the traversal stack"; err = cudaErrorUnknown; goto done; }
+            RT_TRY(cudaMemsetAsync(counters + 2, 0, sizeof(int), stream));
+            collapseKernel<<<blocksFor(nJobs, 64), 64, 0, stream>>>(out.binNodes, out.order, out.primLo, out.primHi, tris,
+                                                                    jobs, nJobs, jobsB,
+                                                                    reinterpret_cast<WideNode*>(out.wideNodes),
+                                                                    out.packedTris, counters, wideCapacity, jobCapacity, n);
+            RT_TRY(cudaGetLastError());
+            RT_TRY(cudaMemcpyAsync(hostCounters, counters, 8 * sizeof(int), cudaMemcpyDeviceToHost, stream));
+            RT_TRY(cudaStreamSynchronize(stream));
+            if (hostCounters[3]) { *failure = "wide BVH collapse ran out of capacity"; err = cudaErrorMemoryAllocation; goto done; }
+            std::swap(jobs, jobsB);
+            nJobs = hostCounters[2];
+        }
+        RT_TRY(cudaEventRecord(e2, stream));
+        RT_TRY(cudaEventSynchronize(e2));
+        if (hostCounters[1] != n) { *failure = "wide BVH collapse lost triangles"; err = cudaErrorUnknown; goto done; }
+        result.wideNodes = hostCounters[0];
+        result.wideDepth = wideDepth;
+        RT_TRY(cudaEventElapsedTime(&result.buildMs, e0, e1));
+        RT_TRY(cudaEventElapsedTime(&result.collapseMs, e1, e2));
+    }
+done:
+#undef RT_TRY
+    cudaFree(cent); cudaFree(orderB); cudaFree(posTask); cudaFree(posTaskB); cudaFree(tasks); cudaFree(tasksB);
+    cudaFree(bins); cudaFree(splits); cudaFree(flags); cudaFree(prefix); cudaFree(blockSums); cudaFree(counters);
+    cudaFree(rawNodes); cudaFree(interior); cudaFree(rank); cudaFree(newIndex); cudaFree(jobs); cudaFree(jobsB);
+    if (hostCounters) cudaFreeHost(hostCounters);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (e2) cudaEventDestroy(e2);
+    if (err != cudaSuccess) freeBvh(out);
+    return err;
+}
+
+}  // namespace rt

@@ -1,0 +1,41 @@
+// GPU BVH construction: binned SAH (the reference's exact split rules) and
+// collapse into the 8-wide compressed traversal layout.
+#pragma once
+#include "rt_bvh.cuh"
+
+namespace rt {
+
+// Device-side scene record: the ABI Triangle (116 bytes) after sRGB decoding.
+struct SceneTri {
+    float3 origin, edge1, edge2, color;
+    float emission; int oneSided;
+    float3 normal0, normal1, normal2;
+    int mesh;
+    float3 specularColor;
+    float smoothness, specularProbability;
+};
+static_assert(sizeof(SceneTri) == 116, "Triangle layout");
+
+struct BuildResult {
+    int binaryNodes = 0, binaryDepth = 0, wideNodes = 0, wideDepth = 0;
+    float buildMs = 0, collapseMs = 0;
+};
+
+// Device buffers owned by a built scene. All pointers are device pointers.
+struct BuiltBvh {
+    BinNode* binNodes = nullptr;   // reference layout, numbered depth-first like Native/bvh.cuh
+    int* order = nullptr;          // primitive order of the binary leaves
+    uint4* wideNodes = nullptr;    // WideNode records (5 x uint4 each)
+    float4* packedTris = nullptr;  // 3 x float4 per triangle, in wide-leaf order
+    float4* primLo = nullptr;      // padded primitive boxes (kept for checks)
+    float4* primHi = nullptr;
+};
+
+// Builds the BVH for n device triangles on `stream`. Returns a CUDA error code
+// (cudaSuccess on success) and fills `out`/`result`. `scratchBytes` is the
+// peak temporary memory used, for reporting. Timing uses events on `stream`.
+cudaError_t buildBvh(const SceneTri* tris, int n, cudaStream_t stream, BuiltBvh& out, BuildResult& result,
+                     const char** failure);
+void freeBvh(BuiltBvh& bvh);
+
+}  // namespace rt

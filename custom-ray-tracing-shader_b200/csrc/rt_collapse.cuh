@@ -1,0 +1,222 @@
+// Collapse of the binary BVH into 8-wide compressed nodes (host and device).
+//
+// One job per wide node. A job is either a binary node (interior or leaf) or
+// a range of primitives (a leaf too large for one node). For a binary node,
+// the children start as its two children; the interior child with the largest
+// surface area is opened (replaced by its two children) while the result
+// still fits in eight slots, where a leaf of k <= 24 triangles needs
+// ceil(k / 3) slots (groups of up to three triangles) and anything else one
+// slot. Leaves that still do not fit become wide children of their own.
+// Slots are assigned by ray octant (slot s holds the child nearest along
+// direction signs s), and child boxes are quantised outward against the
+// node's grid, checked with the same fused multiply-add the traversal uses.
+#pragma once
+#include "rt_build.cuh"
+
+namespace rt {
+
+RT_HD int imin(int a, int b) { return a < b ? a : b; }
+RT_HD int imax(int a, int b) { return a > b ? a : b; }
+RT_HD int portableAdd(int* p, int v) {
+#ifdef __CUDA_ARCH__
+    return atomicAdd(p, v);
+#else
+    int old = *p; *p += v; return old;
+#endif
+}
+RT_HD void portableSet(int* p, int v) {
+#ifdef __CUDA_ARCH__
+    atomicExch(p, v);
+#else
+    *p = v;
+#endif
+}
+RT_HD float collapseHalfArea(const float lo[3], const float hi[3]) {
+    float x = fmaxf(0.0f, hi[0] - lo[0]), y = fmaxf(0.0f, hi[1] - lo[1]), z = fmaxf(0.0f, hi[2] - lo[2]);
+    return x * y + x * z + y * z;
+}
+RT_HD void collapseGrow(float lo[3], float hi[3], const float olo[3], const float ohi[3]) {
+    for (int a = 0; a < 3; a++) { lo[a] = fminf(lo[a], olo[a]); hi[a] = fmaxf(hi[a], ohi[a]); }
+}
+
+struct Job { int kind; int node; int first; int count; int wide; };  // kind 0 binary node, 1 primitive range
+struct Kid { int kind; int node; int first; int count; float lo[3], hi[3]; };  // kind 0/1 wide child, 2 triangle group
+
+RT_HD int slotsOf(const BinNode& n) {
+    if (n.count == 0) return 1;
+    return n.count <= 24 ? (n.count + 2) / 3 : 1;
+}
+
+// Builds wide node J.wide for one job: chooses up to eight children, assigns
+// slots, quantises child boxes, packs leaf triangles and emits jobs for the
+// interior children. counters: [0] wide nodes, [1] packed triangles,
+// [2] next-level jobs, [3] error code. Host and device (atomics through
+// portableAdd), so the collapse can be checked on the CPU.
+RT_HD void collapseJob(Job J, const BinNode* bn, const int* order, const float4* plo, const float4* phi,
+                       const SceneTri* tris, Job* nextJobs, WideNode* wide, float4* packed, int* counters,
+                       int wideCapacity, int jobCapacity, int triCapacity) {
+    if (J.kind == 0 && bn[J.node].count > 0) { J.kind = 1; J.first = bn[J.node].first; J.count = bn[J.node].count; }
+    Kid kids[8];
+    int nk = 0;
+    if (J.kind == 0) {
+        int cand[8], nc = 2;
+        bool asNode[8] = {false, false, false, false, false, false, false, false};
+        cand[0] = bn[J.node].first; cand[1] = cand[0] + 1;
+        for (;;) {
+            int total = 0;
+            for (int i = 0; i < nc; i++) total += slotsOf(bn[cand[i]]);
+            int best = -1; float bestArea = -1.0f;
+            for (int i = 0; i < nc; i++) {
+                const BinNode& c = bn[cand[i]];
+                if (c.count != 0 || nc >= 8) continue;
+                int after = total - 1 + slotsOf(bn[c.first]) + slotsOf(bn[c.first + 1]);
+                if (after > 8) continue;
+                float lo[3] = {c.low.x, c.low.y, c.low.z}, hi[3] = {c.high.x, c.high.y, c.high.z};
+                float a = collapseHalfArea(lo, hi);
+                if (a > bestArea) { bestArea = a; best = i; }
+            }
+            if (best < 0) break;
+            int opened = cand[best];
+            cand[best] = bn[opened].first;
+            cand[nc++] = bn[opened].first + 1;
+        }
+        // Leaves that do not fit inline become wide children of their own.
+        for (;;) {
+            int total = 0;
+            for (int i = 0; i < nc; i++) total += asNode[i] ? 1 : slotsOf(bn[cand[i]]);
+            if (total <= 8) break;
+            int pick = -1, most = 0;
+            for (int i = 0; i < nc; i++) {
+                const BinNode& c = bn[cand[i]];
+                if (!asNode[i] && c.count > 3 && c.count > most) { most = c.count; pick = i; }
+            }
+            if (pick < 0) break;
+            asNode[pick] = true;
+        }
+        for (int i = 0; i < nc && nk < 8; i++) {
+            const BinNode& c = bn[cand[i]];
+            if (c.count == 0) {
+                kids[nk++] = Kid{0, cand[i], 0, 0, {c.low.x, c.low.y, c.low.z}, {c.high.x, c.high.y, c.high.z}};
+            } else if (asNode[i] || c.count > 24) {
+                kids[nk++] = Kid{1, -1, c.first, c.count, {c.low.x, c.low.y, c.low.z}, {c.high.x, c.high.y, c.high.z}};
+            } else {
+                for (int g = 0; g < c.count && nk < 8; g += 3)
+                    kids[nk++] = Kid{2, -1, c.first + g, imin(3, c.count - g), {0, 0, 0}, {0, 0, 0}};
+            }
+        }
+    } else if (J.count <= 24) {
+        for (int g = 0; g < J.count && nk < 8; g += 3) kids[nk++] = Kid{2, -1, J.first + g, imin(3, J.count - g), {0, 0, 0}, {0, 0, 0}};
+    } else {
+        int chunk = (J.count + 7) / 8;
+        for (int g = 0; g < J.count && nk < 8; g += chunk) {
+            int c = imin(chunk, J.count - g);
+            kids[nk++] = Kid{c <= 3 ? 2 : 1, -1, J.first + g, c, {0, 0, 0}, {0, 0, 0}};
+        }
+    }
+    // Boxes of primitive-range kids: union of padded primitive boxes.
+    float nlo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, nhi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    for (int k = 0; k < nk; k++) {
+        Kid& K = kids[k];
+        if (K.kind != 0) {
+            float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+            for (int i = 0; i < K.count; i++) {
+                int p = order[K.first + i];
+                float4 a = plo[p], b = phi[p];
+                lo[0] = fminf(lo[0], a.x); lo[1] = fminf(lo[1], a.y); lo[2] = fminf(lo[2], a.z);
+                hi[0] = fmaxf(hi[0], b.x); hi[1] = fmaxf(hi[1], b.y); hi[2] = fmaxf(hi[2], b.z);
+            }
+            for (int a = 0; a < 3; a++) { K.lo[a] = lo[a]; K.hi[a] = hi[a]; }
+        }
+        collapseGrow(nlo, nhi, K.lo, K.hi);
+    }
+    // Slot assignment: slot s holds the kid met first by rays whose direction
+    // signs are s (bit 2 = x negative, bit 1 = y, bit 0 = z).
+    int slotKid[8] = {-1, -1, -1, -1, -1, -1, -1, -1};
+    {
+        float cn[3], ck[8][3];
+        for (int a = 0; a < 3; a++) cn[a] = 0.5f * (nlo[a] + nhi[a]);
+        for (int k = 0; k < nk; k++)
+            for (int a = 0; a < 3; a++) ck[k][a] = 0.5f * (kids[k].lo[a] + kids[k].hi[a]) - cn[a];
+        bool kidUsed[8] = {false, false, false, false, false, false, false, false};
+        for (int round = 0; round < nk; round++) {
+            float best = FLT_MAX; int bk = -1, bs = -1;
+            for (int k = 0; k < nk; k++) {
+                if (kidUsed[k]) continue;
+                for (int s = 0; s < 8; s++) {
+                    if (slotKid[s] >= 0) continue;
+                    float c = ((s & 4) ? -ck[k][0] : ck[k][0]) + ((s & 2) ? -ck[k][1] : ck[k][1]) + ((s & 1) ? -ck[k][2] : ck[k][2]);
+                    if (c < best) { best = c; bk = k; bs = s; }
+                }
+            }
+            if (bk < 0) {  // non-finite costs: first free kid into the first free slot
+                for (int k = 0; k < nk && bk < 0; k++) if (!kidUsed[k]) bk = k;
+                for (int s = 0; s < 8 && bs < 0; s++) if (slotKid[s] < 0) bs = s;
+            }
+            kidUsed[bk] = true; slotKid[bs] = bk;
+        }
+    }
+    int nInterior = 0, nTris = 0;
+    for (int k = 0; k < nk; k++) { if (kids[k].kind == 2) nTris += kids[k].count; else nInterior++; }
+    int childBase = nInterior ? portableAdd(&counters[0], nInterior) : 0;
+    int triBase = nTris ? portableAdd(&counters[1], nTris) : 0;
+    if (childBase + nInterior > wideCapacity || triBase + nTris > triCapacity) { portableSet(&counters[3], 3); return; }
+    WideNode W;
+    W.px = nlo[0]; W.py = nlo[1]; W.pz = nlo[2];
+    float sc[3];
+    unsigned char ebits[3];
+    for (int a = 0; a < 3; a++) {
+        float extent = nhi[a] - nlo[a];
+        int ex = -126;
+        if (extent > 0.0f) { frexpf(extent / 255.0f, &ex); }
+        ex = imax(-126, imin(127, ex));
+        ebits[a] = (unsigned char)(ex + 127);
+        sc[a] = bitsToFloat((unsigned)ebits[a] << 23);
+    }
+    W.ex = ebits[0]; W.ey = ebits[1]; W.ez = ebits[2];
+    W.imask = 0;
+    W.childBase = (unsigned)childBase;
+    W.triBase = (unsigned)triBase;
+    int interiorSeen = 0, triOffset = 0;
+    for (int s = 0; s < 8; s++) {
+        int k = slotKid[s];
+        if (k < 0) {
+            W.meta[s] = 0;
+            for (int a = 0; a < 3; a++) { W.qlo[a][s] = 0; W.qhi[a][s] = 0; }
+            continue;
+        }
+        const Kid& K = kids[k];
+        for (int a = 0; a < 3; a++) {
+            float p = a == 0 ? W.px : (a == 1 ? W.py : W.pz);
+            int ql = (int)floorf((K.lo[a] - p) / sc[a]);
+            int qh = (int)ceilf((K.hi[a] - p) / sc[a]);
+            ql = imax(0, imin(255, ql));
+            qh = imax(0, imin(255, qh));
+            while (ql > 0 && fmaRn((float)ql, sc[a], p) > K.lo[a]) ql--;
+            while (qh < 255 && fmaRn((float)qh, sc[a], p) < K.hi[a]) qh++;
+            W.qlo[a][s] = (unsigned char)ql;
+            W.qhi[a][s] = (unsigned char)qh;
+        }
+        if (K.kind == 2) {
+            W.meta[s] = (unsigned char)((((1u << K.count) - 1u) << 5) | (unsigned)triOffset);
+            for (int i = 0; i < K.count; i++) {
+                int p = order[K.first + i];
+                const SceneTri& t = tris[p];
+                float4* dst = packed + (size_t)(triBase + triOffset + i) * 3;
+                dst[0] = make_float4(t.origin.x, t.origin.y, t.origin.z, t.edge1.x);
+                dst[1] = make_float4(t.edge1.y, t.edge1.z, t.edge2.x, t.edge2.y);
+                dst[2] = make_float4(t.edge2.z, bitsToFloat(t.oneSided != 0 ? 1u : 0u), bitsToFloat((unsigned)p), 0.0f);
+            }
+            triOffset += K.count;
+        } else {
+            W.meta[s] = (unsigned char)(0x20u | (24u + (unsigned)s));
+            W.imask |= (unsigned char)(1u << s);
+            int q = portableAdd(&counters[2], 1);
+            if (q >= jobCapacity) { portableSet(&counters[3], 4); continue; }
+            nextJobs[q] = Job{K.kind == 0 ? 0 : 1, K.node, K.first, K.count, childBase + interiorSeen};
+            interiorSeen++;
+        }
+    }
+    wide[J.wide] = W;
+}
+
+}  // namespace rt

@@ -1,0 +1,58 @@
+// Launch interface of the render, query, sampler and denoise kernels.
+#pragma once
+#include "rt_integrator.cuh"
+
+namespace rt {
+
+struct RenderLaunch {
+    SceneView scene;
+    Camera cam;
+    Settings set;
+    int w, h;
+    unsigned sample0;            // paths already accumulated per pixel
+    const unsigned* passXor;     // [raysPerPixel][kSobolDims]
+    const unsigned* seedHash;    // [kSobolDims]
+    Accum* sums;                 // w*h running sums (read when sample0 > 0)
+    uchar4* pixels;              // w*h display image
+    unsigned long long* counters;  // [0] primary, [1] secondary, [2] shadow rays
+    int* errorFlag;              // set to 1 on traversal stack overflow
+};
+
+// Work buffers of the wavefront integrator, sized for `capacity` paths in flight.
+struct WavefrontBuffers {
+    int capacity = 0;
+    float4* pathA = nullptr;     // origin.xyz, prevPdf
+    float4* pathB = nullptr;     // dir.xyz, pixel index (bits)
+    float4* pathC = nullptr;     // throughput.xyz, sample row r (bits)
+    float4* radiance = nullptr;  // radiance.xyz, covered (bits)
+    float4* albedo = nullptr;    // albedo.xyz
+    float4* normal = nullptr;    // normal.xyz
+    float4* hits = nullptr;      // per queue slot: distance, u, v, index (bits)
+    int* queue[2] = {nullptr, nullptr};   // active path ids, ping-pong
+    float4* shadowRay = nullptr;      // origin.xyz, limit
+    float4* shadowDir = nullptr;      // dir.xyz, path id (bits)
+    float4* shadowContrib = nullptr;  // contribution.xyz
+    int* counts = nullptr;            // [0..1] queue sizes, [2] shadow queue size
+};
+
+cudaError_t allocWavefront(WavefrontBuffers& b, int capacity);
+void freeWavefront(WavefrontBuffers& b);
+
+cudaError_t buildSobolTables(const unsigned* dirs, unsigned sample0, int rpp, unsigned seed, unsigned* passXor,
+                             unsigned* seedHash, cudaStream_t stream);
+// One kernel per path: returns the number of kernel launches in *launches.
+cudaError_t launchMegakernel(const RenderLaunch& L, cudaStream_t stream, int* launches);
+// Wavefront: generate -> (extend -> shade -> shadow)* per wave. Timing of the
+// traversal kernels is accumulated into extendMs/shadowMs when timing != 0.
+cudaError_t launchWavefront(const RenderLaunch& L, WavefrontBuffers& b, int blockSize, cudaStream_t stream,
+                            int* launches, float* extendMs, float* shadowMs, bool timing);
+
+cudaError_t launchQueries(const uint4* wide, const float4* packed, const float4* queries /*2 per query*/, int count,
+                          int any, float4* hits, int* errorFlag, cudaStream_t stream);
+cudaError_t launchSobolSamples(const unsigned* dirs, const unsigned* pixel, const unsigned* sample, const unsigned* seed,
+                               int count, int ndim, float* out, cudaStream_t stream);
+// Denoise: prepare guides from the running sums, filter, tonemap into pixels.
+cudaError_t launchDenoise(const Accum* sums, unsigned samples, int w, int h, float exposure, float4* work /*4*w*h*/,
+                          uchar4* pixels, cudaStream_t stream);
+
+}  // namespace rt

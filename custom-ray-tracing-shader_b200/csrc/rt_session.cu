@@ -1,0 +1,568 @@
+// The C ABI (include/cuda_ray_tracer.h): session lifecycle, validation,
+// progressive accumulation and the additive query entry points.
+//
+// Behaviour follows the reference's session layer (Native/renderer.cu:309-458):
+//  - RtInitialize copies the triangles, converts colours from sRGB on the host
+//    and builds the emitter CDF in triangle order (renderer.cu:344-353; the
+//    host conversion keeps the reference's exact powf results), uploads the
+//    scene and builds the BVH on the GPU;
+//  - RtRender validates (renderer.cu:377-382), resets the accumulation when
+//    the backend or the bytes of camera/settings change (renderer.cu:388-389),
+//    renders raysPerPixel paths per pixel, reports compute time and copies the
+//    RGBA8 image out; samples += raysPerPixel (renderer.cu:417);
+//  - backends 0/1 run the same integrator and traversal code compiled for the
+//    host, on one thread or all OpenMP threads; backend 3 (Embree) is not
+//    part of this build and is rejected with a message;
+//  - RtDenoise never changes the accumulation, the sample count or the version.
+#include <omp.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <curand.h>
+#include <string>
+#include <vector>
+
+#include "../../include/cuda_ray_tracer.h"
+#include "rt_render.cuh"
+
+using namespace rt;
+
+static_assert(sizeof(Triangle) == 116 && sizeof(CameraData) == 64 && sizeof(RenderSettings) == 28, "ABI sizes");
+static_assert(sizeof(PixelSum) == 40 && sizeof(BvhNode) == 32, "record sizes");
+static_assert(sizeof(RtxQuery) == 28 && sizeof(RtxHit) == 16, "query sizes");
+
+namespace {
+
+const unsigned* hostSobolDirections(std::string& error) {
+    static curandDirectionVectors32_t* table = nullptr;
+    static curandStatus_t status = curandGetDirectionVectors32(&table, CURAND_DIRECTION_VECTORS_32_JOEKUO6);
+    if (status != CURAND_STATUS_SUCCESS || !table) { error = "Could not load cuRAND Sobol direction vectors"; return nullptr; }
+    return &table[0][0];
+}
+
+struct Session {
+    std::string hostError;
+    cudaError_t error = cudaSuccess;
+    bool ready = false;
+    int width = 0, height = 0, device = 0;
+    int lastBackend = -1, cpuThreads = 0;
+    unsigned samples = 0, accumulationVersion = 0;
+    CameraData lastCamera{};
+    RenderSettings lastSettings{};
+    // Host scene (colours linear) and emitters.
+    std::vector<SceneTri> tris;
+    std::vector<Light> lights;
+    float lightArea = 0;
+    // Device scene.
+    cudaStream_t stream = nullptr;
+    cudaEvent_t start = nullptr, stop = nullptr;
+    SceneTri* dTris = nullptr;
+    Light* dLights = nullptr;
+    unsigned* dDirs = nullptr;
+    unsigned* dPassXor = nullptr;
+    unsigned* dSeedHash = nullptr;
+    Accum* dSum = nullptr;
+    uchar4* dPixels = nullptr;
+    unsigned long long* dCounters = nullptr;
+    int* dError = nullptr;
+    float4* dDenoise = nullptr;
+    BuiltBvh bvh;
+    BuildResult build;
+    WavefrontBuffers wave;
+    // Host mirrors for the CPU backends (filled on first use).
+    std::vector<Accum> hostSum;
+    std::vector<uint4> hostWide;
+    std::vector<float4> hostPacked;
+    bool hostBvhReady = false;
+    // Statistics and tuning.
+    RtxRenderStats stats{};
+    double sahCost = -1.0;
+    int integrator = 0, blockSize = 128, pathsInFlight = 0;
+};
+
+bool fail(Session* s, cudaError_t e, const char* what = nullptr) {
+    s->error = e;
+    if (what) s->hostError = what;
+    return false;
+}
+
+void releaseScene(Session* s) {
+    freeBvh(s->bvh);
+    freeWavefront(s->wave);
+    void* owned[] = {s->dTris, s->dLights, s->dDirs, s->dPassXor, s->dSeedHash, s->dSum, s->dPixels, s->dCounters,
+                     s->dError, s->dDenoise};
+    for (void* p : owned)
+        if (p) cudaFree(p);
+    s->dTris = nullptr; s->dLights = nullptr; s->dDirs = nullptr; s->dPassXor = nullptr; s->dSeedHash = nullptr;
+    s->dSum = nullptr; s->dPixels = nullptr; s->dCounters = nullptr; s->dError = nullptr; s->dDenoise = nullptr;
+    if (s->start) cudaEventDestroy(s->start);
+    if (s->stop) cudaEventDestroy(s->stop);
+    s->start = s->stop = nullptr;
+    if (s->stream) cudaStreamDestroy(s->stream);
+    s->stream = nullptr;
+    s->tris.clear(); s->lights.clear(); s->hostSum.clear(); s->hostWide.clear(); s->hostPacked.clear();
+    s->tris.shrink_to_fit(); s->hostWide.shrink_to_fit(); s->hostPacked.shrink_to_fit();
+    s->hostBvhReady = false;
+    s->ready = false;
+    s->width = s->height = 0;
+    s->samples = 0;
+    s->lightArea = 0;
+    s->lastBackend = -1;
+    s->build = BuildResult{};
+    s->sahCost = -1.0;
+    s->stats = RtxRenderStats{};
+}
+
+bool validSettings(const RenderSettings* st) {
+    return st->raysPerPixel >= 1 && st->raysPerPixel <= 16 && st->maxBounces >= 1 && st->maxBounces <= 32 &&
+           st->exposure > 0 && st->aperture >= 0 && st->focusDistance > 0 && st->skyStrength >= 0;
+}
+
+SceneView deviceView(Session* s) {
+    return SceneView{s->dTris, s->bvh.wideNodes, s->bvh.packedTris, s->dLights, (int)s->lights.size(), s->lightArea};
+}
+
+bool ensureWave(Session* s) {
+    int pixels = s->width * s->height;
+    int cap = s->pathsInFlight > 0 ? std::min(s->pathsInFlight, pixels) : pixels;
+    if (s->wave.capacity == cap) return true;
+    cudaError_t e = allocWavefront(s->wave, cap);
+    if (e != cudaSuccess) return fail(s, e, "could not allocate wavefront buffers");
+    return true;
+}
+
+// Common render path of RtRender / RtxRenderDevice for backend 2.
+bool renderDevice(Session* s, const CameraData* camera, const RenderSettings* settings, float* computeMs, bool timing) {
+    Camera cam; Settings set;
+    std::memcpy(&cam, camera, sizeof(cam));
+    std::memcpy(&set, settings, sizeof(set));
+    cudaError_t e;
+    if ((e = buildSobolTables(s->dDirs, s->samples, set.raysPerPixel, set.seed, s->dPassXor, s->dSeedHash, s->stream)) != cudaSuccess) return fail(s, e);
+    if ((e = cudaMemsetAsync(s->dCounters, 0, 4 * sizeof(unsigned long long), s->stream)) != cudaSuccess) return fail(s, e);
+    if ((e = cudaMemsetAsync(s->dError, 0, sizeof(int), s->stream)) != cudaSuccess) return fail(s, e);
+    RenderLaunch L{deviceView(s), cam, set, s->width, s->height, s->samples, s->dPassXor, s->dSeedHash,
+                   s->dSum, s->dPixels, s->dCounters, s->dError};
+    int launches = 0;
+    float extendMs = 0, shadowMs = 0;
+    if ((e = cudaEventRecord(s->start, s->stream)) != cudaSuccess) return fail(s, e);
+    if (s->integrator == 1) {
+        e = launchMegakernel(L, s->stream, &launches);
+    } else {
+        if (!ensureWave(s)) return false;
+        e = launchWavefront(L, s->wave, s->blockSize, s->stream, &launches, &extendMs, &shadowMs, timing);
+    }
+    if (e != cudaSuccess) return fail(s, e);
+    if ((e = cudaEventRecord(s->stop, s->stream)) != cudaSuccess) return fail(s, e);
+    if ((e = cudaEventSynchronize(s->stop)) != cudaSuccess) return fail(s, e);
+    if ((e = cudaEventElapsedTime(computeMs, s->start, s->stop)) != cudaSuccess) return fail(s, e);
+    unsigned long long counters[4];
+    int overflow = 0;
+    if ((e = cudaMemcpy(counters, s->dCounters, sizeof(counters), cudaMemcpyDeviceToHost)) != cudaSuccess) return fail(s, e);
+    if ((e = cudaMemcpy(&overflow, s->dError, sizeof(int), cudaMemcpyDeviceToHost)) != cudaSuccess) return fail(s, e);
+    if (overflow) return fail(s, cudaErrorUnknown, "BVH traversal stack overflow");
+    s->stats.primaryRays = counters[0];
+    s->stats.secondaryRays = counters[1];
+    s->stats.shadowRays = counters[2];
+    s->stats.paths = (unsigned long long)s->width * s->height * set.raysPerPixel;
+    s->stats.renderMs = *computeMs;
+    s->stats.extendMs = extendMs;
+    s->stats.shadowMs = shadowMs;
+    s->stats.kernelLaunches = launches + 1;  // + the sampler-table kernel
+    return true;
+}
+
+bool ensureHostBvh(Session* s) {
+    if (s->hostBvhReady) return true;
+    s->hostWide.resize((size_t)s->build.wideNodes * 5);
+    s->hostPacked.resize(s->tris.size() * 3);
+    cudaError_t e = cudaMemcpy(s->hostWide.data(), s->bvh.wideNodes, s->hostWide.size() * sizeof(uint4), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(s->hostPacked.data(), s->bvh.packedTris, s->hostPacked.size() * sizeof(float4), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return fail(s, e);
+    s->hostBvhReady = true;
+    return true;
+}
+
+// Backends 0 and 1: the integrator compiled for the host (renderer.cu:405-415).
+bool renderHost(Session* s, const CameraData* camera, const RenderSettings* settings, unsigned char* output, int backend,
+                float* computeMs) {
+    if (!ensureHostBvh(s)) return false;
+    std::string err;
+    const unsigned* dirs = hostSobolDirections(err);
+    if (!dirs) { s->hostError = err; return false; }
+    Camera cam; Settings set;
+    std::memcpy(&cam, camera, sizeof(cam));
+    std::memcpy(&set, settings, sizeof(set));
+    std::vector<unsigned> passXor((size_t)set.raysPerPixel * kSobolDims), seedHash(kSobolDims);
+    for (int r = 0; r < set.raysPerPixel; r++)
+        for (int d = 0; d < kSobolDims; d++) passXor[(size_t)r * kSobolDims + d] = sobolXor(dirs, s->samples + (unsigned)r, (unsigned)d);
+    for (int d = 0; d < kSobolDims; d++) seedHash[d] = sobolHash(set.seed + (unsigned)d * 0x9e3779b9u);
+    if (s->hostSum.size() != (size_t)s->width * s->height) s->hostSum.assign((size_t)s->width * s->height, Accum{});
+    SceneView sc{s->tris.data(), s->hostWide.data(), s->hostPacked.data(), s->lights.data(), (int)s->lights.size(), s->lightArea};
+    const int w = s->width, h = s->height;
+    const unsigned sample0 = s->samples;
+    Accum* sums = s->hostSum.data();
+    uchar4* pixels = reinterpret_cast<uchar4*>(output);
+    unsigned long long nPrimary = 0, nSecondary = 0, nShadow = 0;
+    int overflow = 0, threads = 1;
+    auto begin = std::chrono::steady_clock::now();
+#pragma omp parallel num_threads(backend == 1 ? omp_get_max_threads() : 1) reduction(+ : nPrimary, nSecondary, nShadow) reduction(| : overflow)
+    {
+#pragma omp single
+        threads = omp_get_num_threads();
+        uint2 stack[kStackCapacity];
+        unsigned p = 0, q = 0, sh = 0;
+#pragma omp for schedule(dynamic, 1)
+        for (int y = 0; y < h; y++)
+            for (int x = 0; x < w; x++)
+                renderPixel(sc, cam, set, x, y, w, h, sample0, passXor.data(), seedHash.data(), sums, pixels, stack, 1,
+                            &overflow, p, q, sh);
+        nPrimary += p; nSecondary += q; nShadow += sh;
+    }
+    *computeMs = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - begin).count();
+    if (overflow) { s->hostError = "BVH traversal stack overflow"; return false; }
+    s->cpuThreads = threads;
+    s->stats = RtxRenderStats{};
+    s->stats.primaryRays = nPrimary; s->stats.secondaryRays = nSecondary; s->stats.shadowRays = nShadow;
+    s->stats.paths = (unsigned long long)w * h * set.raysPerPixel;
+    s->stats.renderMs = *computeMs;
+    return true;
+}
+
+// Shared front half of RtRender and RtxRenderDevice (renderer.cu:376-390).
+bool beginRender(Session* s, const CameraData* camera, const RenderSettings* settings, int backend) {
+    if (s->ready && s->device >= 0) cudaSetDevice(s->device);
+    if (backend == 3) {
+        s->hostError = "Embree backend (3) is not available in this build";
+        s->error = cudaErrorInvalidValue;
+        return false;
+    }
+    s->hostError.clear();
+    if (s->lastBackend != backend || std::memcmp(camera, &s->lastCamera, sizeof(CameraData)) ||
+        std::memcmp(settings, &s->lastSettings, sizeof(RenderSettings))) {
+        s->samples = 0;
+        s->accumulationVersion++;
+    }
+    s->lastBackend = backend;
+    s->lastCamera = *camera;
+    s->lastSettings = *settings;
+    s->cpuThreads = 0;
+    return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+void* RtCreate(void) { return new Session(); }
+
+void RtReset(void* p) {
+    Session* s = static_cast<Session*>(p);
+    if (s) { s->samples = 0; s->accumulationVersion++; }
+}
+unsigned RtAccumulationVersion(void* p) { return p ? static_cast<Session*>(p)->accumulationVersion : 0u; }
+unsigned RtSampleCount(void* p) { return p ? static_cast<Session*>(p)->samples : 0u; }
+float RtEmbreeBuildMilliseconds(void*) { return 0.0f; }
+int RtCpuThreadCount(void* p) { return p ? static_cast<Session*>(p)->cpuThreads : 0; }
+void RtBvhInfo(void* p, int* nodes, int* depth, float* buildMs) {
+    Session* s = static_cast<Session*>(p);
+    if (nodes) *nodes = s ? s->build.binaryNodes : 0;
+    if (depth) *depth = s ? s->build.binaryDepth : 0;
+    if (buildMs) *buildMs = s ? s->build.buildMs : 0.0f;
+}
+const char* RtLastError(void* p) {
+    Session* s = static_cast<Session*>(p);
+    if (s && !s->hostError.empty()) return s->hostError.c_str();
+    return cudaGetErrorString(s ? s->error : cudaErrorInvalidValue);
+}
+void RtShutdown(void* p) {
+    Session* s = static_cast<Session*>(p);
+    if (!s) return;
+    if (s->device >= 0 && s->stream) cudaSetDevice(s->device);
+    releaseScene(s);
+    s->hostError.clear();
+}
+void RtDestroy(void* p) {
+    Session* s = static_cast<Session*>(p);
+    if (s) { RtShutdown(s); delete s; }
+}
+
+int RtInitialize(void* p, const Triangle* triangles, int count, int width, int height) {
+    Session* s = static_cast<Session*>(p);
+    if (!s) return 0;
+    RtShutdown(s);
+    if (!triangles || count <= 0 || width <= 0 || height <= 0 || width > 4096 || height > 4096) {
+        s->hostError = "RtInitialize: need triangles, count > 0 and 1 <= width, height <= 4096";
+        s->error = cudaErrorInvalidValue;
+        return 0;
+    }
+    cudaError_t e = cudaGetDevice(&s->device);
+    if (e != cudaSuccess) { fail(s, e); return 0; }
+    // Host preparation, as the reference does it (renderer.cu:344-353).
+    s->tris.resize((size_t)count);
+    std::memcpy(s->tris.data(), triangles, sizeof(Triangle) * (size_t)count);
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < count; i++) {
+        SceneTri& t = s->tris[i];
+        t.color = v3(srgbToLinear(t.color.x), srgbToLinear(t.color.y), srgbToLinear(t.color.z));
+        t.specularColor = v3(srgbToLinear(t.specularColor.x), srgbToLinear(t.specularColor.y), srgbToLinear(t.specularColor.z));
+    }
+    for (int i = 0; i < count; i++) {
+        const SceneTri& t = s->tris[i];
+        if (t.emission > 0) {
+            float3 an = cross(t.edge1, t.edge2);
+            s->lightArea += .5f * sqrtf(dot(an, an));
+            s->lights.push_back(Light{i, s->lightArea});
+        }
+    }
+    std::string err;
+    const unsigned* dirs = hostSobolDirections(err);
+    if (!dirs) { s->hostError = err; return 0; }
+#define RT_CHECK(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) { fail(s, e_); releaseScene(s); return 0; } } while (0)
+    RT_CHECK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    RT_CHECK(cudaEventCreate(&s->start));
+    RT_CHECK(cudaEventCreate(&s->stop));
+    RT_CHECK(cudaMalloc(&s->dTris, sizeof(SceneTri) * (size_t)count));
+    RT_CHECK(cudaMemcpy(s->dTris, s->tris.data(), sizeof(SceneTri) * (size_t)count, cudaMemcpyHostToDevice));
+    if (!s->lights.empty()) {
+        RT_CHECK(cudaMalloc(&s->dLights, sizeof(Light) * s->lights.size()));
+        RT_CHECK(cudaMemcpy(s->dLights, s->lights.data(), sizeof(Light) * s->lights.size(), cudaMemcpyHostToDevice));
+    }
+    RT_CHECK(cudaMalloc(&s->dDirs, sizeof(unsigned) * kSobolDims * 32));
+    RT_CHECK(cudaMemcpy(s->dDirs, dirs, sizeof(unsigned) * kSobolDims * 32, cudaMemcpyHostToDevice));
+    RT_CHECK(cudaMalloc(&s->dPassXor, sizeof(unsigned) * 16 * kSobolDims));
+    RT_CHECK(cudaMalloc(&s->dSeedHash, sizeof(unsigned) * kSobolDims));
+    RT_CHECK(cudaMalloc(&s->dSum, sizeof(Accum) * (size_t)width * height));
+    RT_CHECK(cudaMalloc(&s->dPixels, sizeof(uchar4) * (size_t)width * height));
+    RT_CHECK(cudaMalloc(&s->dCounters, 4 * sizeof(unsigned long long)));
+    RT_CHECK(cudaMalloc(&s->dError, sizeof(int)));
+    const char* why = nullptr;
+    e = buildBvh(s->dTris, count, s->stream, s->bvh, s->build, &why);
+    if (e != cudaSuccess) {
+        fail(s, e, why);
+        std::string keep = s->hostError;
+        releaseScene(s);
+        s->hostError = keep;
+        return 0;
+    }
+#undef RT_CHECK
+    s->width = width;
+    s->height = height;
+    s->ready = true;
+    return 1;
+}
+
+int RtRender(void* p, const CameraData* camera, const RenderSettings* settings, unsigned char* output, int outputBytes,
+             int backend, float* computeMs) {
+    Session* s = static_cast<Session*>(p);
+    if (!s) return 0;
+    if (!camera || !settings || !output || !computeMs || !s->ready || backend < 0 || backend > 3 || outputBytes < 0 ||
+        (size_t)outputBytes < (size_t)s->width * s->height * 4 || !validSettings(settings)) {
+        s->error = cudaErrorInvalidValue;
+        s->hostError = !s->ready ? "RtRender: session is not initialised"
+                                 : "RtRender: invalid camera, settings, backend or output buffer";
+        return 0;
+    }
+    if (!beginRender(s, camera, settings, backend)) return 0;
+    if (backend == 2) {
+        if (!renderDevice(s, camera, settings, computeMs, false)) return 0;
+        cudaError_t e = cudaMemcpy(output, s->dPixels, (size_t)s->width * s->height * 4, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) { fail(s, e); return 0; }
+    } else {
+        if (!renderHost(s, camera, settings, output, backend, computeMs)) return 0;
+    }
+    s->samples += (unsigned)settings->raysPerPixel;
+    s->error = cudaSuccess;
+    return 1;
+}
+
+int RtDenoise(void* p, unsigned char* output, int outputBytes, float* milliseconds) {
+    Session* s = static_cast<Session*>(p);
+    if (!s) return 0;
+    if (!s->ready || !s->samples || !output || !milliseconds || outputBytes < 0 ||
+        (size_t)outputBytes < (size_t)s->width * s->height * 4) {
+        s->error = cudaErrorInvalidValue;
+        s->hostError = !s->ready ? "RtDenoise: session is not initialised"
+                     : !s->samples ? "RtDenoise: render at least one pass before denoising"
+                                   : "RtDenoise: invalid output buffer";
+        return 0;
+    }
+    cudaSetDevice(s->device);
+    auto begin = std::chrono::steady_clock::now();
+    s->hostError.clear();
+    size_t count = (size_t)s->width * s->height;
+    cudaError_t e;
+    if (!s->dDenoise && (e = cudaMalloc(&s->dDenoise, sizeof(float4) * 4 * count)) != cudaSuccess) { fail(s, e); return 0; }
+    if (s->lastBackend != 2) {
+        if ((e = cudaMemcpy(s->dSum, s->hostSum.data(), count * sizeof(Accum), cudaMemcpyHostToDevice)) != cudaSuccess) { fail(s, e); return 0; }
+    }
+    if ((e = launchDenoise(s->dSum, s->samples, s->width, s->height, s->lastSettings.exposure, s->dDenoise, s->dPixels, s->stream)) != cudaSuccess) { fail(s, e); return 0; }
+    if ((e = cudaStreamSynchronize(s->stream)) != cudaSuccess) { fail(s, e); return 0; }
+    if ((e = cudaMemcpy(output, s->dPixels, count * 4, cudaMemcpyDeviceToHost)) != cudaSuccess) { fail(s, e); return 0; }
+    *milliseconds = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - begin).count();
+    if (!(*milliseconds > 0)) *milliseconds = 1e-6f;
+    s->error = cudaSuccess;
+    return 1;
+}
+
+// ---- additive entry points ----
+
+int RtxQueryRays(void* p, const RtxQuery* queries, int count, int any, RtxHit* hits) {
+    Session* s = static_cast<Session*>(p);
+    if (!s) return 0;
+    if (!s->ready || !queries || !hits || count < 0) { s->error = cudaErrorInvalidValue; s->hostError = "RtxQueryRays: invalid arguments"; return 0; }
+    if (count == 0) return 1;
+    cudaSetDevice(s->device);
+    std::vector<float4> packed((size_t)count * 2);
+    for (int i = 0; i < count; i++) {
+        const RtxQuery& q = queries[i];
+        packed[2 * (size_t)i] = make_float4(q.origin.x, q.origin.y, q.origin.z, q.direction.x);
+        packed[2 * (size_t)i + 1] = make_float4(q.direction.y, q.direction.z, q.limit, 0.0f);
+    }
+    float4 *dq = nullptr, *dh = nullptr;
+    std::vector<float4> out((size_t)count);
+    int overflow = 0;
+    cudaError_t e = cudaMalloc(&dq, sizeof(float4) * packed.size());
+    if (e == cudaSuccess) e = cudaMalloc(&dh, sizeof(float4) * (size_t)count);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dq, packed.data(), sizeof(float4) * packed.size(), cudaMemcpyHostToDevice, s->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->dError, 0, sizeof(int), s->stream);
+    if (e == cudaSuccess) e = launchQueries(s->bvh.wideNodes, s->bvh.packedTris, dq, count, any, dh, s->dError, s->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out.data(), dh, sizeof(float4) * (size_t)count, cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&overflow, s->dError, sizeof(int), cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    cudaFree(dq); cudaFree(dh);
+    if (e != cudaSuccess) { fail(s, e); return 0; }
+    if (overflow) { s->hostError = "BVH traversal stack overflow"; return 0; }
+    for (int i = 0; i < count; i++) {
+        int index;
+        std::memcpy(&index, &out[i].x, 4);
+        hits[i] = RtxHit{index, out[i].y, out[i].z, out[i].w};
+    }
+    return 1;
+}
+
+int RtxSobolSamples(const unsigned* pixel, const unsigned* sample, const unsigned* seed, int count, int ndim, float* out) {
+    if (!pixel || !sample || !seed || !out || count < 0 || ndim < 0 || ndim > kSobolDims) return 0;
+    if (count == 0 || ndim == 0) return 1;
+    std::string err;
+    const unsigned* dirs = hostSobolDirections(err);
+    if (!dirs) return 0;
+    unsigned *dd = nullptr, *dp = nullptr, *ds = nullptr, *dseed = nullptr;
+    float* dout = nullptr;
+    size_t n = (size_t)count;
+    cudaError_t e = cudaMalloc(&dd, sizeof(unsigned) * kSobolDims * 32);
+    if (e == cudaSuccess) e = cudaMalloc(&dp, sizeof(unsigned) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&ds, sizeof(unsigned) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&dseed, sizeof(unsigned) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&dout, sizeof(float) * n * ndim);
+    if (e == cudaSuccess) e = cudaMemcpy(dd, dirs, sizeof(unsigned) * kSobolDims * 32, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(dp, pixel, sizeof(unsigned) * n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(ds, sample, sizeof(unsigned) * n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(dseed, seed, sizeof(unsigned) * n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = launchSobolSamples(dd, dp, ds, dseed, count, ndim, dout, 0);
+    if (e == cudaSuccess) e = cudaMemcpy(out, dout, sizeof(float) * n * ndim, cudaMemcpyDeviceToHost);
+    cudaFree(dd); cudaFree(dp); cudaFree(ds); cudaFree(dseed); cudaFree(dout);
+    return e == cudaSuccess ? 1 : 0;
+}
+
+int RtxExportBvh(void* p, BvhNode* nodes, int nodeCapacity, int* order, int orderCapacity) {
+    Session* s = static_cast<Session*>(p);
+    if (!s) return 0;
+    if (!s->ready || (nodes && nodeCapacity < s->build.binaryNodes) || (order && orderCapacity < (int)s->tris.size())) {
+        s->error = cudaErrorInvalidValue; s->hostError = "RtxExportBvh: not initialised or buffers too small"; return 0;
+    }
+    cudaSetDevice(s->device);
+    cudaError_t e = cudaSuccess;
+    if (nodes) e = cudaMemcpy(nodes, s->bvh.binNodes, sizeof(BvhNode) * (size_t)s->build.binaryNodes, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && order) e = cudaMemcpy(order, s->bvh.order, sizeof(int) * s->tris.size(), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) { fail(s, e); return 0; }
+    return 1;
+}
+
+int RtxBvhStatsGet(void* p, RtxBvhStats* out) {
+    Session* s = static_cast<Session*>(p);
+    if (!s || !out) return 0;
+    if (!s->ready) { s->hostError = "RtxBvhStatsGet: session is not initialised"; return 0; }
+    if (s->sahCost < 0) {
+        std::vector<BvhNode> nodes((size_t)s->build.binaryNodes);
+        cudaSetDevice(s->device);
+        cudaError_t e = cudaMemcpy(nodes.data(), s->bvh.binNodes, sizeof(BvhNode) * nodes.size(), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) { fail(s, e); return 0; }
+        auto area = [](const BvhNode& n) {
+            double x = std::max(0.0, (double)n.high.x - n.low.x), y = std::max(0.0, (double)n.high.y - n.low.y),
+                   z = std::max(0.0, (double)n.high.z - n.low.z);
+            return x * y + x * z + y * z;
+        };
+        double root = area(nodes[0]), total = 0;
+        for (const BvhNode& n : nodes) total += n.count > 0 ? area(n) * n.count : area(n);
+        s->sahCost = root > 0 ? total / root : 0.0;
+    }
+    out->binaryNodes = s->build.binaryNodes;
+    out->binaryDepth = s->build.binaryDepth;
+    out->wideNodes = s->build.wideNodes;
+    out->wideDepth = s->build.wideDepth;
+    out->buildMs = s->build.buildMs;
+    out->collapseMs = s->build.collapseMs;
+    out->sahCost = s->sahCost;
+    return 1;
+}
+
+int RtxReadAccumulation(void* p, PixelSum* out, int count) {
+    Session* s = static_cast<Session*>(p);
+    if (!s) return 0;
+    size_t need = (size_t)s->width * s->height;
+    if (!s->ready || !out || count < 0 || (size_t)count < need) {
+        s->error = cudaErrorInvalidValue; s->hostError = "RtxReadAccumulation: not initialised or buffer too small"; return 0;
+    }
+    if (s->lastBackend == 0 || s->lastBackend == 1) {
+        if (s->hostSum.size() != need) return 0;
+        std::memcpy(out, s->hostSum.data(), need * sizeof(PixelSum));
+        return 1;
+    }
+    cudaSetDevice(s->device);
+    cudaError_t e = cudaMemcpy(out, s->dSum, need * sizeof(PixelSum), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) { fail(s, e); return 0; }
+    return 1;
+}
+
+int RtxRenderStatsGet(void* p, RtxRenderStats* out) {
+    Session* s = static_cast<Session*>(p);
+    if (!s || !out) return 0;
+    *out = s->stats;
+    return 1;
+}
+
+int RtxRenderDevice(void* p, const CameraData* camera, const RenderSettings* settings, float* computeMs) {
+    Session* s = static_cast<Session*>(p);
+    if (!s) return 0;
+    if (!camera || !settings || !computeMs || !s->ready || !validSettings(settings)) {
+        s->error = cudaErrorInvalidValue;
+        s->hostError = "RtxRenderDevice: invalid arguments or session not initialised";
+        return 0;
+    }
+    if (!beginRender(s, camera, settings, 2)) return 0;
+    if (!renderDevice(s, camera, settings, computeMs, true)) return 0;
+    s->samples += (unsigned)settings->raysPerPixel;
+    s->error = cudaSuccess;
+    return 1;
+}
+
+int RtxSetIntegrator(void* p, int mode) {
+    Session* s = static_cast<Session*>(p);
+    if (!s || mode < 0 || mode > 1) return 0;
+    s->integrator = mode;
+    return 1;
+}
+
+int RtxSetTuning(void* p, int blockSize, int pathsInFlight) {
+    Session* s = static_cast<Session*>(p);
+    if (!s) return 0;
+    if (blockSize != 0 && (blockSize < 64 || blockSize > 1024 || blockSize % 32)) return 0;
+    if (pathsInFlight != 0 && pathsInFlight < 1024) return 0;
+    if (blockSize) s->blockSize = blockSize;
+    if (pathsInFlight) s->pathsInFlight = pathsInFlight;
+    return 1;
+}
+
+}  // extern "C"

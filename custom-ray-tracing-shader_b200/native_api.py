@@ -1,0 +1,252 @@
+"""ctypes bindings of libCudaRayTracer.so, mirroring the reference's Tools/native_api.py.
+
+The structures, the size checks (116/64/28 bytes, Tools/native_api.py:26), the
+RAYTRACER_LIBRARY override (:29), the argument types set by load_library
+(:28-43) and unpack() for Unity JSON snapshots (:45-48) keep the reference's
+names and meaning, so scripts written against the reference bind this library
+unchanged. Additions: numpy record dtypes for bulk triangle arrays and the
+additive Rtx* entry points declared in include/cuda_ray_tracer.h.
+"""
+import ctypes as c
+import os
+from pathlib import Path
+
+import numpy as np
+
+
+class Vector(c.Structure):
+    _fields_ = [(axis, c.c_float) for axis in 'xyz']
+
+
+class Triangle(c.Structure):
+    _fields_ = [(name, Vector) for name in ('origin', 'edge1', 'edge2', 'color')]
+    _fields_ += [('emission', c.c_float), ('oneSided', c.c_int)]
+    _fields_ += [(name, Vector) for name in ('normal0', 'normal1', 'normal2')]
+    _fields_ += [('mesh', c.c_int), ('specularColor', Vector), ('smoothness', c.c_float),
+                 ('specularProbability', c.c_float)]
+
+
+class Camera(c.Structure):
+    _fields_ = [(name, Vector) for name in ('origin', 'right', 'up', 'forward')]
+    _fields_ += [('tanHalfFov', c.c_float), ('aspect', c.c_float), ('orthographicSize', c.c_float),
+                 ('orthographic', c.c_int)]
+
+
+class Settings(c.Structure):
+    _fields_ = [('maxBounces', c.c_int)]
+    _fields_ += [(name, c.c_float) for name in ('exposure', 'aperture', 'focusDistance', 'skyStrength')]
+    _fields_ += [('seed', c.c_uint), ('raysPerPixel', c.c_int)]
+
+
+class PixelSum(c.Structure):
+    _fields_ = [('radiance', Vector), ('albedo', Vector), ('normal', Vector), ('covered', c.c_uint)]
+
+
+class BvhNode(c.Structure):
+    _fields_ = [('low', Vector), ('first', c.c_int), ('high', Vector), ('count', c.c_int)]
+
+
+class RtxQuery(c.Structure):
+    _fields_ = [('origin', Vector), ('direction', Vector), ('limit', c.c_float)]
+
+
+class RtxHit(c.Structure):
+    _fields_ = [('index', c.c_int), ('distance', c.c_float), ('u', c.c_float), ('v', c.c_float)]
+
+
+class RtxRenderStats(c.Structure):
+    _fields_ = [('primaryRays', c.c_ulonglong), ('secondaryRays', c.c_ulonglong), ('shadowRays', c.c_ulonglong),
+                ('paths', c.c_ulonglong), ('renderMs', c.c_float), ('extendMs', c.c_float),
+                ('shadowMs', c.c_float), ('kernelLaunches', c.c_int)]
+
+
+class RtxBvhStats(c.Structure):
+    _fields_ = [('binaryNodes', c.c_int), ('binaryDepth', c.c_int), ('wideNodes', c.c_int),
+                ('wideDepth', c.c_int), ('buildMs', c.c_float), ('collapseMs', c.c_float),
+                ('sahCost', c.c_double)]
+
+
+assert (c.sizeof(Triangle), c.sizeof(Camera), c.sizeof(Settings)) == (116, 64, 28)
+assert (c.sizeof(PixelSum), c.sizeof(BvhNode), c.sizeof(RtxQuery), c.sizeof(RtxHit)) == (40, 32, 28, 16)
+
+# numpy views of the same records, for scenes of millions of triangles.
+VEC = [('x', '<f4'), ('y', '<f4'), ('z', '<f4')]
+TRIANGLE_DTYPE = np.dtype([('origin', VEC), ('edge1', VEC), ('edge2', VEC), ('color', VEC),
+                           ('emission', '<f4'), ('oneSided', '<i4'), ('normal0', VEC), ('normal1', VEC),
+                           ('normal2', VEC), ('mesh', '<i4'), ('specularColor', VEC), ('smoothness', '<f4'),
+                           ('specularProbability', '<f4')])
+PIXELSUM_DTYPE = np.dtype([('radiance', VEC), ('albedo', VEC), ('normal', VEC), ('covered', '<u4')])
+NODE_DTYPE = np.dtype([('low', VEC), ('first', '<i4'), ('high', VEC), ('count', '<i4')])
+QUERY_DTYPE = np.dtype([('origin', VEC), ('direction', VEC), ('limit', '<f4')])
+HIT_DTYPE = np.dtype([('index', '<i4'), ('distance', '<f4'), ('u', '<f4'), ('v', '<f4')])
+assert (TRIANGLE_DTYPE.itemsize, PIXELSUM_DTYPE.itemsize, NODE_DTYPE.itemsize) == (116, 40, 32)
+
+ROOT = Path(__file__).resolve().parent
+LIBRARY = ROOT / 'libCudaRayTracer.so'
+
+# Every symbol the header declares (include/cuda_ray_tracer.h).
+EXPORTS = ('RtCreate', 'RtDestroy', 'RtShutdown', 'RtInitialize', 'RtRender', 'RtDenoise', 'RtReset',
+           'RtAccumulationVersion', 'RtSampleCount', 'RtEmbreeBuildMilliseconds', 'RtCpuThreadCount',
+           'RtBvhInfo', 'RtLastError', 'RtxQueryRays', 'RtxSobolSamples', 'RtxExportBvh', 'RtxBvhStatsGet',
+           'RtxReadAccumulation', 'RtxRenderStatsGet', 'RtxRenderDevice', 'RtxSetIntegrator', 'RtxSetTuning')
+
+
+def load_library(path=None):
+    """Loads the library and declares argument types (Tools/native_api.py:28-43)."""
+    path = path or os.environ.get('RAYTRACER_LIBRARY', LIBRARY)
+    path = Path(path).resolve()
+    if not path.exists():
+        raise FileNotFoundError(f'{path} is not built: run `make -C {ROOT}` (or __graft_entry__.build())')
+    lib = c.CDLL(str(path))
+    vp = c.c_void_p
+    lib.RtCreate.restype = vp
+    lib.RtDestroy.argtypes = lib.RtShutdown.argtypes = lib.RtReset.argtypes = lib.RtSampleCount.argtypes = [vp]
+    lib.RtSampleCount.restype = c.c_uint
+    lib.RtInitialize.argtypes = [vp, c.c_void_p, c.c_int, c.c_int, c.c_int]
+    lib.RtRender.argtypes = [vp, c.POINTER(Camera), c.POINTER(Settings), c.POINTER(c.c_ubyte), c.c_int, c.c_int,
+                             c.POINTER(c.c_float)]
+    lib.RtLastError.argtypes = [vp]
+    lib.RtLastError.restype = c.c_char_p
+    lib.RtCpuThreadCount.argtypes = [vp]
+    lib.RtDenoise.argtypes = [vp, c.POINTER(c.c_ubyte), c.c_int, c.POINTER(c.c_float)]
+    lib.RtAccumulationVersion.argtypes = [vp]
+    lib.RtAccumulationVersion.restype = c.c_uint
+    lib.RtEmbreeBuildMilliseconds.argtypes = [vp]
+    lib.RtEmbreeBuildMilliseconds.restype = c.c_float
+    lib.RtBvhInfo.argtypes = [vp, c.POINTER(c.c_int), c.POINTER(c.c_int), c.POINTER(c.c_float)]
+    lib.RtxQueryRays.argtypes = [vp, c.c_void_p, c.c_int, c.c_int, c.c_void_p]
+    lib.RtxSobolSamples.argtypes = [c.c_void_p, c.c_void_p, c.c_void_p, c.c_int, c.c_int, c.c_void_p]
+    lib.RtxExportBvh.argtypes = [vp, c.c_void_p, c.c_int, c.c_void_p, c.c_int]
+    lib.RtxBvhStatsGet.argtypes = [vp, c.POINTER(RtxBvhStats)]
+    lib.RtxReadAccumulation.argtypes = [vp, c.c_void_p, c.c_int]
+    lib.RtxRenderStatsGet.argtypes = [vp, c.POINTER(RtxRenderStats)]
+    lib.RtxRenderDevice.argtypes = [vp, c.POINTER(Camera), c.POINTER(Settings), c.POINTER(c.c_float)]
+    lib.RtxSetIntegrator.argtypes = [vp, c.c_int]
+    lib.RtxSetTuning.argtypes = [vp, c.c_int, c.c_int]
+    return lib
+
+
+def unpack(structure, values):
+    """Read Unity's JSON snapshot without changing its float inputs (Tools/native_api.py:45-48)."""
+    return structure(**{name: Vector(**values[name]) if field is Vector else values[name]
+                        for name, field in structure._fields_})
+
+
+def triangles_array(records):
+    """A contiguous TRIANGLE_DTYPE array from numpy records or a ctypes Triangle array."""
+    if isinstance(records, np.ndarray):
+        return np.ascontiguousarray(records, dtype=TRIANGLE_DTYPE)
+    return np.frombuffer(bytes(records), dtype=TRIANGLE_DTYPE).copy()
+
+
+class NativeError(RuntimeError):
+    pass
+
+
+class Session:
+    """Thin owner of one native session (RtCreate/RtDestroy) with checked calls."""
+
+    def __init__(self, lib=None):
+        self.lib = lib or load_library()
+        self.handle = self.lib.RtCreate()
+        self.width = self.height = 0
+
+    def close(self):
+        if self.handle:
+            self.lib.RtDestroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def error(self):
+        return self.lib.RtLastError(self.handle).decode()
+
+    def check(self, ok):
+        if not ok:
+            raise NativeError(self.error())
+
+    def initialize(self, triangles, width, height):
+        tris = triangles_array(triangles)
+        self.check(self.lib.RtInitialize(self.handle, tris.ctypes.data, len(tris), width, height))
+        self.width, self.height = width, height
+        return self
+
+    def render(self, camera, settings, backend=2, output=None):
+        output = output if output is not None else np.zeros(self.width * self.height * 4, np.uint8)
+        ms = c.c_float()
+        self.check(self.lib.RtRender(self.handle, c.byref(camera), c.byref(settings),
+                                     output.ctypes.data_as(c.POINTER(c.c_ubyte)), output.size, backend, c.byref(ms)))
+        return output, ms.value
+
+    def render_device(self, camera, settings):
+        ms = c.c_float()
+        self.check(self.lib.RtxRenderDevice(self.handle, c.byref(camera), c.byref(settings), c.byref(ms)))
+        return ms.value
+
+    def denoise(self, output=None):
+        output = output if output is not None else np.zeros(self.width * self.height * 4, np.uint8)
+        ms = c.c_float()
+        self.check(self.lib.RtDenoise(self.handle, output.ctypes.data_as(c.POINTER(c.c_ubyte)), output.size,
+                                      c.byref(ms)))
+        return output, ms.value
+
+    def accumulation(self):
+        out = np.zeros(self.width * self.height, PIXELSUM_DTYPE)
+        self.check(self.lib.RtxReadAccumulation(self.handle, out.ctypes.data, out.size))
+        return out
+
+    def query(self, queries, any_hit=False):
+        q = np.ascontiguousarray(queries, dtype=QUERY_DTYPE)
+        out = np.zeros(len(q), HIT_DTYPE)
+        self.check(self.lib.RtxQueryRays(self.handle, q.ctypes.data, len(q), int(any_hit), out.ctypes.data))
+        return out
+
+    def bvh_info(self):
+        nodes, depth, ms = c.c_int(), c.c_int(), c.c_float()
+        self.lib.RtBvhInfo(self.handle, c.byref(nodes), c.byref(depth), c.byref(ms))
+        return nodes.value, depth.value, ms.value
+
+    def bvh_stats(self):
+        st = RtxBvhStats()
+        self.check(self.lib.RtxBvhStatsGet(self.handle, c.byref(st)))
+        return {name: getattr(st, name) for name, _ in st._fields_}
+
+    def export_bvh(self, triangle_count):
+        n = self.bvh_info()[0]
+        nodes = np.zeros(n, NODE_DTYPE)
+        order = np.zeros(triangle_count, np.int32)
+        self.check(self.lib.RtxExportBvh(self.handle, nodes.ctypes.data, n, order.ctypes.data, triangle_count))
+        return nodes, order
+
+    def render_stats(self):
+        st = RtxRenderStats()
+        self.check(self.lib.RtxRenderStatsGet(self.handle, c.byref(st)))
+        return {name: getattr(st, name) for name, _ in st._fields_}
+
+    def set_integrator(self, mode):
+        self.check(self.lib.RtxSetIntegrator(self.handle, mode))
+
+    def set_tuning(self, block_size=0, paths_in_flight=0):
+        self.check(self.lib.RtxSetTuning(self.handle, block_size, paths_in_flight))
+
+    def sample_count(self):
+        return self.lib.RtSampleCount(self.handle)
+
+    def version(self):
+        return self.lib.RtAccumulationVersion(self.handle)
+
+
+def sobol_samples(lib, pixel, sample, seed, ndim):
+    """Device sampler values, shape (count, ndim)."""
+    pixel = np.ascontiguousarray(pixel, np.uint32)
+    sample = np.ascontiguousarray(sample, np.uint32)
+    seed = np.ascontiguousarray(seed, np.uint32)
+    out = np.zeros((len(pixel), ndim), np.float32)
+    if not lib.RtxSobolSamples(pixel.ctypes.data, sample.ctypes.data, seed.ctypes.data, len(pixel), ndim,
+                               out.ctypes.data):
+        raise NativeError('RtxSobolSamples failed')
+    return out

@@ -1,0 +1,264 @@
+"""Seeded synthetic scenes for the renderer's workloads and checks.
+
+Every generator is deterministic for a given seed (numpy PCG64 streams) and
+returns triangles as TRIANGLE_DTYPE records in the ABI layout, with colours
+given sRGB-encoded as the ABI expects (the library linearises them at
+RtInitialize, as the reference does at Native/renderer.cu:347).
+
+Workloads:
+  cornell_sphere()   - 10-triangle open box + 2-triangle ceiling light
+                       (emission 15) around a level-4 icosphere (5,120
+                       triangles, radius 0.3, +-2% seeded normal
+                       displacement); per-object albedo uniform in
+                       [0.2, 0.8]^3; 256x256, max depth 4.
+  displaced_sphere_room() - the same kind of room (10 walls + 2 light
+                       triangles) around a geodesic sphere with f = 224
+                       subdivisions per icosahedron edge (1,003,520
+                       triangles, the geodesic count closest to one million)
+                       and +-5% radial noise; 1920x1080, max depth 3,
+                       diffuse only.
+Check scenes mirror the geometry categories of the reference's own
+verifiers (Tools/verify_native.py, Tools/verify_bvh.cu).
+"""
+import math
+
+import numpy as np
+
+from native_api import Camera, Settings, Vector, TRIANGLE_DTYPE
+
+_PHI = (1.0 + 5.0 ** 0.5) / 2.0
+_ICO_V = np.array([(-1, _PHI, 0), (1, _PHI, 0), (-1, -_PHI, 0), (1, -_PHI, 0), (0, -1, _PHI), (0, 1, _PHI),
+                   (0, -1, -_PHI), (0, 1, -_PHI), (_PHI, 0, -1), (_PHI, 0, 1), (-_PHI, 0, -1), (-_PHI, 0, 1)],
+                  dtype=np.float64)
+_ICO_F = np.array([(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2),
+                   (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5),
+                   (2, 4, 11), (6, 2, 10), (8, 6, 7), (9, 8, 1)], dtype=np.int64)
+
+
+def records(v0, v1, v2, color=(1, 1, 1), emission=0.0, one_sided=0, normals=None, mesh=0, specular_color=(1, 1, 1),
+            smoothness=0.0, specular_probability=0.0):
+    """Triangle records from corner arrays (N,3); edges are float32 differences."""
+    v0 = np.asarray(v0, np.float32).reshape(-1, 3)
+    v1 = np.asarray(v1, np.float32).reshape(-1, 3)
+    v2 = np.asarray(v2, np.float32).reshape(-1, 3)
+    n = len(v0)
+    out = np.zeros(n, TRIANGLE_DTYPE)
+    e1 = v1 - v0
+    e2 = v2 - v0
+
+    def put(field, arr):
+        arr = np.broadcast_to(np.asarray(arr, np.float32), (n, 3))
+        out[field]['x'], out[field]['y'], out[field]['z'] = arr[:, 0], arr[:, 1], arr[:, 2]
+
+    put('origin', v0)
+    put('edge1', e1)
+    put('edge2', e2)
+    put('color', color)
+    put('specularColor', specular_color)
+    if normals is None:
+        fn = np.cross(e1.astype(np.float64), e2.astype(np.float64))
+        fn /= np.maximum(np.linalg.norm(fn, axis=1, keepdims=True), 1e-30)
+        normals = (fn, fn, fn)
+    for k, name in enumerate(('normal0', 'normal1', 'normal2')):
+        put(name, normals[k])
+    out['emission'] = emission
+    out['oneSided'] = one_sided
+    out['mesh'] = mesh
+    out['smoothness'] = smoothness
+    out['specularProbability'] = specular_probability
+    return out
+
+
+def quad(x0, x1, y0, y1, z, **kwargs):
+    """Two triangles covering [x0,x1]x[y0,y1] at depth z (Tools/verify_native.py:105-107)."""
+    a, b, c, d = (x0, y0, z), (x1, y0, z), (x1, y1, z), (x0, y1, z)
+    return records([a, a], [b, c], [c, d], **kwargs)
+
+
+def box_quad(p, u, v, **kwargs):
+    """Two triangles of the parallelogram p, p+u, p+u+v, p+v (winding p->p+u->p+u+v)."""
+    p, u, v = (np.asarray(x, np.float64) for x in (p, u, v))
+    return records([p, p], [p + u, p + u + v], [p + u + v, p + v], **kwargs)
+
+
+def geodesic_sphere(subdivisions, radius, center, noise, rng):
+    """Icosahedron with every face split into subdivisions^2 triangles, projected
+    to a sphere; each distinct vertex is moved along its radius by a factor
+    (1 + U(-noise, noise)). Returns corner arrays and smooth vertex normals."""
+    f = int(subdivisions)
+    ico = _ICO_V / np.linalg.norm(_ICO_V, axis=1, keepdims=True)
+    ii, jj = np.meshgrid(np.arange(f + 1), np.arange(f + 1), indexing='ij')
+    keep = ii + jj <= f
+    ii, jj = ii[keep], jj[keep]
+    local = {(int(a), int(b)): k for k, (a, b) in enumerate(zip(ii, jj))}
+    up_a = [(a, b) for a in range(f) for b in range(f - a)]
+    dn_a = [(a, b) for a in range(f - 1) for b in range(f - 1 - a)]
+    up = np.array([[local[(a, b)], local[(a + 1, b)], local[(a, b + 1)]] for a, b in up_a], np.int64)
+    dn = np.array([[local[(a + 1, b)], local[(a + 1, b + 1)], local[(a, b + 1)]] for a, b in dn_a], np.int64)
+    tri_local = np.concatenate([up, dn]) if len(dn) else up
+    pts = []
+    tris = []
+    for face_index, (A, B, C) in enumerate(_ICO_F):
+        a, b, c = ico[A], ico[B], ico[C]
+        p = a[None, :] + (b - a)[None, :] * (ii[:, None] / f) + (c - a)[None, :] * (jj[:, None] / f)
+        pts.append(p / np.linalg.norm(p, axis=1, keepdims=True))
+        tris.append(tri_local + face_index * len(ii))
+    pts = np.concatenate(pts)
+    tris = np.concatenate(tris)
+    keys = np.round(pts * (1 << 24)).astype(np.int64)
+    _, first, inverse = np.unique(keys, axis=0, return_index=True, return_inverse=True)
+    unique_pts = pts[first]
+    scale_f = 1.0 + rng.uniform(-noise, noise, len(unique_pts))
+    verts = unique_pts * (radius * scale_f)[:, None] + np.asarray(center, np.float64)[None, :]
+    corners = inverse.reshape(-1)[tris]
+    # Area-weighted vertex normals.
+    v0, v1, v2 = verts[corners[:, 0]], verts[corners[:, 1]], verts[corners[:, 2]]
+    fn = np.cross(v1 - v0, v2 - v0)
+    vn = np.zeros_like(verts)
+    for k in range(3):
+        for axis in range(3):
+            vn[:, axis] += np.bincount(corners[:, k], weights=fn[:, axis], minlength=len(verts))
+    vn /= np.maximum(np.linalg.norm(vn, axis=1, keepdims=True), 1e-30)
+    return v0, v1, v2, (vn[corners[:, 0]], vn[corners[:, 1]], vn[corners[:, 2]])
+
+
+def open_box(lo, hi, colors, light_half, light_y, emission):
+    """Five inward-facing walls (floor, ceiling, back, left, right: 10
+    triangles, open at z = lo.z) and a 2-triangle ceiling light facing down."""
+    x0, y0, z0 = lo
+    x1, y1, z1 = hi
+    walls = [
+        box_quad((x0, y0, z0), (0, 0, z1 - z0), (x1 - x0, 0, 0), color=colors[0], mesh=1),   # floor, normal +y
+        box_quad((x0, y1, z0), (x1 - x0, 0, 0), (0, 0, z1 - z0), color=colors[1], mesh=2),   # ceiling, normal -y
+        box_quad((x0, y0, z1), (0, y1 - y0, 0), (x1 - x0, 0, 0), color=colors[2], mesh=3),   # back, normal -z
+        box_quad((x0, y0, z0), (0, y1 - y0, 0), (0, 0, z1 - z0), color=colors[3], mesh=4),   # left, normal +x
+        box_quad((x1, y0, z0), (0, 0, z1 - z0), (0, y1 - y0, 0), color=colors[4], mesh=5),   # right, normal -x
+    ]
+    cx, cz = 0.5 * (x0 + x1), 0.5 * (z0 + z1)
+    h = light_half
+    light = box_quad((cx - h, light_y, cz - h), (2 * h, 0, 0), (0, 0, 2 * h), color=(1, 1, 1), emission=emission,
+                     mesh=6)
+    return np.concatenate(walls + [light])
+
+
+def camera(origin, target, tan_half_fov, aspect, up=(0.0, 1.0, 0.0)):
+    o = np.asarray(origin, np.float64)
+    fwd = np.asarray(target, np.float64) - o
+    fwd /= np.linalg.norm(fwd)
+    right = np.cross(np.asarray(up, np.float64), fwd)
+    right /= np.linalg.norm(right)
+    upv = np.cross(fwd, right)
+    v = lambda a: Vector(*(float(x) for x in a))
+    return Camera(v(o), v(right), v(upv), v(fwd), float(tan_half_fov), float(aspect), 1.0, 0)
+
+
+def cornell_sphere(seed=7, width=256, height=256, bounces=4):
+    """Config 'plain method, small': 5,132 triangles, 256x256, depth 4."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    colors = rng.uniform(0.2, 0.8, (6, 3))
+    room = open_box((-1.0, 0.0, -1.0), (1.0, 2.0, 1.0), colors[:5], 0.25, 1.98, 15.0)
+    v0, v1, v2, normals = geodesic_sphere(16, 0.3, (0.0, 0.55, 0.1), 0.02, rng)
+    sphere = records(v0, v1, v2, color=colors[5], normals=normals, mesh=7)
+    tris = np.concatenate([room, sphere])
+    cam = camera((0.0, 1.0, -3.4), (0.0, 1.0, 0.0), math.tan(math.radians(19.0)), width / height)
+    settings = Settings(bounces, 1.0, 0.0, 1.0, 0.0, 42, 1)
+    return tris, cam, settings, width, height
+
+
+def displaced_sphere_room(seed=11, width=1920, height=1080, bounces=3, subdivisions=224):
+    """Config 'traversal and build at scale': 1,003,520 + 12 triangles, 1920x1080, depth 3."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    colors = rng.uniform(0.2, 0.8, (6, 3))
+    room = open_box((-2.5, 0.0, -2.5), (2.5, 4.0, 2.5), colors[:5], 0.6, 3.98, 15.0)
+    v0, v1, v2, normals = geodesic_sphere(subdivisions, 1.3, (0.0, 1.45, 0.3), 0.05, rng)
+    sphere = records(v0, v1, v2, color=colors[5], normals=normals, mesh=7)
+    tris = np.concatenate([room, sphere])
+    cam = camera((0.0, 2.0, -7.0), (0.0, 1.6, 0.0), math.tan(math.radians(24.0)), width / height)
+    settings = Settings(bounces, 1.0, 0.0, 1.0, 0.0, 42, 1)
+    return tris, cam, settings, width, height
+
+
+# ---- check geometry, after the categories of Tools/verify_bvh.cu:115-139 ----
+
+def _tri(a, b, c, one_sided=0):
+    return records([a], [b], [c], color=(1, 1, 1), one_sided=one_sided)
+
+
+def edge_case_triangles():
+    """Shared edges, a one-sided face, a duplicate and a zero-area triangle."""
+    t0 = _tri((-1, -1, 0), (1, -1, 0), (1, 1, 0))
+    t1 = _tri((-1, -1, 0), (1, 1, 0), (-1, 1, 0), one_sided=1)
+    zero = _tri((0, 0, 0), (0, 0, 0), (0, 0, 0))
+    return np.concatenate([t0, t1, t0, zero])
+
+
+def scattered_triangles(rng, count=3000):
+    a = rng.uniform(-10, 10, (count, 3)).astype(np.float32)
+    b = a + np.array([.2, .3, 0], np.float32)
+    c = a + np.array([0, .1, .4], np.float32)
+    out = records(a, b, c, color=(1, 1, 1))
+    out['oneSided'] = np.arange(count) % 2
+    return out
+
+
+def overlapping_triangles(count=256):
+    return np.concatenate([_tri((-1, -1, 0), (1, -1, 0), (1, 1, 0))] * count)
+
+
+def exponential_triangles():
+    xs = []
+    for i in range(200):
+        x = 1.5 ** i
+        if not np.isfinite(np.float32(x)):
+            break
+        xs.append(x)
+    xs = np.array(xs, np.float64)
+    a = np.stack([xs, -np.ones_like(xs), np.zeros_like(xs)], 1)
+    b = np.stack([xs, np.ones_like(xs), np.zeros_like(xs)], 1)
+    c = np.stack([xs, np.zeros_like(xs), np.ones_like(xs)], 1)
+    return records(a, b, c, color=(1, 1, 1))
+
+
+def random_rays(rng, count=12000):
+    """Rays like Tools/verify_bvh.cu:105-114: random origins in [-10,10]^3, unit
+    directions with every 4th axis-aligned and every 5th carrying a 1e-40
+    (subnormal) x component; odd rays unbounded (1e30), even ones finite."""
+    from native_api import QUERY_DTYPE
+    q = np.zeros(count, QUERY_DTYPE)
+    o = rng.uniform(-10, 10, (count, 3)).astype(np.float32)
+    d = rng.uniform(-10, 10, (count, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    d = d.astype(np.float32)
+    i = np.arange(count)
+    axis = i % 3
+    aligned = i % 4 == 0
+    d[aligned] = 0
+    d[aligned, axis[aligned]] = 1
+    d[i % 5 == 0, 0] = np.float32(1e-40)
+    limit = np.where(i % 2 == 1, np.float32(1e30), np.abs(rng.uniform(-10, 10, count)).astype(np.float32))
+    for k, ax in enumerate('xyz'):
+        q['origin'][ax] = o[:, k]
+        q['direction'][ax] = d[:, k]
+    q['limit'] = limit
+    return q
+
+
+def edge_grid_rays():
+    """Axis-parallel rays from grid points on the test faces (Tools/verify_bvh.cu:120-122)."""
+    from native_api import QUERY_DTYPE
+    rows = []
+    for z in (-1.0, 0.0, 1.0):
+        for x in (-1.0, 0.0, 1.0):
+            for d in ((0, 0, 1), (0, 0, -1), (0, 1, 0), (1e-40, 0, 1)):
+                for limit in (.5, 1.0, 2.0, 1e30):
+                    rows.append(((x, x, z), d, limit))
+    q = np.zeros(len(rows), QUERY_DTYPE)
+    for k, (o, d, limit) in enumerate(rows):
+        q[k]['origin'] = tuple(np.float32(v) for v in o)
+        q[k]['direction'] = tuple(np.float32(v) for v in d)
+        q[k]['limit'] = np.float32(limit)
+    return q
+
+
+def concat_queries(*parts):
+    return np.concatenate(parts)

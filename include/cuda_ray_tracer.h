@@ -1,0 +1,175 @@
+/*
+ * C ABI of libCudaRayTracer.so: a drop-in for the reference renderer's native
+ * library (Ekansh-K/custom-ray-tracing-shader, Native/renderer.cu), rebuilt for
+ * NVIDIA B200 (sm_100a).
+ *
+ * The thirteen Rt* entry points keep the reference's names, argument meaning,
+ * return convention (1 = success, 0 = failure, message in RtLastError) and
+ * struct layouts, so the Unity P/Invoke bindings
+ * (UnityRayTracer/Assets/RayTracing/RayTraceSession.cs:36-63) and the ctypes
+ * bindings (Tools/native_api.py:28-43) load it unchanged.
+ *
+ * The Rtx* entry points are additive: they have no counterpart in the
+ * reference's exported ABI. Each one names the reference test harness whose
+ * job it takes over (per-ray queries, sampler values, the built BVH, the raw
+ * accumulation buffer, ray counters).
+ *
+ * All entry points use plain C types and pointers. A session is not
+ * thread-safe; use one session per thread (the reference's rule).
+ */
+#ifndef CUDA_RAY_TRACER_H
+#define CUDA_RAY_TRACER_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- records (layouts fixed by Native/renderer.cu:11-30,46 and Native/bvh.cuh:7) ---- */
+
+typedef struct RtVector { float x, y, z; } RtVector;
+
+/* Scene primitive, 116 bytes (Native/renderer.cu:11-18). Colours are sRGB
+ * encoded; the library converts them to linear at RtInitialize
+ * (Native/renderer.cu:347). */
+typedef struct Triangle {
+    RtVector origin, edge1, edge2, color;
+    float emission;
+    int oneSided;
+    RtVector normal0, normal1, normal2;
+    int mesh;
+    RtVector specularColor;
+    float smoothness, specularProbability;
+} Triangle;
+
+/* Camera, 64 bytes (Native/renderer.cu:21-24). */
+typedef struct CameraData {
+    RtVector origin, right, up, forward;
+    float tanHalfFov, aspect, orthographicSize;
+    int orthographic;
+} CameraData;
+
+/* Per-call settings, 28 bytes (Native/renderer.cu:25-30). */
+typedef struct RenderSettings {
+    int maxBounces;
+    float exposure, aperture, focusDistance, skyStrength;
+    unsigned seed;
+    int raysPerPixel;
+} RenderSettings;
+
+/* Progressive accumulation record, 40 bytes per pixel, row-major with row 0 at
+ * the bottom of the image (Native/renderer.cu:46, :291). */
+typedef struct PixelSum {
+    RtVector radiance, albedo, normal;
+    unsigned covered;
+} PixelSum;
+
+/* Binary BVH node in the reference layout, 32 bytes (Native/bvh.cuh:7). A
+ * leaf has count > 0 and covers order[first .. first+count); an interior node
+ * has count == 0 and children first, first+1. */
+typedef struct BvhNode {
+    RtVector low;
+    int first;
+    RtVector high;
+    int count;
+} BvhNode;
+
+/* Ray query and its result (Tools/verify_bvh.cu:8 and Native/renderer.cu:43). */
+typedef struct RtxQuery { RtVector origin, direction; float limit; } RtxQuery;
+typedef struct RtxHit { int index; float distance, u, v; } RtxHit;
+
+/* Counters and timings of the last successful RtRender / RtxRenderDevice. */
+typedef struct RtxRenderStats {
+    unsigned long long primaryRays;   /* closest-hit queries at bounce 0 */
+    unsigned long long secondaryRays; /* closest-hit queries at bounces >= 1 */
+    unsigned long long shadowRays;    /* any-hit queries for light sampling */
+    unsigned long long paths;         /* width * height * raysPerPixel */
+    float renderMs;                   /* device time of the render kernels (CUDA events) */
+    float extendMs;                   /* part of renderMs spent in closest-hit traversal kernels */
+    float shadowMs;                   /* part of renderMs spent in any-hit traversal kernels */
+    int kernelLaunches;               /* kernels launched by the render */
+} RtxRenderStats;
+
+/* Summary of the acceleration structure built at RtInitialize. */
+typedef struct RtxBvhStats {
+    int binaryNodes;        /* reference-layout nodes (same count as Native/bvh.cuh) */
+    int binaryDepth;        /* deepest binary node (the reference's maxDepth) */
+    int wideNodes;          /* 8-wide compressed nodes used for traversal */
+    int wideDepth;          /* deepest wide node */
+    float buildMs;          /* device time of the binned-SAH build (CUDA events) */
+    float collapseMs;       /* device time of the wide collapse and triangle packing */
+    double sahCost;         /* SAH cost of the binary tree, normalised by the root area */
+} RtxBvhStats;
+
+/* ---- the reference's thirteen exports ---- */
+
+/* Native/renderer.cu:309. Returns a new, empty session. */
+void* RtCreate(void);
+/* Native/renderer.cu:332. Frees the session and everything it owns. */
+void RtDestroy(void* session);
+/* Native/renderer.cu:319. Frees scene and image buffers; the session stays usable. */
+void RtShutdown(void* session);
+/* Native/renderer.cu:340. Copies the triangles, builds the BVH on the GPU and
+ * allocates a width x height image. 1 <= width, height <= 4096, count > 0. */
+int RtInitialize(void* session, const Triangle* triangles, int count, int width, int height);
+/* Native/renderer.cu:374. Adds settings->raysPerPixel paths per pixel to the
+ * accumulation and writes the tonemapped RGBA8 image (width*height*4 bytes,
+ * bottom row first) to output. backend: 0 CPU one thread, 1 CPU all threads,
+ * 2 CUDA, 3 Embree (not available in this build: returns 0). computeMs
+ * receives the render time (CUDA events for backend 2). */
+int RtRender(void* session, const CameraData* camera, const RenderSettings* settings,
+             unsigned char* output, int outputBytes, int backend, float* computeMs);
+/* Native/renderer.cu:436. Filters the current accumulation into output without
+ * changing it, the sample count or the accumulation version. */
+int RtDenoise(void* session, unsigned char* output, int outputBytes, float* milliseconds);
+/* Native/renderer.cu:310. Clears the accumulation and bumps its version. */
+void RtReset(void* session);
+/* Native/renderer.cu:311. */
+unsigned RtAccumulationVersion(void* session);
+/* Native/renderer.cu:312. Paths accumulated per pixel since the last reset. */
+unsigned RtSampleCount(void* session);
+/* Native/renderer.cu:313. Always 0: this build has no Embree backend. */
+float RtEmbreeBuildMilliseconds(void* session);
+/* Native/renderer.cu:314. 0 after a CUDA render, else the CPU thread count. */
+int RtCpuThreadCount(void* session);
+/* Native/renderer.cu:315. Binary node count, depth and BVH build time in ms. */
+void RtBvhInfo(void* session, int* nodes, int* depth, float* buildMs);
+/* Native/renderer.cu:318. Message for the last failure on this session. */
+const char* RtLastError(void* session);
+
+/* ---- additive entry points (no counterpart in the reference's exported ABI) ---- */
+
+/* Per-ray BVH queries on the GPU for a host array of rays, closest hit
+ * (any = 0) or any hit (any != 0), against the session's scene. Takes over the
+ * job of the reference's differential checker kernel (Tools/verify_bvh.cu:26-34). */
+int RtxQueryRays(void* session, const RtxQuery* queries, int count, int any, RtxHit* hits);
+/* Sampler values on the GPU: out[i*ndim + d] = sample d of the path
+ * (pixel[i], sample[i], seed[i]); ndim <= 260. Takes over the job of the
+ * reference's sampler check kernel (Tools/verify_sampling.cu:8-13). */
+int RtxSobolSamples(const unsigned* pixel, const unsigned* sample, const unsigned* seed, int count, int ndim, float* out);
+/* Copies the GPU-built binary BVH in the reference layout (node count from
+ * RtBvhInfo) and its primitive order (one int per triangle). The BVH checker
+ * reads the same arrays from the reference session (Tools/verify_bvh.cu:42-66). */
+int RtxExportBvh(void* session, BvhNode* nodes, int nodeCapacity, int* order, int orderCapacity);
+/* BVH summary (node counts, depths, build times, SAH cost). */
+int RtxBvhStatsGet(void* session, RtxBvhStats* stats);
+/* Copies the raw accumulation (width*height PixelSum records) of the last
+ * backend used. The reference keeps it private (Native/renderer.cu:55,61). */
+int RtxReadAccumulation(void* session, PixelSum* out, int count);
+/* Counters and device timings of the last render. */
+int RtxRenderStatsGet(void* session, RtxRenderStats* stats);
+/* RtRender on the CUDA backend without the image copy to the host: the
+ * accumulation and the device-side RGBA8 image are updated in HBM. Same
+ * validation, auto-reset and sample-count rules as RtRender. */
+int RtxRenderDevice(void* session, const CameraData* camera, const RenderSettings* settings, float* computeMs);
+/* Selects the CUDA integrator: 0 = wavefront (queues per bounce, default),
+ * 1 = one-kernel path tracer. Both give bit-identical accumulations. */
+int RtxSetIntegrator(void* session, int mode);
+/* Tunables of the wavefront integrator: threads per block of the traversal
+ * kernels (64..1024, multiple of 32) and paths in flight per wave (>= 1024).
+ * 0 keeps the current value. */
+int RtxSetTuning(void* session, int blockSize, int pathsInFlight);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CUDA_RAY_TRACER_H */
