@@ -1,0 +1,487 @@
+#!/usr/bin/env python3
+"""Benchmark: Mrays/s of the progressive path tracer on its at-scale workload.
+
+Workload (one step = one progressive pass of 16 paths per pixel):
+  displaced_sphere_room - a seeded geodesic sphere of 1,003,520 triangles
+  (+-5% radial noise) in a 12-triangle room with one quad light,
+  1920x1080, 16 paths per pixel per step, maximum depth 3, diffuse only.
+  Rays = closest-hit queries (primary + secondary) + shadow (any-hit)
+  queries, counted on the device.
+
+Line fields beyond the common contract:
+  roofline      dominant traversal kernel against measured HBM bandwidth;
+                algorithmic bytes per ray = 64 * interior nodes + 44 *
+                triangles that the reference's binary-BVH traversal
+                (Native/renderer.cu:136-178) visits for the same rays, counted
+                by the oracle on a pixel sample of the workload
+  cpu_baseline  the reference's own CPU backend (Native/renderer.cu compiled
+                from its sources into oracle/_ref, else the oracle port) on a
+                bounded row sample, all host threads
+  build         GPU BVH build (binned SAH + wide collapse), Mtris/s
+  reference_cuda  the reference's own CUDA renderer built for sm_100a, same
+                scene and settings, when oracle/_ref is present
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+For N > 1 run under torch.distributed.run; each rank renders its own copy of
+the workload on its own GPU (replicas, weak scaling) and the step time is the
+maximum over ranks.
+"""
+import argparse
+import ctypes as c
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / 'custom-ray-tracing-shader_b200'))
+sys.path.insert(0, str(ROOT / 'oracle'))
+
+WORKLOAD = 'displaced_sphere_room'
+METRIC = 'Mrays/s'
+SPP_PER_STEP = 16
+
+
+def parse():
+    p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    p.add_argument('--gpus', type=int, default=1)
+    p.add_argument('--steps', type=int, default=10)
+    p.add_argument('--warmup', type=int, default=3)
+    p.add_argument('--impl', choices=('ours', 'reference'), default='ours')
+    p.add_argument('--integrator', choices=('auto', 'wavefront', 'megakernel'), default='auto')
+    p.add_argument('--cpu-seconds', type=float, default=12.0, help='budget of the CPU-baseline sample')
+    p.add_argument('--no-cpu-baseline', action='store_true')
+    p.add_argument('--no-reference-cuda', action='store_true')
+    p.add_argument('--resolution', default=None, help='WxH override, for small profiling cases')
+    p.add_argument('--spp', type=int, default=SPP_PER_STEP, help='paths per pixel per step (1..16)')
+    return p.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get('RANK', 0)), int(os.environ.get('LOCAL_RANK', 0)), int(os.environ.get('WORLD_SIZE', 1))
+
+
+class Dist:
+    """torch.distributed plumbing for N > 1 (barrier, max over ranks)."""
+
+    def __init__(self, world):
+        self.world = world
+        self.pg = None
+        if world > 1:
+            import datetime
+            import torch
+            import torch.distributed as dist
+            backend = 'nccl' if torch.cuda.is_available() else 'gloo'
+            if backend == 'nccl':
+                torch.cuda.set_device(0)
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+            self.torch, self.dist, self.backend = torch, dist, backend
+
+    def barrier(self):
+        if self.world > 1:
+            self.dist.barrier()
+
+    def max(self, value):
+        if self.world == 1:
+            return value
+        t = self.torch.tensor([float(value)], dtype=self.torch.float64,
+                              device='cuda' if self.backend == 'nccl' else 'cpu')
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, value):
+        if self.world == 1:
+            return value
+        t = self.torch.tensor([float(value)], dtype=self.torch.float64,
+                              device='cuda' if self.backend == 'nccl' else 'cpu')
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.world > 1:
+            self.dist.barrier()
+            self.dist.destroy_process_group()
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+    FIELDS = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+              'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+              'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, gpu_index):
+        self.gpu_index = gpu_index
+        self.proc = None
+        self.path = Path(os.environ.get('TMPDIR', '/tmp')) / f'bench_clocks_{os.getpid()}.csv'
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(['nvidia-smi', '-i', str(self.gpu_index), f'--query-gpu={self.FIELDS}',
+                                          '--format=csv,noheader,nounits', '-lms', '200'],
+                                         stdout=open(self.path, 'w'), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['nvidia-smi unavailable']}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, sm_max, power, reasons = [], None, [], set()
+        names = ('hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap')
+        for line in self.path.read_text().splitlines():
+            parts = [p.strip() for p in line.split(',')]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                sm_max = float(parts[2])
+                power.append(float(parts[3]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower().startswith('active'):
+                    reasons.add(name)
+        self.path.unlink(missing_ok=True)
+        if not sm:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['no samples']}
+        under_load = [s for s, p in zip(sm, power) if p > 0.5 * max(power)] or sm
+        return {'sm_mhz': statistics.median(under_load), 'sm_max_mhz': sm_max, 'reasons': sorted(reasons),
+                'samples': len(sm)}
+
+
+def measured_peaks():
+    path = ROOT / 'MEASURED_PEAKS.json'
+    if path.exists():
+        data = json.loads(path.read_text())
+        return float(data['hbm_gbs']), 'measured'
+    return 6650.0, 'fallback'
+
+
+def workload(args=None):
+    import scenes
+    kwargs = {}
+    if args is not None and args.resolution:
+        kwargs['width'], kwargs['height'] = (int(v) for v in args.resolution.lower().split('x'))
+    tris, cam, settings, w, h = scenes.displaced_sphere_room(**kwargs)
+    settings.raysPerPixel = args.spp if args is not None else SPP_PER_STEP
+    return tris, cam, settings, w, h
+
+
+def sample_rows(h, stride):
+    return list(range(stride // 2, h, stride))
+
+
+def algorithmic_bytes(tris, cam, settings, w, h, pixel_count=4096):
+    """Bytes per closest and per shadow query of the reference's traversal,
+    from the oracle's counters on a seeded pixel sample of the workload."""
+    import numpy as np
+    from oracle_api import Oracle
+    o = Oracle()
+    sc = o.scene(tris)
+    rng = np.random.Generator(np.random.PCG64(5))
+    pixels = rng.choice(w * h, pixel_count, replace=False)
+    _, _, counts = o.render_pixels(sc, cam, settings, w, h, pixels)
+    sc.close()
+    closest_q, closest_int, closest_tri = counts[3], counts[4], counts[6]
+    shadow_q, shadow_int, shadow_tri = counts[7], counts[8], counts[10]
+    return {
+        'closest': (64.0 * closest_int + 44.0 * closest_tri) / max(closest_q, 1),
+        'shadow': (64.0 * shadow_int + 44.0 * shadow_tri) / max(shadow_q, 1),
+        'sample_pixels': int(pixel_count),
+        'interior_per_closest': float(closest_int / max(closest_q, 1)),
+        'triangles_per_closest': float(closest_tri / max(closest_q, 1)),
+    }
+
+
+def cpu_baseline(tris, cam, settings, w, h, budget_s):
+    """The reference's CPU backend on all host threads over a bounded row sample."""
+    from oracle_api import Oracle, Reference, reference_available
+    kind = 'reference' if reference_available() else 'port'
+    impl = Reference() if kind == 'reference' else Oracle()
+    threads = impl.max_threads()
+    sc = impl.scene(tris)
+    # Size the sample: one probe row, then enough evenly spaced rows for the budget.
+    t0 = time.perf_counter()
+    impl.render(sc, cam, settings, w, h, rows=(h // 2, h // 2 + 1), threads=threads)
+    per_row = max(time.perf_counter() - t0, 1e-4)
+    nrows = int(max(1, min(h, budget_s / per_row)))
+    stride = max(1, h // nrows)
+    rows = sample_rows(h, stride)
+    t0 = time.perf_counter()
+    for y in rows:
+        impl.render(sc, cam, settings, w, h, rows=(y, y + 1), threads=threads)
+    elapsed = time.perf_counter() - t0
+    sc.close()
+    # Ray count of the same rows, from the oracle's counters (identical paths).
+    o = Oracle()
+    osc = o.scene(tris)
+    rays = 0
+    for y in rows:
+        _, _, counts = o.render(osc, cam, settings, w, h, rows=(y, y + 1))
+        rays += int(counts[0] + counts[1] + counts[2])
+    osc.close()
+    return {
+        'value': rays / elapsed / 1e6, 'unit': METRIC, 'cores': threads, 'kind': kind,
+        'sample': f'{len(rows)} of {h} rows (every {stride}th) x {w} px x {settings.raysPerPixel} spp, '
+                  f'{rays} rays in {elapsed:.2f} s',
+        'seconds': elapsed, 'rays': rays,
+    }
+
+
+def reference_cuda(tris, cam, settings, w, h, rays_per_step, steps=3):
+    """The reference's own CUDA renderer (oracle/_ref, built for sm_100a)."""
+    from oracle_api import Reference, ReferenceSession, reference_available
+    if not reference_available():
+        return None
+    ref = ReferenceSession(Reference())
+    try:
+        ref.initialize(tris, w, h)
+        times = []
+        for _ in range(steps + 1):
+            _, ms = ref.render(cam, settings)
+            times.append(ms)
+        ms = statistics.median(times[1:])
+        return {'value': rays_per_step / ms / 1e3, 'unit': METRIC, 'ms_per_step': ms,
+                'note': 'Native/renderer.cu renderKernel built for sm_100a, same scene, settings and ray count'}
+    finally:
+        ref.close()
+
+
+def l2_flusher():
+    try:
+        import torch
+        if torch.cuda.is_available():
+            buf = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device='cuda')  # 256 MB > 126 MB L2
+
+            def flush():
+                buf.fill_(1.0)
+                torch.cuda.synchronize()
+            return flush, 'flushed between steps (256 MB write)'
+    except Exception:
+        pass
+    return (lambda: None), 'inputs larger than L2 (1.0M triangles: 116 MB records + 48 MB packed + 8.5 MB nodes)'
+
+
+def run_ours(args, rank, local_rank, world):
+    import numpy as np
+    from native_api import Session, load_library
+    dist = Dist(world)
+    lib = load_library()
+    tris, cam, settings, w, h = workload(args)
+    s = Session(lib)
+    s.initialize(tris, w, h)
+    bvh = s.bvh_stats()
+    # Integrator choice: both give identical sums; pick the faster on warm-up.
+    candidates = {'wavefront': 0, 'megakernel': 1}
+    if args.integrator != 'auto':
+        candidates = {args.integrator: candidates[args.integrator]}
+    flush, l2_note = l2_flusher()
+    best, best_ms = None, None
+    for name, mode in candidates.items():
+        s.set_integrator(mode)
+        times = []
+        for _ in range(max(args.warmup, 1)):
+            flush()
+            times.append(s.render_device(cam, settings))
+        ms = min(times)
+        if best_ms is None or ms < best_ms:
+            best, best_ms = name, ms
+    s.set_integrator(candidates[best])
+    for _ in range(args.warmup):
+        flush()
+        s.render_device(cam, settings)
+    # Timed region: K passes, device time from CUDA events around each pass.
+    gpu_index = int((os.environ.get('CUDA_VISIBLE_DEVICES') or str(local_rank)).split(',')[0]) if world > 1 else 0
+    if world == 1 and os.environ.get('CUDA_VISIBLE_DEVICES'):
+        gpu_index = int(os.environ['CUDA_VISIBLE_DEVICES'].split(',')[0])
+    clocks = Clocks(gpu_index)
+    rays = launches = 0
+    device_ms = extend_ms = shadow_ms = 0.0
+    per_kind = {'primaryRays': 0, 'secondaryRays': 0, 'shadowRays': 0}
+    dist.barrier()
+    clocks.start()
+    wall0 = time.perf_counter()
+    for _ in range(args.steps):
+        flush()
+        device_ms += s.render_device(cam, settings)
+        st = s.render_stats()
+        rays += st['primaryRays'] + st['secondaryRays'] + st['shadowRays']
+        for k in per_kind:
+            per_kind[k] += st[k]
+        launches += st['kernelLaunches']
+        extend_ms += st['extendMs']
+        shadow_ms += st['shadowMs']
+    wall = time.perf_counter() - wall0
+    clock_info = clocks.stop()
+    dist.barrier()
+    t_max = dist.max(device_ms)
+    total_rays = dist.sum(rays)
+    value = total_rays / t_max / 1e3
+    # End to end: RtRender through the C ABI into pinned host memory.
+    out_buf, pinned = None, False
+    try:
+        import torch
+        if torch.cuda.is_available():
+            t = torch.empty(w * h * 4, dtype=torch.uint8, pin_memory=True)
+            out_buf = np.frombuffer((c.c_ubyte * (w * h * 4)).from_address(t.data_ptr()), np.uint8)
+            pinned = True
+    except Exception:
+        pass
+    if out_buf is None:
+        out_buf = np.zeros(w * h * 4, np.uint8)
+    for _ in range(args.warmup):
+        s.render(cam, settings, output=out_buf)
+    dist.barrier()
+    e2e_rays = 0
+    e0 = time.perf_counter()
+    for _ in range(args.steps):
+        s.render(cam, settings, output=out_buf)
+        st = s.render_stats()
+        e2e_rays += st['primaryRays'] + st['secondaryRays'] + st['shadowRays']
+    e2e_s = dist.max(time.perf_counter() - e0)
+    e2e_value = dist.sum(e2e_rays) / e2e_s / 1e6
+    peak, peak_kind = measured_peaks()
+    result = None
+    if rank == 0:
+        alg = algorithmic_bytes(tris, cam, settings, w, h)
+        if best == 'wavefront':
+            kernel = 'extendKernel (closest-hit traversal)'
+            closest = per_kind['primaryRays'] + per_kind['secondaryRays']
+            achieved = closest * alg['closest'] / (extend_ms / 1e3) / 1e9 if extend_ms > 0 else None
+        else:
+            kernel = 'megakernel (closest + shadow traversal and shading)'
+            achieved = ((per_kind['primaryRays'] + per_kind['secondaryRays']) * alg['closest'] +
+                        per_kind['shadowRays'] * alg['shadow']) / (device_ms / 1e3) / 1e9
+        # DRAM traffic of the dominant kernel per launch, from the committed
+        # ncu summary (bytes per ray of a capture of this kernel), scaled to
+        # the rays of one launch here.
+        closest_step = (per_kind['primaryRays'] + per_kind['secondaryRays']) / args.steps
+        if best == 'wavefront':
+            launches_step = settings.raysPerPixel * settings.maxBounces  # one wave per sample row
+            rays_per_launch = closest_step / launches_step
+        else:
+            rays_per_launch = sum(per_kind.values()) / args.steps
+        traffic = None
+        tfile = ROOT / 'profiles' / 'traffic.json'
+        if tfile.exists():
+            tdata = json.loads(tfile.read_text()).get(best)
+            if tdata:
+                traffic = tdata['dram_bytes_per_ray'] * rays_per_launch
+        roofline = {'bound': 'hbm', 'kernel': kernel, 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
+                    'frac': (achieved / peak) if achieved else None, 'traffic': traffic,
+                    'peak_source': f'{peak_kind} hbm_gbs (MEASURED_PEAKS.json)' if peak_kind == 'measured' else
+                                   'fallback 6.65 TB/s',
+                    'bytes_per_closest_query': alg['closest'], 'bytes_per_shadow_query': alg['shadow'],
+                    'model': '64 B per interior node + 44 B per triangle the reference traversal visits',
+                    'sample_pixels': alg['sample_pixels']}
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            cpu = cpu_baseline(tris, cam, settings, w, h, args.cpu_seconds)
+            cpu.pop('seconds', None)
+            cpu.pop('rays', None)
+        ref_cuda = None
+        if world == 1 and not args.no_reference_cuda:
+            try:
+                ref_cuda = reference_cuda(tris, cam, settings, w, h, rays / args.steps)
+            except Exception as exc:
+                ref_cuda = {'unavailable': str(exc)}
+        result = {
+            'metric': METRIC, 'value': value, 'unit': METRIC, 'n_gpus': world, 'steps': args.steps,
+            'warmup': args.warmup, 'ms_per_step': t_max / args.steps, 'higher_is_better': True,
+            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic (seeded procedural scene)',
+            'config': {'workload': WORKLOAD, 'triangles': len(tris), 'width': w, 'height': h,
+                       'spp_per_step': settings.raysPerPixel, 'max_depth': settings.maxBounces,
+                       'integrator': best, 'l2': l2_note, 'parallelism': f'replicas x{world}'},
+            'e2e': {'value': e2e_value, 'unit': METRIC, 'h2d_bytes_per_step': 64 + 28,
+                    'd2h_bytes_per_step': w * h * 4, 'pinned_output': pinned},
+            'gpu_launches': launches,
+            'clocks': clock_info,
+            'roofline': roofline,
+            'cpu_baseline': cpu,
+            'rays': {k: v // args.steps for k, v in per_kind.items()},
+            'wall_ms_per_step': wall * 1e3 / args.steps,
+            'build': {'ms': bvh['buildMs'] + bvh['collapseMs'], 'binned_sah_ms': bvh['buildMs'],
+                      'collapse_ms': bvh['collapseMs'],
+                      'mtris_per_s': len(tris) / (bvh['buildMs'] + bvh['collapseMs']) / 1e3,
+                      'binary_nodes': bvh['binaryNodes'], 'binary_depth': bvh['binaryDepth'],
+                      'wide_nodes': bvh['wideNodes'], 'sah_cost': bvh['sahCost']},
+            'reference_cuda': ref_cuda,
+            'time_to_35db': None,
+        }
+    s.close()
+    dist.close()
+    return result
+
+
+def run_reference(args, rank, world):
+    """The reference's own CPU implementation on this machine's host cores."""
+    if rank != 0:
+        return None
+    from oracle_api import Oracle, Reference, reference_available
+    tris, cam, settings, w, h = workload(args)
+    kind = 'reference' if reference_available() else 'port'
+    impl = Reference() if kind == 'reference' else Oracle()
+    threads = impl.max_threads()
+    sc = impl.scene(tris)
+    t0 = time.perf_counter()
+    impl.render(sc, cam, settings, w, h, rows=(h // 2, h // 2 + 1), threads=threads)
+    per_row = max(time.perf_counter() - t0, 1e-4)
+    budget = max(0.5, 60.0 / max(1, args.steps + args.warmup))
+    stride = max(1, int(h / max(1, budget / per_row)))
+    rows = sample_rows(h, stride)
+    for _ in range(args.warmup):
+        for y in rows[:1]:
+            impl.render(sc, cam, settings, w, h, rows=(y, y + 1), threads=threads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        for y in rows:
+            impl.render(sc, cam, settings, w, h, rows=(y, y + 1), threads=threads)
+        times.append(time.perf_counter() - t0)
+    sc.close()
+    o = Oracle()
+    osc = o.scene(tris)
+    rays = 0
+    for y in rows:
+        _, _, counts = o.render(osc, cam, settings, w, h, rows=(y, y + 1))
+        rays += int(counts[0] + counts[1] + counts[2])
+    osc.close()
+    total = sum(times)
+    value = rays * args.steps / total / 1e6
+    sample = f'{len(rows)} of {h} rows (every {stride}th) x {w} px x {settings.raysPerPixel} spp per step'
+    return {
+        'impl': 'reference', 'metric': METRIC, 'value': value, 'unit': METRIC, 'n_gpus': world,
+        'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': total * 1e3 / args.steps,
+        'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32',
+        'data': 'synthetic (seeded procedural scene)',
+        'config': {'workload': WORKLOAD, 'triangles': len(tris), 'width': w, 'height': h,
+                   'spp_per_step': settings.raysPerPixel, 'max_depth': settings.maxBounces,
+                   'parallelism': 'host cores'},
+        'cpu_baseline': {'value': value, 'unit': METRIC, 'cores': threads, 'kind': kind, 'sample': sample},
+        'e2e': {'value': value, 'unit': METRIC, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
+    }
+
+
+def main():
+    args = parse()
+    rank, local_rank, world = dist_env()
+    if world > 1 and args.impl == 'ours':
+        os.environ['CUDA_VISIBLE_DEVICES'] = str(local_rank) if 'CUDA_VISIBLE_DEVICES' not in os.environ else \
+            os.environ['CUDA_VISIBLE_DEVICES'].split(',')[local_rank]
+    if args.impl == 'reference':
+        result = run_reference(args, rank, world)
+    else:
+        result = run_ours(args, rank, local_rank, world)
+    if rank == 0 and result is not None:
+        print(json.dumps(result), flush=True)
+
+
+if __name__ == '__main__':
+    main()

@@ -395,11 +395,12 @@ __global__ void renumberKernel(const BinNode* nodes, int count, const int* newIn
 // ---- collapse into wide nodes (logic in rt_collapse.cuh) ----
 __global__ void collapseKernel(const BinNode* bn, const int* order, const float4* plo, const float4* phi,
                                const SceneTri* tris, const Job* jobs, int nJobs, Job* nextJobs, WideNode* wide,
-                               float4* packed, int* counters, int wideCapacity, int jobCapacity, int triCapacity) {
+                               float4* packed, int* counters, int wideCapacity, int jobCapacity, int triCapacity,
+                               int group) {
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= nJobs) return;
     collapseJob(jobs[j], bn, order, plo, phi, tris, nextJobs, wide, packed, counters, wideCapacity, jobCapacity,
-                triCapacity);
+                triCapacity, group);
 }
 
 inline int blocksFor(long long n, int block) { return (int)((n + block - 1) / block); }
@@ -417,7 +418,7 @@ void freeBvh(BuiltBvh& b) {
 }
 
 cudaError_t buildBvh(const SceneTri* tris, int n, cudaStream_t stream, BuiltBvh& out, BuildResult& result,
-                     const char** failure) {
+                     const char** failure, int leafGroup) {
     *failure = nullptr;
     cudaError_t err = cudaSuccess;
     const int nodeCapacity = 2 * n + 2;
@@ -524,7 +525,8 @@ cudaError_t buildBvh(const SceneTri* tris, int n, cudaStream_t stream, BuiltBvh&
             collapseKernel<<<blocksFor(nJobs, 64), 64, 0, stream>>>(out.binNodes, out.order, out.primLo, out.primHi, tris,
                                                                     jobs, nJobs, jobsB,
                                                                     reinterpret_cast<WideNode*>(out.wideNodes),
-                                                                    out.packedTris, counters, wideCapacity, jobCapacity, n);
+                                                                    out.packedTris, counters, wideCapacity, jobCapacity, n,
+                                                                    leafGroup);
             RT_TRY(cudaGetLastError());
             RT_TRY(cudaMemcpyAsync(hostCounters, counters, 8 * sizeof(int), cudaMemcpyDeviceToHost, stream));
             RT_TRY(cudaStreamSynchronize(stream));

@@ -82,16 +82,28 @@ RT_HD float4 loadVec(const float4* p) {
     return *p;
 #endif
 }
-RT_HD unsigned byteOf(unsigned lo4, unsigned hi4, int i) { return ((i < 4 ? lo4 : hi4) >> (8 * (i & 3))) & 0xFFu; }
+// (float) of byte b (0..3) of w, exact. On the device 0x4B0000bb read as a
+// float is 2^23 + bb, which avoids an integer-to-float conversion.
+RT_HD float quantum(unsigned w, unsigned b) {
+#ifdef __CUDA_ARCH__
+    return __uint_as_float(__byte_perm(w, 0x4B000000u, b | 0x7440u)) - 8388608.0f;
+#else
+    return (float)((w >> (8 * b)) & 0xFFu);
+#endif
+}
 
 // Tests the eight child boxes of a wide node against [0, tmax]. Returns the
 // node's hit mask: bits 24-31 interior children (octant-ordered), bits 0-23
 // triangles relative to triBase. Also returns childBase/triBase/imask.
+// Per axis the near plane is the lower bound when the inverse direction is
+// non-negative and the upper bound otherwise, so each child needs one fused
+// multiply-add per plane and no min/max pairs; fma is monotonic in q, so this
+// equals taking min/max of the two plane distances.
 RT_HD unsigned intersectWideNode(const uint4* node, const RaySetup& r, float tmax, unsigned& childBase,
                                  unsigned& triBase, unsigned& imask) {
     uint4 w0 = loadVec(node + 0), w1 = loadVec(node + 1), w2 = loadVec(node + 2), w3 = loadVec(node + 3),
           w4 = loadVec(node + 4);
-    float3 p = v3(bitsToFloat(w0.x), bitsToFloat(w0.y), bitsToFloat(w0.z));
+    float px = bitsToFloat(w0.x), py = bitsToFloat(w0.y), pz = bitsToFloat(w0.z);
     float sx = bitsToFloat((w0.w & 0xFFu) << 23), sy = bitsToFloat(((w0.w >> 8) & 0xFFu) << 23),
           sz = bitsToFloat(((w0.w >> 16) & 0xFFu) << 23);
     imask = w0.w >> 24;
@@ -99,34 +111,41 @@ RT_HD unsigned intersectWideNode(const uint4* node, const RaySetup& r, float tma
     triBase = w1.y;
     // t(q) = (p + q*s - o) * inv = q * (s*inv) + (p - o)*inv
     float ax = sx * r.inv.x, ay = sy * r.inv.y, az = sz * r.inv.z;
-    float bx = (p.x - r.o.x) * r.inv.x, by = (p.y - r.o.y) * r.inv.y, bz = (p.z - r.o.z) * r.inv.z;
+    float bx = (px - r.o.x) * r.inv.x, by = (py - r.o.y) * r.inv.y, bz = (pz - r.o.z) * r.inv.z;
+    // Words of the lower (lo) and upper (hi) planes, children 0-3 and 4-7.
+    const bool nx = r.inv.x < 0.0f, ny = r.inv.y < 0.0f, nz = r.inv.z < 0.0f;
+    uint2 nearX = nx ? make_uint2(w3.z, w3.w) : make_uint2(w2.x, w2.y);
+    uint2 farX = nx ? make_uint2(w2.x, w2.y) : make_uint2(w3.z, w3.w);
+    uint2 nearY = ny ? make_uint2(w4.x, w4.y) : make_uint2(w2.z, w2.w);
+    uint2 farY = ny ? make_uint2(w2.z, w2.w) : make_uint2(w4.x, w4.y);
+    uint2 nearZ = nz ? make_uint2(w4.z, w4.w) : make_uint2(w3.x, w3.y);
+    uint2 farZ = nz ? make_uint2(w3.x, w3.y) : make_uint2(w4.z, w4.w);
     unsigned mask = 0;
 #pragma unroll
     for (int i = 0; i < 8; i++) {
-        unsigned meta = byteOf(w1.z, w1.w, i);
-        if (meta == 0) continue;
-        float qlx = (float)byteOf(w2.x, w2.y, i), qly = (float)byteOf(w2.z, w2.w, i), qlz = (float)byteOf(w3.x, w3.y, i);
-        float qhx = (float)byteOf(w3.z, w3.w, i), qhy = (float)byteOf(w4.x, w4.y, i), qhz = (float)byteOf(w4.z, w4.w, i);
-        float x0 = fmaRn(qlx, ax, bx), x1 = fmaRn(qhx, ax, bx);
-        float y0 = fmaRn(qly, ay, by), y1 = fmaRn(qhy, ay, by);
-        float z0 = fmaRn(qlz, az, bz), z1 = fmaRn(qhz, az, bz);
-        float tnx = fminf(x0, x1), tfx = fmaxf(x0, x1);
-        float tny = fminf(y0, y1), tfy = fmaxf(y0, y1);
-        float tnz = fminf(z0, z1), tfz = fmaxf(z0, z1);
+        const unsigned b = (unsigned)(i & 3);
+        const bool hiHalf = i >= 4;
+        unsigned meta = ((hiHalf ? w1.w : w1.z) >> (8 * b)) & 0xFFu;
+        float qnx = quantum(hiHalf ? nearX.y : nearX.x, b), qfx = quantum(hiHalf ? farX.y : farX.x, b);
+        float qny = quantum(hiHalf ? nearY.y : nearY.x, b), qfy = quantum(hiHalf ? farY.y : farY.x, b);
+        float qnz = quantum(hiHalf ? nearZ.y : nearZ.x, b), qfz = quantum(hiHalf ? farZ.y : farZ.x, b);
+        float tnx = fmaRn(qnx, ax, bx), tfx = fmaRn(qfx, ax, bx);
+        float tny = fmaRn(qny, ay, by), tfy = fmaRn(qfy, ay, by);
+        float tnz = fmaRn(qnz, az, bz), tfz = fmaRn(qfz, az, bz);
         if (r.parMask) {
-            // Reference semantics for axes parallel to the ray: inside the
-            // slab (bounds inclusive) imposes no limit, outside misses.
-            if (r.parMask & 1u) { bool in = r.o.x >= fmaRn(qlx, sx, p.x) && r.o.x <= fmaRn(qhx, sx, p.x); tnx = in ? -FLT_MAX : FLT_MAX; tfx = FLT_MAX; }
-            if (r.parMask & 2u) { bool in = r.o.y >= fmaRn(qly, sy, p.y) && r.o.y <= fmaRn(qhy, sy, p.y); tny = in ? -FLT_MAX : FLT_MAX; tfy = FLT_MAX; }
-            if (r.parMask & 4u) { bool in = r.o.z >= fmaRn(qlz, sz, p.z) && r.o.z <= fmaRn(qhz, sz, p.z); tnz = in ? -FLT_MAX : FLT_MAX; tfz = FLT_MAX; }
+            // Reference semantics for axes parallel to the ray (renderer.cu:120):
+            // inside the slab (bounds inclusive) imposes no limit, outside
+            // misses. inv is +0 on those axes, so near = lower bound.
+            if (r.parMask & 1u) { bool in = r.o.x >= fmaRn(qnx, sx, px) && r.o.x <= fmaRn(qfx, sx, px); tnx = in ? -FLT_MAX : FLT_MAX; tfx = FLT_MAX; }
+            if (r.parMask & 2u) { bool in = r.o.y >= fmaRn(qny, sy, py) && r.o.y <= fmaRn(qfy, sy, py); tny = in ? -FLT_MAX : FLT_MAX; tfy = FLT_MAX; }
+            if (r.parMask & 4u) { bool in = r.o.z >= fmaRn(qnz, sz, pz) && r.o.z <= fmaRn(qfz, sz, pz); tnz = in ? -FLT_MAX : FLT_MAX; tfz = FLT_MAX; }
         }
         float tmin = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f));
         float tmaxc = fminf(fminf(tfx, tfy), fminf(tfz, tmax));
-        if (tmin <= tmaxc) {
-            unsigned index = meta & 0x1Fu;
-            if ((meta & 0x18u) == 0x18u) index ^= r.octInv;
-            mask |= (meta >> 5) << index;
-        }
+        unsigned index = meta & 0x1Fu;
+        if ((meta & 0x18u) == 0x18u) index ^= r.octInv;
+        unsigned bits = (meta != 0u && tmin <= tmaxc) ? (meta >> 5) : 0u;
+        mask |= bits << index;
     }
     return mask;
 }

@@ -4,9 +4,9 @@
 // a range of primitives (a leaf too large for one node). For a binary node,
 // the children start as its two children; the interior child with the largest
 // surface area is opened (replaced by its two children) while the result
-// still fits in eight slots, where a leaf of k <= 24 triangles needs
-// ceil(k / 3) slots (groups of up to three triangles) and anything else one
-// slot. Leaves that still do not fit become wide children of their own.
+// still fits in eight slots, where a leaf of k <= 8 * group triangles needs
+// ceil(k / group) slots (groups of up to `group` triangles, 1..3, each with
+// its own box) and anything else one slot. Leaves that still do not fit become wide children of their own.
 // Slots are assigned by ray octant (slot s holds the child nearest along
 // direction signs s), and child boxes are quantised outward against the
 // node's grid, checked with the same fused multiply-add the traversal uses.
@@ -42,9 +42,11 @@ RT_HD void collapseGrow(float lo[3], float hi[3], const float olo[3], const floa
 struct Job { int kind; int node; int first; int count; int wide; };  // kind 0 binary node, 1 primitive range
 struct Kid { int kind; int node; int first; int count; float lo[3], hi[3]; };  // kind 0/1 wide child, 2 triangle group
 
-RT_HD int slotsOf(const BinNode& n) {
+// Slots a binary child needs: one for an interior node, ceil(k / group) for a
+// leaf of k <= 8 * group triangles held inline, one for a larger leaf.
+RT_HD int slotsOf(const BinNode& n, int group) {
     if (n.count == 0) return 1;
-    return n.count <= 24 ? (n.count + 2) / 3 : 1;
+    return n.count <= 8 * group ? (n.count + group - 1) / group : 1;
 }
 
 // Builds wide node J.wide for one job: chooses up to eight children, assigns
@@ -54,7 +56,7 @@ RT_HD int slotsOf(const BinNode& n) {
 // portableAdd), so the collapse can be checked on the CPU.
 RT_HD void collapseJob(Job J, const BinNode* bn, const int* order, const float4* plo, const float4* phi,
                        const SceneTri* tris, Job* nextJobs, WideNode* wide, float4* packed, int* counters,
-                       int wideCapacity, int jobCapacity, int triCapacity) {
+                       int wideCapacity, int jobCapacity, int triCapacity, int group) {
     if (J.kind == 0 && bn[J.node].count > 0) { J.kind = 1; J.first = bn[J.node].first; J.count = bn[J.node].count; }
     Kid kids[8];
     int nk = 0;
@@ -64,12 +66,12 @@ RT_HD void collapseJob(Job J, const BinNode* bn, const int* order, const float4*
         cand[0] = bn[J.node].first; cand[1] = cand[0] + 1;
         for (;;) {
             int total = 0;
-            for (int i = 0; i < nc; i++) total += slotsOf(bn[cand[i]]);
+            for (int i = 0; i < nc; i++) total += slotsOf(bn[cand[i]], group);
             int best = -1; float bestArea = -1.0f;
             for (int i = 0; i < nc; i++) {
                 const BinNode& c = bn[cand[i]];
                 if (c.count != 0 || nc >= 8) continue;
-                int after = total - 1 + slotsOf(bn[c.first]) + slotsOf(bn[c.first + 1]);
+                int after = total - 1 + slotsOf(bn[c.first], group) + slotsOf(bn[c.first + 1], group);
                 if (after > 8) continue;
                 float lo[3] = {c.low.x, c.low.y, c.low.z}, hi[3] = {c.high.x, c.high.y, c.high.z};
                 float a = collapseHalfArea(lo, hi);
@@ -83,12 +85,12 @@ RT_HD void collapseJob(Job J, const BinNode* bn, const int* order, const float4*
         // Leaves that do not fit inline become wide children of their own.
         for (;;) {
             int total = 0;
-            for (int i = 0; i < nc; i++) total += asNode[i] ? 1 : slotsOf(bn[cand[i]]);
+            for (int i = 0; i < nc; i++) total += asNode[i] ? 1 : slotsOf(bn[cand[i]], group);
             if (total <= 8) break;
             int pick = -1, most = 0;
             for (int i = 0; i < nc; i++) {
                 const BinNode& c = bn[cand[i]];
-                if (!asNode[i] && c.count > 3 && c.count > most) { most = c.count; pick = i; }
+                if (!asNode[i] && c.count > group && c.count > most) { most = c.count; pick = i; }
             }
             if (pick < 0) break;
             asNode[pick] = true;
@@ -97,20 +99,21 @@ RT_HD void collapseJob(Job J, const BinNode* bn, const int* order, const float4*
             const BinNode& c = bn[cand[i]];
             if (c.count == 0) {
                 kids[nk++] = Kid{0, cand[i], 0, 0, {c.low.x, c.low.y, c.low.z}, {c.high.x, c.high.y, c.high.z}};
-            } else if (asNode[i] || c.count > 24) {
+            } else if (asNode[i] || c.count > 8 * group) {
                 kids[nk++] = Kid{1, -1, c.first, c.count, {c.low.x, c.low.y, c.low.z}, {c.high.x, c.high.y, c.high.z}};
             } else {
-                for (int g = 0; g < c.count && nk < 8; g += 3)
-                    kids[nk++] = Kid{2, -1, c.first + g, imin(3, c.count - g), {0, 0, 0}, {0, 0, 0}};
+                for (int g = 0; g < c.count && nk < 8; g += group)
+                    kids[nk++] = Kid{2, -1, c.first + g, imin(group, c.count - g), {0, 0, 0}, {0, 0, 0}};
             }
         }
-    } else if (J.count <= 24) {
-        for (int g = 0; g < J.count && nk < 8; g += 3) kids[nk++] = Kid{2, -1, J.first + g, imin(3, J.count - g), {0, 0, 0}, {0, 0, 0}};
+    } else if (J.count <= 8 * group) {
+        for (int g = 0; g < J.count && nk < 8; g += group)
+            kids[nk++] = Kid{2, -1, J.first + g, imin(group, J.count - g), {0, 0, 0}, {0, 0, 0}};
     } else {
         int chunk = (J.count + 7) / 8;
         for (int g = 0; g < J.count && nk < 8; g += chunk) {
             int c = imin(chunk, J.count - g);
-            kids[nk++] = Kid{c <= 3 ? 2 : 1, -1, J.first + g, c, {0, 0, 0}, {0, 0, 0}};
+            kids[nk++] = Kid{c <= group ? 2 : 1, -1, J.first + g, c, {0, 0, 0}, {0, 0, 0}};
         }
     }
     // Boxes of primitive-range kids: union of padded primitive boxes.

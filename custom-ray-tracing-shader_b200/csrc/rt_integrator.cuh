@@ -69,6 +69,7 @@ struct SceneView {
     const Light* lights;
     int lightCount;
     float lightArea;
+    int wideDepth;           // levels of the wide BVH (bounds the traversal stack)
 };
 
 // ---- BRDF and sky (renderer.cu:181-196) ----

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "rt_render.cuh"
+#include "rt_trace.cuh"
 
 namespace rt {
 namespace {
@@ -83,24 +84,25 @@ __global__ void generateKernel(WaveArgs A, WavefrontBuffers B) {
     if (p == 0) { B.counts[0] = A.n; B.counts[1] = 0; B.counts[2] = 0; }
 }
 
-// Closest hit for every queued path (grid-stride over the device-side count).
-__global__ void extendKernel(const uint4* wide, const float4* packed, WavefrontBuffers B, int q,
-                             unsigned long long* counter, int* errorFlag) {
-    extern __shared__ uint2 smemStack[];
-    uint2* stack = smemStack + threadIdx.x;
-    int count = B.counts[q];
-    int overflow = 0;
-    unsigned done = 0;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
-        int p = B.queue[q][k];
-        float4 a = B.pathA[p], b = B.pathB[p];
-        Hit h = traverse<false>(wide, packed, v3(a.x, a.y, a.z), v3(b.x, b.y, b.z), 1e30f, stack, blockDim.x, &overflow, nullptr);
-        B.hits[p] = make_float4(h.distance, h.u, h.v, __int_as_float(h.index));
-        done++;
+// Closest hit for every queued path (persistent, dynamic fetch).
+struct ExtendIO {
+    const int* queue;
+    const float4 *pathA, *pathB;
+    float4* hits;
+    __device__ void load(int k, float3& o, float3& d, float& limit) const {
+        int p = queue[k];
+        float4 a = pathA[p], b = pathB[p];
+        o = v3(a.x, a.y, a.z); d = v3(b.x, b.y, b.z); limit = 1e30f;
     }
-    unsigned s = __reduce_add_sync(0xFFFFFFFFu, done);
-    if ((threadIdx.x & 31) == 0 && s) atomicAdd(counter, (unsigned long long)s);
-    if (overflow) atomicExch(errorFlag, 1);
+    __device__ void store(int k, const Hit& h) const {
+        hits[queue[k]] = make_float4(h.distance, h.u, h.v, __int_as_float(h.index));
+    }
+};
+__global__ void __launch_bounds__(kTraceBlock) extendKernel(const uint4* wide, const float4* packed, WavefrontBuffers B,
+                                                            int q, unsigned long long* counter, int* errorFlag,
+                                                            int postponeBelow, int refill) {
+    ExtendIO io{B.queue[q], B.pathA, B.pathB, B.hits};
+    persistentTrace<false>(io, B.counts[q], wide, packed, &B.counts[3], counter, errorFlag, postponeBelow, refill);
 }
 
 // Appends to a queue with one atomic per warp.
@@ -160,30 +162,31 @@ __global__ void shadeKernel(WaveArgs A, WavefrontBuffers B, int q, int bounce) {
     }
 }
 
-__global__ void shadowKernel(const uint4* wide, const float4* packed, WavefrontBuffers B, unsigned long long* counter,
-                             int* errorFlag) {
-    extern __shared__ uint2 smemStack[];
-    uint2* stack = smemStack + threadIdx.x;
-    int count = B.counts[2];
-    int overflow = 0;
-    unsigned done = 0;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
-        float4 o = B.shadowRay[k], d = B.shadowDir[k];
-        Hit h = traverse<true>(wide, packed, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), o.w, stack, blockDim.x, &overflow, nullptr);
-        if (h.index < 0) {
-            int p = __float_as_int(d.w);
-            float4 c = B.shadowContrib[k], rad = B.radiance[p];
-            B.radiance[p] = make_float4(rad.x + c.x, rad.y + c.y, rad.z + c.z, rad.w);
-        }
-        done++;
+// Light-sample visibility for every queued shadow ray (persistent, dynamic
+// fetch); unoccluded samples add their contribution to the path's radiance.
+struct ShadowIO {
+    const float4 *ray, *dir, *contrib;
+    float4* radiance;
+    __device__ void load(int k, float3& o, float3& d, float& limit) const {
+        float4 a = ray[k], b = dir[k];
+        o = v3(a.x, a.y, a.z); d = v3(b.x, b.y, b.z); limit = a.w;
     }
-    unsigned s = __reduce_add_sync(0xFFFFFFFFu, done);
-    if ((threadIdx.x & 31) == 0 && s) atomicAdd(counter, (unsigned long long)s);
-    if (overflow) atomicExch(errorFlag, 1);
+    __device__ void store(int k, const Hit& h) const {
+        if (h.index >= 0) return;
+        int p = __float_as_int(dir[k].w);
+        float4 c = contrib[k], rad = radiance[p];
+        radiance[p] = make_float4(rad.x + c.x, rad.y + c.y, rad.z + c.z, rad.w);
+    }
+};
+__global__ void __launch_bounds__(kTraceBlock) shadowKernel(const uint4* wide, const float4* packed, WavefrontBuffers B,
+                                                            unsigned long long* counter, int* errorFlag,
+                                                            int postponeBelow, int refill) {
+    ShadowIO io{B.shadowRay, B.shadowDir, B.shadowContrib, B.radiance};
+    persistentTrace<true>(io, B.counts[2], wide, packed, &B.counts[4], counter, errorFlag, postponeBelow, refill);
 }
 
 __global__ void resetQueuesKernel(WavefrontBuffers B, int q) {
-    if (threadIdx.x == 0) { B.counts[q ^ 1] = 0; B.counts[2] = 0; }
+    if (threadIdx.x == 0) { B.counts[q ^ 1] = 0; B.counts[2] = 0; B.counts[3] = 0; B.counts[4] = 0; }
 }
 
 __global__ void accumulateKernel(WaveArgs A, WavefrontBuffers B) {
@@ -202,19 +205,23 @@ __global__ void accumulateKernel(WaveArgs A, WavefrontBuffers B) {
 }
 
 // ---- per-ray queries, sampler values ----
-__global__ void queryKernel(const uint4* wide, const float4* packed, const float4* q, int count, int any, float4* out,
-                            int* errorFlag) {
-    extern __shared__ uint2 smemStack[];
-    uint2* stack = smemStack + threadIdx.x;
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    int overflow = 0;
-    if (i < count) {
-        float4 a = q[2 * i], b = q[2 * i + 1];
-        Hit h = any ? traverse<true>(wide, packed, v3(a.x, a.y, a.z), v3(a.w, b.x, b.y), b.z, stack, blockDim.x, &overflow, nullptr)
-                    : traverse<false>(wide, packed, v3(a.x, a.y, a.z), v3(a.w, b.x, b.y), b.z, stack, blockDim.x, &overflow, nullptr);
-        out[i] = make_float4(__int_as_float(h.index), h.distance, h.u, h.v);
+struct QueryIO {
+    const float4* q;
+    float4* out;
+    __device__ void load(int k, float3& o, float3& d, float& limit) const {
+        float4 a = q[2 * k], b = q[2 * k + 1];
+        o = v3(a.x, a.y, a.z); d = v3(a.w, b.x, b.y); limit = b.z;
     }
-    if (overflow) atomicExch(errorFlag, 1);
+    __device__ void store(int k, const Hit& h) const {
+        out[k] = make_float4(__int_as_float(h.index), h.distance, h.u, h.v);
+    }
+};
+template <bool ANY>
+__global__ void __launch_bounds__(kTraceBlock) queryKernel(const uint4* wide, const float4* packed, const float4* q,
+                                                           int count, float4* out, int* fetch, int* errorFlag,
+                                                           int postponeBelow, int refill) {
+    QueryIO io{q, out};
+    persistentTrace<ANY>(io, count, wide, packed, fetch, nullptr, errorFlag, postponeBelow, refill);
 }
 
 __global__ void sobolSamplesKernel(const unsigned* dirs, const unsigned* pixel, const unsigned* sample,
@@ -277,7 +284,7 @@ __global__ void denoisePresentKernel(const Accum* sums, const float4* color, int
 
 inline int blocks(long long n, int b) { return (int)((n + b - 1) / b); }
 
-int persistentBlocks(int blockSize) {
+int smCount() {
     static int sms = 0;
     if (!sms) {
         int dev = 0;
@@ -285,9 +292,21 @@ int persistentBlocks(int blockSize) {
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if (sms <= 0) sms = 148;
     }
-    int perSm = 2048 / blockSize;
-    return sms * (perSm > 0 ? perSm : 1);
+    return sms;
 }
+int persistentBlocks(int blockSize) {
+    int perSm = 2048 / blockSize;
+    return smCount() * (perSm > 0 ? perSm : 1);
+}
+// Resident blocks of a traversal kernel, for a grid of exactly one wave.
+template <class K>
+int traceBlocks(K kernel, size_t smem) {
+    int perSm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, kTraceBlock, smem) != cudaSuccess || perSm <= 0)
+        perSm = 1;
+    return smCount() * perSm;
+}
+constexpr size_t kTraceSmem = sizeof(uint2) * kSharedStack * kTraceBlock;
 
 }  // namespace
 
@@ -300,7 +319,7 @@ cudaError_t allocWavefront(WavefrontBuffers& b, int capacity) {
     RT_ALLOC(b.radiance, n); RT_ALLOC(b.albedo, n); RT_ALLOC(b.normal, n); RT_ALLOC(b.hits, n);
     RT_ALLOC(b.queue[0], n); RT_ALLOC(b.queue[1], n);
     RT_ALLOC(b.shadowRay, n); RT_ALLOC(b.shadowDir, n); RT_ALLOC(b.shadowContrib, n);
-    RT_ALLOC(b.counts, 4);
+    RT_ALLOC(b.counts, 8);
 #undef RT_ALLOC
     b.capacity = capacity;
     return cudaSuccess;
@@ -333,16 +352,16 @@ cudaError_t launchMegakernel(const RenderLaunch& L, cudaStream_t stream, int* la
     return cudaGetLastError();
 }
 
-cudaError_t launchWavefront(const RenderLaunch& L, WavefrontBuffers& B, int blockSize, cudaStream_t stream,
+cudaError_t launchWavefront(const RenderLaunch& L, WavefrontBuffers& B, const TraceTuning& tuning, cudaStream_t stream,
                             int* launches, float* extendMs, float* shadowMs, bool timing) {
-    size_t smem = sizeof(uint2) * kStackCapacity * (size_t)blockSize;
-    static size_t configured = 0;
-    if (configured < smem) {
-        cudaFuncSetAttribute(extendKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        cudaFuncSetAttribute(shadowKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        configured = smem;
+    static int extendBlocks = 0, shadowBlocks = 0;
+    if (!extendBlocks) {
+        extendBlocks = traceBlocks(extendKernel, kTraceSmem);
+        shadowBlocks = traceBlocks(shadowKernel, kTraceSmem);
     }
-    int travBlocks = persistentBlocks(blockSize);
+    const size_t smem = kTraceSmem;
+    const int postponeBelow = tuning.postpone ? kStackCapacity - L.scene.wideDepth - 2 : 0;
+    const int refill = tuning.refill;
     int shadeBlocks = persistentBlocks(256);
     int pixels = L.w * L.h;
     int n = 0;
@@ -364,14 +383,15 @@ cudaError_t launchWavefront(const RenderLaunch& L, WavefrontBuffers& B, int bloc
                 resetQueuesKernel<<<1, 32, 0, stream>>>(B, q);
                 Mark m{nullptr, nullptr, false};
                 if (timing) { m.a = event(ev++); m.b = event(ev++); cudaEventRecord(m.a, stream); }
-                extendKernel<<<travBlocks, blockSize, smem, stream>>>(L.scene.wide, L.scene.packed, B, q,
-                                                                      &L.counters[bounce == 0 ? 0 : 1], L.errorFlag);
+                extendKernel<<<extendBlocks, kTraceBlock, smem, stream>>>(L.scene.wide, L.scene.packed, B, q,
+                                                                          &L.counters[bounce == 0 ? 0 : 1], L.errorFlag,
+                                                                          postponeBelow, refill);
                 if (timing) { cudaEventRecord(m.b, stream); marks.push_back(m); }
                 shadeKernel<<<shadeBlocks, 256, 0, stream>>>(A, B, q, bounce);
                 Mark s{nullptr, nullptr, true};
                 if (timing) { s.a = event(ev++); s.b = event(ev++); cudaEventRecord(s.a, stream); }
-                shadowKernel<<<travBlocks, blockSize, smem, stream>>>(L.scene.wide, L.scene.packed, B, &L.counters[2],
-                                                                      L.errorFlag);
+                shadowKernel<<<shadowBlocks, kTraceBlock, smem, stream>>>(L.scene.wide, L.scene.packed, B, &L.counters[2],
+                                                                          L.errorFlag, postponeBelow, refill);
                 if (timing) { cudaEventRecord(s.b, stream); marks.push_back(s); }
                 n += 4;
                 q ^= 1;
@@ -397,10 +417,21 @@ cudaError_t launchWavefront(const RenderLaunch& L, WavefrontBuffers& B, int bloc
 }
 
 cudaError_t launchQueries(const uint4* wide, const float4* packed, const float4* queries, int count, int any,
-                          float4* hits, int* errorFlag, cudaStream_t stream) {
-    const int block = 128;
-    size_t smem = sizeof(uint2) * kStackCapacity * block;
-    queryKernel<<<blocks(count, block), block, smem, stream>>>(wide, packed, queries, count, any, hits, errorFlag);
+                          float4* hits, int* fetch, int* errorFlag, int wideDepth, const TraceTuning& tuning,
+                          cudaStream_t stream) {
+    const int postponeBelow = tuning.postpone ? kStackCapacity - wideDepth - 2 : 0;
+    const int refill = tuning.refill;
+    cudaError_t e = cudaMemsetAsync(fetch, 0, sizeof(int), stream);
+    if (e != cudaSuccess) return e;
+    if (any) {
+        static int blocks = traceBlocks(queryKernel<true>, kTraceSmem);
+        queryKernel<true><<<blocks, kTraceBlock, kTraceSmem, stream>>>(wide, packed, queries, count, hits, fetch, errorFlag,
+                                                                      postponeBelow, refill);
+    } else {
+        static int blocks = traceBlocks(queryKernel<false>, kTraceSmem);
+        queryKernel<false><<<blocks, kTraceBlock, kTraceSmem, stream>>>(wide, packed, queries, count, hits, fetch, errorFlag,
+                                                                       postponeBelow, refill);
+    }
     return cudaGetLastError();
 }
 

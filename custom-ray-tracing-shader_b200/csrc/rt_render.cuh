@@ -32,7 +32,13 @@ struct WavefrontBuffers {
     float4* shadowRay = nullptr;      // origin.xyz, limit
     float4* shadowDir = nullptr;      // dir.xyz, path id (bits)
     float4* shadowContrib = nullptr;  // contribution.xyz
-    int* counts = nullptr;            // [0..1] queue sizes, [2] shadow queue size
+    int* counts = nullptr;            // [0..1] queue sizes, [2] shadow queue size, [3..4] fetch counters
+};
+
+// Speed-only knobs of the persistent traversal kernels.
+struct TraceTuning {
+    int postpone = 0;  // postpone triangle tests in sparse warps (measured neutral on B200)
+    int refill = 28;   // refill idle lanes when fewer lanes than this are busy
 };
 
 cudaError_t allocWavefront(WavefrontBuffers& b, int capacity);
@@ -44,11 +50,13 @@ cudaError_t buildSobolTables(const unsigned* dirs, unsigned sample0, int rpp, un
 cudaError_t launchMegakernel(const RenderLaunch& L, cudaStream_t stream, int* launches);
 // Wavefront: generate -> (extend -> shade -> shadow)* per wave. Timing of the
 // traversal kernels is accumulated into extendMs/shadowMs when timing != 0.
-cudaError_t launchWavefront(const RenderLaunch& L, WavefrontBuffers& b, int blockSize, cudaStream_t stream,
+cudaError_t launchWavefront(const RenderLaunch& L, WavefrontBuffers& b, const TraceTuning& tuning, cudaStream_t stream,
                             int* launches, float* extendMs, float* shadowMs, bool timing);
 
+// fetch: one device int of scratch (the work counter of the persistent kernel).
 cudaError_t launchQueries(const uint4* wide, const float4* packed, const float4* queries /*2 per query*/, int count,
-                          int any, float4* hits, int* errorFlag, cudaStream_t stream);
+                          int any, float4* hits, int* fetch, int* errorFlag, int wideDepth, const TraceTuning& tuning,
+                          cudaStream_t stream);
 cudaError_t launchSobolSamples(const unsigned* dirs, const unsigned* pixel, const unsigned* sample, const unsigned* seed,
                                int count, int ndim, float* out, cudaStream_t stream);
 // Denoise: prepare guides from the running sums, filter, tonemap into pixels.

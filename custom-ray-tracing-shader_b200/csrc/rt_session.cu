@@ -78,7 +78,8 @@ struct Session {
     // Statistics and tuning.
     RtxRenderStats stats{};
     double sahCost = -1.0;
-    int integrator = 0, blockSize = 128, pathsInFlight = 0;
+    int integrator = 0, pathsInFlight = 0;
+    TraceTuning tuning;
 };
 
 bool fail(Session* s, cudaError_t e, const char* what = nullptr) {
@@ -120,7 +121,8 @@ bool validSettings(const RenderSettings* st) {
 }
 
 SceneView deviceView(Session* s) {
-    return SceneView{s->dTris, s->bvh.wideNodes, s->bvh.packedTris, s->dLights, (int)s->lights.size(), s->lightArea};
+    return SceneView{s->dTris, s->bvh.wideNodes, s->bvh.packedTris, s->dLights, (int)s->lights.size(), s->lightArea,
+                     s->build.wideDepth};
 }
 
 bool ensureWave(Session* s) {
@@ -150,7 +152,7 @@ bool renderDevice(Session* s, const CameraData* camera, const RenderSettings* se
         e = launchMegakernel(L, s->stream, &launches);
     } else {
         if (!ensureWave(s)) return false;
-        e = launchWavefront(L, s->wave, s->blockSize, s->stream, &launches, &extendMs, &shadowMs, timing);
+        e = launchWavefront(L, s->wave, s->tuning, s->stream, &launches, &extendMs, &shadowMs, timing);
     }
     if (e != cudaSuccess) return fail(s, e);
     if ((e = cudaEventRecord(s->stop, s->stream)) != cudaSuccess) return fail(s, e);
@@ -199,7 +201,8 @@ bool renderHost(Session* s, const CameraData* camera, const RenderSettings* sett
         for (int d = 0; d < kSobolDims; d++) passXor[(size_t)r * kSobolDims + d] = sobolXor(dirs, s->samples + (unsigned)r, (unsigned)d);
     for (int d = 0; d < kSobolDims; d++) seedHash[d] = sobolHash(set.seed + (unsigned)d * 0x9e3779b9u);
     if (s->hostSum.size() != (size_t)s->width * s->height) s->hostSum.assign((size_t)s->width * s->height, Accum{});
-    SceneView sc{s->tris.data(), s->hostWide.data(), s->hostPacked.data(), s->lights.data(), (int)s->lights.size(), s->lightArea};
+    SceneView sc{s->tris.data(), s->hostWide.data(), s->hostPacked.data(), s->lights.data(), (int)s->lights.size(),
+                 s->lightArea, s->build.wideDepth};
     const int w = s->width, h = s->height;
     const unsigned sample0 = s->samples;
     Accum* sums = s->hostSum.data();
@@ -336,7 +339,7 @@ int RtInitialize(void* p, const Triangle* triangles, int count, int width, int h
     RT_CHECK(cudaMalloc(&s->dSum, sizeof(Accum) * (size_t)width * height));
     RT_CHECK(cudaMalloc(&s->dPixels, sizeof(uchar4) * (size_t)width * height));
     RT_CHECK(cudaMalloc(&s->dCounters, 4 * sizeof(unsigned long long)));
-    RT_CHECK(cudaMalloc(&s->dError, sizeof(int)));
+    RT_CHECK(cudaMalloc(&s->dError, 2 * sizeof(int)));
     const char* why = nullptr;
     e = buildBvh(s->dTris, count, s->stream, s->bvh, s->build, &why);
     if (e != cudaSuccess) {
@@ -427,7 +430,8 @@ int RtxQueryRays(void* p, const RtxQuery* queries, int count, int any, RtxHit* h
     if (e == cudaSuccess) e = cudaMalloc(&dh, sizeof(float4) * (size_t)count);
     if (e == cudaSuccess) e = cudaMemcpyAsync(dq, packed.data(), sizeof(float4) * packed.size(), cudaMemcpyHostToDevice, s->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(s->dError, 0, sizeof(int), s->stream);
-    if (e == cudaSuccess) e = launchQueries(s->bvh.wideNodes, s->bvh.packedTris, dq, count, any, dh, s->dError, s->stream);
+    if (e == cudaSuccess) e = launchQueries(s->bvh.wideNodes, s->bvh.packedTris, dq, count, any, dh, s->dError + 1, s->dError,
+                                            s->build.wideDepth, s->tuning, s->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(out.data(), dh, sizeof(float4) * (size_t)count, cudaMemcpyDeviceToHost, s->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&overflow, s->dError, sizeof(int), cudaMemcpyDeviceToHost, s->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
@@ -555,14 +559,25 @@ int RtxSetIntegrator(void* p, int mode) {
     return 1;
 }
 
-int RtxSetTuning(void* p, int blockSize, int pathsInFlight) {
+int RtxSetTuning(void* p, int key, int value) {
     Session* s = static_cast<Session*>(p);
     if (!s) return 0;
-    if (blockSize != 0 && (blockSize < 64 || blockSize > 1024 || blockSize % 32)) return 0;
-    if (pathsInFlight != 0 && pathsInFlight < 1024) return 0;
-    if (blockSize) s->blockSize = blockSize;
-    if (pathsInFlight) s->pathsInFlight = pathsInFlight;
-    return 1;
+    switch (key) {
+        case RTX_TUNE_PATHS_IN_FLIGHT:
+            if (value < 1024) return 0;
+            s->pathsInFlight = value;
+            return 1;
+        case RTX_TUNE_POSTPONE:
+            if (value != 0 && value != 1) return 0;
+            s->tuning.postpone = value;
+            return 1;
+        case RTX_TUNE_REFILL:
+            if (value < 1 || value > 32) return 0;
+            s->tuning.refill = value;
+            return 1;
+        default:
+            return 0;
+    }
 }
 
 }  // extern "C"

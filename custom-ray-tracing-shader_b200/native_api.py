@@ -230,8 +230,13 @@ class Session:
     def set_integrator(self, mode):
         self.check(self.lib.RtxSetIntegrator(self.handle, mode))
 
-    def set_tuning(self, block_size=0, paths_in_flight=0):
-        self.check(self.lib.RtxSetTuning(self.handle, block_size, paths_in_flight))
+    TUNE_PATHS_IN_FLIGHT, TUNE_POSTPONE, TUNE_REFILL = 1, 2, 3
+
+    def set_tuning(self, paths_in_flight=None, postpone=None, refill=None):
+        for key, value in ((self.TUNE_PATHS_IN_FLIGHT, paths_in_flight), (self.TUNE_POSTPONE, postpone),
+                           (self.TUNE_REFILL, refill)):
+            if value is not None:
+                self.check(self.lib.RtxSetTuning(self.handle, key, int(value)))
 
     def sample_count(self):
         return self.lib.RtSampleCount(self.handle)

@@ -164,10 +164,18 @@ int RtxRenderDevice(void* session, const CameraData* camera, const RenderSetting
 /* Selects the CUDA integrator: 0 = wavefront (queues per bounce, default),
  * 1 = one-kernel path tracer. Both give bit-identical accumulations. */
 int RtxSetIntegrator(void* session, int mode);
-/* Tunables of the wavefront integrator: threads per block of the traversal
- * kernels (64..1024, multiple of 32) and paths in flight per wave (>= 1024).
- * 0 keeps the current value. */
-int RtxSetTuning(void* session, int blockSize, int pathsInFlight);
+/* Tunables of the wavefront integrator, one key at a time. Results do not
+ * depend on them, only speed does. Returns 0 for an unknown key or a value
+ * out of range.
+ *   RTX_TUNE_PATHS_IN_FLIGHT  paths per wave (>= 1024; default: all pixels)
+ *   RTX_TUNE_POSTPONE         1 = postpone triangle tests in sparse warps,
+ *                             0 = off (default)
+ *   RTX_TUNE_REFILL           refill a warp's idle lanes when fewer than this
+ *                             many lanes are busy (1..32, default 28) */
+#define RTX_TUNE_PATHS_IN_FLIGHT 1
+#define RTX_TUNE_POSTPONE 2
+#define RTX_TUNE_REFILL 3
+int RtxSetTuning(void* session, int key, int value);
 
 #ifdef __cplusplus
 }

@@ -550,14 +550,15 @@ void orc_render(void* s, const void* camera, const void* settings, int w, int h,
 }
 
 // Sampled pixels: render only the listed pixel indices (for bounded CPU timing
-// on large frames). sums/rgba are full-frame buffers.
+// on large frames). sums/rgba are full-frame buffers. counts (nullable) as in
+// orc_render.
 void orc_render_pixels(void* s, const void* camera, const void* settings, int w, int h, unsigned sample, void* sums,
                        unsigned char* rgba, const int* pixels, int npix, int threads, long long* counts) {
     const OScene& sc = *static_cast<OScene*>(s);
     const Camera& cam = *static_cast<const Camera*>(camera);
     const Settings& set = *static_cast<const Settings*>(settings);
     Sum* sum = static_cast<Sum*>(sums);
-    std::atomic<long long> c[3];
+    std::atomic<long long> c[11];
     for (auto& x : c) x = 0;
     #pragma omp parallel num_threads(threads > 0 ? threads : 1)
     {
@@ -565,9 +566,13 @@ void orc_render_pixels(void* s, const void* camera, const void* settings, int w,
         #pragma omp for schedule(dynamic, 64)
         for (int k = 0; k < npix; k++)
             shadePixel(sc, cam, set, pixels[k] % w, pixels[k] / w, w, h, sample, sum, rgba, counts ? &rc : nullptr);
-        if (counts) { c[0] += rc.primary; c[1] += rc.secondary; c[2] += rc.shadow; }
+        if (counts) {
+            c[0] += rc.primary; c[1] += rc.secondary; c[2] += rc.shadow;
+            c[3] += rc.closestWork.queries; c[4] += rc.closestWork.interior; c[5] += rc.closestWork.pops; c[6] += rc.closestWork.tris;
+            c[7] += rc.shadowWork.queries; c[8] += rc.shadowWork.interior; c[9] += rc.shadowWork.pops; c[10] += rc.shadowWork.tris;
+        }
     }
-    if (counts) for (int i = 0; i < 3; i++) counts[i] = c[i];
+    if (counts) for (int i = 0; i < 11; i++) counts[i] = c[i];
 }
 
 // Tonemap used for display (renderer.cu:86-90), exposed for tests.

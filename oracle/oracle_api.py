@@ -158,7 +158,7 @@ class Oracle:
     def render_pixels(self, scene, camera, settings, w, h, pixels, sample=0, threads=0):
         sums = np.zeros(w * h, PIXELSUM_DTYPE)
         rgba = np.zeros(w * h * 4, np.uint8)
-        counts = np.zeros(3, np.int64)
+        counts = np.zeros(11, np.int64)
         pixels = np.ascontiguousarray(pixels, np.int32)
         self.lib.orc_render_pixels(scene.handle, c.byref(camera), c.byref(settings), w, h, sample, sums.ctypes.data,
                                    rgba.ctypes.data, pixels.ctypes.data, len(pixels), threads or self.max_threads(),

@@ -39,7 +39,7 @@ static void primBoxes(const SceneTri* tris, int n, std::vector<float4>& lo, std:
 // Collapses a reference-layout binary BVH. result: [0] wide nodes, [1] depth,
 // [2] error code, [3] packed triangle count.
 int hc_collapse(const BinNode* bn, const int* order, const SceneTri* tris, int n, uint4* wideOut, int wideCapacity,
-                float4* packedOut, int* result) {
+                float4* packedOut, int* result, int group) {
     std::vector<float4> plo, phi;
     primBoxes(tris, n, plo, phi);
     int jobCapacity = 2 * n + 8;
@@ -51,7 +51,7 @@ int hc_collapse(const BinNode* bn, const int* order, const SceneTri* tris, int n
         counters[2] = 0;
         for (const Job& j : jobs)
             collapseJob(j, bn, order, plo.data(), phi.data(), tris, next.data(), reinterpret_cast<WideNode*>(wideOut),
-                        packedOut, counters, wideCapacity, jobCapacity, n);
+                        packedOut, counters, wideCapacity, jobCapacity, n, group);
         if (counters[3]) break;
         jobs.assign(next.begin(), next.begin() + counters[2]);
     }
@@ -65,7 +65,7 @@ int hc_collapse(const BinNode* bn, const int* order, const SceneTri* tris, int n
 // Ray queries (28-byte origin/direction/limit records) against a wide BVH.
 // stats: [0] node visits, [1] triangle tests, [2] stack overflows.
 void hc_query(const uint4* wide, const float4* packed, const float* queries, int count, int any, Hit* out,
-              unsigned long long* stats) {
+              unsigned long long* stats, unsigned* perRay) {
     uint2 stack[kStackCapacity];
     for (int i = 0; i < count; i++) {
         const float* q = queries + 7 * (size_t)i;
@@ -75,6 +75,7 @@ void hc_query(const uint4* wide, const float4* packed, const float* queries, int
         out[i] = any ? traverse<true>(wide, packed, o, d, q[6], stack, 1, &overflow, &tc)
                      : traverse<false>(wide, packed, o, d, q[6], stack, 1, &overflow, &tc);
         stats[0] += tc.nodes; stats[1] += tc.tris; stats[2] += (unsigned)overflow;
+        if (perRay) { perRay[2 * (size_t)i] = tc.nodes; perRay[2 * (size_t)i + 1] = tc.tris; }
     }
 }
 
@@ -87,7 +88,7 @@ int hc_render(const SceneTri* tris, const Light* lights, int lightCount, float l
     for (int r = 0; r < set->raysPerPixel; r++)
         for (int d = 0; d < kSobolDims; d++) passXor[(size_t)r * kSobolDims + d] = sobolXor(dirs, sample0 + (unsigned)r, (unsigned)d);
     for (int d = 0; d < kSobolDims; d++) seedHash[d] = sobolHash(set->seed + (unsigned)d * 0x9e3779b9u);
-    SceneView sc{tris, wide, packed, lights, lightCount, lightArea};
+    SceneView sc{tris, wide, packed, lights, lightCount, lightArea, 0};
     uint2 stack[kStackCapacity];
     int overflow = 0;
     unsigned p = 0, q = 0, s = 0;

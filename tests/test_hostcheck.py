@@ -29,13 +29,13 @@ def hc():
                         '-Xcompiler=-fPIC', str(HERE / 'host_check.cu'), '-o', str(LIB)], check=True)
     lib = c.CDLL(str(LIB))
     vp = c.c_void_p
-    lib.hc_collapse.argtypes = [vp, vp, vp, c.c_int, vp, c.c_int, vp, vp]
-    lib.hc_query.argtypes = [vp, vp, vp, c.c_int, c.c_int, vp, vp]
+    lib.hc_collapse.argtypes = [vp, vp, vp, c.c_int, vp, c.c_int, vp, vp, c.c_int]
+    lib.hc_query.argtypes = [vp, vp, vp, c.c_int, c.c_int, vp, vp, vp]
     lib.hc_render.argtypes = [vp, vp, c.c_int, c.c_float, vp, vp, vp, vp, vp, c.c_int, c.c_int, c.c_uint, vp, vp, vp]
     return lib
 
 
-def collapse(hc, scene):
+def collapse(hc, scene, group=3):
     nodes, order, lin = scene.nodes(), scene.order(), scene.linear_triangles()
     n = len(lin)
     cap = 2 * n + 8
@@ -43,22 +43,23 @@ def collapse(hc, scene):
     packed = np.zeros(n * 12, np.float32)
     res = np.zeros(4, np.int32)
     assert hc.hc_collapse(nodes.ctypes.data, order.ctypes.data, lin.ctypes.data, n, wide.ctypes.data, cap,
-                          packed.ctypes.data, res.ctypes.data)
+                          packed.ctypes.data, res.ctypes.data, group)
     assert res[3] == n, 'every triangle packed exactly once'
     return wide, packed, res
 
 
+@pytest.mark.parametrize('group', (1, 2, 3))
 @pytest.mark.parametrize('name', SETS)
-def test_wide_traversal_matches_reference(hc, oracle, name):
+def test_wide_traversal_matches_reference(hc, oracle, name, group):
     g = golden(f'bvh_{name}.npz')
     sc = oracle.scene(GEOMETRY[name])
-    wide, packed, res = collapse(hc, sc)
+    wide, packed, res = collapse(hc, sc, group)
     assert res[1] <= 48
     for any_hit in (0, 1):
         out = np.zeros(len(RAYS), HIT_DTYPE)
         stats = np.zeros(3, np.uint64)
         hc.hc_query(wide.ctypes.data, packed.ctypes.data, np.ascontiguousarray(RAYS).ctypes.data, len(RAYS), any_hit,
-                    out.ctypes.data, stats.ctypes.data)
+                    out.ctypes.data, stats.ctypes.data, None)
         assert stats[2] == 0
         if any_hit:
             assert ((out['index'] >= 0) == (g['any_index'] >= 0)).all()
