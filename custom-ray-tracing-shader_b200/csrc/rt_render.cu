@@ -306,7 +306,7 @@ int traceBlocks(K kernel, size_t smem) {
         perSm = 1;
     return smCount() * perSm;
 }
-constexpr size_t kTraceSmem = sizeof(uint2) * kSharedStack * kTraceBlock;
+constexpr size_t kTraceSmem = traceSharedBytes(kTraceBlock);
 
 }  // namespace
 

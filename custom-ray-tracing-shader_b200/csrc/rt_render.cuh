@@ -38,7 +38,7 @@ struct WavefrontBuffers {
 // Speed-only knobs of the persistent traversal kernels.
 struct TraceTuning {
     int postpone = 0;  // postpone triangle tests in sparse warps (measured neutral on B200)
-    int refill = 28;   // refill idle lanes when fewer lanes than this are busy
+    int refill = 24;   // refill idle lanes when fewer lanes than this are busy
 };
 
 cudaError_t allocWavefront(WavefrontBuffers& b, int capacity);

@@ -84,31 +84,130 @@ __device__ __forceinline__ bool nodeStep(LaneRay& L, const uint4* nodes, uint2* 
     return false;
 }
 
+// Per-warp shared scratch of the cooperative triangle phase.
+struct WarpTriangles {
+    float4 origin[32];              // each lane's ray origin
+    float4 dir[32];                 // each lane's ray direction
+    unsigned long long best[32];    // (distance bits << 32 | index) of each lane's best hit
+    float2 uv[32];                  // barycentrics of that hit
+    unsigned end[32];               // inclusive prefix sum of pending triangle counts
+    uint2 group[32];                // each lane's pending triangle group
+};
+constexpr size_t traceSharedBytes(int block) {
+    return sizeof(uint2) * kSharedStack * block + sizeof(WarpTriangles) * (block / 32);
+}
+
+// Position of the k-th (0-based) set bit of m; m has more than k set bits.
+__device__ __forceinline__ unsigned selectBit(unsigned m, unsigned k) {
+    unsigned pos = 0;
+#pragma unroll
+    for (unsigned width = 16; width > 0; width >>= 1) {
+        unsigned low = __popc(m & ((1u << width) - 1u));
+        if (k >= low) { k -= low; m >>= width; pos += width; }
+    }
+    return pos;
+}
+
+// Key ordering hits like the reference's acceptance rule (renderer.cu:153):
+// smaller distance first, then smaller triangle index. Distances are
+// positive, so their bit patterns order like the values. Before any hit the
+// best is (limit, index -1) and the rule accepts only distances below the
+// limit (i < -1 never holds), so that state is keyed with low word 0: a
+// candidate at exactly the limit has a key >= it and is rejected.
+__device__ __forceinline__ unsigned long long hitKey(float distance, int index) {
+    return ((unsigned long long)__float_as_uint(distance) << 32) | (unsigned)(index < 0 ? 0 : index);
+}
+
+// Cooperative triangle phase: the warp's pending triangles (all lanes' groups)
+// are dealt out one per lane per iteration; each candidate hit is merged into
+// its ray's best with a shared-memory 64-bit atomicMin on hitKey. The result
+// is the minimum over the same candidate set as testing them one by one, so
+// it equals the sequential outcome. Returns true for a lane whose any-hit
+// query is answered.
+template <bool ANY>
+__device__ __forceinline__ bool warpTrianglePhase(LaneRay& L, bool busy, const float4* tris, WarpTriangles& W,
+                                                  unsigned lane) {
+    const unsigned count = busy ? __popc(L.triGroup.y) : 0u;
+    unsigned incl = count;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        unsigned v = __shfl_up_sync(0xFFFFFFFFu, incl, off);
+        if ((int)lane >= off) incl += v;
+    }
+    const unsigned total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+    if (total == 0u) return false;
+    const unsigned long long key0 = busy ? hitKey(L.hit.distance, L.hit.index) : ~0ull;
+    W.origin[lane] = make_float4(L.r.o.x, L.r.o.y, L.r.o.z, 0.0f);
+    W.dir[lane] = make_float4(L.r.d.x, L.r.d.y, L.r.d.z, 0.0f);
+    W.best[lane] = key0;
+    W.end[lane] = incl;
+    W.group[lane] = busy ? L.triGroup : make_uint2(0u, 0u);
+    __syncwarp();
+    for (unsigned base = 0; base < total; base += 32u) {
+        const unsigned w = base + lane;
+        unsigned long long key = ~0ull;
+        unsigned owner = 0;
+        float u = 0.0f, v = 0.0f;
+        if (w < total) {
+            unsigned pos = 0;
+#pragma unroll
+            for (unsigned step = 16; step > 0; step >>= 1)
+                if (W.end[pos + step - 1] <= w) pos += step;
+            owner = pos;
+            const uint2 g = W.group[owner];
+            const unsigned bit = selectBit(g.y, w - (W.end[owner] - __popc(g.y)));
+            const float4* t = tris + (size_t)(g.x + bit) * 3;
+            float4 a = __ldg(t), b = __ldg(t + 1), c = __ldg(t + 2);
+            float4 o4 = W.origin[owner], d4 = W.dir[owner];
+            float dist = intersectTriangle(v3(o4.x, o4.y, o4.z), v3(d4.x, d4.y, d4.z), a, b, c, u, v);
+            if (dist > 0) {
+                unsigned long long k = hitKey(dist, __float_as_int(c.z));
+                if (k < W.best[owner]) { atomicMin(&W.best[owner], k); key = k; }
+            }
+        }
+        __syncwarp();
+        if (key != ~0ull && W.best[owner] == key) W.uv[owner] = make_float2(u, v);
+        __syncwarp();
+    }
+    bool answered = false;
+    if (busy) {
+        const unsigned long long b = W.best[lane];
+        if (b != key0) {
+            L.hit.distance = __uint_as_float((unsigned)(b >> 32));
+            L.hit.index = (int)(unsigned)(b & 0xFFFFFFFFull);
+            const float2 uv = W.uv[lane];
+            L.hit.u = uv.x; L.hit.v = uv.y;
+            answered = ANY;
+        }
+        L.triGroup.y = 0u;
+    }
+    __syncwarp();
+    return answered;
+}
+
 // Persistent query loop over `count` rays of an IO object providing
 //   __device__ void load(int k, float3& o, float3& d, float& limit);
 //   __device__ void store(int k, const Hit& h);
 // `fetch` must be zero at launch. Adds the number of finished queries to
-// *done and sets *errorFlag on stack overflow.
+// *done and sets *errorFlag on stack overflow. Dynamic shared memory:
+// traceSharedBytes(blockDim.x).
 //
-// Each round has a triangle phase, in which every lane with pending
-// triangles tests one per iteration until no lane has any, and a node phase,
+// Each round has a triangle phase, in which the warp tests all pending
+// triangles of its lanes cooperatively (warpTrianglePhase), and a node phase,
 // in which every busy lane takes one node step. The node step (eight box
 // tests) is the costly one, so running it in lockstep for all busy lanes
-// keeps the warp's lanes doing useful work.
-//
-// Triangle postponement (Ylitie et al. 2017): at the start of a triangle
-// phase, when fewer than a fifth of the busy lanes have triangles, a lane
-// that also has interior children to visit pushes its triangle group and
-// takes part in the node phase instead. A lane postpones only while its stack
-// has room for a full descent of the tree afterwards (postponeBelow =
-// capacity minus the tree depth), so postponement never causes an overflow.
+// keeps the warp's lanes doing useful work. postponeBelow is unused by this
+// schedule and kept for the tuning interface.
 template <bool ANY, class IO>
 __device__ __forceinline__ void persistentTrace(IO& io, int count, const uint4* nodes, const float4* tris, int* fetch,
                                                 unsigned long long* done, int* errorFlag, int postponeBelow,
                                                 int refill) {
+    (void)postponeBelow;
     extern __shared__ uint2 smemStack[];
     uint2* sstack = smemStack + threadIdx.x;
     const int stride = blockDim.x;
+    WarpTriangles* warps = reinterpret_cast<WarpTriangles*>(smemStack + kSharedStack * blockDim.x);
+    WarpTriangles& W = warps[threadIdx.x >> 5];
     uint2 lstack[kStackCapacity - kSharedStack];
     const unsigned lane = threadIdx.x & 31u;
     const unsigned below = (1u << lane) - 1u;
@@ -130,8 +229,15 @@ __device__ __forceinline__ void persistentTrace(IO& io, int count, const uint4* 
                         float3 o, d;
                         float limit;
                         io.load(mine, o, d, limit);
-                        laneStart(L, o, d, limit);
-                        k = mine;
+                        if (limit > 0.0f) {
+                            laneStart(L, o, d, limit);
+                            k = mine;
+                        } else {
+                            // No distance can be accepted (limit <= 0 or NaN):
+                            // the reference's answer is "no hit" at once.
+                            io.store(mine, Hit{-1, limit, 0.0f, 0.0f});
+                            finished++;
+                        }
                     }
                 }
             }
@@ -139,25 +245,11 @@ __device__ __forceinline__ void persistentTrace(IO& io, int count, const uint4* 
         if (!__any_sync(0xFFFFFFFFu, k >= 0)) break;
         const int threshold = drained ? 1 : refill;
         for (;;) {
-            // Triangle phase.
-            const bool busy = k >= 0;
-            const unsigned busyLanes = __popc(__ballot_sync(0xFFFFFFFFu, busy));
-            const unsigned triLanes = __popc(__ballot_sync(0xFFFFFFFFu, busy && L.triGroup.y != 0u));
-            if (busy && L.triGroup.y != 0u && triLanes * 5u < busyLanes && L.group.y > 0x00FFFFFFu &&
-                L.top < postponeBelow) {
-                if (L.top < kSharedStack) sstack[L.top * stride] = L.triGroup;
-                else lstack[L.top - kSharedStack] = L.triGroup;
-                L.top++;
-                L.triGroup.y = 0u;
+            if (warpTrianglePhase<ANY>(L, k >= 0, tris, W, lane)) {
+                io.store(k, L.hit);
+                k = -1;
+                finished++;
             }
-            while (__any_sync(0xFFFFFFFFu, k >= 0 && L.triGroup.y != 0u)) {
-                if (k >= 0 && L.triGroup.y != 0u && triangleStep<ANY>(L, tris)) {
-                    io.store(k, L.hit);
-                    k = -1;
-                    finished++;
-                }
-            }
-            // Node phase.
             if (k >= 0 && nodeStep(L, nodes, sstack, stride, lstack, overflow)) {
                 io.store(k, L.hit);
                 k = -1;

@@ -171,7 +171,7 @@ int RtxSetIntegrator(void* session, int mode);
  *   RTX_TUNE_POSTPONE         1 = postpone triangle tests in sparse warps,
  *                             0 = off (default)
  *   RTX_TUNE_REFILL           refill a warp's idle lanes when fewer than this
- *                             many lanes are busy (1..32, default 28) */
+ *                             many lanes are busy (1..32, default 24) */
 #define RTX_TUNE_PATHS_IN_FLIGHT 1
 #define RTX_TUNE_POSTPONE 2
 #define RTX_TUNE_REFILL 3
