@@ -20,6 +20,7 @@
 #include <chrono>
 #include <cstring>
 #include <curand.h>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -581,3 +582,99 @@ int RtxSetTuning(void* p, int key, int value) {
 }
 
 }  // extern "C"
+
+// ---- ray queries without device allocation ----
+//
+// RtxQueryRaysStatic serves callers that must not allocate device memory
+// during the call: code that runs while another thread captures CUDA work
+// into a graph, or latency-critical loops where cudaMalloc/cudaFree would
+// serialise with the whole device, or hosts whose device memory is owned by
+// a pool the library must not touch. It stages rays and hits in one
+// file-scope device array instead of cudaMalloc'd buffers.
+namespace {
+
+constexpr int kStaticQueryRays = 16384;  // largest count one call accepts
+constexpr size_t kStaticPacked = 0;                                    // 2 float4 per ray, kernel layout
+constexpr size_t kStaticHits = 2 * (size_t)kStaticQueryRays;           // 1 float4 per ray, RtxHit layout
+constexpr size_t kStaticRaw = 3 * (size_t)kStaticQueryRays;            // caller's 28-byte RtxQuery records
+constexpr size_t kStaticCounters = kStaticRaw + (7 * (size_t)kStaticQueryRays + 3) / 4;  // work counter, error flag
+constexpr size_t kStaticFloat4s = kStaticCounters + 1;                 // 1.25 MiB in total
+constexpr int kStaticMaxDevices = 64;
+
+// One copy per GPU that loads the library, held until the process exits.
+// Every call on a device shares it: calls whose GPU work overlaps race.
+static __device__ __align__(256) float4 g_staticQueryScratch[kStaticFloat4s];
+
+std::mutex g_staticScratchLock;
+float4* g_staticScratchAddress[kStaticMaxDevices] = {};
+
+// Device address of g_staticQueryScratch on the current device, looked up
+// once per device (the host-side symbol is not a device address).
+float4* staticQueryScratch(int device, std::string& error) {
+    if (device < 0 || device >= kStaticMaxDevices) { error = "RtxQueryRaysStatic: device index out of range"; return nullptr; }
+    std::lock_guard<std::mutex> guard(g_staticScratchLock);
+    if (!g_staticScratchAddress[device]) {
+        void* address = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&address, g_staticQueryScratch);
+        if (e != cudaSuccess || !address) {
+            error = std::string("RtxQueryRaysStatic: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e);
+            return nullptr;
+        }
+        g_staticScratchAddress[device] = static_cast<float4*>(address);
+    }
+    return g_staticScratchAddress[device];
+}
+
+// 28-byte RtxQuery records -> the query kernel's two-float4 layout.
+__global__ void packStaticQueriesKernel(const float* raw, float4* packed, int count) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const float* q = raw + 7 * (size_t)i;
+    packed[2 * (size_t)i] = make_float4(q[0], q[1], q[2], q[3]);
+    packed[2 * (size_t)i + 1] = make_float4(q[4], q[5], q[6], 0.0f);
+}
+
+}  // namespace
+
+extern "C" int RtxQueryRaysStatic(void* p, const RtxQuery* queries, int count, int any, RtxHit* hits) {
+    Session* s = static_cast<Session*>(p);
+    if (!s) return 0;
+    if (!s->ready || !queries || !hits || count < 0) {
+        s->error = cudaErrorInvalidValue;
+        s->hostError = "RtxQueryRaysStatic: invalid arguments or session not initialised";
+        return 0;
+    }
+    if (count > kStaticQueryRays) {
+        s->error = cudaErrorInvalidValue;
+        s->hostError = "RtxQueryRaysStatic: count exceeds the static scratch capacity of 16384 rays per call";
+        return 0;
+    }
+    if (count == 0) return 1;
+    cudaError_t e = cudaSetDevice(s->device);
+    if (e != cudaSuccess) { fail(s, e); return 0; }
+    std::string why;
+    float4* scratch = staticQueryScratch(s->device, why);
+    if (!scratch) { s->hostError = why; return 0; }
+    float4* packed = scratch + kStaticPacked;
+    float4* deviceHits = scratch + kStaticHits;
+    float* raw = reinterpret_cast<float*>(scratch + kStaticRaw);
+    int* counters = reinterpret_cast<int*>(scratch + kStaticCounters);  // [0] work counter, [1] error flag
+    int overflow = 0;
+    e = cudaMemcpyAsync(raw, queries, sizeof(RtxQuery) * (size_t)count, cudaMemcpyHostToDevice, s->stream);
+    if (e == cudaSuccess) {
+        packStaticQueriesKernel<<<(count + 255) / 256, 256, 0, s->stream>>>(raw, packed, count);
+        e = cudaGetLastError();
+    }
+    // The array keeps the previous call's contents: clear the counters.
+    if (e == cudaSuccess) e = cudaMemsetAsync(counters, 0, 2 * sizeof(int), s->stream);
+    if (e == cudaSuccess)
+        e = launchQueries(s->bvh.wideNodes, s->bvh.packedTris, packed, count, any, deviceHits, counters, counters + 1,
+                          s->build.wideDepth, s->tuning, s->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(hits, deviceHits, sizeof(RtxHit) * (size_t)count, cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&overflow, counters + 1, sizeof(int), cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) { fail(s, e); return 0; }
+    if (overflow) { s->hostError = "BVH traversal stack overflow"; return 0; }
+    return 1;
+}

@@ -88,7 +88,8 @@ LIBRARY = ROOT / 'libCudaRayTracer.so'
 EXPORTS = ('RtCreate', 'RtDestroy', 'RtShutdown', 'RtInitialize', 'RtRender', 'RtDenoise', 'RtReset',
            'RtAccumulationVersion', 'RtSampleCount', 'RtEmbreeBuildMilliseconds', 'RtCpuThreadCount',
            'RtBvhInfo', 'RtLastError', 'RtxQueryRays', 'RtxSobolSamples', 'RtxExportBvh', 'RtxBvhStatsGet',
-           'RtxReadAccumulation', 'RtxRenderStatsGet', 'RtxRenderDevice', 'RtxSetIntegrator', 'RtxSetTuning')
+           'RtxReadAccumulation', 'RtxRenderStatsGet', 'RtxRenderDevice', 'RtxSetIntegrator', 'RtxSetTuning',
+           'RtxQueryRaysStatic')
 
 
 def load_library(path=None):
@@ -123,6 +124,7 @@ def load_library(path=None):
     lib.RtxRenderDevice.argtypes = [vp, c.POINTER(Camera), c.POINTER(Settings), c.POINTER(c.c_float)]
     lib.RtxSetIntegrator.argtypes = [vp, c.c_int]
     lib.RtxSetTuning.argtypes = [vp, c.c_int, c.c_int]
+    lib.RtxQueryRaysStatic.argtypes = [vp, c.c_void_p, c.c_int, c.c_int, c.c_void_p]
     return lib
 
 
@@ -203,6 +205,15 @@ class Session:
         q = np.ascontiguousarray(queries, dtype=QUERY_DTYPE)
         out = np.zeros(len(q), HIT_DTYPE)
         self.check(self.lib.RtxQueryRays(self.handle, q.ctypes.data, len(q), int(any_hit), out.ctypes.data))
+        return out
+
+    STATIC_QUERY_CAPACITY = 16384
+
+    def query_static(self, queries, any_hit=False):
+        """RtxQueryRaysStatic: the same answers as query(), staged without device allocation."""
+        q = np.ascontiguousarray(queries, dtype=QUERY_DTYPE)
+        out = np.zeros(len(q), HIT_DTYPE)
+        self.check(self.lib.RtxQueryRaysStatic(self.handle, q.ctypes.data, len(q), int(any_hit), out.ctypes.data))
         return out
 
     def bvh_info(self):

@@ -176,6 +176,18 @@ int RtxSetIntegrator(void* session, int mode);
 #define RTX_TUNE_POSTPONE 2
 #define RTX_TUNE_REFILL 3
 int RtxSetTuning(void* session, int key, int value);
+/* RtxQueryRays without any device allocation; no counterpart in the reference.
+ * For callers that must not allocate device memory during the call (work
+ * running beside a CUDA graph capture, latency-critical loops where
+ * cudaMalloc/cudaFree would synchronise the device, hosts whose device memory
+ * belongs to a pool). Rays and hits are staged in a file-scope device array
+ * of 1.25 MiB that every GPU loading the library keeps until the process
+ * exits; count may be at most 16384 per call (larger counts return 0 with a
+ * message). The first call on each device looks up that array's device
+ * address, so make it before any stream capture. All calls on a device share
+ * the array: calls whose GPU work overlaps race and must be serialised by the
+ * caller. Results equal RtxQueryRays. */
+int RtxQueryRaysStatic(void* session, const RtxQuery* queries, int count, int any, RtxHit* hits);
 
 #ifdef __cplusplus
 }
