@@ -57,6 +57,10 @@ def parse():
     p.add_argument('--no-reference-cuda', action='store_true')
     p.add_argument('--resolution', default=None, help='WxH override, for small profiling cases')
     p.add_argument('--spp', type=int, default=SPP_PER_STEP, help='paths per pixel per step (1..16)')
+    p.add_argument('--quality', action='store_true',
+                   help='also measure time to 35 dB PSNR vs a 4096-spp render on the 2M-triangle scene')
+    p.add_argument('--quality-resolution', default=None, help='WxH override of the quality scene')
+    p.add_argument('--oracle-spp', type=int, default=4096)
     return p.parse_args()
 
 
@@ -254,6 +258,100 @@ def reference_cuda(tris, cam, settings, w, h, rays_per_step, steps=3):
         ref.close()
 
 
+def psnr8(image, reference):
+    """PSNR in dB of 8-bit RGB display values (alpha ignored)."""
+    import numpy as np
+    a = image.reshape(-1, 4)[:, :3].astype(np.float64)
+    b = reference.reshape(-1, 4)[:, :3].astype(np.float64)
+    mse = float(np.mean((a - b) ** 2))
+    return (float('inf') if mse == 0 else float(20.0 * np.log10(255.0 / np.sqrt(mse)))), float(np.sqrt(mse))
+
+
+def quality_run(lib, args, target_db=35.0):
+    """Time to reach target_db PSNR against a high-spp render of the
+    end-to-end scene (2M triangles, depth 5, constant 0.1 environment):
+    plain progressive accumulation vs 8 spp followed by RtDenoise. PSNR is
+    taken on the 8-bit display images (the reference's own quality tool
+    compares 8-bit RGB, Tools/verify_quality.py:53-54); the high-spp render
+    uses a different sampler seed than the arms."""
+    import numpy as np
+    import scenes
+    from native_api import Session, Settings
+    kwargs = {}
+    if args.quality_resolution:
+        kwargs['width'], kwargs['height'] = (int(v) for v in args.quality_resolution.lower().split('x'))
+    tris, cam, st, w, h = scenes.end_to_end_room(**kwargs)
+    s = Session(lib)
+    try:
+        s.initialize(tris, w, h)
+        s.set_environment(0.1)
+        oracle_settings = Settings(st.maxBounces, st.exposure, st.aperture, st.focusDistance, st.skyStrength,
+                                   20261023, 16)
+        oracle_ms = 0.0
+        passes = max(1, args.oracle_spp // 16)
+        for _ in range(passes - 1):
+            oracle_ms += s.render_device(cam, oracle_settings)
+        oracle, ms = s.render(cam, oracle_settings)
+        oracle_ms += ms
+        oracle = oracle.copy()
+        # Plain progressive accumulation: PSNR after every pass of 4 paths per
+        # pixel up to 64 spp, then every 16.
+        spp, device_ms, wall0 = 0, 0.0, time.perf_counter()
+        curve = []
+        reached = None
+        while spp < args.oracle_spp // 2:
+            st.raysPerPixel = 4 if spp < 64 else 16
+            img, ms = s.render(cam, st)
+            device_ms += ms
+            spp += st.raysPerPixel
+            db, rmse = psnr8(img, oracle)
+            curve.append([spp, round(device_ms, 2), round(db, 3)])
+            if db >= target_db:
+                reached = {'spp': spp, 'device_ms': device_ms, 'psnr_db': db, 'rmse_8bit': rmse}
+                break
+        plain_wall_ms = (time.perf_counter() - wall0) * 1e3
+        # Denoised: 8 spp, then more paths per pixel until the filtered image
+        # reaches the target (each budget rendered from scratch).
+        trials = []
+        denoised = None
+        for budget in (8, 16, 32, 64, 128, 256):
+            s.lib.RtReset(s.handle)
+            render_ms, done = 0.0, 0
+            while done < budget:
+                st.raysPerPixel = min(16, budget - done)
+                img, ms = s.render(cam, st)
+                render_ms += ms
+                done += st.raysPerPixel
+            raw_db, _ = psnr8(img, oracle)
+            den, denoise_ms = s.denoise()
+            den_db, den_rmse = psnr8(den, oracle)
+            trial = {'spp': budget, 'render_ms': render_ms, 'denoise_ms': denoise_ms, 'psnr_db': den_db,
+                     'rmse_8bit': den_rmse, 'raw_psnr_db': raw_db}
+            trials.append(trial)
+            if den_db >= target_db:
+                denoised = dict(trial, reaches_target=True)
+                break
+        if denoised is None:
+            denoised = dict(trials[-1], reaches_target=False)
+        denoised['denoiser'] = 'guided a-trous wavelet filter (RtDenoise)'
+        denoised['at_8spp'] = trials[0]
+        result = {
+            'workload': 'end_to_end_room', 'triangles': len(tris), 'width': w, 'height': h,
+            'max_depth': st.maxBounces, 'environment': 0.1, 'exposure': st.exposure, 'target_db': target_db,
+            'oracle_spp': passes * 16, 'oracle_device_ms': oracle_ms,
+            'plain': dict(reached or {'spp': spp, 'device_ms': device_ms, 'psnr_db': curve[-1][2] if curve else None},
+                          reaches_target=reached is not None, wall_ms=plain_wall_ms),
+            'denoised': denoised,
+            'psnr_metric': '20 log10(255 / RMSE) over 8-bit RGB display values',
+            'curve_every_4spp': curve[:: max(1, len(curve) // 32)],
+        }
+        if reached and denoised['reaches_target']:
+            result['speedup_denoised_vs_plain'] = reached['device_ms'] / (denoised['render_ms'] + denoised['denoise_ms'])
+        return result
+    finally:
+        s.close()
+
+
 def l2_flusher():
     try:
         import torch
@@ -275,6 +373,13 @@ def run_ours(args, rank, local_rank, world):
     dist = Dist(world)
     lib = load_library()
     tris, cam, settings, w, h = workload(args)
+    # Load every kernel once (CUDA loads modules lazily at first launch), so
+    # the reported build time is the build's, not one-time module loading.
+    import scenes
+    with Session(lib) as warm:
+        small = scenes.cornell_sphere(width=32, height=32)
+        warm.initialize(small[0], 32, 32)
+        warm.render(small[1], small[2])
     s = Session(lib)
     s.initialize(tris, w, h)
     bvh = s.bvh_stats()
@@ -413,7 +518,7 @@ def run_ours(args, rank, local_rank, world):
                       'binary_nodes': bvh['binaryNodes'], 'binary_depth': bvh['binaryDepth'],
                       'wide_nodes': bvh['wideNodes'], 'sah_cost': bvh['sahCost']},
             'reference_cuda': ref_cuda,
-            'time_to_35db': None,
+            'time_to_35db': quality_run(lib, args) if (args.quality and world == 1) else None,
         }
     s.close()
     dist.close()

@@ -70,6 +70,8 @@ struct SceneView {
     int lightCount;
     float lightArea;
     int wideDepth;           // levels of the wide BVH (bounds the traversal stack)
+    int environmentMode;     // 0: the reference's sky gradient x skyStrength; 1: constant radiance
+    float3 environment;      // the constant radiance of mode 1
 };
 
 // ---- BRDF and sky (renderer.cu:181-196) ----
@@ -91,6 +93,12 @@ RT_HD float3 evaluateBsdf(const SceneTri& t, float3 n, float3 refl, float3 dir, 
 RT_HD float3 skyRadiance(float3 d, float strength) {
     float t = fminf(1.0f, fmaxf(0.0f, d.y));
     return scale(add(scale(v3(.65f, .72f, .82f), 1.0f - t), scale(v3(.15f, .32f, .65f), t)), strength);
+}
+// Radiance of rays that leave the scene after the first bounce
+// (renderer.cu:218-221). Mode 0 is the reference's sky; mode 1, a constant
+// environment, is an addition that leaves mode 0's results untouched.
+RT_HD float3 environmentRadiance(const SceneView& sc, float3 d, float skyStrength) {
+    return sc.environmentMode == 1 ? sc.environment : skyRadiance(d, skyStrength);
 }
 RT_HD float3 orientAround(float3 axis, float cosine, float angle) {
     float3 tangent = normalize(cross(fabsf(axis.y) < .999f ? v3(0, 1, 0) : v3(1, 0, 0), axis));
@@ -143,7 +151,7 @@ struct ShadowRequest { float3 origin, dir; float limit; float3 contribution; };
 RT_HD unsigned shadeBounce(const SceneView& sc, const Settings& set, int bounce, PathState& st, const Hit& hit,
                            const Sampler& rng, ShadowRequest& req) {
     if (hit.index < 0) {
-        if (bounce > 0) st.radiance = add(st.radiance, mul(st.throughput, skyRadiance(st.dir, set.skyStrength)));
+        if (bounce > 0) st.radiance = add(st.radiance, mul(st.throughput, environmentRadiance(sc, st.dir, set.skyStrength)));
         return 0;
     }
     const SceneTri& t = sc.tris[hit.index];

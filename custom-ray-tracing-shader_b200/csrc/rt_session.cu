@@ -81,6 +81,8 @@ struct Session {
     double sahCost = -1.0;
     int integrator = 0, pathsInFlight = 0;
     TraceTuning tuning;
+    int environmentMode = 0;
+    float3 environment = make_float3(0.0f, 0.0f, 0.0f);
 };
 
 bool fail(Session* s, cudaError_t e, const char* what = nullptr) {
@@ -123,7 +125,7 @@ bool validSettings(const RenderSettings* st) {
 
 SceneView deviceView(Session* s) {
     return SceneView{s->dTris, s->bvh.wideNodes, s->bvh.packedTris, s->dLights, (int)s->lights.size(), s->lightArea,
-                     s->build.wideDepth};
+                     s->build.wideDepth, s->environmentMode, s->environment};
 }
 
 bool ensureWave(Session* s) {
@@ -203,7 +205,7 @@ bool renderHost(Session* s, const CameraData* camera, const RenderSettings* sett
     for (int d = 0; d < kSobolDims; d++) seedHash[d] = sobolHash(set.seed + (unsigned)d * 0x9e3779b9u);
     if (s->hostSum.size() != (size_t)s->width * s->height) s->hostSum.assign((size_t)s->width * s->height, Accum{});
     SceneView sc{s->tris.data(), s->hostWide.data(), s->hostPacked.data(), s->lights.data(), (int)s->lights.size(),
-                 s->lightArea, s->build.wideDepth};
+                 s->lightArea, s->build.wideDepth, s->environmentMode, s->environment};
     const int w = s->width, h = s->height;
     const unsigned sample0 = s->samples;
     Accum* sums = s->hostSum.data();
@@ -557,6 +559,23 @@ int RtxSetIntegrator(void* p, int mode) {
     Session* s = static_cast<Session*>(p);
     if (!s || mode < 0 || mode > 1) return 0;
     s->integrator = mode;
+    return 1;
+}
+
+int RtxSetEnvironment(void* p, int mode, float r, float g, float b) {
+    Session* s = static_cast<Session*>(p);
+    if (!s) return 0;
+    if (mode < 0 || mode > 1 || !(r >= 0) || !(g >= 0) || !(b >= 0)) {
+        s->error = cudaErrorInvalidValue;
+        s->hostError = "RtxSetEnvironment: mode 0 or 1 and non-negative radiance";
+        return 0;
+    }
+    float3 c = mode == 1 ? make_float3(r, g, b) : make_float3(0.0f, 0.0f, 0.0f);
+    if (mode != s->environmentMode || std::memcmp(&c, &s->environment, sizeof(c))) {
+        s->environmentMode = mode;
+        s->environment = c;
+        RtReset(s);  // a different light field: restart the accumulation
+    }
     return 1;
 }
 

@@ -89,7 +89,7 @@ EXPORTS = ('RtCreate', 'RtDestroy', 'RtShutdown', 'RtInitialize', 'RtRender', 'R
            'RtAccumulationVersion', 'RtSampleCount', 'RtEmbreeBuildMilliseconds', 'RtCpuThreadCount',
            'RtBvhInfo', 'RtLastError', 'RtxQueryRays', 'RtxSobolSamples', 'RtxExportBvh', 'RtxBvhStatsGet',
            'RtxReadAccumulation', 'RtxRenderStatsGet', 'RtxRenderDevice', 'RtxSetIntegrator', 'RtxSetTuning',
-           'RtxQueryRaysStatic')
+           'RtxQueryRaysStatic', 'RtxSetEnvironment')
 
 
 def load_library(path=None):
@@ -125,6 +125,7 @@ def load_library(path=None):
     lib.RtxSetIntegrator.argtypes = [vp, c.c_int]
     lib.RtxSetTuning.argtypes = [vp, c.c_int, c.c_int]
     lib.RtxQueryRaysStatic.argtypes = [vp, c.c_void_p, c.c_int, c.c_int, c.c_void_p]
+    lib.RtxSetEnvironment.argtypes = [vp, c.c_int, c.c_float, c.c_float, c.c_float]
     return lib
 
 
@@ -248,6 +249,14 @@ class Session:
                            (self.TUNE_REFILL, refill)):
             if value is not None:
                 self.check(self.lib.RtxSetTuning(self.handle, key, int(value)))
+
+    def set_environment(self, constant=None):
+        """None: the reference's sky gradient; a float or RGB triple: constant radiance."""
+        if constant is None:
+            self.check(self.lib.RtxSetEnvironment(self.handle, 0, 0.0, 0.0, 0.0))
+        else:
+            r, g, b = (constant,) * 3 if isinstance(constant, (int, float)) else constant
+            self.check(self.lib.RtxSetEnvironment(self.handle, 1, r, g, b))
 
     def sample_count(self):
         return self.lib.RtSampleCount(self.handle)

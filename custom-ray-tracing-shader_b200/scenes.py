@@ -17,6 +17,9 @@ Workloads:
                        triangles, the geodesic count closest to one million)
                        and +-5% radial noise; 1920x1080, max depth 3,
                        diffuse only.
+  end_to_end_room()  - four smoothly displaced spheres (1,997,120 triangles)
+                       in the same kind of room with a shaded uplight,
+                       1920x1080, max depth 5, constant 0.1 environment.
 Check scenes mirror the geometry categories of the reference's own
 verifiers (Tools/verify_native.py, Tools/verify_bvh.cu).
 """
@@ -81,10 +84,12 @@ def box_quad(p, u, v, **kwargs):
     return records([p, p], [p + u, p + u + v], [p + u + v, p + v], **kwargs)
 
 
-def geodesic_sphere(subdivisions, radius, center, noise, rng):
+def geodesic_sphere(subdivisions, radius, center, noise, rng, smooth=False):
     """Icosahedron with every face split into subdivisions^2 triangles, projected
     to a sphere; each distinct vertex is moved along its radius by a factor
-    (1 + U(-noise, noise)). Returns corner arrays and smooth vertex normals."""
+    (1 + U(-noise, noise)) (independent per vertex), or with smooth=True by
+    (1 + noise * n(p)) where n is a seeded sum of eight random plane waves
+    scaled to [-1, 1]. Returns corner arrays and smooth vertex normals."""
     f = int(subdivisions)
     ico = _ICO_V / np.linalg.norm(_ICO_V, axis=1, keepdims=True)
     ii, jj = np.meshgrid(np.arange(f + 1), np.arange(f + 1), indexing='ij')
@@ -108,7 +113,13 @@ def geodesic_sphere(subdivisions, radius, center, noise, rng):
     keys = np.round(pts * (1 << 24)).astype(np.int64)
     _, first, inverse = np.unique(keys, axis=0, return_index=True, return_inverse=True)
     unique_pts = pts[first]
-    scale_f = 1.0 + rng.uniform(-noise, noise, len(unique_pts))
+    if smooth:
+        waves = rng.normal(size=(8, 3)) * rng.uniform(2.0, 6.0, (8, 1))
+        phases = rng.uniform(0, 2 * np.pi, 8)
+        field = np.sin(unique_pts @ waves.T + phases).sum(axis=1)
+        scale_f = 1.0 + noise * field / max(np.abs(field).max(), 1e-12)
+    else:
+        scale_f = 1.0 + rng.uniform(-noise, noise, len(unique_pts))
     verts = unique_pts * (radius * scale_f)[:, None] + np.asarray(center, np.float64)[None, :]
     corners = inverse.reshape(-1)[tris]
     # Area-weighted vertex normals.
@@ -175,6 +186,35 @@ def displaced_sphere_room(seed=11, width=1920, height=1080, bounces=3, subdivisi
     tris = np.concatenate([room, sphere])
     cam = camera((0.0, 2.0, -7.0), (0.0, 1.6, 0.0), math.tan(math.radians(24.0)), width / height)
     settings = Settings(bounces, 1.0, 0.0, 1.0, 0.0, 42, 1)
+    return tris, cam, settings, width, height
+
+
+def end_to_end_room(seed=17, width=1920, height=1080, bounces=5, subdivisions=158, light_half=0.4, emission=40.0,
+                    eye=(0.0, 2.0, -2.8), target=(0.0, 1.5, 2.0), half_fov_deg=38.0, light_y=3.5, shade=True,
+                    exposure=1.5):
+    """Config 'end-to-end equal quality': four displaced geodesic spheres of
+    20 * 158^2 = 499,280 triangles each (smooth +-5% radial displacement,
+    different radii and albedo) in the 12-triangle room with one quad light
+    and a 2-triangle shade under it, so the room is lit through the ceiling
+    (mostly indirect light): 1,997,134 triangles, 1920x1080, max depth 5,
+    camera inside the room. The workload's constant 0.1 environment is set
+    on the session with RtxSetEnvironment."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    colors = rng.uniform(0.2, 0.8, (9, 3))
+    room = open_box((-3.0, 0.0, -3.0), (3.0, 4.0, 3.0), colors[:5], light_half, light_y, emission)
+    parts = [room]
+    if shade:
+        # A diffuse shade just under the (two-sided) light: the room below is
+        # lit only through the ceiling, by indirect light.
+        h = 1.5 * light_half
+        parts.append(box_quad((-h, light_y - 0.05, -h), (2 * h, 0, 0), (0, 0, 2 * h), color=(0.8, 0.8, 0.8), mesh=20))
+    layout = (((-1.4, 0.8, 0.6), 0.8), ((1.3, 0.9, 1.0), 0.9), ((-0.2, 0.55, -1.0), 0.55), ((0.6, 2.2, 1.6), 0.6))
+    for k, (center, radius) in enumerate(layout):
+        v0, v1, v2, normals = geodesic_sphere(subdivisions, radius, center, 0.05, rng, smooth=True)
+        parts.append(records(v0, v1, v2, color=colors[5 + k], normals=normals, mesh=8 + k))
+    tris = np.concatenate(parts)
+    cam = camera(eye, target, math.tan(math.radians(half_fov_deg)), width / height)
+    settings = Settings(bounces, exposure, 0.0, 1.0, 0.0, 42, 1)
     return tris, cam, settings, width, height
 
 

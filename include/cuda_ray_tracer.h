@@ -176,6 +176,13 @@ int RtxSetIntegrator(void* session, int mode);
 #define RTX_TUNE_POSTPONE 2
 #define RTX_TUNE_REFILL 3
 int RtxSetTuning(void* session, int key, int value);
+/* Light arriving from outside the scene on rays that leave it after the first
+ * bounce (primary misses stay black, as in the reference). mode 0: the
+ * reference's sky gradient times settings->skyStrength (Native/renderer.cu:
+ * 193-196, the default); mode 1: constant radiance (r, g, b), skyStrength
+ * ignored. A change resets the accumulation. No counterpart in the
+ * reference's exported ABI. */
+int RtxSetEnvironment(void* session, int mode, float r, float g, float b);
 /* RtxQueryRays without any device allocation; no counterpart in the reference.
  * For callers that must not allocate device memory during the call (work
  * running beside a CUDA graph capture, latency-critical loops where

@@ -88,7 +88,7 @@ int hc_render(const SceneTri* tris, const Light* lights, int lightCount, float l
     for (int r = 0; r < set->raysPerPixel; r++)
         for (int d = 0; d < kSobolDims; d++) passXor[(size_t)r * kSobolDims + d] = sobolXor(dirs, sample0 + (unsigned)r, (unsigned)d);
     for (int d = 0; d < kSobolDims; d++) seedHash[d] = sobolHash(set->seed + (unsigned)d * 0x9e3779b9u);
-    SceneView sc{tris, wide, packed, lights, lightCount, lightArea, 0};
+    SceneView sc{tris, wide, packed, lights, lightCount, lightArea, 0, 0, make_float3(0.0f, 0.0f, 0.0f)};
     uint2 stack[kStackCapacity];
     int overflow = 0;
     unsigned p = 0, q = 0, s = 0;

@@ -247,3 +247,28 @@ def test_denoise_behaviour(drv):
     assert all(value == (255 if i % 4 == 3 else 0) for i, value in enumerate(ai))
     lib.RtShutdown(drv.session)
     assert not lib.RtDenoise(drv.session, first, len(first), c.byref(ms))
+
+
+def test_constant_environment_extension(drv):
+    """RtxSetEnvironment mode 1 lights bounces with a constant radiance and
+    leaves primary misses black; it resets the accumulation; mode 0 is the
+    reference's sky. CPU and CUDA backends agree within 1/255."""
+    lib = drv.lib
+    w, h = 33, 25
+    camera = Camera(Vector(0, 0, -3), Vector(1, 0, 0), Vector(0, 1, 0), Vector(0, 0, 1), .3, w / h, 1, 0)
+    floor = scenes.quad(-2, 2, -2, 2, 0)
+    drv.initialize(floor, w, h)
+    lit = Settings(8, 1, 0, 3, 0, 42, 1)
+    dark = drv.agree(camera, w, h, lit, 8)
+    assert centre(dark, w, h) == (0, 0, 0, 255)
+    version = lib.RtAccumulationVersion(drv.session)
+    assert lib.RtxSetEnvironment(drv.session, 1, 0.5, 0.5, 0.5)
+    assert lib.RtAccumulationVersion(drv.session) == version + 1 and lib.RtSampleCount(drv.session) == 0
+    bright = drv.agree(camera, w, h, lit, 8)
+    assert centre(bright, w, h)[0] > 60
+    camera.origin.x = 20
+    empty = drv.agree(camera, w, h, lit)
+    assert all(empty[i:i + 4] == bytes((0, 0, 0, 255)) for i in range(0, len(empty), 4))
+    assert not lib.RtxSetEnvironment(drv.session, 2, 0, 0, 0)
+    assert not lib.RtxSetEnvironment(drv.session, 1, -1, 0, 0)
+    assert lib.RtxSetEnvironment(drv.session, 0, 0, 0, 0)
