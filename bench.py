@@ -295,15 +295,17 @@ def quality_run(lib, args, target_db=35.0):
         oracle_ms += ms
         oracle = oracle.copy()
         # Plain progressive accumulation: PSNR after every pass of 4 paths per
-        # pixel up to 64 spp, then every 16.
+        # pixel (one pass size throughout: RtRender restarts the accumulation
+        # when any setting changes, renderer.cu:388-389).
         spp, device_ms, wall0 = 0, 0.0, time.perf_counter()
         curve = []
         reached = None
+        st.raysPerPixel = 4
+        s.lib.RtReset(s.handle)
         while spp < args.oracle_spp // 2:
-            st.raysPerPixel = 4 if spp < 64 else 16
             img, ms = s.render(cam, st)
             device_ms += ms
-            spp += st.raysPerPixel
+            spp = s.sample_count()
             db, rmse = psnr8(img, oracle)
             curve.append([spp, round(device_ms, 2), round(db, 3)])
             if db >= target_db:

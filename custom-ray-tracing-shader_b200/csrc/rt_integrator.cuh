@@ -113,6 +113,7 @@ struct PathState {
     float prevPdf;
     float3 radiance, albedo, normal;
     unsigned covered;
+    float depth;  // distance to the first hit (0 on a primary miss); an added AOV
 };
 
 // Camera ray and initial state (renderer.cu:198-214). rng.base must be 0.
@@ -136,6 +137,7 @@ RT_HD PathState startPath(const Camera& cam, const Settings& set, int x, int y, 
     s.prevPdf = 0;
     s.radiance = v3(0, 0, 0); s.albedo = v3(0, 0, 0); s.normal = v3(0, 0, 0);
     s.covered = 0;
+    s.depth = 0.0f;
     return s;
 }
 
@@ -159,6 +161,7 @@ RT_HD unsigned shadeBounce(const SceneView& sc, const Settings& set, int bounce,
     if (dot(g, st.dir) > 0) g = scale(g, -1.0f);
     if (bounce == 0) {
         st.covered = 1;
+        st.depth = hit.distance;
         st.albedo = t.emission > 0 ? v3(1, 1, 1)
                                    : add(scale(t.color, 1.0f - t.specularProbability), scale(t.specularColor, t.specularProbability));
         st.normal = g;
@@ -240,10 +243,11 @@ RT_HD uchar4 displayPixel(const Accum& total, unsigned samples, float exposure) 
 // one-kernel-per-pixel integrator and the host backends.
 RT_HD void renderPixel(const SceneView& sc, const Camera& cam, const Settings& set, int x, int y, int w, int h,
                        unsigned sample0, const unsigned* passXor, const unsigned* seedHash, Accum* sums,
-                       uchar4* pixels, uint2* stack, int stackStride, int* overflow, unsigned& nPrimary,
-                       unsigned& nSecondary, unsigned& nShadow) {
+                       float* depthSums, uchar4* pixels, uint2* stack, int stackStride, int* overflow,
+                       unsigned& nPrimary, unsigned& nSecondary, unsigned& nShadow) {
     size_t i = (size_t)y * w + x;
     Accum total = sample0 ? sums[i] : Accum{v3(0, 0, 0), v3(0, 0, 0), v3(0, 0, 0), 0u};
+    float depthTotal = sample0 ? depthSums[i] : 0.0f;
     for (int r = 0; r < set.raysPerPixel; r++) {
         Sampler rng{passXor + r * kSobolDims, seedHash, (unsigned)(y * w + x), 0u};
         PathState st = startPath(cam, set, x, y, w, h, rng);
@@ -261,8 +265,10 @@ RT_HD void renderPixel(const SceneView& sc, const Camera& cam, const Settings& s
             if (!(f & kContinue)) break;
         }
         addPath(total, st);
+        depthTotal += st.depth;
     }
     sums[i] = total;
+    depthSums[i] = depthTotal;
     pixels[i] = displayPixel(total, sample0 + (unsigned)set.raysPerPixel, set.exposure);
 }
 

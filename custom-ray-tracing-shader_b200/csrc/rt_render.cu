@@ -54,8 +54,8 @@ __global__ void __launch_bounds__(kMegaBlock) megakernel(RenderLaunch L) {
     unsigned nPrimary = 0, nSecondary = 0, nShadow = 0;
     int overflow = 0;
     if (x < L.w && y < L.h)
-        renderPixel(L.scene, L.cam, L.set, x, y, L.w, L.h, L.sample0, L.passXor, L.seedHash, L.sums, L.pixels, stack,
-                    stride, &overflow, nPrimary, nSecondary, nShadow);
+        renderPixel(L.scene, L.cam, L.set, x, y, L.w, L.h, L.sample0, L.passXor, L.seedHash, L.sums, L.depthSums,
+                    L.pixels, stack, stride, &overflow, nPrimary, nSecondary, nShadow);
     flushCounters(L.counters, nPrimary, nSecondary, nShadow);
     if (overflow) atomicExch(L.errorFlag, 1);
 }
@@ -137,6 +137,7 @@ __global__ void shadeKernel(WaveArgs A, WavefrontBuffers B, int q, int bounce) {
             st.radiance = v3(rad.x, rad.y, rad.z); st.covered = __float_as_uint(rad.w);
             float4 al = B.albedo[p], no = B.normal[p];
             st.albedo = v3(al.x, al.y, al.z); st.normal = v3(no.x, no.y, no.z);
+            st.depth = al.w;
             Hit h{__float_as_int(hv.w), hv.x, hv.y, hv.z};
             Sampler rng{A.L.passXor + A.r * kSobolDims, A.L.seedHash, (unsigned)(A.pixStart + p), 4u + 8u * (unsigned)bounce};
             unsigned f = shadeBounce(A.L.scene, A.L.set, bounce, st, h, rng, req);
@@ -147,7 +148,7 @@ __global__ void shadeKernel(WaveArgs A, WavefrontBuffers B, int q, int bounce) {
             B.pathC[p] = make_float4(st.throughput.x, st.throughput.y, st.throughput.z, 0.0f);
             B.radiance[p] = make_float4(st.radiance.x, st.radiance.y, st.radiance.z, __uint_as_float(st.covered));
             if (bounce == 0) {
-                B.albedo[p] = make_float4(st.albedo.x, st.albedo.y, st.albedo.z, 0.0f);
+                B.albedo[p] = make_float4(st.albedo.x, st.albedo.y, st.albedo.z, st.depth);
                 B.normal[p] = make_float4(st.normal.x, st.normal.y, st.normal.z, 0.0f);
             }
         }
@@ -193,13 +194,16 @@ __global__ void accumulateKernel(WaveArgs A, WavefrontBuffers B) {
     int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= A.n) return;
     size_t i = (size_t)(A.pixStart + p);
-    Accum total = (A.r == 0 && A.L.sample0 == 0) ? Accum{v3(0, 0, 0), v3(0, 0, 0), v3(0, 0, 0), 0u} : A.L.sums[i];
+    const bool first = A.r == 0 && A.L.sample0 == 0;
+    Accum total = first ? Accum{v3(0, 0, 0), v3(0, 0, 0), v3(0, 0, 0), 0u} : A.L.sums[i];
+    float depthTotal = first ? 0.0f : A.L.depthSums[i];
     float4 rad = B.radiance[p], al = B.albedo[p], no = B.normal[p];
     PathState st;
     st.radiance = v3(rad.x, rad.y, rad.z); st.covered = __float_as_uint(rad.w);
     st.albedo = v3(al.x, al.y, al.z); st.normal = v3(no.x, no.y, no.z);
     addPath(total, st);
     A.L.sums[i] = total;
+    A.L.depthSums[i] = depthTotal + al.w;
     if (A.r == A.L.set.raysPerPixel - 1)
         A.L.pixels[i] = displayPixel(total, A.L.sample0 + (unsigned)A.L.set.raysPerPixel, A.L.set.exposure);
 }
@@ -279,6 +283,27 @@ __global__ void denoisePresentKernel(const Accum* sums, const float4* color, int
     if (i >= count) return;
     float4 c4 = color[i];
     float3 c = sums[i].covered ? v3(c4.x, c4.y, c4.z) : v3(0, 0, 0);
+    pixels[i] = make_uchar4(tonemap(c.x, exposure), tonemap(c.y, exposure), tonemap(c.z, exposure), 255);
+}
+
+__global__ void aovKernel(const Accum* sums, const float* depthSums, unsigned samples, int count, float* aov) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    Accum s = sums[i];
+    float inv = 1.0f / (float)samples;
+    float3 c = scale(s.radiance, inv), a = scale(s.albedo, inv), n = normalize(s.normal);
+    float* o = aov + (size_t)i * 10;
+    o[0] = c.x; o[1] = c.y; o[2] = c.z;
+    o[3] = a.x; o[4] = a.y; o[5] = a.z;
+    o[6] = n.x; o[7] = n.y; o[8] = n.z;
+    o[9] = depthSums[i] * inv;
+}
+__global__ void presentRadianceKernel(const Accum* sums, const float* radiance, int count, float exposure,
+                                      uchar4* pixels) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const float* r = radiance + (size_t)i * 3;
+    float3 c = sums[i].covered ? v3(r[0], r[1], r[2]) : v3(0, 0, 0);
     pixels[i] = make_uchar4(tonemap(c.x, exposure), tonemap(c.y, exposure), tonemap(c.z, exposure), 255);
 }
 
@@ -456,6 +481,17 @@ cudaError_t launchDenoise(const Accum* sums, unsigned samples, int w, int h, flo
         phi *= 0.5f;
     }
     denoisePresentKernel<<<blocks(count, 256), 256, 0, stream>>>(sums, src, count, exposure, pixels);
+    return cudaGetLastError();
+}
+
+cudaError_t launchAovs(const Accum* sums, const float* depthSums, unsigned samples, int count, float* aov,
+                       cudaStream_t stream) {
+    aovKernel<<<blocks(count, 256), 256, 0, stream>>>(sums, depthSums, samples, count, aov);
+    return cudaGetLastError();
+}
+cudaError_t launchPresentRadiance(const Accum* sums, const float* radiance, int count, float exposure, uchar4* pixels,
+                                  cudaStream_t stream) {
+    presentRadianceKernel<<<blocks(count, 256), 256, 0, stream>>>(sums, radiance, count, exposure, pixels);
     return cudaGetLastError();
 }
 

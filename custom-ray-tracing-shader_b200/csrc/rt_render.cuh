@@ -13,6 +13,7 @@ struct RenderLaunch {
     const unsigned* passXor;     // [raysPerPixel][kSobolDims]
     const unsigned* seedHash;    // [kSobolDims]
     Accum* sums;                 // w*h running sums (read when sample0 > 0)
+    float* depthSums;            // w*h running sums of first-hit distance (an added AOV)
     uchar4* pixels;              // w*h display image
     unsigned long long* counters;  // [0] primary, [1] secondary, [2] shadow rays
     int* errorFlag;              // set to 1 on traversal stack overflow
@@ -62,5 +63,14 @@ cudaError_t launchSobolSamples(const unsigned* dirs, const unsigned* pixel, cons
 // Denoise: prepare guides from the running sums, filter, tonemap into pixels.
 cudaError_t launchDenoise(const Accum* sums, unsigned samples, int w, int h, float exposure, float4* work /*4*w*h*/,
                           uchar4* pixels, cudaStream_t stream);
+
+// Denoiser input: per pixel colour = radiance / samples, albedo / samples,
+// normalised normal sum (renderer.cu:422-428) and depth / samples (10 floats).
+cudaError_t launchAovs(const Accum* sums, const float* depthSums, unsigned samples, int count, float* aov,
+                       cudaStream_t stream);
+// Tonemap linear radiance (3 floats per pixel) into the display image;
+// uncovered pixels stay black (renderer.cu:429-435).
+cudaError_t launchPresentRadiance(const Accum* sums, const float* radiance, int count, float exposure, uchar4* pixels,
+                                  cudaStream_t stream);
 
 }  // namespace rt

@@ -26,12 +26,20 @@
 
 #include "../../include/cuda_ray_tracer.h"
 #include "rt_render.cuh"
+#include "rt_unet.cuh"
 
 using namespace rt;
 
 static_assert(sizeof(Triangle) == 116 && sizeof(CameraData) == 64 && sizeof(RenderSettings) == 28, "ABI sizes");
 static_assert(sizeof(PixelSum) == 40 && sizeof(BvhNode) == 32, "record sizes");
 static_assert(sizeof(RtxQuery) == 28 && sizeof(RtxHit) == 16, "query sizes");
+
+// A denoising network with its last error message (RtxUnet* entry points).
+struct UnetHandle {
+    rt::Unet net;
+    std::string error;
+    explicit UnetHandle(unsigned seed) : net(seed) {}
+};
 
 namespace {
 
@@ -64,6 +72,7 @@ struct Session {
     unsigned* dPassXor = nullptr;
     unsigned* dSeedHash = nullptr;
     Accum* dSum = nullptr;
+    float* dDepth = nullptr;      // running sums of first-hit distance (added AOV)
     uchar4* dPixels = nullptr;
     unsigned long long* dCounters = nullptr;
     int* dError = nullptr;
@@ -73,6 +82,7 @@ struct Session {
     WavefrontBuffers wave;
     // Host mirrors for the CPU backends (filled on first use).
     std::vector<Accum> hostSum;
+    std::vector<float> hostDepth;
     std::vector<uint4> hostWide;
     std::vector<float4> hostPacked;
     bool hostBvhReady = false;
@@ -83,6 +93,7 @@ struct Session {
     TraceTuning tuning;
     int environmentMode = 0;
     float3 environment = make_float3(0.0f, 0.0f, 0.0f);
+    UnetHandle* denoiser = nullptr;  // learned denoiser used by RtDenoise (not owned)
 };
 
 bool fail(Session* s, cudaError_t e, const char* what = nullptr) {
@@ -94,18 +105,20 @@ bool fail(Session* s, cudaError_t e, const char* what = nullptr) {
 void releaseScene(Session* s) {
     freeBvh(s->bvh);
     freeWavefront(s->wave);
-    void* owned[] = {s->dTris, s->dLights, s->dDirs, s->dPassXor, s->dSeedHash, s->dSum, s->dPixels, s->dCounters,
-                     s->dError, s->dDenoise};
+    void* owned[] = {s->dTris, s->dLights, s->dDirs, s->dPassXor, s->dSeedHash, s->dSum, s->dDepth, s->dPixels,
+                     s->dCounters, s->dError, s->dDenoise};
     for (void* p : owned)
         if (p) cudaFree(p);
     s->dTris = nullptr; s->dLights = nullptr; s->dDirs = nullptr; s->dPassXor = nullptr; s->dSeedHash = nullptr;
-    s->dSum = nullptr; s->dPixels = nullptr; s->dCounters = nullptr; s->dError = nullptr; s->dDenoise = nullptr;
+    s->dSum = nullptr; s->dDepth = nullptr; s->dPixels = nullptr; s->dCounters = nullptr; s->dError = nullptr;
+    s->dDenoise = nullptr;
     if (s->start) cudaEventDestroy(s->start);
     if (s->stop) cudaEventDestroy(s->stop);
     s->start = s->stop = nullptr;
     if (s->stream) cudaStreamDestroy(s->stream);
     s->stream = nullptr;
-    s->tris.clear(); s->lights.clear(); s->hostSum.clear(); s->hostWide.clear(); s->hostPacked.clear();
+    s->tris.clear(); s->lights.clear(); s->hostSum.clear(); s->hostDepth.clear(); s->hostWide.clear();
+    s->hostPacked.clear();
     s->tris.shrink_to_fit(); s->hostWide.shrink_to_fit(); s->hostPacked.shrink_to_fit();
     s->hostBvhReady = false;
     s->ready = false;
@@ -147,7 +160,7 @@ bool renderDevice(Session* s, const CameraData* camera, const RenderSettings* se
     if ((e = cudaMemsetAsync(s->dCounters, 0, 4 * sizeof(unsigned long long), s->stream)) != cudaSuccess) return fail(s, e);
     if ((e = cudaMemsetAsync(s->dError, 0, sizeof(int), s->stream)) != cudaSuccess) return fail(s, e);
     RenderLaunch L{deviceView(s), cam, set, s->width, s->height, s->samples, s->dPassXor, s->dSeedHash,
-                   s->dSum, s->dPixels, s->dCounters, s->dError};
+                   s->dSum, s->dDepth, s->dPixels, s->dCounters, s->dError};
     int launches = 0;
     float extendMs = 0, shadowMs = 0;
     if ((e = cudaEventRecord(s->start, s->stream)) != cudaSuccess) return fail(s, e);
@@ -204,6 +217,8 @@ bool renderHost(Session* s, const CameraData* camera, const RenderSettings* sett
         for (int d = 0; d < kSobolDims; d++) passXor[(size_t)r * kSobolDims + d] = sobolXor(dirs, s->samples + (unsigned)r, (unsigned)d);
     for (int d = 0; d < kSobolDims; d++) seedHash[d] = sobolHash(set.seed + (unsigned)d * 0x9e3779b9u);
     if (s->hostSum.size() != (size_t)s->width * s->height) s->hostSum.assign((size_t)s->width * s->height, Accum{});
+    if (s->hostDepth.size() != (size_t)s->width * s->height) s->hostDepth.assign((size_t)s->width * s->height, 0.0f);
+    float* depthSums = s->hostDepth.data();
     SceneView sc{s->tris.data(), s->hostWide.data(), s->hostPacked.data(), s->lights.data(), (int)s->lights.size(),
                  s->lightArea, s->build.wideDepth, s->environmentMode, s->environment};
     const int w = s->width, h = s->height;
@@ -222,8 +237,8 @@ bool renderHost(Session* s, const CameraData* camera, const RenderSettings* sett
 #pragma omp for schedule(dynamic, 1)
         for (int y = 0; y < h; y++)
             for (int x = 0; x < w; x++)
-                renderPixel(sc, cam, set, x, y, w, h, sample0, passXor.data(), seedHash.data(), sums, pixels, stack, 1,
-                            &overflow, p, q, sh);
+                renderPixel(sc, cam, set, x, y, w, h, sample0, passXor.data(), seedHash.data(), sums, depthSums, pixels,
+                            stack, 1, &overflow, p, q, sh);
         nPrimary += p; nSecondary += q; nShadow += sh;
     }
     *computeMs = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - begin).count();
@@ -340,6 +355,7 @@ int RtInitialize(void* p, const Triangle* triangles, int count, int width, int h
     RT_CHECK(cudaMalloc(&s->dPassXor, sizeof(unsigned) * 16 * kSobolDims));
     RT_CHECK(cudaMalloc(&s->dSeedHash, sizeof(unsigned) * kSobolDims));
     RT_CHECK(cudaMalloc(&s->dSum, sizeof(Accum) * (size_t)width * height));
+    RT_CHECK(cudaMalloc(&s->dDepth, sizeof(float) * (size_t)width * height));
     RT_CHECK(cudaMalloc(&s->dPixels, sizeof(uchar4) * (size_t)width * height));
     RT_CHECK(cudaMalloc(&s->dCounters, 4 * sizeof(unsigned long long)));
     RT_CHECK(cudaMalloc(&s->dError, 2 * sizeof(int)));
@@ -403,7 +419,18 @@ int RtDenoise(void* p, unsigned char* output, int outputBytes, float* millisecon
     if (s->lastBackend != 2) {
         if ((e = cudaMemcpy(s->dSum, s->hostSum.data(), count * sizeof(Accum), cudaMemcpyHostToDevice)) != cudaSuccess) { fail(s, e); return 0; }
     }
-    if ((e = launchDenoise(s->dSum, s->samples, s->width, s->height, s->lastSettings.exposure, s->dDenoise, s->dPixels, s->stream)) != cudaSuccess) { fail(s, e); return 0; }
+    if (s->lastBackend != 2 && s->hostDepth.size() == count) {
+        if ((e = cudaMemcpy(s->dDepth, s->hostDepth.data(), count * sizeof(float), cudaMemcpyHostToDevice)) != cudaSuccess) { fail(s, e); return 0; }
+    }
+    if (s->denoiser) {
+        // Learned denoiser: AOVs -> U-Net -> display, all on the session stream.
+        float* aov = reinterpret_cast<float*>(s->dDenoise);
+        float* radiance = aov + 10 * count;
+        std::string why;
+        if ((e = launchAovs(s->dSum, s->dDepth, s->samples, (int)count, aov, s->stream)) != cudaSuccess) { fail(s, e); return 0; }
+        if ((e = s->denoiser->net.inferDevice(aov, s->height, s->width, radiance, s->stream, why)) != cudaSuccess) { fail(s, e, why.empty() ? nullptr : why.c_str()); return 0; }
+        if ((e = launchPresentRadiance(s->dSum, radiance, (int)count, s->lastSettings.exposure, s->dPixels, s->stream)) != cudaSuccess) { fail(s, e); return 0; }
+    } else if ((e = launchDenoise(s->dSum, s->samples, s->width, s->height, s->lastSettings.exposure, s->dDenoise, s->dPixels, s->stream)) != cudaSuccess) { fail(s, e); return 0; }
     if ((e = cudaStreamSynchronize(s->stream)) != cudaSuccess) { fail(s, e); return 0; }
     if ((e = cudaMemcpy(output, s->dPixels, count * 4, cudaMemcpyDeviceToHost)) != cudaSuccess) { fail(s, e); return 0; }
     *milliseconds = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - begin).count();
@@ -559,6 +586,100 @@ int RtxSetIntegrator(void* p, int mode) {
     Session* s = static_cast<Session*>(p);
     if (!s || mode < 0 || mode > 1) return 0;
     s->integrator = mode;
+    return 1;
+}
+
+// ---- learned denoiser ----
+
+void* RtxUnetCreate(unsigned seed) {
+    UnetHandle* h = new UnetHandle(seed);
+    if (cudaGetLastError() != cudaSuccess) { delete h; return nullptr; }
+    return h;
+}
+void RtxUnetDestroy(void* p) { delete static_cast<UnetHandle*>(p); }
+long long RtxUnetParamCount(void* p) { return p ? (long long)static_cast<UnetHandle*>(p)->net.paramCount() : 0; }
+const char* RtxUnetLastError(void* p) { return p ? static_cast<UnetHandle*>(p)->error.c_str() : "null network"; }
+static int unetResult(UnetHandle* h, cudaError_t e, const std::string& why) {
+    if (e == cudaSuccess) { h->error.clear(); return 1; }
+    h->error = why.empty() ? cudaGetErrorString(e) : why;
+    return 0;
+}
+int RtxUnetGetParams(void* p, float* out) {
+    UnetHandle* h = static_cast<UnetHandle*>(p);
+    if (!h || !out) return 0;
+    return unetResult(h, h->net.getParams(out), "");
+}
+int RtxUnetSetParams(void* p, const float* in) {
+    UnetHandle* h = static_cast<UnetHandle*>(p);
+    if (!h || !in) return 0;
+    return unetResult(h, h->net.setParams(in), "");
+}
+int RtxUnetLossGrad(void* p, const float* aovs, const float* targets, int n, int h, int w, float* loss, float* grads) {
+    UnetHandle* u = static_cast<UnetHandle*>(p);
+    if (!u || !aovs || !targets || !loss || n < 1 || h < 16 || w < 16) return 0;
+    std::string why;
+    return unetResult(u, u->net.lossAndGradient(aovs, targets, n, h, w, loss, grads, why), why);
+}
+int RtxUnetTrain(void* p, const float* aovs, const float* targets, int count, int h, int w, int steps, int batch,
+                 float lr, unsigned seed, float* losses) {
+    UnetHandle* u = static_cast<UnetHandle*>(p);
+    if (!u || !aovs || !targets || count < 1 || steps < 0 || batch < 1 || !(lr > 0)) return 0;
+    std::string why;
+    return unetResult(u, u->net.train(aovs, targets, count, h, w, steps, batch, lr, seed, losses, why), why);
+}
+int RtxUnetInfer(void* p, const float* aovs, int h, int w, float* radiance) {
+    UnetHandle* u = static_cast<UnetHandle*>(p);
+    if (!u || !aovs || !radiance || h < 1 || w < 1) return 0;
+    float *dIn = nullptr, *dOut = nullptr;
+    size_t px = (size_t)w * h;
+    std::string why;
+    cudaError_t e = cudaMalloc(&dIn, sizeof(float) * px * 10);
+    if (e == cudaSuccess) e = cudaMalloc(&dOut, sizeof(float) * px * 3);
+    if (e == cudaSuccess) e = cudaMemcpy(dIn, aovs, sizeof(float) * px * 10, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = u->net.inferDevice(dIn, h, w, dOut, 0, why);
+    if (e == cudaSuccess) e = cudaMemcpy(radiance, dOut, sizeof(float) * px * 3, cudaMemcpyDeviceToHost);
+    cudaFree(dIn); cudaFree(dOut);
+    return unetResult(u, e, why);
+}
+int RtxUnetSave(void* p, const char* path, int optimizerState) {
+    UnetHandle* u = static_cast<UnetHandle*>(p);
+    if (!u || !path) return 0;
+    std::string why;
+    return unetResult(u, u->net.save(path, optimizerState != 0, why), why);
+}
+int RtxUnetLoad(void* p, const char* path) {
+    UnetHandle* u = static_cast<UnetHandle*>(p);
+    if (!u || !path) return 0;
+    std::string why;
+    return unetResult(u, u->net.load(path, why), why);
+}
+int RtxSetDenoiser(void* p, void* net) {
+    Session* s = static_cast<Session*>(p);
+    if (!s) return 0;
+    s->denoiser = static_cast<UnetHandle*>(net);
+    return 1;
+}
+int RtxReadAovs(void* p, float* out, int count) {
+    Session* s = static_cast<Session*>(p);
+    if (!s) return 0;
+    size_t need = (size_t)s->width * s->height;
+    if (!s->ready || !s->samples || !out || count < 0 || (size_t)count < need) {
+        s->error = cudaErrorInvalidValue;
+        s->hostError = "RtxReadAovs: render first, and pass room for width*height pixels";
+        return 0;
+    }
+    cudaSetDevice(s->device);
+    cudaError_t e;
+    if (!s->dDenoise && (e = cudaMalloc(&s->dDenoise, sizeof(float4) * 4 * need)) != cudaSuccess) { fail(s, e); return 0; }
+    if (s->lastBackend != 2) {
+        if ((e = cudaMemcpy(s->dSum, s->hostSum.data(), need * sizeof(Accum), cudaMemcpyHostToDevice)) != cudaSuccess) { fail(s, e); return 0; }
+        if (s->hostDepth.size() == need &&
+            (e = cudaMemcpy(s->dDepth, s->hostDepth.data(), need * sizeof(float), cudaMemcpyHostToDevice)) != cudaSuccess) { fail(s, e); return 0; }
+    }
+    float* aov = reinterpret_cast<float*>(s->dDenoise);
+    if ((e = launchAovs(s->dSum, s->dDepth, s->samples, (int)need, aov, s->stream)) != cudaSuccess) { fail(s, e); return 0; }
+    if ((e = cudaStreamSynchronize(s->stream)) != cudaSuccess) { fail(s, e); return 0; }
+    if ((e = cudaMemcpy(out, aov, need * 10 * sizeof(float), cudaMemcpyDeviceToHost)) != cudaSuccess) { fail(s, e); return 0; }
     return 1;
 }
 

@@ -83,13 +83,17 @@ assert (TRIANGLE_DTYPE.itemsize, PIXELSUM_DTYPE.itemsize, NODE_DTYPE.itemsize) =
 
 ROOT = Path(__file__).resolve().parent
 LIBRARY = ROOT / 'libCudaRayTracer.so'
+# Trained parameters of the learned denoiser (train_denoiser.py writes them).
+DENOISER_WEIGHTS = ROOT / 'weights' / 'denoiser_unet.bin'
 
 # Every symbol the header declares (include/cuda_ray_tracer.h).
 EXPORTS = ('RtCreate', 'RtDestroy', 'RtShutdown', 'RtInitialize', 'RtRender', 'RtDenoise', 'RtReset',
            'RtAccumulationVersion', 'RtSampleCount', 'RtEmbreeBuildMilliseconds', 'RtCpuThreadCount',
            'RtBvhInfo', 'RtLastError', 'RtxQueryRays', 'RtxSobolSamples', 'RtxExportBvh', 'RtxBvhStatsGet',
            'RtxReadAccumulation', 'RtxRenderStatsGet', 'RtxRenderDevice', 'RtxSetIntegrator', 'RtxSetTuning',
-           'RtxQueryRaysStatic', 'RtxSetEnvironment')
+           'RtxQueryRaysStatic', 'RtxSetEnvironment', 'RtxUnetCreate', 'RtxUnetDestroy', 'RtxUnetParamCount',
+           'RtxUnetLastError', 'RtxUnetGetParams', 'RtxUnetSetParams', 'RtxUnetLossGrad', 'RtxUnetTrain',
+           'RtxUnetInfer', 'RtxUnetSave', 'RtxUnetLoad', 'RtxSetDenoiser', 'RtxReadAovs')
 
 
 def load_library(path=None):
@@ -126,6 +130,22 @@ def load_library(path=None):
     lib.RtxSetTuning.argtypes = [vp, c.c_int, c.c_int]
     lib.RtxQueryRaysStatic.argtypes = [vp, c.c_void_p, c.c_int, c.c_int, c.c_void_p]
     lib.RtxSetEnvironment.argtypes = [vp, c.c_int, c.c_float, c.c_float, c.c_float]
+    lib.RtxUnetCreate.restype = vp
+    lib.RtxUnetCreate.argtypes = [c.c_uint]
+    lib.RtxUnetDestroy.argtypes = [vp]
+    lib.RtxUnetParamCount.argtypes = [vp]
+    lib.RtxUnetParamCount.restype = c.c_longlong
+    lib.RtxUnetLastError.argtypes = [vp]
+    lib.RtxUnetLastError.restype = c.c_char_p
+    lib.RtxUnetGetParams.argtypes = lib.RtxUnetSetParams.argtypes = [vp, c.c_void_p]
+    lib.RtxUnetLossGrad.argtypes = [vp, c.c_void_p, c.c_void_p, c.c_int, c.c_int, c.c_int, c.c_void_p, c.c_void_p]
+    lib.RtxUnetTrain.argtypes = [vp, c.c_void_p, c.c_void_p, c.c_int, c.c_int, c.c_int, c.c_int, c.c_int, c.c_float,
+                                 c.c_uint, c.c_void_p]
+    lib.RtxUnetInfer.argtypes = [vp, c.c_void_p, c.c_int, c.c_int, c.c_void_p]
+    lib.RtxUnetSave.argtypes = [vp, c.c_char_p, c.c_int]
+    lib.RtxUnetLoad.argtypes = [vp, c.c_char_p]
+    lib.RtxSetDenoiser.argtypes = [vp, vp]
+    lib.RtxReadAovs.argtypes = [vp, c.c_void_p, c.c_int]
     return lib
 
 
@@ -258,6 +278,15 @@ class Session:
             r, g, b = (constant,) * 3 if isinstance(constant, (int, float)) else constant
             self.check(self.lib.RtxSetEnvironment(self.handle, 1, r, g, b))
 
+    def aovs(self):
+        """Denoiser inputs of the current accumulation, shape (height, width, 10)."""
+        out = np.zeros((self.height, self.width, 10), np.float32)
+        self.check(self.lib.RtxReadAovs(self.handle, out.ctypes.data, self.width * self.height))
+        return out
+
+    def set_denoiser(self, net):
+        self.check(self.lib.RtxSetDenoiser(self.handle, net.handle if net is not None else None))
+
     def sample_count(self):
         return self.lib.RtSampleCount(self.handle)
 
@@ -275,3 +304,74 @@ def sobol_samples(lib, pixel, sample, seed, ndim):
                                out.ctypes.data):
         raise NativeError('RtxSobolSamples failed')
     return out
+
+
+class Unet:
+    """The learned denoiser (RtxUnet* entry points)."""
+
+    def __init__(self, lib=None, seed=1):
+        self.lib = lib or load_library()
+        self.handle = self.lib.RtxUnetCreate(seed)
+        if not self.handle:
+            raise NativeError('RtxUnetCreate failed')
+
+    def close(self):
+        if self.handle:
+            self.lib.RtxUnetDestroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def check(self, ok):
+        if not ok:
+            raise NativeError(self.lib.RtxUnetLastError(self.handle).decode())
+
+    @property
+    def param_count(self):
+        return self.lib.RtxUnetParamCount(self.handle)
+
+    def params(self):
+        out = np.zeros(self.param_count, np.float32)
+        self.check(self.lib.RtxUnetGetParams(self.handle, out.ctypes.data))
+        return out
+
+    def set_params(self, params):
+        p = np.ascontiguousarray(params, np.float32)
+        assert p.size == self.param_count
+        self.check(self.lib.RtxUnetSetParams(self.handle, p.ctypes.data))
+
+    def loss_grad(self, aovs, targets):
+        a = np.ascontiguousarray(aovs, np.float32)
+        t = np.ascontiguousarray(targets, np.float32)
+        n, h, w = a.shape[:3]
+        loss = np.zeros(1, np.float32)
+        grads = np.zeros(self.param_count, np.float32)
+        self.check(self.lib.RtxUnetLossGrad(self.handle, a.ctypes.data, t.ctypes.data, n, h, w, loss.ctypes.data,
+                                            grads.ctypes.data))
+        return float(loss[0]), grads
+
+    def train(self, aovs, targets, steps, batch=16, lr=1e-3, seed=0):
+        a = np.ascontiguousarray(aovs, np.float32)
+        t = np.ascontiguousarray(targets, np.float32)
+        n, h, w = a.shape[:3]
+        losses = np.zeros(max(steps, 1), np.float32)
+        self.check(self.lib.RtxUnetTrain(self.handle, a.ctypes.data, t.ctypes.data, n, h, w, steps, batch, lr, seed,
+                                         losses.ctypes.data))
+        return losses[:steps]
+
+    def infer(self, aovs):
+        a = np.ascontiguousarray(aovs, np.float32)
+        h, w = a.shape[:2]
+        out = np.zeros((h, w, 3), np.float32)
+        self.check(self.lib.RtxUnetInfer(self.handle, a.ctypes.data, h, w, out.ctypes.data))
+        return out
+
+    def save(self, path, optimizer_state=False):
+        self.check(self.lib.RtxUnetSave(self.handle, str(path).encode(), int(optimizer_state)))
+
+    def load(self, path):
+        self.check(self.lib.RtxUnetLoad(self.handle, str(path).encode()))

@@ -218,6 +218,73 @@ def end_to_end_room(seed=17, width=1920, height=1080, bounces=5, subdivisions=15
     return tris, cam, settings, width, height
 
 
+def cuboid(center, size, yaw, **kwargs):
+    """Closed box of 12 triangles with outward windings, rotated by yaw about +y."""
+    cx, cy, cz = center
+    sx, sy, sz = (0.5 * v for v in size)
+    c, s = math.cos(yaw), math.sin(yaw)
+    ex, ez = np.array([c, 0, -s]) * sx, np.array([s, 0, c]) * sz
+    ey = np.array([0.0, sy, 0.0])
+    o = np.array([cx, cy, cz], np.float64)
+    faces = []
+    for axis, pair in ((ex, (ey, ez)), (ey, (ez, ex)), (ez, (ex, ey))):
+        for sign in (1, -1):
+            u, v = (2 * e for e in (pair if sign > 0 else pair[::-1]))
+            p = o + sign * axis - 0.5 * u - 0.5 * v
+            faces.append(box_quad(p, u, v, **kwargs))
+    return np.concatenate(faces)
+
+
+def random_room(seed, width=256, height=256):
+    """Training scene for the learned denoiser (not a benchmark workload):
+    an open room of random size and wall colours lit by a ceiling quad
+    light (random size, height and power, half the time under a diffuse
+    shade, sometimes with a second small light), two to seven objects
+    (faceted or smooth displaced spheres, boxes; a quarter of them glossy),
+    a random camera inside the room, depth 3 to 6. Returns the triangles,
+    camera, settings and the environment (None: the sky gradient, else a
+    constant radiance)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    hx, top, hz = rng.uniform(1.5, 4.0), rng.uniform(2.2, 4.5), rng.uniform(1.5, 4.0)
+    colors = rng.uniform(0.08, 0.9, (5, 3))
+    light_half = rng.uniform(0.15, 0.8)
+    light_y = top - rng.uniform(0.02, 0.5)
+    emission = float(rng.uniform(6.0, 60.0))
+    parts = [open_box((-hx, 0.0, -hz), (hx, top, hz), colors, light_half, light_y, emission)]
+    if rng.random() < 0.5:
+        h = light_half * rng.uniform(1.2, 2.0)
+        parts.append(box_quad((-h, light_y - rng.uniform(0.03, 0.3), -h), (2 * h, 0, 0), (0, 0, 2 * h),
+                              color=rng.uniform(0.3, 0.9, 3), mesh=20))
+    if rng.random() < 0.3:
+        q = rng.uniform(0.05, 0.25)
+        lx, lz = rng.uniform(-hx + q, hx - q), rng.uniform(-hz + q, hz - q)
+        parts.append(box_quad((lx - q, top - 0.01, lz - q), (2 * q, 0, 0), (0, 0, 2 * q), emission=emission,
+                              mesh=21))
+    for k in range(int(rng.integers(2, 8))):
+        size = rng.uniform(0.2, 0.35 * min(hx, hz, top))
+        center = (rng.uniform(-hx + size, hx - size), rng.uniform(size, top - size), rng.uniform(-hz + size, hz - size))
+        material = dict(color=rng.uniform(0.05, 0.95, 3), mesh=30 + k)
+        if rng.random() < 0.25:
+            material.update(smoothness=float(rng.uniform(0.6, 1.0)), specular_probability=float(rng.uniform(0.1, 0.6)),
+                            specular_color=rng.uniform(0.6, 1.0, 3))
+        if rng.random() < 0.6:
+            v0, v1, v2, normals = geodesic_sphere(int(rng.integers(3, 40)), size, center, rng.uniform(0, 0.1), rng,
+                                                  smooth=bool(rng.random() < 0.5))
+            parts.append(records(v0, v1, v2, normals=normals if rng.random() < 0.7 else None, **material))
+        else:
+            dims = rng.uniform(0.5, 1.8, 3) * size
+            center = (center[0], 0.5 * dims[1] if rng.random() < 0.6 else center[1], center[2])
+            parts.append(cuboid(center, dims, rng.uniform(0, math.pi), **material))
+    tris = np.concatenate(parts)
+    eye = (rng.uniform(-0.7, 0.7) * hx, rng.uniform(0.4, top - 0.3), -hz + rng.uniform(0.1, 0.6) * hz)
+    target = (rng.uniform(-0.6, 0.6) * hx, rng.uniform(0.2, 0.8) * top, rng.uniform(0.0, 0.9) * hz)
+    cam = camera(eye, target, math.tan(math.radians(rng.uniform(22.0, 45.0))), width / height)
+    settings = Settings(int(rng.integers(3, 7)), float(rng.uniform(0.7, 2.0)), 0.0, 1.0,
+                        float(rng.uniform(0.0, 1.0)), 42, 1)
+    environment = None if rng.random() < 0.4 else float(rng.uniform(0.0, 0.3))
+    return tris, cam, settings, environment
+
+
 # ---- check geometry, after the categories of Tools/verify_bvh.cu:115-139 ----
 
 def _tri(a, b, c, one_sided=0):

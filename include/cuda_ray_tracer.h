@@ -183,6 +183,37 @@ int RtxSetTuning(void* session, int key, int value);
  * ignored. A change resets the accumulation. No counterpart in the
  * reference's exported ABI. */
 int RtxSetEnvironment(void* session, int mode, float r, float g, float b);
+/* Learned denoiser (no counterpart in the reference: it replaces the OptiX
+ * denoiser of Native/denoiser.cuh). A 5-level convolutional U-Net (widths
+ * 32-48-64-96-128, about 1.01M parameters) on BF16 tensor cores with FP32
+ * accumulation. Input per pixel: the 10 floats RtxReadAovs returns; output:
+ * linear radiance RGB. Returns 1 on success, 0 on failure (RtxUnetLastError).
+ *   RtxUnetCreate     new network, He-normal initialisation from seed
+ *   RtxUnetGetParams / RtxUnetSetParams  FP32 parameters, RtxUnetParamCount floats
+ *   RtxUnetLossGrad   one forward/backward over n crops (h, w multiples of 16):
+ *                     L1 loss on log(1 + radiance) and its gradient
+ *   RtxUnetTrain      Adam steps over random batches (with flips) of a data set
+ *   RtxUnetInfer      host-to-host inference for any h, w
+ *   RtxUnetSave / RtxUnetLoad  checkpoint: parameters, and the Adam state
+ *                     when optimizerState is non-zero
+ *   RtxSetDenoiser    RtDenoise runs this network (NULL: guided filter) */
+void* RtxUnetCreate(unsigned seed);
+void RtxUnetDestroy(void* net);
+long long RtxUnetParamCount(void* net);
+const char* RtxUnetLastError(void* net);
+int RtxUnetGetParams(void* net, float* params);
+int RtxUnetSetParams(void* net, const float* params);
+int RtxUnetLossGrad(void* net, const float* aovs, const float* targets, int n, int h, int w, float* loss, float* grads);
+int RtxUnetTrain(void* net, const float* aovs, const float* targets, int count, int h, int w, int steps, int batch,
+                 float learningRate, unsigned seed, float* losses);
+int RtxUnetInfer(void* net, const float* aovs, int h, int w, float* radiance);
+int RtxUnetSave(void* net, const char* path, int optimizerState);
+int RtxUnetLoad(void* net, const char* path);
+int RtxSetDenoiser(void* session, void* net);
+/* Denoiser inputs of the current accumulation, 10 floats per pixel: colour
+ * (radiance / samples), albedo / samples, normalised normal sum, first-hit
+ * distance / samples (the distance is an added AOV). */
+int RtxReadAovs(void* session, float* aovs, int count);
 /* RtxQueryRays without any device allocation; no counterpart in the reference.
  * For callers that must not allocate device memory during the call (work
  * running beside a CUDA graph capture, latency-critical loops where

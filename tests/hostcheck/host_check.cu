@@ -92,10 +92,12 @@ int hc_render(const SceneTri* tris, const Light* lights, int lightCount, float l
     uint2 stack[kStackCapacity];
     int overflow = 0;
     unsigned p = 0, q = 0, s = 0;
+    static std::vector<float> depth;
+    if (sample0 == 0 || depth.size() != (size_t)w * h) depth.assign((size_t)w * h, 0.0f);
     for (int y = 0; y < h; y++)
         for (int x = 0; x < w; x++)
-            renderPixel(sc, *cam, *set, x, y, w, h, sample0, passXor.data(), seedHash.data(), sums, pixels, stack, 1,
-                        &overflow, p, q, s);
+            renderPixel(sc, *cam, *set, x, y, w, h, sample0, passXor.data(), seedHash.data(), sums, depth.data(),
+                        pixels, stack, 1, &overflow, p, q, s);
     counts[0] = p; counts[1] = q; counts[2] = s;
     return overflow == 0;
 }
