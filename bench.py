@@ -61,6 +61,9 @@ def parse():
                    help='also measure time to 35 dB PSNR vs a 4096-spp render on the 2M-triangle scene')
     p.add_argument('--quality-resolution', default=None, help='WxH override of the quality scene')
     p.add_argument('--oracle-spp', type=int, default=4096)
+    p.add_argument('--batch', action='store_true',
+                   help='also measure batched multi-scene tracing (8 scenes, 64 views) against per-view launches')
+    p.add_argument('--batch-frames', type=int, default=3)
     return p.parse_args()
 
 
@@ -276,7 +279,7 @@ def quality_run(lib, args, target_db=35.0):
     uses a different sampler seed than the arms."""
     import numpy as np
     import scenes
-    from native_api import Session, Settings
+    from native_api import DENOISER_WEIGHTS, Session, Settings, Unet
     kwargs = {}
     if args.quality_resolution:
         kwargs['width'], kwargs['height'] = (int(v) for v in args.quality_resolution.lower().split('x'))
@@ -312,31 +315,47 @@ def quality_run(lib, args, target_db=35.0):
                 reached = {'spp': spp, 'device_ms': device_ms, 'psnr_db': db, 'rmse_8bit': rmse}
                 break
         plain_wall_ms = (time.perf_counter() - wall0) * 1e3
-        # Denoised: 8 spp, then more paths per pixel until the filtered image
-        # reaches the target (each budget rendered from scratch).
-        trials = []
-        denoised = None
-        for budget in (8, 16, 32, 64, 128, 256):
-            s.lib.RtReset(s.handle)
-            render_ms, done = 0.0, 0
-            while done < budget:
-                st.raysPerPixel = min(16, budget - done)
-                img, ms = s.render(cam, st)
-                render_ms += ms
-                done += st.raysPerPixel
-            raw_db, _ = psnr8(img, oracle)
-            den, denoise_ms = s.denoise()
-            den_db, den_rmse = psnr8(den, oracle)
-            trial = {'spp': budget, 'render_ms': render_ms, 'denoise_ms': denoise_ms, 'psnr_db': den_db,
-                     'rmse_8bit': den_rmse, 'raw_psnr_db': raw_db}
-            trials.append(trial)
-            if den_db >= target_db:
-                denoised = dict(trial, reaches_target=True)
-                break
-        if denoised is None:
-            denoised = dict(trials[-1], reaches_target=False)
-        denoised['denoiser'] = 'guided a-trous wavelet filter (RtDenoise)'
-        denoised['at_8spp'] = trials[0]
+        def denoised_arm(name):
+            """8 spp, then more paths per pixel until the denoised image
+            reaches the target (each budget rendered from scratch; a budget
+            above 16 spp is several passes of 16 with one setting)."""
+            trials, arm = [], None
+            for budget in (8, 16, 32, 64, 128, 256):
+                per = min(16, budget)
+                st.raysPerPixel = per
+                s.lib.RtReset(s.handle)
+                render_ms = 0.0
+                while s.sample_count() < budget:
+                    img, ms = s.render(cam, st)
+                    render_ms += ms
+                raw_db, _ = psnr8(img, oracle)
+                den, denoise_ms = s.denoise()
+                den_db, den_rmse = psnr8(den, oracle)
+                trial = {'spp': budget, 'render_ms': render_ms, 'denoise_ms': denoise_ms, 'psnr_db': den_db,
+                         'rmse_8bit': den_rmse, 'raw_psnr_db': raw_db}
+                trials.append(trial)
+                if den_db >= target_db:
+                    arm = dict(trial, reaches_target=True)
+                    break
+            arm = arm or dict(trials[-1], reaches_target=False)
+            arm['denoiser'] = name
+            arm['at_8spp'] = trials[0]
+            return arm
+
+        denoised = denoised_arm('guided a-trous wavelet filter (RtDenoise without a network)')
+        learned = None
+        if DENOISER_WEIGHTS.exists():
+            net = Unet(lib)
+            try:
+                net.load(DENOISER_WEIGHTS)
+                s.set_denoiser(net)
+                # The first inference at this size allocates the activations.
+                s.denoise()
+                learned = denoised_arm(f'learned U-Net ({net.param_count:,} parameters, BF16 tensor cores; '
+                                       f'RtDenoise with RtxSetDenoiser)')
+            finally:
+                s.set_denoiser(None)
+                net.close()
         result = {
             'workload': 'end_to_end_room', 'triangles': len(tris), 'width': w, 'height': h,
             'max_depth': st.maxBounces, 'environment': 0.1, 'exposure': st.exposure, 'target_db': target_db,
@@ -344,14 +363,90 @@ def quality_run(lib, args, target_db=35.0):
             'plain': dict(reached or {'spp': spp, 'device_ms': device_ms, 'psnr_db': curve[-1][2] if curve else None},
                           reaches_target=reached is not None, wall_ms=plain_wall_ms),
             'denoised': denoised,
+            'learned': learned,
             'psnr_metric': '20 log10(255 / RMSE) over 8-bit RGB display values',
             'curve_every_4spp': curve[:: max(1, len(curve) // 32)],
         }
         if reached and denoised['reaches_target']:
             result['speedup_denoised_vs_plain'] = reached['device_ms'] / (denoised['render_ms'] + denoised['denoise_ms'])
+        if reached and learned and learned['reaches_target']:
+            result['speedup_learned_vs_plain'] = reached['device_ms'] / (learned['render_ms'] + learned['denoise_ms'])
         return result
     finally:
         s.close()
+
+
+def batch_run(lib, args):
+    """Batched multi-scene tracing: eight scenes of 10K-2M triangles (log-
+    uniform), 64 views of 256^2, 512^2 or 1024^2, 8 paths per pixel, depth 4.
+    The batch (one wave of paths across all views per traversal launch,
+    frames replayed from a CUDA graph, launch shape and BVH width from the
+    autotuner) against the same views rendered one by one through RtRender's
+    device path (one session per scene and resolution). Rays: closest-hit
+    plus shadow queries counted on the device."""
+    import scenes
+    from native_api import Batch, Session
+    t0 = time.perf_counter()
+    scene_list, views, st = scenes.batch_workload()
+    gen_s = time.perf_counter() - t0
+    b = Batch(lib)
+    try:
+        for tris in scene_list:
+            b.add_scene(tris)
+        for k, cam, w, h in views:
+            b.add_view(k, cam, w, h)
+        built = b.stats()
+        t1 = time.perf_counter()
+        tried = b.autotune(st)
+        tune_s = time.perf_counter() - t1
+
+        def frames(graph):
+            b.set_tuning(graph=graph)
+            b.reset()
+            b.render(st)  # warm-up (and graph capture)
+            ms = []
+            rays = 0
+            for _ in range(args.batch_frames):
+                b.reset()  # samples 0..7 again: the paths (and rays) of the per-view renders
+                ms.append(b.render(st))
+                stats = b.stats()
+                rays = stats['primaryRays'] + stats['secondaryRays'] + stats['shadowRays']
+            best = min(ms)
+            return {'frame_ms': best, 'mrays_per_s': rays / best / 1e3, 'rays_per_frame': rays,
+                    'kernel_launches': stats['kernelLaunches']}
+        graph = frames(1)
+        launches = frames(0)
+        tuned = b.stats()
+    finally:
+        b.close()
+    # Per-view launches: every view alone through the single-view device path.
+    sessions = {}
+    per_view_ms, per_view_rays = 0.0, 0
+    try:
+        for k, cam, w, h in views:
+            s = sessions.get((k, w, h))
+            if s is None:
+                s = sessions[(k, w, h)] = Session(lib).initialize(scene_list[k], w, h)
+                s.render_device(cam, st)  # warm-up of this session
+            per_view_ms += s.render_device(cam, st)
+            r = s.render_stats()
+            per_view_rays += r['primaryRays'] + r['secondaryRays'] + r['shadowRays']
+    finally:
+        for s in sessions.values():
+            s.close()
+    per_view = {'frame_ms': per_view_ms, 'mrays_per_s': per_view_rays / per_view_ms / 1e3,
+                'rays_per_frame': per_view_rays}
+    return {
+        'workload': 'batch_workload (8 scenes, 64 views)', 'scenes': len(scene_list),
+        'triangles': [len(t) for t in scene_list], 'views': len(views), 'pixels': built['pixels'],
+        'spp_per_frame': st.raysPerPixel, 'max_depth': st.maxBounces,
+        'build_ms': built['buildMs'], 'build_mtris_per_s': built['triangles'] / built['buildMs'] / 1e3,
+        'generate_s': gen_s, 'autotune_s': tune_s, 'autotune': tried,
+        'tuned': {k: tuned[k] for k in ('block', 'capacity', 'refill', 'width')},
+        'batched_graph': graph, 'batched_launches': launches, 'per_view_launches': per_view,
+        'speedup_vs_per_view': per_view['frame_ms'] / graph['frame_ms'],
+        'same_rays': graph['rays_per_frame'] == per_view_rays,
+    }
 
 
 def l2_flusher():
@@ -521,6 +616,7 @@ def run_ours(args, rank, local_rank, world):
                       'wide_nodes': bvh['wideNodes'], 'sah_cost': bvh['sahCost']},
             'reference_cuda': ref_cuda,
             'time_to_35db': quality_run(lib, args) if (args.quality and world == 1) else None,
+            'batch': batch_run(lib, args) if (args.batch and world == 1) else None,
         }
     s.close()
     dist.close()

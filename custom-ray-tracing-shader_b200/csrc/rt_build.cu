@@ -396,11 +396,11 @@ __global__ void renumberKernel(const BinNode* nodes, int count, const int* newIn
 __global__ void collapseKernel(const BinNode* bn, const int* order, const float4* plo, const float4* phi,
                                const SceneTri* tris, const Job* jobs, int nJobs, Job* nextJobs, WideNode* wide,
                                float4* packed, int* counters, int wideCapacity, int jobCapacity, int triCapacity,
-                               int group) {
+                               int group, int width) {
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= nJobs) return;
     collapseJob(jobs[j], bn, order, plo, phi, tris, nextJobs, wide, packed, counters, wideCapacity, jobCapacity,
-                triCapacity, group);
+                triCapacity, group, width);
 }
 
 inline int blocksFor(long long n, int block) { return (int)((n + block - 1) / block); }
@@ -418,7 +418,8 @@ void freeBvh(BuiltBvh& b) {
 }
 
 cudaError_t buildBvh(const SceneTri* tris, int n, cudaStream_t stream, BuiltBvh& out, BuildResult& result,
-                     const char** failure, int leafGroup) {
+                     const char** failure, int leafGroup, int width) {
+    if (width != 4 && width != 8) { *failure = "BVH width must be 4 or 8"; return cudaErrorInvalidValue; }
     *failure = nullptr;
     cudaError_t err = cudaSuccess;
     const int nodeCapacity = 2 * n + 2;
@@ -526,7 +527,7 @@ cudaError_t buildBvh(const SceneTri* tris, int n, cudaStream_t stream, BuiltBvh&
                                                                     jobs, nJobs, jobsB,
                                                                     reinterpret_cast<WideNode*>(out.wideNodes),
                                                                     out.packedTris, counters, wideCapacity, jobCapacity, n,
-                                                                    leafGroup);
+                                                                    leafGroup, width);
             RT_TRY(cudaGetLastError());
             RT_TRY(cudaMemcpyAsync(hostCounters, counters, 8 * sizeof(int), cudaMemcpyDeviceToHost, stream));
             RT_TRY(cudaStreamSynchronize(stream));

@@ -34,9 +34,10 @@ struct BuiltBvh {
 // Builds the BVH for n device triangles on `stream`. Returns a CUDA error code
 // (cudaSuccess on success) and fills `out`/`result`. `scratchBytes` is the
 // peak temporary memory used, for reporting. Timing uses events on `stream`.
-// leafGroup (1..3): most triangles under one wide-node slot.
+// leafGroup (1..3): most triangles under one wide-node slot. width (4 or 8):
+// most children per wide node.
 cudaError_t buildBvh(const SceneTri* tris, int n, cudaStream_t stream, BuiltBvh& out, BuildResult& result,
-                     const char** failure, int leafGroup = 3);
+                     const char** failure, int leafGroup = 3, int width = 8);
 void freeBvh(BuiltBvh& bvh);
 
 }  // namespace rt

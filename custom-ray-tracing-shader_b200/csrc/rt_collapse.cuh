@@ -43,20 +43,21 @@ struct Job { int kind; int node; int first; int count; int wide; };  // kind 0 b
 struct Kid { int kind; int node; int first; int count; float lo[3], hi[3]; };  // kind 0/1 wide child, 2 triangle group
 
 // Slots a binary child needs: one for an interior node, ceil(k / group) for a
-// leaf of k <= 8 * group triangles held inline, one for a larger leaf.
-RT_HD int slotsOf(const BinNode& n, int group) {
+// leaf of k <= width * group triangles held inline, one for a larger leaf.
+RT_HD int slotsOf(const BinNode& n, int group, int width) {
     if (n.count == 0) return 1;
-    return n.count <= 8 * group ? (n.count + group - 1) / group : 1;
+    return n.count <= width * group ? (n.count + group - 1) / group : 1;
 }
 
 // Builds wide node J.wide for one job: chooses up to eight children, assigns
 // slots, quantises child boxes, packs leaf triangles and emits jobs for the
 // interior children. counters: [0] wide nodes, [1] packed triangles,
 // [2] next-level jobs, [3] error code. Host and device (atomics through
-// portableAdd), so the collapse can be checked on the CPU.
+// portableAdd), so the collapse can be checked on the CPU. width (4 or 8):
+// most children per node; the node format keeps eight slots either way.
 RT_HD void collapseJob(Job J, const BinNode* bn, const int* order, const float4* plo, const float4* phi,
                        const SceneTri* tris, Job* nextJobs, WideNode* wide, float4* packed, int* counters,
-                       int wideCapacity, int jobCapacity, int triCapacity, int group) {
+                       int wideCapacity, int jobCapacity, int triCapacity, int group, int width = 8) {
     if (J.kind == 0 && bn[J.node].count > 0) { J.kind = 1; J.first = bn[J.node].first; J.count = bn[J.node].count; }
     Kid kids[8];
     int nk = 0;
@@ -66,13 +67,13 @@ RT_HD void collapseJob(Job J, const BinNode* bn, const int* order, const float4*
         cand[0] = bn[J.node].first; cand[1] = cand[0] + 1;
         for (;;) {
             int total = 0;
-            for (int i = 0; i < nc; i++) total += slotsOf(bn[cand[i]], group);
+            for (int i = 0; i < nc; i++) total += slotsOf(bn[cand[i]], group, width);
             int best = -1; float bestArea = -1.0f;
             for (int i = 0; i < nc; i++) {
                 const BinNode& c = bn[cand[i]];
-                if (c.count != 0 || nc >= 8) continue;
-                int after = total - 1 + slotsOf(bn[c.first], group) + slotsOf(bn[c.first + 1], group);
-                if (after > 8) continue;
+                if (c.count != 0 || nc >= width) continue;
+                int after = total - 1 + slotsOf(bn[c.first], group, width) + slotsOf(bn[c.first + 1], group, width);
+                if (after > width) continue;
                 float lo[3] = {c.low.x, c.low.y, c.low.z}, hi[3] = {c.high.x, c.high.y, c.high.z};
                 float a = collapseHalfArea(lo, hi);
                 if (a > bestArea) { bestArea = a; best = i; }
@@ -85,8 +86,8 @@ RT_HD void collapseJob(Job J, const BinNode* bn, const int* order, const float4*
         // Leaves that do not fit inline become wide children of their own.
         for (;;) {
             int total = 0;
-            for (int i = 0; i < nc; i++) total += asNode[i] ? 1 : slotsOf(bn[cand[i]], group);
-            if (total <= 8) break;
+            for (int i = 0; i < nc; i++) total += asNode[i] ? 1 : slotsOf(bn[cand[i]], group, width);
+            if (total <= width) break;
             int pick = -1, most = 0;
             for (int i = 0; i < nc; i++) {
                 const BinNode& c = bn[cand[i]];
@@ -95,23 +96,23 @@ RT_HD void collapseJob(Job J, const BinNode* bn, const int* order, const float4*
             if (pick < 0) break;
             asNode[pick] = true;
         }
-        for (int i = 0; i < nc && nk < 8; i++) {
+        for (int i = 0; i < nc && nk < width; i++) {
             const BinNode& c = bn[cand[i]];
             if (c.count == 0) {
                 kids[nk++] = Kid{0, cand[i], 0, 0, {c.low.x, c.low.y, c.low.z}, {c.high.x, c.high.y, c.high.z}};
-            } else if (asNode[i] || c.count > 8 * group) {
+            } else if (asNode[i] || c.count > width * group) {
                 kids[nk++] = Kid{1, -1, c.first, c.count, {c.low.x, c.low.y, c.low.z}, {c.high.x, c.high.y, c.high.z}};
             } else {
-                for (int g = 0; g < c.count && nk < 8; g += group)
+                for (int g = 0; g < c.count && nk < width; g += group)
                     kids[nk++] = Kid{2, -1, c.first + g, imin(group, c.count - g), {0, 0, 0}, {0, 0, 0}};
             }
         }
-    } else if (J.count <= 8 * group) {
-        for (int g = 0; g < J.count && nk < 8; g += group)
+    } else if (J.count <= width * group) {
+        for (int g = 0; g < J.count && nk < width; g += group)
             kids[nk++] = Kid{2, -1, J.first + g, imin(group, J.count - g), {0, 0, 0}, {0, 0, 0}};
     } else {
-        int chunk = (J.count + 7) / 8;
-        for (int g = 0; g < J.count && nk < 8; g += chunk) {
+        int chunk = (J.count + width - 1) / width;
+        for (int g = 0; g < J.count && nk < width; g += chunk) {
             int c = imin(chunk, J.count - g);
             kids[nk++] = Kid{c <= group ? 2 : 1, -1, J.first + g, c, {0, 0, 0}, {0, 0, 0}};
         }

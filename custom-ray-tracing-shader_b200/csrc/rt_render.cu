@@ -89,7 +89,7 @@ struct ExtendIO {
     const int* queue;
     const float4 *pathA, *pathB;
     float4* hits;
-    __device__ void load(int k, float3& o, float3& d, float& limit) const {
+    __device__ void load(int k, float3& o, float3& d, float& limit, unsigned&) const {
         int p = queue[k];
         float4 a = pathA[p], b = pathB[p];
         o = v3(a.x, a.y, a.z); d = v3(b.x, b.y, b.z); limit = 1e30f;
@@ -168,7 +168,7 @@ __global__ void shadeKernel(WaveArgs A, WavefrontBuffers B, int q, int bounce) {
 struct ShadowIO {
     const float4 *ray, *dir, *contrib;
     float4* radiance;
-    __device__ void load(int k, float3& o, float3& d, float& limit) const {
+    __device__ void load(int k, float3& o, float3& d, float& limit, unsigned&) const {
         float4 a = ray[k], b = dir[k];
         o = v3(a.x, a.y, a.z); d = v3(b.x, b.y, b.z); limit = a.w;
     }
@@ -212,7 +212,7 @@ __global__ void accumulateKernel(WaveArgs A, WavefrontBuffers B) {
 struct QueryIO {
     const float4* q;
     float4* out;
-    __device__ void load(int k, float3& o, float3& d, float& limit) const {
+    __device__ void load(int k, float3& o, float3& d, float& limit, unsigned&) const {
         float4 a = q[2 * k], b = q[2 * k + 1];
         o = v3(a.x, a.y, a.z); d = v3(a.w, b.x, b.y); limit = b.z;
     }

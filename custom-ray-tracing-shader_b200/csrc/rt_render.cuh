@@ -1,8 +1,13 @@
 // Launch interface of the render, query, sampler and denoise kernels.
 #pragma once
+#include <string>
+
 #include "rt_integrator.cuh"
 
 namespace rt {
+
+// cuRAND's Sobol direction numbers (host copy), or null with a message.
+const unsigned* hostSobolDirections(std::string& error);
 
 struct RenderLaunch {
     SceneView scene;

@@ -41,14 +41,18 @@ struct UnetHandle {
     explicit UnetHandle(unsigned seed) : net(seed) {}
 };
 
-namespace {
-
+namespace rt {
+// The sampler's direction numbers: cuRAND's JOEKUO6 table, fetched at run
+// time like the reference (sampling.cuh:10), 260 dimensions x 32 words.
 const unsigned* hostSobolDirections(std::string& error) {
     static curandDirectionVectors32_t* table = nullptr;
     static curandStatus_t status = curandGetDirectionVectors32(&table, CURAND_DIRECTION_VECTORS_32_JOEKUO6);
     if (status != CURAND_STATUS_SUCCESS || !table) { error = "Could not load cuRAND Sobol direction vectors"; return nullptr; }
     return &table[0][0];
 }
+}  // namespace rt
+
+namespace {
 
 struct Session {
     std::string hostError;

@@ -28,10 +28,12 @@ struct LaneRay {
     int top;
 };
 
-__device__ __forceinline__ void laneStart(LaneRay& L, float3 o, float3 d, float limit) {
+// root: index of the ray's root node (0 for a single scene; the scene's
+// first node when several scenes share one node array).
+__device__ __forceinline__ void laneStart(LaneRay& L, float3 o, float3 d, float limit, unsigned root) {
     L.r = setupRay(o, d);
     L.hit = Hit{-1, limit, 0.0f, 0.0f};
-    L.group = make_uint2(0u, 0x80000000u);
+    L.group = make_uint2(root, 0x80000000u);
     L.triGroup = make_uint2(0u, 0u);
     L.top = 0;
 }
@@ -186,7 +188,7 @@ __device__ __forceinline__ bool warpTrianglePhase(LaneRay& L, bool busy, const f
 }
 
 // Persistent query loop over `count` rays of an IO object providing
-//   __device__ void load(int k, float3& o, float3& d, float& limit);
+//   __device__ void load(int k, float3& o, float3& d, float& limit, unsigned& root);
 //   __device__ void store(int k, const Hit& h);
 // `fetch` must be zero at launch. Adds the number of finished queries to
 // *done and sets *errorFlag on stack overflow. Dynamic shared memory:
@@ -228,9 +230,10 @@ __device__ __forceinline__ void persistentTrace(IO& io, int count, const uint4* 
                     if (mine < count) {
                         float3 o, d;
                         float limit;
-                        io.load(mine, o, d, limit);
+                        unsigned root = 0;
+                        io.load(mine, o, d, limit, root);
                         if (limit > 0.0f) {
-                            laneStart(L, o, d, limit);
+                            laneStart(L, o, d, limit, root);
                             k = mine;
                         } else {
                             // No distance can be accepted (limit <= 0 or NaN):

@@ -66,7 +66,21 @@ class RtxBvhStats(c.Structure):
                 ('sahCost', c.c_double)]
 
 
+class RtxBatchTune(c.Structure):
+    _fields_ = [('block', c.c_int), ('capacity', c.c_int), ('refill', c.c_int), ('width', c.c_int),
+                ('frameMs', c.c_float)]
+
+
+class RtxBatchStats(c.Structure):
+    _fields_ = [('primaryRays', c.c_ulonglong), ('secondaryRays', c.c_ulonglong), ('shadowRays', c.c_ulonglong),
+                ('paths', c.c_ulonglong), ('frameMs', c.c_float), ('buildMs', c.c_float),
+                ('triangles', c.c_longlong), ('pixels', c.c_longlong), ('scenes', c.c_int), ('views', c.c_int),
+                ('kernelLaunches', c.c_int), ('graph', c.c_int), ('block', c.c_int), ('capacity', c.c_int),
+                ('refill', c.c_int), ('width', c.c_int)]
+
+
 assert (c.sizeof(Triangle), c.sizeof(Camera), c.sizeof(Settings)) == (116, 64, 28)
+assert (c.sizeof(RtxBatchTune), c.sizeof(RtxBatchStats)) == (20, 88)
 assert (c.sizeof(PixelSum), c.sizeof(BvhNode), c.sizeof(RtxQuery), c.sizeof(RtxHit)) == (40, 32, 28, 16)
 
 # numpy views of the same records, for scenes of millions of triangles.
@@ -93,7 +107,10 @@ EXPORTS = ('RtCreate', 'RtDestroy', 'RtShutdown', 'RtInitialize', 'RtRender', 'R
            'RtxReadAccumulation', 'RtxRenderStatsGet', 'RtxRenderDevice', 'RtxSetIntegrator', 'RtxSetTuning',
            'RtxQueryRaysStatic', 'RtxSetEnvironment', 'RtxUnetCreate', 'RtxUnetDestroy', 'RtxUnetParamCount',
            'RtxUnetLastError', 'RtxUnetGetParams', 'RtxUnetSetParams', 'RtxUnetLossGrad', 'RtxUnetTrain',
-           'RtxUnetInfer', 'RtxUnetSave', 'RtxUnetLoad', 'RtxSetDenoiser', 'RtxReadAovs')
+           'RtxUnetInfer', 'RtxUnetSave', 'RtxUnetLoad', 'RtxSetDenoiser', 'RtxReadAovs',
+           'RtxBatchCreate', 'RtxBatchDestroy', 'RtxBatchLastError', 'RtxBatchAddScene', 'RtxBatchAddView',
+           'RtxBatchSetEnvironment', 'RtxBatchRender', 'RtxBatchReset', 'RtxBatchSampleCount', 'RtxBatchReadImage',
+           'RtxBatchReadAccumulation', 'RtxBatchSetTuning', 'RtxBatchAutotune', 'RtxBatchStatsGet')
 
 
 def load_library(path=None):
@@ -146,6 +163,24 @@ def load_library(path=None):
     lib.RtxUnetLoad.argtypes = [vp, c.c_char_p]
     lib.RtxSetDenoiser.argtypes = [vp, vp]
     lib.RtxReadAovs.argtypes = [vp, c.c_void_p, c.c_int]
+    lib.RtxBatchCreate.restype = vp
+    lib.RtxBatchCreate.argtypes = []
+    lib.RtxBatchDestroy.argtypes = [vp]
+    lib.RtxBatchLastError.argtypes = [vp]
+    lib.RtxBatchLastError.restype = c.c_char_p
+    lib.RtxBatchAddScene.argtypes = [vp, c.c_void_p, c.c_int]
+    lib.RtxBatchAddView.argtypes = [vp, c.c_int, c.POINTER(Camera), c.c_int, c.c_int]
+    lib.RtxBatchSetEnvironment.argtypes = [vp, c.c_int, c.c_float, c.c_float, c.c_float]
+    lib.RtxBatchRender.argtypes = [vp, c.POINTER(Settings), c.POINTER(c.c_float)]
+    lib.RtxBatchReset.argtypes = [vp]
+    lib.RtxBatchSampleCount.argtypes = [vp]
+    lib.RtxBatchSampleCount.restype = c.c_uint
+    lib.RtxBatchReadImage.argtypes = [vp, c.c_int, c.c_void_p, c.c_int]
+    lib.RtxBatchReadAccumulation.argtypes = [vp, c.c_int, c.c_void_p, c.c_int]
+    lib.RtxBatchSetTuning.argtypes = [vp, c.c_int, c.c_int]
+    lib.RtxBatchAutotune.argtypes = [vp, c.POINTER(Settings), c.POINTER(RtxBatchTune), c.c_int,
+                                     c.POINTER(c.c_int)]
+    lib.RtxBatchStatsGet.argtypes = [vp, c.POINTER(RtxBatchStats)]
     return lib
 
 
@@ -375,3 +410,91 @@ class Unet:
 
     def load(self, path):
         self.check(self.lib.RtxUnetLoad(self.handle, str(path).encode()))
+
+
+class Batch:
+    """Many views of many scenes rendered together (RtxBatch* entry points)."""
+
+    BLOCK, CAPACITY, REFILL, GRAPH, WIDTH = 1, 2, 3, 4, 5
+
+    def __init__(self, lib=None):
+        self.lib = lib or load_library()
+        self.handle = self.lib.RtxBatchCreate()
+        self.views = []
+
+    def close(self):
+        if self.handle:
+            self.lib.RtxBatchDestroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def error(self):
+        return self.lib.RtxBatchLastError(self.handle).decode()
+
+    def check(self, ok):
+        if not ok:
+            raise NativeError(self.error())
+
+    def add_scene(self, triangles):
+        tris = triangles_array(triangles)
+        k = self.lib.RtxBatchAddScene(self.handle, tris.ctypes.data, len(tris))
+        self.check(k >= 0)
+        return k
+
+    def add_view(self, scene, camera, width, height):
+        k = self.lib.RtxBatchAddView(self.handle, scene, c.byref(camera), width, height)
+        self.check(k >= 0)
+        self.views.append((width, height))
+        return k
+
+    def set_environment(self, constant=None):
+        if constant is None:
+            self.check(self.lib.RtxBatchSetEnvironment(self.handle, 0, 0.0, 0.0, 0.0))
+        else:
+            r, g, b = (constant,) * 3 if isinstance(constant, (int, float)) else constant
+            self.check(self.lib.RtxBatchSetEnvironment(self.handle, 1, r, g, b))
+
+    def render(self, settings):
+        ms = c.c_float()
+        self.check(self.lib.RtxBatchRender(self.handle, c.byref(settings), c.byref(ms)))
+        return ms.value
+
+    def reset(self):
+        self.lib.RtxBatchReset(self.handle)
+
+    def sample_count(self):
+        return self.lib.RtxBatchSampleCount(self.handle)
+
+    def image(self, view):
+        w, h = self.views[view]
+        out = np.zeros(w * h * 4, np.uint8)
+        self.check(self.lib.RtxBatchReadImage(self.handle, view, out.ctypes.data, out.size))
+        return out
+
+    def accumulation(self, view):
+        w, h = self.views[view]
+        out = np.zeros(w * h, PIXELSUM_DTYPE)
+        self.check(self.lib.RtxBatchReadAccumulation(self.handle, view, out.ctypes.data, out.size))
+        return out
+
+    def set_tuning(self, block=None, capacity=None, refill=None, graph=None, width=None):
+        for key, value in ((self.BLOCK, block), (self.CAPACITY, capacity), (self.REFILL, refill),
+                           (self.GRAPH, graph), (self.WIDTH, width)):
+            if value is not None:
+                self.check(self.lib.RtxBatchSetTuning(self.handle, key, int(value)))
+
+    def autotune(self, settings, max_results=64):
+        results = (RtxBatchTune * max_results)()
+        count = c.c_int()
+        self.check(self.lib.RtxBatchAutotune(self.handle, c.byref(settings), results, max_results, c.byref(count)))
+        return [{name: getattr(r, name) for name, _ in RtxBatchTune._fields_} for r in results[:count.value]]
+
+    def stats(self):
+        st = RtxBatchStats()
+        self.check(self.lib.RtxBatchStatsGet(self.handle, c.byref(st)))
+        return {name: getattr(st, name) for name, _ in st._fields_}

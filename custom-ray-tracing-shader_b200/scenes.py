@@ -285,6 +285,67 @@ def random_room(seed, width=256, height=256):
     return tris, cam, settings, environment
 
 
+def random_scene(seed, triangles):
+    """A room (12 triangles with its light) holding displaced geodesic spheres
+    and boxes with random transforms, about `triangles` triangles in all:
+    one to six spheres share the budget (20 f^2 triangles each), plus up to
+    six boxes of 12."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    colors = rng.uniform(0.2, 0.8, (5, 3))
+    room = open_box((-4.0, 0.0, -4.0), (4.0, 4.0, 4.0), colors, rng.uniform(0.3, 0.8), 3.98, rng.uniform(10.0, 30.0))
+    parts = [room]
+    boxes = int(rng.integers(0, 7))
+    for k in range(boxes):
+        size = rng.uniform(0.3, 1.2, 3)
+        center = (rng.uniform(-3.0, 3.0), rng.uniform(0.2, 3.0), rng.uniform(-3.0, 3.0))
+        parts.append(cuboid(center, size, rng.uniform(0, math.pi), color=rng.uniform(0.1, 0.9, 3), mesh=20 + k))
+    budget = max(triangles - 12 - 12 * boxes, 20)
+    spheres = int(rng.integers(1, 7))
+    shares = rng.dirichlet(np.ones(spheres)) * budget
+    for k, share in enumerate(shares):
+        f = max(1, int(round(math.sqrt(share / 20.0))))
+        radius = rng.uniform(0.3, 1.3)
+        center = (rng.uniform(-2.5, 2.5), rng.uniform(radius, 4.0 - radius), rng.uniform(-2.5, 2.5))
+        v0, v1, v2, normals = geodesic_sphere(f, radius, center, rng.uniform(0.0, 0.08), rng,
+                                              smooth=bool(rng.random() < 0.5))
+        # Random anisotropic scale and rotation about the centre.
+        q = rng.normal(size=4)
+        q /= np.linalg.norm(q)
+        w, x, y, z = q
+        rot = np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)],
+                        [2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)],
+                        [2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)]])
+        m = rot * rng.uniform(0.7, 1.3, 3)[None, :]
+        c = np.asarray(center)
+        v0, v1, v2 = ((v - c) @ m.T + c for v in (v0, v1, v2))
+        inv_t = np.linalg.inv(m).T
+        normals = tuple(n @ inv_t.T / np.linalg.norm(n @ inv_t.T, axis=1, keepdims=True) for n in normals)
+        parts.append(records(v0, v1, v2, color=rng.uniform(0.1, 0.9, 3), normals=normals, mesh=40 + k))
+    return np.concatenate(parts)
+
+
+def batch_workload(seed=23, scene_count=8, cameras=64, low=10_000, high=2_000_000,
+                   resolutions=(256, 512, 1024)):
+    """Config 'batched multi-scene tracing': scene_count scenes (random_scene)
+    with triangle counts log-uniform in [low, high], `cameras` cameras spread
+    evenly over them, each at a square resolution drawn uniformly from
+    `resolutions`, looking into the room from random points. Returns the
+    scenes, the views as (scene, camera, width, height) and the settings
+    (depth 4, 8 paths per pixel)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    counts = np.exp(rng.uniform(math.log(low), math.log(high), scene_count)).astype(int)
+    scene_list = [random_scene(seed * 1000 + k, int(t)) for k, t in enumerate(counts)]
+    views = []
+    for i in range(cameras):
+        k = i % scene_count
+        size = int(rng.choice(resolutions))
+        eye = (rng.uniform(-3.0, 3.0), rng.uniform(0.8, 3.2), rng.uniform(-3.8, -2.5))
+        target = (rng.uniform(-1.5, 1.5), rng.uniform(0.5, 2.5), rng.uniform(-1.0, 2.5))
+        views.append((k, camera(eye, target, math.tan(math.radians(rng.uniform(25.0, 45.0))), 1.0), size, size))
+    settings = Settings(4, 1.0, 0.0, 1.0, 0.5, 42, 8)
+    return scene_list, views, settings
+
+
 # ---- check geometry, after the categories of Tools/verify_bvh.cu:115-139 ----
 
 def _tri(a, b, c, one_sided=0):

@@ -9,9 +9,13 @@ crops with random flips and an L1 loss on log(1 + radiance). Held-out rooms
 report PSNR on 8-bit display values (exposure tonemap and sRGB, as RtRender
 displays) for the input, the guided filter and the network.
 
+Defaults follow the training configuration of the denoiser: 200 rooms,
+4,800 crops of 128x128 (six inputs of 4 to 32 paths per pixel per room),
+1024-path targets, Adam at lr 1e-3 (cosine decay), 20K steps at batch 32.
+
 Usage:
-  python train_denoiser.py [--scenes 160] [--holdout 12] [--size 256]
-      [--target-spp 2048] [--steps 4000] [--out weights/denoiser_unet.bin]
+  python train_denoiser.py [--scenes 200] [--holdout 12] [--size 256]
+      [--target-spp 1024] [--steps 20000] [--out weights/denoiser_unet.bin]
 """
 import argparse
 import json
@@ -29,7 +33,7 @@ if str(HERE) not in sys.path:
 import scenes  # noqa: E402
 from native_api import DENOISER_WEIGHTS, Session, Settings, Unet, load_library  # noqa: E402
 
-INPUT_SPP = (4, 8, 8, 16, 16, 32)
+INPUT_SPP = (4, 4, 8, 8, 16, 32)
 
 
 def display(radiance, exposure):
@@ -86,14 +90,14 @@ def crops(images, crop):
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split('\n\n')[0])
-    ap.add_argument('--scenes', type=int, default=160, help='training rooms')
+    ap.add_argument('--scenes', type=int, default=200, help='training rooms')
     ap.add_argument('--holdout', type=int, default=12, help='validation rooms (other seeds)')
     ap.add_argument('--size', type=int, default=256, help='render resolution (square)')
     ap.add_argument('--crop', type=int, default=128)
-    ap.add_argument('--target-spp', type=int, default=2048)
-    ap.add_argument('--inputs-per-room', type=int, default=2)
-    ap.add_argument('--steps', type=int, default=4000)
-    ap.add_argument('--batch', type=int, default=16)
+    ap.add_argument('--target-spp', type=int, default=1024)
+    ap.add_argument('--inputs-per-room', type=int, default=6)
+    ap.add_argument('--steps', type=int, default=20000)
+    ap.add_argument('--batch', type=int, default=32)
     ap.add_argument('--lr', type=float, default=1e-3)
     ap.add_argument('--seed', type=int, default=1)
     ap.add_argument('--out', default=str(DENOISER_WEIGHTS))
@@ -118,7 +122,7 @@ def main(argv=None):
 
     net = Unet(lib, seed=args.seed)
     t1 = time.perf_counter()
-    chunk, history = 250, []
+    chunk, history = 500, []
     for start in range(0, args.steps, chunk):
         steps = min(chunk, args.steps - start)
         # Cosine decay to 5% of the initial rate.

@@ -214,6 +214,64 @@ int RtxSetDenoiser(void* session, void* net);
  * (radiance / samples), albedo / samples, normalised normal sum, first-hit
  * distance / samples (the distance is an added AOV). */
 int RtxReadAovs(void* session, float* aovs, int count);
+/* ---- Batched multi-scene rendering (no counterpart in the reference) ----
+ * Many views of many scenes of uneven size, rendered together: every frame
+ * traces the paths of all views in shared waves, so each traversal launch
+ * serves rays of every scene (the scenes' BVHs live in one node array, each
+ * ray starting at its scene's root), and the frame's kernel sequence is
+ * replayed from a CUDA graph. A view rendered in a batch accumulates exactly
+ * what RtRender (backend 2) accumulates for the same scene, camera and
+ * settings: the same Sobol pixel index (y * width + x of the view), sample
+ * numbers and seed.
+ *   RtxBatchAddScene   copies and prepares triangles like RtInitialize and
+ *                      builds its BVH; returns the scene id (>= 0) or -1
+ *   RtxBatchAddView    a camera on a scene with its own resolution (1..4096)
+ *                      and accumulation; returns the view id or -1
+ *   RtxBatchRender     one frame: raysPerPixel paths for every pixel of every
+ *                      view; the accumulation restarts when the settings
+ *                      bytes change or a view or scene is added
+ *   RtxBatchReadImage / RtxBatchReadAccumulation  one view's RGBA8 image /
+ *                      PixelSum records (bottom-up rows like RtRender)
+ *   RtxBatchSetTuning  RTX_BATCH_* keys below
+ *   RtxBatchAutotune   times candidate block sizes, queue capacities, refill
+ *                      thresholds and BVH widths on this batch (frames of
+ *                      one path per pixel), keeps the fastest and writes
+ *                      the candidates to results (up to maxResults)
+ * Returns 1 on success and 0 on failure (RtxBatchLastError) unless noted. */
+#define RTX_BATCH_BLOCK 1     /* threads per block of the traversal kernels: 64, 128 or 256 */
+#define RTX_BATCH_CAPACITY 2  /* paths in flight per wave (>= 1024) */
+#define RTX_BATCH_REFILL 3    /* refill threshold of the persistent traversal (1..32) */
+#define RTX_BATCH_GRAPH 4     /* 1: replay frames from a CUDA graph (default), 0: launch kernels */
+#define RTX_BATCH_WIDTH 5     /* BVH node width: 4 or 8 (default 8); rebuilds every scene */
+typedef struct RtxBatchTune {
+    int block, capacity, refill, width;
+    float frameMs;  /* device time of one frame of one path per pixel */
+} RtxBatchTune;
+typedef struct RtxBatchStats {
+    unsigned long long primaryRays, secondaryRays, shadowRays, paths;  /* of the last frame */
+    float frameMs;                 /* device time of the last frame (CUDA events) */
+    float buildMs;                 /* total BVH build time of all scenes */
+    long long triangles, pixels;   /* over all scenes / views */
+    int scenes, views;
+    int kernelLaunches;            /* kernels in one frame (graph nodes when replayed) */
+    int graph;                     /* 1 if the last frame was a graph launch */
+    int block, capacity, refill, width;  /* tuning in use */
+} RtxBatchStats;
+void* RtxBatchCreate(void);
+void RtxBatchDestroy(void* batch);
+const char* RtxBatchLastError(void* batch);
+int RtxBatchAddScene(void* batch, const Triangle* triangles, int count);
+int RtxBatchAddView(void* batch, int scene, const CameraData* camera, int width, int height);
+int RtxBatchSetEnvironment(void* batch, int mode, float r, float g, float b);
+int RtxBatchRender(void* batch, const RenderSettings* settings, float* milliseconds);
+void RtxBatchReset(void* batch);
+unsigned RtxBatchSampleCount(void* batch);
+int RtxBatchReadImage(void* batch, int view, unsigned char* output, int outputBytes);
+int RtxBatchReadAccumulation(void* batch, int view, PixelSum* sums, int count);
+int RtxBatchSetTuning(void* batch, int key, int value);
+int RtxBatchAutotune(void* batch, const RenderSettings* settings, RtxBatchTune* results, int maxResults, int* count);
+int RtxBatchStatsGet(void* batch, RtxBatchStats* stats);
+
 /* RtxQueryRays without any device allocation; no counterpart in the reference.
  * For callers that must not allocate device memory during the call (work
  * running beside a CUDA graph capture, latency-critical loops where

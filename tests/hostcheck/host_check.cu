@@ -39,7 +39,7 @@ static void primBoxes(const SceneTri* tris, int n, std::vector<float4>& lo, std:
 // Collapses a reference-layout binary BVH. result: [0] wide nodes, [1] depth,
 // [2] error code, [3] packed triangle count.
 int hc_collapse(const BinNode* bn, const int* order, const SceneTri* tris, int n, uint4* wideOut, int wideCapacity,
-                float4* packedOut, int* result, int group) {
+                float4* packedOut, int* result, int group, int width) {
     std::vector<float4> plo, phi;
     primBoxes(tris, n, plo, phi);
     int jobCapacity = 2 * n + 8;
@@ -51,7 +51,7 @@ int hc_collapse(const BinNode* bn, const int* order, const SceneTri* tris, int n
         counters[2] = 0;
         for (const Job& j : jobs)
             collapseJob(j, bn, order, plo.data(), phi.data(), tris, next.data(), reinterpret_cast<WideNode*>(wideOut),
-                        packedOut, counters, wideCapacity, jobCapacity, n, group);
+                        packedOut, counters, wideCapacity, jobCapacity, n, group, width);
         if (counters[3]) break;
         jobs.assign(next.begin(), next.begin() + counters[2]);
     }

@@ -29,13 +29,13 @@ def hc():
                         '-Xcompiler=-fPIC', str(HERE / 'host_check.cu'), '-o', str(LIB)], check=True)
     lib = c.CDLL(str(LIB))
     vp = c.c_void_p
-    lib.hc_collapse.argtypes = [vp, vp, vp, c.c_int, vp, c.c_int, vp, vp, c.c_int]
+    lib.hc_collapse.argtypes = [vp, vp, vp, c.c_int, vp, c.c_int, vp, vp, c.c_int, c.c_int]
     lib.hc_query.argtypes = [vp, vp, vp, c.c_int, c.c_int, vp, vp, vp]
     lib.hc_render.argtypes = [vp, vp, c.c_int, c.c_float, vp, vp, vp, vp, vp, c.c_int, c.c_int, c.c_uint, vp, vp, vp]
     return lib
 
 
-def collapse(hc, scene, group=3):
+def collapse(hc, scene, group=3, width=8):
     nodes, order, lin = scene.nodes(), scene.order(), scene.linear_triangles()
     n = len(lin)
     cap = 2 * n + 8
@@ -43,17 +43,20 @@ def collapse(hc, scene, group=3):
     packed = np.zeros(n * 12, np.float32)
     res = np.zeros(4, np.int32)
     assert hc.hc_collapse(nodes.ctypes.data, order.ctypes.data, lin.ctypes.data, n, wide.ctypes.data, cap,
-                          packed.ctypes.data, res.ctypes.data, group)
+                          packed.ctypes.data, res.ctypes.data, group, width)
     assert res[3] == n, 'every triangle packed exactly once'
     return wide, packed, res
 
 
-@pytest.mark.parametrize('group', (1, 2, 3))
+@pytest.mark.parametrize('group,width', ((1, 8), (2, 8), (3, 8), (3, 4), (1, 4)))
 @pytest.mark.parametrize('name', SETS)
-def test_wide_traversal_matches_reference(hc, oracle, name, group):
+def test_wide_traversal_matches_reference(hc, oracle, name, group, width):
     g = golden(f'bvh_{name}.npz')
     sc = oracle.scene(GEOMETRY[name])
-    wide, packed, res = collapse(hc, sc, group)
+    wide, packed, res = collapse(hc, sc, group, width)
+    W = wide[:res[0] * 20].reshape(-1, 20)
+    children = np.array([[m != 0 for m in node.view(np.uint8)[24:32]] for node in W[:200]])
+    assert children.sum(axis=1).max() <= width
     assert res[1] <= 48
     for any_hit in (0, 1):
         out = np.zeros(len(RAYS), HIT_DTYPE)
