@@ -57,13 +57,14 @@ def parse():
     p.add_argument('--no-reference-cuda', action='store_true')
     p.add_argument('--resolution', default=None, help='WxH override, for small profiling cases')
     p.add_argument('--spp', type=int, default=SPP_PER_STEP, help='paths per pixel per step (1..16)')
-    p.add_argument('--quality', action='store_true',
-                   help='also measure time to 35 dB PSNR vs a 4096-spp render on the 2M-triangle scene')
+    p.add_argument('--no-quality', dest='quality', action='store_false',
+                   help='skip time to 35 dB PSNR vs a 4096-spp render of the 2M-triangle scene (1 GPU runs it by default)')
     p.add_argument('--quality-resolution', default=None, help='WxH override of the quality scene')
     p.add_argument('--oracle-spp', type=int, default=4096)
-    p.add_argument('--batch', action='store_true',
-                   help='also measure batched multi-scene tracing (8 scenes, 64 views) against per-view launches')
+    p.add_argument('--no-batch', dest='batch', action='store_false',
+                   help='skip batched multi-scene tracing (8 scenes, 64 views; 1 GPU runs it by default)')
     p.add_argument('--batch-frames', type=int, default=3)
+    p.set_defaults(quality=True, batch=True)
     return p.parse_args()
 
 
@@ -428,6 +429,7 @@ def batch_run(lib, args):
             if s is None:
                 s = sessions[(k, w, h)] = Session(lib).initialize(scene_list[k], w, h)
                 s.render_device(cam, st)  # warm-up of this session
+            s.lib.RtReset(s.handle)  # samples 0..7, as in the batch frames
             per_view_ms += s.render_device(cam, st)
             r = s.render_stats()
             per_view_rays += r['primaryRays'] + r['secondaryRays'] + r['shadowRays']
