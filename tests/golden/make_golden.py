@@ -2,7 +2,7 @@
 
 Run from the repository root where the reference sources exist:
     make -C oracle            # builds oracle/_ref/libref.so from Native/renderer.cu
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [snapshot]
 Every array here is produced by the reference's own host code (BvhBuilder,
 collision, PathSampler, pixel) through oracle/_ref/libref.so, on the seeded
 scenes of custom-ray-tracing-shader_b200/scenes.py. The tests compare the
@@ -93,6 +93,19 @@ def main():
     print('golden fixtures written to', OUT)
 
 
+def snapshot_fixture(reference_root=Path('/root/reference')):
+    """The reference's Suzanne-room snapshot (Benchmarks/embree/scene.json,
+    982 triangles) as scene_io loads it, with the size, depth and node-array
+    hash of the reference builder's BVH for it."""
+    import scene_io
+    tris, cam, st, w, h = scene_io.load_snapshot(reference_root / 'Benchmarks/embree/scene.json')
+    sc = Reference().scene(tris)
+    np.savez_compressed(OUT / 'snapshot_room982.npz', triangles=tris, camera=np.frombuffer(bytes(cam), np.uint8),
+                        settings=np.frombuffer(bytes(st), np.uint8), width=w, height=h, node_count=sc.node_count,
+                        depth=sc.depth, nodes_sha256=sha(sc.nodes()), order_sha256=sha(sc.order()))
+    sc.close()
+
+
 def feature_scene():
     """Mirror, glossy Phong, one-sided faces, sky light, depth of field,
     orthographic and Russian roulette (depth 8) in one small scene."""
@@ -123,4 +136,8 @@ def feature_scene():
 
 
 if __name__ == '__main__':
-    main()
+    if sys.argv[1:] == ['snapshot']:
+        snapshot_fixture()   # only the snapshot fixture
+    else:
+        main()
+        snapshot_fixture()
