@@ -480,7 +480,9 @@ def run_ours(args, rank, local_rank, world):
         warm.initialize(small[0], 32, 32)
         warm.render(small[1], small[2])
     s = Session(lib)
+    t_init = time.perf_counter()
     s.initialize(tris, w, h)
+    init_wall_ms = (time.perf_counter() - t_init) * 1e3
     bvh = s.bvh_stats()
     # Integrator choice: both give identical sums; pick the faster on warm-up.
     candidates = {'wavefront': 0, 'megakernel': 1}
@@ -615,7 +617,9 @@ def run_ours(args, rank, local_rank, world):
                       'collapse_ms': bvh['collapseMs'],
                       'mtris_per_s': len(tris) / (bvh['buildMs'] + bvh['collapseMs']) / 1e3,
                       'binary_nodes': bvh['binaryNodes'], 'binary_depth': bvh['binaryDepth'],
-                      'wide_nodes': bvh['wideNodes'], 'sah_cost': bvh['sahCost']},
+                      'wide_nodes': bvh['wideNodes'], 'sah_cost': bvh['sahCost'],
+                      'initialize_wall_ms': init_wall_ms, 'upload_ms': bvh['uploadMs'],
+                      'distinct_colours': bvh['distinctColours']},
             'reference_cuda': ref_cuda,
             'time_to_35db': quality_run(lib, args) if (args.quality and world == 1) else None,
             'batch': batch_run(lib, args) if (args.batch and world == 1) else None,

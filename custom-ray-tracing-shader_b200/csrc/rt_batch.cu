@@ -28,6 +28,7 @@
 #include "rt_build.cuh"
 #include "rt_render.cuh"
 #include "rt_trace.cuh"
+#include "rt_upload.cuh"
 
 namespace rt {
 namespace {
@@ -669,29 +670,25 @@ int RtxBatchAddScene(void* p, const Triangle* triangles, int count) {
     if (!triangles || count <= 0) { b->error = "RtxBatchAddScene: need triangles and count > 0"; return -1; }
     if (!ensureBase(b)) return -1;
     cudaSetDevice(b->device);
-    // Host preparation as RtInitialize does it (renderer.cu:344-353).
-    std::vector<SceneTri> tris((size_t)count);
-    std::memcpy(tris.data(), triangles, sizeof(Triangle) * (size_t)count);
+    // Prepared on the device like RtInitialize's scenes (rt_upload.cuh); the
+    // emitters come back to the host for the arena's emitter list.
     BatchSceneData S;
     S.count = count;
-    for (int i = 0; i < count; i++) {
-        SceneTri& t = tris[i];
-        t.color = v3(srgbToLinear(t.color.x), srgbToLinear(t.color.y), srgbToLinear(t.color.z));
-        t.specularColor = v3(srgbToLinear(t.specularColor.x), srgbToLinear(t.specularColor.y),
-                             srgbToLinear(t.specularColor.z));
-        if (t.emission > 0) {
-            float3 an = cross(t.edge1, t.edge2);
-            S.lightArea += .5f * sqrtf(dot(an, an));
-            S.lights.push_back(Light{i, S.lightArea});
-        }
-    }
-    cudaError_t e;
-    if ((e = cudaMalloc(&S.dTris, sizeof(SceneTri) * (size_t)count)) != cudaSuccess) { failB(b, e, "scene"); return -1; }
-    if ((e = cudaMemcpy(S.dTris, tris.data(), sizeof(SceneTri) * (size_t)count, cudaMemcpyHostToDevice)) != cudaSuccess) {
+    Light* dLights = nullptr;
+    UploadResult up;
+    std::string why;
+    cudaError_t e = uploadScene(triangles, count, b->stream, &S.dTris, &dLights, up, why);
+    if (e != cudaSuccess) { b->error = why; return -1; }
+    S.lightArea = up.lightArea;
+    S.lights.resize((size_t)up.lightCount);
+    if (up.lightCount &&
+        (e = cudaMemcpy(S.lights.data(), dLights, sizeof(Light) * S.lights.size(), cudaMemcpyDeviceToHost)) != cudaSuccess) {
+        cudaFree(dLights);
         cudaFree(S.dTris);
         failB(b, e, "scene");
         return -1;
     }
+    cudaFree(dLights);
     if (!buildScene(b, S)) { freeBvh(S.bvh); cudaFree(S.dTris); return -1; }
     b->scenes.push_back(S);
     b->stats.buildMs += S.build.buildMs + S.build.collapseMs;

@@ -181,9 +181,17 @@ RT_HD unsigned shadeBounce(const SceneView& sc, const Settings& set, int bounce,
     st.origin = add(p, scale(g, .0005f));
     unsigned flags = 0;
     if (sc.lightCount > 0) {
+        // The reference scans the cumulative areas (renderer.cu:250) for the
+        // first light with pick < cumulativeArea, else the last light. The
+        // test is monotone in l (cumulative areas never decrease; once one is
+        // NaN all later ones are), so a binary search picks the same light.
         float pick = rng(0) * sc.lightArea;
-        int l = 0;
-        while (l < sc.lightCount - 1 && pick >= sc.lights[l].cumulativeArea) l++;
+        int l = 0, hi = sc.lightCount - 1;
+        while (l < hi) {
+            int mid = (l + hi) >> 1;
+            if (pick >= sc.lights[mid].cumulativeArea) l = mid + 1;
+            else hi = mid;
+        }
         const SceneTri& L = sc.tris[sc.lights[l].triangle];
         float root = sqrtf(rng(1)), v = rng(2);
         float3 target = add(L.origin, add(scale(L.edge1, root * (1.0f - v)), scale(L.edge2, root * v)));

@@ -27,6 +27,7 @@
 #include "../../include/cuda_ray_tracer.h"
 #include "rt_render.cuh"
 #include "rt_unet.cuh"
+#include "rt_upload.cuh"
 
 using namespace rt;
 
@@ -63,10 +64,15 @@ struct Session {
     unsigned samples = 0, accumulationVersion = 0;
     CameraData lastCamera{};
     RenderSettings lastSettings{};
-    // Host scene (colours linear) and emitters.
+    // Scene size and emitters (prepared on the device at RtInitialize); host
+    // copies of the prepared triangles and emitters for the CPU backends,
+    // fetched on their first use.
+    int triCount = 0, lightCount = 0;
+    float lightArea = 0;
     std::vector<SceneTri> tris;
     std::vector<Light> lights;
-    float lightArea = 0;
+    bool hostSceneReady = false;
+    UploadResult upload;
     // Device scene.
     cudaStream_t stream = nullptr;
     cudaEvent_t start = nullptr, stop = nullptr;
@@ -125,6 +131,10 @@ void releaseScene(Session* s) {
     s->hostPacked.clear();
     s->tris.shrink_to_fit(); s->hostWide.shrink_to_fit(); s->hostPacked.shrink_to_fit();
     s->hostBvhReady = false;
+    s->hostSceneReady = false;
+    s->triCount = 0;
+    s->lightCount = 0;
+    s->upload = UploadResult{};
     s->ready = false;
     s->width = s->height = 0;
     s->samples = 0;
@@ -141,7 +151,7 @@ bool validSettings(const RenderSettings* st) {
 }
 
 SceneView deviceView(Session* s) {
-    return SceneView{s->dTris, s->bvh.wideNodes, s->bvh.packedTris, s->dLights, (int)s->lights.size(), s->lightArea,
+    return SceneView{s->dTris, s->bvh.wideNodes, s->bvh.packedTris, s->dLights, s->lightCount, s->lightArea,
                      s->build.wideDepth, s->environmentMode, s->environment};
 }
 
@@ -194,10 +204,24 @@ bool renderDevice(Session* s, const CameraData* camera, const RenderSettings* se
     return true;
 }
 
+// Host copies of the prepared triangles and emitters (CPU backends).
+bool ensureHostScene(Session* s) {
+    if (s->hostSceneReady) return true;
+    s->tris.resize((size_t)s->triCount);
+    s->lights.resize((size_t)s->lightCount);
+    cudaError_t e = cudaMemcpy(s->tris.data(), s->dTris, sizeof(SceneTri) * s->tris.size(), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && s->lightCount)
+        e = cudaMemcpy(s->lights.data(), s->dLights, sizeof(Light) * s->lights.size(), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return fail(s, e);
+    s->hostSceneReady = true;
+    return true;
+}
+
 bool ensureHostBvh(Session* s) {
+    if (!ensureHostScene(s)) return false;
     if (s->hostBvhReady) return true;
     s->hostWide.resize((size_t)s->build.wideNodes * 5);
-    s->hostPacked.resize(s->tris.size() * 3);
+    s->hostPacked.resize((size_t)s->triCount * 3);
     cudaError_t e = cudaMemcpy(s->hostWide.data(), s->bvh.wideNodes, s->hostWide.size() * sizeof(uint4), cudaMemcpyDeviceToHost);
     if (e == cudaSuccess)
         e = cudaMemcpy(s->hostPacked.data(), s->bvh.packedTris, s->hostPacked.size() * sizeof(float4), cudaMemcpyDeviceToHost);
@@ -324,23 +348,6 @@ int RtInitialize(void* p, const Triangle* triangles, int count, int width, int h
     }
     cudaError_t e = cudaGetDevice(&s->device);
     if (e != cudaSuccess) { fail(s, e); return 0; }
-    // Host preparation, as the reference does it (renderer.cu:344-353).
-    s->tris.resize((size_t)count);
-    std::memcpy(s->tris.data(), triangles, sizeof(Triangle) * (size_t)count);
-#pragma omp parallel for schedule(static)
-    for (int i = 0; i < count; i++) {
-        SceneTri& t = s->tris[i];
-        t.color = v3(srgbToLinear(t.color.x), srgbToLinear(t.color.y), srgbToLinear(t.color.z));
-        t.specularColor = v3(srgbToLinear(t.specularColor.x), srgbToLinear(t.specularColor.y), srgbToLinear(t.specularColor.z));
-    }
-    for (int i = 0; i < count; i++) {
-        const SceneTri& t = s->tris[i];
-        if (t.emission > 0) {
-            float3 an = cross(t.edge1, t.edge2);
-            s->lightArea += .5f * sqrtf(dot(an, an));
-            s->lights.push_back(Light{i, s->lightArea});
-        }
-    }
     std::string err;
     const unsigned* dirs = hostSobolDirections(err);
     if (!dirs) { s->hostError = err; return 0; }
@@ -348,12 +355,19 @@ int RtInitialize(void* p, const Triangle* triangles, int count, int width, int h
     RT_CHECK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
     RT_CHECK(cudaEventCreate(&s->start));
     RT_CHECK(cudaEventCreate(&s->stop));
-    RT_CHECK(cudaMalloc(&s->dTris, sizeof(SceneTri) * (size_t)count));
-    RT_CHECK(cudaMemcpy(s->dTris, s->tris.data(), sizeof(SceneTri) * (size_t)count, cudaMemcpyHostToDevice));
-    if (!s->lights.empty()) {
-        RT_CHECK(cudaMalloc(&s->dLights, sizeof(Light) * s->lights.size()));
-        RT_CHECK(cudaMemcpy(s->dLights, s->lights.data(), sizeof(Light) * s->lights.size(), cudaMemcpyHostToDevice));
+    // The triangles go to the device as they are; sRGB decode and the
+    // emitter list are computed there with the reference's results
+    // (renderer.cu:344-353; rt_upload.cuh).
+    e = uploadScene(triangles, count, s->stream, &s->dTris, &s->dLights, s->upload, err);
+    if (e != cudaSuccess) {
+        fail(s, e);
+        releaseScene(s);
+        s->hostError = err;
+        return 0;
     }
+    s->triCount = count;
+    s->lightCount = s->upload.lightCount;
+    s->lightArea = s->upload.lightArea;
     RT_CHECK(cudaMalloc(&s->dDirs, sizeof(unsigned) * kSobolDims * 32));
     RT_CHECK(cudaMemcpy(s->dDirs, dirs, sizeof(unsigned) * kSobolDims * 32, cudaMemcpyHostToDevice));
     RT_CHECK(cudaMalloc(&s->dPassXor, sizeof(unsigned) * 16 * kSobolDims));
@@ -507,13 +521,13 @@ int RtxSobolSamples(const unsigned* pixel, const unsigned* sample, const unsigne
 int RtxExportBvh(void* p, BvhNode* nodes, int nodeCapacity, int* order, int orderCapacity) {
     Session* s = static_cast<Session*>(p);
     if (!s) return 0;
-    if (!s->ready || (nodes && nodeCapacity < s->build.binaryNodes) || (order && orderCapacity < (int)s->tris.size())) {
+    if (!s->ready || (nodes && nodeCapacity < s->build.binaryNodes) || (order && orderCapacity < s->triCount)) {
         s->error = cudaErrorInvalidValue; s->hostError = "RtxExportBvh: not initialised or buffers too small"; return 0;
     }
     cudaSetDevice(s->device);
     cudaError_t e = cudaSuccess;
     if (nodes) e = cudaMemcpy(nodes, s->bvh.binNodes, sizeof(BvhNode) * (size_t)s->build.binaryNodes, cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess && order) e = cudaMemcpy(order, s->bvh.order, sizeof(int) * s->tris.size(), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && order) e = cudaMemcpy(order, s->bvh.order, sizeof(int) * (size_t)s->triCount, cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) { fail(s, e); return 0; }
     return 1;
 }
@@ -543,6 +557,10 @@ int RtxBvhStatsGet(void* p, RtxBvhStats* out) {
     out->buildMs = s->build.buildMs;
     out->collapseMs = s->build.collapseMs;
     out->sahCost = s->sahCost;
+    out->uploadMs = s->upload.ms;
+    out->distinctColours = s->upload.distinctColours;
+    out->lightCount = s->lightCount;
+    out->lightArea = s->lightArea;
     return 1;
 }
 

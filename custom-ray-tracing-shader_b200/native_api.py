@@ -63,7 +63,8 @@ class RtxRenderStats(c.Structure):
 class RtxBvhStats(c.Structure):
     _fields_ = [('binaryNodes', c.c_int), ('binaryDepth', c.c_int), ('wideNodes', c.c_int),
                 ('wideDepth', c.c_int), ('buildMs', c.c_float), ('collapseMs', c.c_float),
-                ('sahCost', c.c_double)]
+                ('sahCost', c.c_double), ('uploadMs', c.c_float), ('distinctColours', c.c_int),
+                ('lightCount', c.c_int), ('lightArea', c.c_float)]
 
 
 class RtxBatchTune(c.Structure):

@@ -98,6 +98,10 @@ typedef struct RtxBvhStats {
     float buildMs;          /* device time of the binned-SAH build (CUDA events) */
     float collapseMs;       /* device time of the wide collapse and triangle packing */
     double sahCost;         /* SAH cost of the binary tree, normalised by the root area */
+    float uploadMs;         /* wall time of the upload with sRGB decode and emitter list on the device */
+    int distinctColours;    /* colour values decoded through the host's powf (the rest on the device) */
+    int lightCount;         /* emitting triangles */
+    float lightArea;        /* their total area */
 } RtxBvhStats;
 
 /* ---- the reference's thirteen exports ---- */

@@ -17,7 +17,7 @@ import pytest
 
 import scenes
 from conftest import golden, sha256
-from native_api import PIXELSUM_DTYPE, Session, sobol_samples
+from native_api import PIXELSUM_DTYPE, Session, Settings, sobol_samples
 from test_oracle_golden import GEOMETRY, RAYS, SETS
 
 pytestmark = pytest.mark.gpu
@@ -198,5 +198,66 @@ def test_gpu_reference_snapshot(session, reference):
             rgba, _ = session.render(cam, st)
             assert rgba.tobytes() == ref_rgba.tobytes()
             assert session.accumulation().tobytes() == ref.sums().tobytes()
+    finally:
+        ref.close()
+
+
+def upload_stress_scene():
+    """Per-triangle colours on both sides of the sRGB threshold (0, the
+    threshold itself, values above 1), 2,000 emitters of random power and
+    size among them zero-area ones, in a small room."""
+    rng = np.random.Generator(np.random.PCG64(4242))
+    room = scenes.open_box((-2.0, 0.0, -2.0), (2.0, 3.0, 2.0), rng.uniform(0.2, 0.8, (5, 3)), 0.4, 2.95, 10.0)
+    a = rng.uniform((-1.9, 0.1, -1.0), (1.9, 2.9, 1.9), (6000, 3)).astype(np.float32)
+    tris = scenes.records(a, a + rng.uniform(-0.15, 0.15, (6000, 3)), a + rng.uniform(-0.15, 0.15, (6000, 3)))
+    tris['oneSided'] = np.arange(len(tris)) % 2
+    for field in ('color', 'specularColor'):
+        for axis in 'xyz':
+            v = rng.uniform(0.0, 1.6, len(tris)).astype(np.float32)
+            v[::97] = np.float32(0.04045)
+            v[::89] = 0.0
+            tris[field][axis] = v
+    lit = rng.choice(len(tris), 2000, replace=False)
+    tris['emission'][lit] = rng.uniform(0.5, 20.0, len(lit)).astype(np.float32)
+    for k in lit[:20]:
+        tris['edge2'][k] = tris['edge1'][k]  # zero-area emitters
+    tris['smoothness'] = rng.uniform(0, 1, len(tris)).astype(np.float32)
+    tris['specularProbability'] = (rng.uniform(0, 1, len(tris)) < 0.3) * np.float32(0.5)
+    return np.concatenate([room, tris])
+
+
+def test_gpu_upload_matches_host_preparation(session, oracle, reference):
+    """Colours decoded and emitters listed on the device (RtInitialize) equal
+    the reference's host preparation: the emitter list and total area equal
+    the oracle's, renders equal the reference CUDA renderer bit for bit (its
+    scene prepared on the host), and the CPU backends read the same scene."""
+    from oracle_api import ReferenceSession
+    tris = upload_stress_scene()
+    w, h = 48, 40
+    cam = scenes.camera((0.0, 1.5, -1.9), (0.0, 1.2, 1.0), 0.8, w / h)
+    st = Settings(4, 1.0, 0.0, 1.0, 0.3, 77, 2)
+    session.initialize(tris, w, h)
+    stats = session.bvh_stats()
+    sc = oracle.scene(tris)
+    try:
+        lights = sc.lights()
+        assert stats['lightCount'] == len(lights) >= 2000
+        assert np.float32(stats['lightArea']) == np.float32(sc.light_area())
+        assert stats['distinctColours'] > 1000
+    finally:
+        sc.close()
+    ref = ReferenceSession(reference)
+    try:
+        ref.initialize(tris, w, h)
+        for _ in range(2):
+            ref_rgba, _ = ref.render(cam, st)
+            rgba, _ = session.render(cam, st)
+            assert rgba.tobytes() == ref_rgba.tobytes()
+            assert session.accumulation().tobytes() == ref.sums().tobytes()
+        gpu = rgba.copy()
+        session.lib.RtReset(session.handle)
+        session.render(cam, st, backend=0)
+        cpu, _ = session.render(cam, st, backend=0)  # host copies of the device-prepared scene
+        assert np.abs(cpu.astype(int) - gpu.astype(int)).max() <= 1
     finally:
         ref.close()
