@@ -64,6 +64,8 @@ def parse():
     p.add_argument('--no-batch', dest='batch', action='store_false',
                    help='skip batched multi-scene tracing (8 scenes, 64 views; 1 GPU runs it by default)')
     p.add_argument('--batch-frames', type=int, default=3)
+    p.add_argument('--denoiser-only', action='store_true',
+                   help='only time learned-denoiser inference at 1920x1080 (a small case for profiling)')
     p.set_defaults(quality=True, batch=True)
     return p.parse_args()
 
@@ -451,6 +453,59 @@ def batch_run(lib, args):
     }
 
 
+def unet_flops_per_pixel():
+    """Forward FLOPs per (padded) pixel of the U-Net: 2 * 9 * cin * cout per
+    3x3 layer at 1/4^level of the pixels, plus the 1x1 output layer."""
+    widths, prev, table = (32, 48, 64, 96, 128), 16, []
+    for level, w in enumerate(widths):
+        table += [(prev, w, level), (w, w, level)]
+        prev = w
+    for level in (3, 2, 1, 0):
+        w = widths[level]
+        table += [(prev + w, w, level), (w, w, level)]
+        prev = w
+    return sum(2 * 9 * ci * co / 4 ** lv for ci, co, lv in table) + 2 * 32 * 3
+
+
+def denoiser_run(lib, args, repeats=10):
+    """Learned-denoiser inference at 1920x1080 through RtDenoise (AOV kernel,
+    U-Net on BF16 tensor cores, tonemap, RGBA8 read-back): wall time per call
+    and the tensor-core rate it implies against the measured bf16 peak."""
+    import scenes
+    from native_api import DENOISER_WEIGHTS, Session, Unet
+    tris, cam, st, _, _ = scenes.cornell_sphere()
+    w, h = 1920, 1080
+    cam.aspect = w / h
+    st.raysPerPixel = 8
+    net = Unet(lib)
+    s = Session(lib)
+    try:
+        net.load(DENOISER_WEIGHTS)
+        s.initialize(tris, w, h)
+        s.render(cam, st)
+        s.set_denoiser(net)
+        s.denoise()  # allocates the activations for this size
+        times = [s.denoise()[1] for _ in range(repeats)]
+    finally:
+        s.set_denoiser(None)
+        s.close()
+        net.close()
+    ms = statistics.median(times)
+    padded = ((h + 15) // 16 * 16) * ((w + 15) // 16 * 16)
+    flops = unet_flops_per_pixel() * padded
+    path = ROOT / 'MEASURED_PEAKS.json'
+    peak, source = (float(json.loads(path.read_text())['bf16_tflops']), 'measured') if path.exists() else \
+        (1590.0, 'fallback')
+    tflops = flops / (ms * 1e-3) / 1e12
+    return {'workload': 'U-Net inference via RtDenoise, 1920x1080 (1920x1088 padded)', 'ms_per_call': ms,
+            'min_ms': min(times), 'mflop_per_pixel': unet_flops_per_pixel() / 1e6, 'gflop_per_call': flops / 1e9,
+            'tflops': tflops, 'roofline': {'bound': 'tensor', 'achieved': tflops, 'peak': peak,
+                                           'unit': 'TFLOP/s', 'frac': tflops / peak if peak else None,
+                                           'peak_source': f'{source} bf16_tflops',
+                                           'note': 'wall time of the whole call (AOVs, network, tonemap, '
+                                                   '8 MB read-back) against bf16 dense peak'}}
+
+
 def l2_flusher():
     try:
         import torch
@@ -623,6 +678,7 @@ def run_ours(args, rank, local_rank, world):
             'reference_cuda': ref_cuda,
             'time_to_35db': quality_run(lib, args) if (args.quality and world == 1) else None,
             'batch': batch_run(lib, args) if (args.batch and world == 1) else None,
+            'denoiser': denoiser_run(lib, args) if world == 1 else None,
         }
     s.close()
     dist.close()
@@ -684,7 +740,10 @@ def main():
     if world > 1 and args.impl == 'ours':
         os.environ['CUDA_VISIBLE_DEVICES'] = str(local_rank) if 'CUDA_VISIBLE_DEVICES' not in os.environ else \
             os.environ['CUDA_VISIBLE_DEVICES'].split(',')[local_rank]
-    if args.impl == 'reference':
+    if args.denoiser_only:
+        from native_api import load_library
+        result = denoiser_run(load_library(), args) if rank == 0 else None
+    elif args.impl == 'reference':
         result = run_reference(args, rank, world)
     else:
         result = run_ours(args, rank, local_rank, world)

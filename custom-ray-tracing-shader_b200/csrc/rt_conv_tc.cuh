@@ -1,0 +1,53 @@
+// 3x3 convolutions of the learned denoiser on the fifth-generation tensor
+// cores (tcgen05.mma, BF16 operands in shared memory, FP32 accumulators in
+// tensor memory).
+//
+// Implicit GEMM: D[pixel][n] = sum over taps and input channels of
+// A[pixel][k] * B[n][k], with A the input shifted by the tap. A block owns
+// 128 consecutive output pixels of one image row (the MMA's M = 128) and all
+// N output channels. The input halo of the tile (3 rows x 130 pixels x a
+// chunk of input channels) sits in shared memory as planes of 8 channels, 16
+// bytes per pixel, which is the no-swizzle K-major operand layout: core
+// matrices of 8 pixels x 8 channels, 8-pixel groups 128 bytes apart (SBO),
+// the two 8-channel halves of an MMA's K = 16 one plane apart (LBO). Each of
+// the 9 taps is the same buffer read from a start address shifted by the
+// tap's pixel offset, so no im2col copy is made. Weights are K-major
+// [tap][n][k] in the same plane form.
+#pragma once
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace rt {
+
+// Instruction descriptor of tcgen05.mma kind::f16: FP32 accumulator (bits
+// 4-5 = 1), BF16 A and B (bits 7-9 and 10-12 = 1), both K-major (bits 15 and
+// 16 = 0), N >> 3 in bits 17-22, M >> 4 in bits 24-28.
+__host__ __device__ constexpr uint32_t ummaInstrDescBf16(int m, int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+}
+
+// Shared-memory matrix descriptor, no swizzle: start address, leading-
+// dimension byte offset (LBO) and stride-dimension byte offset (SBO), each in
+// 16-byte units in 14-bit fields at bits 0, 16 and 32; descriptor version 1
+// (bit 46); base offset, LBO mode and layout type (bits 49-63) zero.
+__host__ __device__ constexpr uint64_t ummaSmemDesc(uint32_t address, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((address >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// out[p][n] = act(bias[n] + sum_tap,k in[p + off(tap)][k] * w[tap'][n][k]) over
+// NHWC BF16 input with Cin channels; w is [9][Cout][Cin] BF16 (K-major) and
+// tap' = 8 - tap when reverseTaps (the data gradient reads the forward
+// weights [tap][cin][cout] this way). Cin and Cout multiples of 16, Cout <=
+// 256. Writes BF16 (outB) or FP32 (outF, added to when accumulate). errorFlag
+// is set if a wait on the tensor cores runs past its limit.
+// With `low` set, the input is the concatenation [upsample2(low), in] read
+// in place: channels [0, lowChannels) from low (h/2 x w/2, nearest) and the
+// rest from `in` (cin - lowChannels channels per pixel); h and w even.
+cudaError_t convTc(const __nv_bfloat16* in, const __nv_bfloat16* low, int lowChannels, int n, int h, int w, int cin,
+                   const __nv_bfloat16* weights, bool reverseTaps, const float* bias, int cout, __nv_bfloat16* outB,
+                   float* outF, bool relu, bool accumulate, int* errorFlag, cudaStream_t stream);
+
+}  // namespace rt

@@ -450,6 +450,10 @@ int RtDenoise(void* p, unsigned char* output, int outputBytes, float* millisecon
         if ((e = launchPresentRadiance(s->dSum, radiance, (int)count, s->lastSettings.exposure, s->dPixels, s->stream)) != cudaSuccess) { fail(s, e); return 0; }
     } else if ((e = launchDenoise(s->dSum, s->samples, s->width, s->height, s->lastSettings.exposure, s->dDenoise, s->dPixels, s->stream)) != cudaSuccess) { fail(s, e); return 0; }
     if ((e = cudaStreamSynchronize(s->stream)) != cudaSuccess) { fail(s, e); return 0; }
+    if (s->denoiser) {
+        std::string why;
+        if ((e = s->denoiser->net.checkConvolutions(why)) != cudaSuccess) { fail(s, e, why.c_str()); return 0; }
+    }
     if ((e = cudaMemcpy(output, s->dPixels, count * 4, cudaMemcpyDeviceToHost)) != cudaSuccess) { fail(s, e); return 0; }
     *milliseconds = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - begin).count();
     if (!(*milliseconds > 0)) *milliseconds = 1e-6f;
@@ -660,6 +664,7 @@ int RtxUnetInfer(void* p, const float* aovs, int h, int w, float* radiance) {
     if (e == cudaSuccess) e = cudaMemcpy(dIn, aovs, sizeof(float) * px * 10, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = u->net.inferDevice(dIn, h, w, dOut, 0, why);
     if (e == cudaSuccess) e = cudaMemcpy(radiance, dOut, sizeof(float) * px * 3, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = u->net.checkConvolutions(why);
     cudaFree(dIn); cudaFree(dOut);
     return unetResult(u, e, why);
 }

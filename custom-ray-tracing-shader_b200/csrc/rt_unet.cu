@@ -1,14 +1,13 @@
 // Learned denoiser (see rt_unet.cuh): kernels, forward, backward, Adam.
 //
-// Convolutions are implicit GEMMs on the BF16 tensor cores (warp-level
-// matrix multiply-accumulate, 16x16x16 tiles, FP32 accumulation) over NHWC
-// BF16 activations with channel counts that are multiples of 16:
+// Activations are NHWC BF16 with channel counts that are multiples of 16.
 //   forward      out[p][co] = b[co] + sum_tap,ci x[p + off(tap)][ci] w[tap][ci][co]
-//   data grad    the same kernel on dY with w'[tap][co][ci] = w[8 - tap][ci][co]
-//   weight grad  dw[tap][ci][co] = sum_p x[p + off(tap)][ci] dY[p][co]
-// A block computes a 16 x 4 pixel tile for up to 64 output channels,
-// staging a 6 x 18 x 16 input halo and the 9 x 16 x 64 weight slice of each
-// 16-channel input chunk in shared memory.
+//                on the fifth-generation tensor cores (convTc, rt_conv_tc.cu)
+//                with K-major weights wT[tap][co][ci]
+//   data grad    convTc on dY with B[ci][co] = w[8 - tap][ci][co]: the forward
+//                weights read with the taps reversed
+//   weight grad  dw[tap][ci][co] = sum_p x[p + off(tap)][ci] dY[p][co] with
+//                16x16x16 warp-level MMA (wgradKernel)
 #include <mma.h>
 
 #include <algorithm>
@@ -17,6 +16,7 @@
 #include <cstring>
 #include <random>
 
+#include "rt_conv_tc.cuh"
 #include "rt_unet.cuh"
 
 namespace rt {
@@ -30,70 +30,6 @@ constexpr int kWidths[5] = {32, 48, 64, 96, 128};
 constexpr int kInputChannels = 10, kInputPadded = 16, kOutChannels = 3;
 
 inline int blocksFor(long long n, int b) { return (int)((n + b - 1) / b); }
-
-// ---- convolution (forward and data gradient) ----
-template <int CT>
-__global__ void __launch_bounds__(128) conv3x3Kernel(const bf16* __restrict__ in, int N, int H, int W, int Cin,
-                                                     const bf16* __restrict__ wt, const float* __restrict__ bias,
-                                                     int Cout, bf16* outB, float* outF, int relu, int accumulate) {
-    __shared__ __align__(32) bf16 sIn[kTileY + 2][kTileX + 2][16];
-    __shared__ __align__(32) bf16 sW[9][16][CT];
-    __shared__ __align__(32) float sOut[kTileY][16][CT];
-    const int coTiles = Cout / CT;
-    const int n = blockIdx.z / coTiles, co0 = (blockIdx.z % coTiles) * CT;
-    const int x0 = blockIdx.x * kTileX, y0 = blockIdx.y * kTileY;
-    const int warp = threadIdx.x >> 5;
-    wmma::fragment<wmma::accumulator, 16, 16, 16, float> acc[CT / 16];
-#pragma unroll
-    for (int f = 0; f < CT / 16; f++) wmma::fill_fragment(acc[f], 0.0f);
-    for (int ci0 = 0; ci0 < Cin; ci0 += 16) {
-        // Halo: (4+2) x (16+2) pixels x 16 channels, two 16-byte halves per pixel.
-        for (int k = threadIdx.x; k < (kTileY + 2) * (kTileX + 2) * 2; k += blockDim.x) {
-            int half = k & 1, pix = k >> 1;
-            int hy = pix / (kTileX + 2), hx = pix % (kTileX + 2);
-            int y = y0 + hy - 1, x = x0 + hx - 1;
-            uint4 v = make_uint4(0u, 0u, 0u, 0u);
-            if (y >= 0 && y < H && x >= 0 && x < W)
-                v = *reinterpret_cast<const uint4*>(in + (((size_t)n * H + y) * W + x) * Cin + ci0 + half * 8);
-            *reinterpret_cast<uint4*>(&sIn[hy][hx][half * 8]) = v;
-        }
-        // Weights: 9 taps x 16 input channels x CT output channels.
-        constexpr int perRow = CT / 8;
-        for (int k = threadIdx.x; k < 9 * 16 * perRow; k += blockDim.x) {
-            int row = k / perRow, part = k % perRow;
-            int tap = row / 16, ci = row % 16;
-            *reinterpret_cast<uint4*>(&sW[tap][ci][part * 8]) =
-                *reinterpret_cast<const uint4*>(wt + ((size_t)tap * Cin + ci0 + ci) * Cout + co0 + part * 8);
-        }
-        __syncthreads();
-#pragma unroll
-        for (int tap = 0; tap < 9; tap++) {
-            const int ky = tap / 3, kx = tap % 3;
-            wmma::fragment<wmma::matrix_a, 16, 16, 16, bf16, wmma::row_major> a;
-            wmma::load_matrix_sync(a, &sIn[warp + ky][kx][0], 16);
-#pragma unroll
-            for (int f = 0; f < CT / 16; f++) {
-                wmma::fragment<wmma::matrix_b, 16, 16, 16, bf16, wmma::row_major> b;
-                wmma::load_matrix_sync(b, &sW[tap][0][f * 16], CT);
-                wmma::mma_sync(acc[f], a, b, acc[f]);
-            }
-        }
-        __syncthreads();
-    }
-#pragma unroll
-    for (int f = 0; f < CT / 16; f++) wmma::store_matrix_sync(&sOut[warp][0][f * 16], acc[f], CT, wmma::mem_row_major);
-    __syncthreads();
-    for (int k = threadIdx.x; k < kTileY * 16 * CT; k += blockDim.x) {
-        int ty = k / (16 * CT), rem = k % (16 * CT), px = rem / CT, c = rem % CT;
-        int y = y0 + ty, x = x0 + px;
-        if (y >= H || x >= W) continue;
-        float v = sOut[ty][px][c] + (bias ? bias[co0 + c] : 0.0f);
-        if (relu) v = fmaxf(v, 0.0f);
-        size_t o = (((size_t)n * H + y) * W + x) * Cout + co0 + c;
-        if (outF) outF[o] = accumulate ? outF[o] + v : v;
-        else outB[o] = __float2bfloat16(v);
-    }
-}
 
 // ---- weight gradient ----
 // Block: one tap, 16 input channels, CT output channels, a chunk of 16-pixel
@@ -175,8 +111,16 @@ __global__ void inputKernel(const float* aov, int n, int h, int w, int H, int W,
         v[6] = a[6]; v[7] = a[7]; v[8] = a[8];
         v[9] = log1pf(fmaxf(a[9], 0.0f));
     }
-    bf16* o = x0 + (size_t)i * kInputPadded;
-    for (int c = 0; c < kInputPadded; c++) o[c] = __float2bfloat16(v[c]);
+    uint4 packed[2];
+    uint32_t* words = reinterpret_cast<uint32_t*>(packed);
+#pragma unroll
+    for (int j = 0; j < kInputPadded / 2; j++) {
+        __nv_bfloat162 pair = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+        words[j] = *reinterpret_cast<uint32_t*>(&pair);
+    }
+    uint4* o = reinterpret_cast<uint4*>(x0 + (size_t)i * kInputPadded);
+    o[0] = packed[0];
+    o[1] = packed[1];
 }
 __global__ void targetKernel(const float* target, int n, int h, int w, float* out, const int* batch,
                              const unsigned char* flips) {
@@ -190,18 +134,29 @@ __global__ void targetKernel(const float* target, int n, int h, int w, float* ou
     const float* t = target + (((size_t)src * h + sy) * w + sx) * 3;
     for (int c = 0; c < 3; c++) out[(size_t)i * 3 + c] = log1pf(fmaxf(t[c], 0.0f));
 }
+// 2x2 average pooling, 8 channels per thread (16-byte loads and stores).
 __global__ void poolKernel(const bf16* in, int N, int H, int W, int C, bf16* out) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    int Ho = H / 2, Wo = W / 2;
-    long long total = (long long)N * Ho * Wo * C;
+    const int Ho = H / 2, Wo = W / 2, C8 = C / 8;
+    long long total = (long long)N * Ho * Wo * C8;
     if (i >= total) return;
-    int c = (int)(i % C);
-    long long p = i / C;
+    int c = (int)(i % C8) * 8;
+    long long p = i / C8;
     int x = (int)(p % Wo), y = (int)((p / Wo) % Ho), n = (int)(p / ((long long)Wo * Ho));
     const bf16* b = in + (((size_t)n * H + 2 * y) * W + 2 * x) * C + c;
-    float s = __bfloat162float(b[0]) + __bfloat162float(b[C]) + __bfloat162float(b[(size_t)W * C]) +
-              __bfloat162float(b[(size_t)W * C + C]);
-    out[i] = __float2bfloat16(0.25f * s);
+    uint4 q[4] = {*reinterpret_cast<const uint4*>(b), *reinterpret_cast<const uint4*>(b + C),
+                  *reinterpret_cast<const uint4*>(b + (size_t)W * C), *reinterpret_cast<const uint4*>(b + (size_t)W * C + C)};
+    const bf16* e[4] = {reinterpret_cast<const bf16*>(&q[0]), reinterpret_cast<const bf16*>(&q[1]),
+                        reinterpret_cast<const bf16*>(&q[2]), reinterpret_cast<const bf16*>(&q[3])};
+    uint4 r;
+    bf16* o = reinterpret_cast<bf16*>(&r);
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        float s = __bfloat162float(e[0][j]) + __bfloat162float(e[1][j]) + __bfloat162float(e[2][j]) +
+                  __bfloat162float(e[3][j]);
+        o[j] = __float2bfloat16(0.25f * s);
+    }
+    *reinterpret_cast<uint4*>(out + (size_t)p * C + c) = r;
 }
 __global__ void poolBackwardKernel(const float* dOut, int N, int H, int W, int C, float* dIn, int accumulate) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -259,12 +214,12 @@ __global__ void biasGradKernel(const bf16* dPre, long long pixels, int C, float*
         s += __bfloat162float(dPre[p * C + c]);
     atomicAdd(&db[c], s);
 }
-// w'[tap][co][ci] = w[8 - tap][ci][co]
-__global__ void flipKernel(const bf16* w, int Cin, int Cout, bf16* out) {
+// K-major copy for the forward convolution: wT[tap][co][ci] = w[tap][ci][co].
+__global__ void transposeKernel(const bf16* w, int Cin, int Cout, bf16* out) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= 9 * Cin * Cout) return;
     int ci = i % Cin, co = (i / Cin) % Cout, tap = i / (Cin * Cout);
-    out[i] = w[((size_t)(8 - tap) * Cin + ci) * Cout + co];
+    out[i] = w[((size_t)tap * Cin + ci) * Cout + co];
 }
 __global__ void toBf16Kernel(const float* in, size_t count, bf16* out) {
     size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -275,9 +230,14 @@ __global__ void outForwardKernel(const bf16* d, long long pixels, int C, const f
     long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= pixels) return;
     float s[kOutChannels] = {b[0], b[1], b[2]};
-    for (int c = 0; c < C; c++) {
-        float v = __bfloat162float(d[p * C + c]);
-        for (int k = 0; k < kOutChannels; k++) s[k] += v * w[c * kOutChannels + k];
+    for (int c8 = 0; c8 < C; c8 += 8) {
+        uint4 q = *reinterpret_cast<const uint4*>(d + p * C + c8);
+        const bf16* e = reinterpret_cast<const bf16*>(&q);
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            float v = __bfloat162float(e[j]);
+            for (int k = 0; k < kOutChannels; k++) s[k] += v * w[(c8 + j) * kOutChannels + k];
+        }
     }
     for (int k = 0; k < kOutChannels; k++) pred[p * kOutChannels + k] = s[k];
 }
@@ -335,20 +295,6 @@ __global__ void outputKernel(const float* pred, int H, int W, int h, int w, floa
     for (int k = 0; k < kOutChannels; k++) out[(size_t)i * 3 + k] = fmaxf(expm1f(p[k]), 0.0f);
 }
 
-template <int CT>
-cudaError_t launchConv(const bf16* in, int N, int H, int W, int Cin, const bf16* wt, const float* bias, int Cout,
-                       bf16* outB, float* outF, bool relu, bool accumulate, cudaStream_t s) {
-    dim3 grid((W + kTileX - 1) / kTileX, (H + kTileY - 1) / kTileY, N * (Cout / CT));
-    conv3x3Kernel<CT><<<grid, 128, 0, s>>>(in, N, H, W, Cin, wt, bias, Cout, outB, outF, relu ? 1 : 0, accumulate ? 1 : 0);
-    return cudaGetLastError();
-}
-cudaError_t conv(const bf16* in, int N, int H, int W, int Cin, const bf16* wt, const float* bias, int Cout, bf16* outB,
-                 float* outF, bool relu, bool accumulate, cudaStream_t s) {
-    if (Cout % 64 == 0) return launchConv<64>(in, N, H, W, Cin, wt, bias, Cout, outB, outF, relu, accumulate, s);
-    if (Cout % 48 == 0) return launchConv<48>(in, N, H, W, Cin, wt, bias, Cout, outB, outF, relu, accumulate, s);
-    if (Cout % 32 == 0) return launchConv<32>(in, N, H, W, Cin, wt, bias, Cout, outB, outF, relu, accumulate, s);
-    return launchConv<16>(in, N, H, W, Cin, wt, bias, Cout, outB, outF, relu, accumulate, s);
-}
 template <int CT>
 cudaError_t launchWgrad(const bf16* x, const bf16* dy, int N, int H, int W, int Cin, int Cout, float* dw, cudaStream_t s) {
     long long segments = (long long)N * H * ((W + 15) / 16);
@@ -448,7 +394,9 @@ Unet::Unet(unsigned seed) {
     cudaMalloc(&adamM_, sizeof(float) * params_);
     cudaMalloc(&adamV_, sizeof(float) * params_);
     cudaMalloc(&wbf_, sizeof(bf16) * params_);
-    cudaMalloc(&wflip_, sizeof(bf16) * params_);
+    cudaMalloc(&wT_, sizeof(bf16) * params_);
+    cudaMalloc(&convError_, sizeof(int));
+    cudaMemset(convError_, 0, sizeof(int));
     cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking);
     cudaMemcpy(master_, host.data(), sizeof(float) * params_, cudaMemcpyHostToDevice);
     cudaMemset(adamM_, 0, sizeof(float) * params_);
@@ -459,7 +407,7 @@ Unet::Unet(unsigned seed) {
 
 Unet::~Unet() {
     delete act_;
-    cudaFree(master_); cudaFree(grad_); cudaFree(adamM_); cudaFree(adamV_); cudaFree(wbf_); cudaFree(wflip_);
+    cudaFree(master_); cudaFree(grad_); cudaFree(adamM_); cudaFree(adamV_); cudaFree(wbf_); cudaFree(wT_); cudaFree(convError_);
     if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -467,9 +415,19 @@ cudaError_t Unet::syncWeights(cudaStream_t s) {
     toBf16Kernel<<<blocksFor((long long)params_, 256), 256, 0, s>>>(master_, params_, wbf_);
     for (size_t l = 0; l + 1 < layers_.size(); l++) {
         const UnetLayer& L = layers_[l];
-        flipKernel<<<blocksFor(9LL * L.cin * L.cout, 256), 256, 0, s>>>(wbf_ + L.wOffset, L.cin, L.cout, wflip_ + L.wOffset);
+        transposeKernel<<<blocksFor(9LL * L.cin * L.cout, 256), 256, 0, s>>>(wbf_ + L.wOffset, L.cin, L.cout, wT_ + L.wOffset);
     }
     return cudaGetLastError();
+}
+
+cudaError_t Unet::checkConvolutions(std::string& error) {
+    int flag = 0;
+    cudaError_t e = cudaMemcpy(&flag, convError_, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return e;
+    if (!flag) return cudaSuccess;
+    cudaMemset(convError_, 0, sizeof(int));
+    error = "tensor-core convolution stopped: a wait on the tensor cores ran past its limit";
+    return cudaErrorLaunchTimeout;
 }
 
 cudaError_t Unet::getParams(float* host) const {
@@ -504,7 +462,7 @@ cudaError_t Unet::ensure(int n, int h, int w, bool training) {
     }
     for (int j = 0; j < 4; j++) {  // decoder level 3 - j
         int level = 3 - j;
-        if ((e = A.make(A.cat[j], px(level) * layers_[10 + 2 * j].cin)) != cudaSuccess) return e;
+        if (training && (e = A.make(A.cat[j], px(level) * layers_[10 + 2 * j].cin)) != cudaSuccess) return e;
         if (training && (e = A.make(A.dCat[j], px(level) * layers_[10 + 2 * j].cin)) != cudaSuccess) return e;
     }
     if ((e = A.make(A.pred, px(0) * kOutChannels)) != cudaSuccess) return e;
@@ -519,7 +477,7 @@ cudaError_t Unet::ensure(int n, int h, int w, bool training) {
     return cudaSuccess;
 }
 
-cudaError_t Unet::forward(cudaStream_t s, bool) {
+cudaError_t Unet::forward(cudaStream_t s, bool training) {
     Activations& A = *act_;
     const int n = A.n;
     cudaError_t e;
@@ -529,25 +487,33 @@ cudaError_t Unet::forward(cudaStream_t s, bool) {
         int H = A.H >> l, W = A.W >> l;
         if (l > 0) {
             int C = kWidths[l - 1];
-            poolKernel<<<blocksFor((long long)n * H * W * C, 256), 256, 0, s>>>(A.a[k - 1], n, H * 2, W * 2, C, A.pool[l - 1]);
+            poolKernel<<<blocksFor((long long)n * H * W * (C / 8), 256), 256, 0, s>>>(A.a[k - 1], n, H * 2, W * 2, C, A.pool[l - 1]);
             x = A.pool[l - 1];
         }
         for (int r = 0; r < 2; r++, k++) {
             const UnetLayer& L = layers_[k];
-            if ((e = conv(x, n, H, W, L.cin, wbf_ + L.wOffset, master_ + L.bOffset, L.cout, A.a[k], nullptr, true, false, s)) != cudaSuccess) return e;
+            if ((e = convTc(x, nullptr, 0, n, H, W, L.cin, wT_ + L.wOffset, false, master_ + L.bOffset, L.cout, A.a[k], nullptr, true, false, convError_, s)) != cudaSuccess) return e;
             x = A.a[k];
         }
     }
     for (int j = 0; j < 4; j++) {
         int level = 3 - j, H = A.H >> level, W = A.W >> level;
         int Cl = layers_[k - 1].cout, Cs = kWidths[level];
+        const bf16* low = A.a[k - 1];
         const bf16* skip = A.a[2 * level + 1];
-        upConcatKernel<<<blocksFor((long long)n * H * W * (Cl + Cs), 256), 256, 0, s>>>(A.a[k - 1], Cl, skip, Cs, n, H, W, A.cat[j]);
-        x = A.cat[j];
         for (int r = 0; r < 2; r++, k++) {
             const UnetLayer& L = layers_[k];
-            if ((e = conv(x, n, H, W, L.cin, wbf_ + L.wOffset, master_ + L.bOffset, L.cout, A.a[k], nullptr, true, false, s)) != cudaSuccess) return e;
-            x = A.a[k];
+            if (r == 0 && training) {
+                // The weight gradient reads the concatenated input: keep it.
+                upConcatKernel<<<blocksFor((long long)n * H * W * (Cl + Cs), 256), 256, 0, s>>>(low, Cl, skip, Cs, n, H, W, A.cat[j]);
+                e = convTc(A.cat[j], nullptr, 0, n, H, W, L.cin, wT_ + L.wOffset, false, master_ + L.bOffset, L.cout, A.a[k], nullptr, true, false, convError_, s);
+            } else if (r == 0) {
+                // Inference: the convolution reads [upsample(low), skip] in place.
+                e = convTc(skip, low, Cl, n, H, W, L.cin, wT_ + L.wOffset, false, master_ + L.bOffset, L.cout, A.a[k], nullptr, true, false, convError_, s);
+            } else {
+                e = convTc(A.a[k - 1], nullptr, 0, n, H, W, L.cin, wT_ + L.wOffset, false, master_ + L.bOffset, L.cout, A.a[k], nullptr, true, false, convError_, s);
+            }
+            if (e != cudaSuccess) return e;
         }
     }
     const UnetLayer& O = layers_[18];
@@ -576,7 +542,7 @@ cudaError_t Unet::backward(cudaStream_t s) {
             A.dPre, (long long)n * H * W, L.cout, grad_ + L.bOffset);
         cudaError_t err = wgrad(input, A.dPre, n, H, W, L.cin, L.cout, grad_ + L.wOffset, s);
         if (err != cudaSuccess) return err;
-        if (dIn) return conv(A.dPre, n, H, W, L.cout, wflip_ + L.wOffset, nullptr, L.cin, nullptr, dIn, false, accumulate, s);
+        if (dIn) return convTc(A.dPre, nullptr, 0, n, H, W, L.cout, wbf_ + L.wOffset, true, nullptr, L.cin, nullptr, dIn, false, accumulate, convError_, s);
         return cudaSuccess;
     };
     int k = 17;
@@ -633,6 +599,7 @@ cudaError_t Unet::lossAndGradient(const float* aovs, const float* targets, int n
     if (e == cudaSuccess) e = cudaMemcpyAsync(loss, A.loss, sizeof(float), cudaMemcpyDeviceToHost, stream_);
     if (e == cudaSuccess && grads) e = cudaMemcpyAsync(grads, grad_, sizeof(float) * params_, cudaMemcpyDeviceToHost, stream_);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+    if (e == cudaSuccess) e = checkConvolutions(error);
     cudaFree(dA); cudaFree(dT);
     return e;
 }
@@ -677,6 +644,7 @@ cudaError_t Unet::train(const float* aovs, const float* targets, int count, int 
     }
     if (e == cudaSuccess && losses) e = cudaMemcpyAsync(losses, dLosses, sizeof(float) * steps, cudaMemcpyDeviceToHost, stream_);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+    if (e == cudaSuccess) e = checkConvolutions(error);
     cudaFree(dA); cudaFree(dT); cudaFree(dLosses);
     return e;
 }

@@ -48,6 +48,9 @@ public:
     cudaError_t inferDevice(const float* aovs, int h, int w, float* radiance, cudaStream_t stream, std::string& error);
     // Checkpoint file: parameters, and the Adam state when optimizerState.
     cudaError_t save(const char* path, bool optimizerState, std::string& error) const;
+    // After the work has finished: an error if a tensor-core convolution gave
+    // up waiting (the flag is cleared).
+    cudaError_t checkConvolutions(std::string& error);
     cudaError_t load(const char* path, std::string& error);
 
 private:
@@ -64,7 +67,8 @@ private:
     float* adamM_ = nullptr;
     float* adamV_ = nullptr;
     __nv_bfloat16* wbf_ = nullptr;   // BF16 3x3 weights [tap][cin][cout] per layer (same offsets)
-    __nv_bfloat16* wflip_ = nullptr; // BF16 transposed, rotated weights for the data gradient
+    __nv_bfloat16* wT_ = nullptr;    // BF16 K-major weights [tap][cout][cin] for the forward convolutions
+    int* convError_ = nullptr;       // set by a tensor-core convolution whose wait ran past its limit
     long long adamStep_ = 0;
     Activations* act_ = nullptr;
     int n_ = 0, h_ = 0, w_ = 0;
