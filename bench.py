@@ -64,6 +64,8 @@ def parse():
     p.add_argument('--no-batch', dest='batch', action='store_false',
                    help='skip batched multi-scene tracing (8 scenes, 64 views; 1 GPU runs it by default)')
     p.add_argument('--batch-frames', type=int, default=3)
+    p.add_argument('--pieces', type=int, default=None,
+                   help='pieces per triangle of the traversal tree (RTX_TUNE_PIECES; default: the library default)')
     p.add_argument('--denoiser-only', action='store_true',
                    help='only time learned-denoiser inference at 1920x1080 (a small case for profiling)')
     p.set_defaults(quality=True, batch=True)
@@ -535,6 +537,8 @@ def run_ours(args, rank, local_rank, world):
         warm.initialize(small[0], 32, 32)
         warm.render(small[1], small[2])
     s = Session(lib)
+    if args.pieces is not None:
+        s.set_tuning(pieces=args.pieces)
     t_init = time.perf_counter()
     s.initialize(tris, w, h)
     init_wall_ms = (time.perf_counter() - t_init) * 1e3
@@ -672,7 +676,9 @@ def run_ours(args, rank, local_rank, world):
                       'collapse_ms': bvh['collapseMs'],
                       'mtris_per_s': len(tris) / (bvh['buildMs'] + bvh['collapseMs']) / 1e3,
                       'binary_nodes': bvh['binaryNodes'], 'binary_depth': bvh['binaryDepth'],
-                      'wide_nodes': bvh['wideNodes'], 'sah_cost': bvh['sahCost'],
+                      'sah_cost': bvh['sahCost'],
+                      'traversal_tree': {'pieces_per_triangle': bvh['pieces'], 'build_ms': bvh['pieceBuildMs'],
+                                         'wide_nodes': bvh['wideNodes'], 'wide_depth': bvh['wideDepth']},
                       'initialize_wall_ms': init_wall_ms, 'upload_ms': bvh['uploadMs'],
                       'distinct_colours': bvh['distinctColours']},
             'reference_cuda': ref_cuda,

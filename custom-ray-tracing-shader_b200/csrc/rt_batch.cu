@@ -6,8 +6,9 @@
 // Scenes are built one by one with the single-scene builder, then copied
 // into arenas: shading triangles, wide nodes, packed triangles and emitters
 // of all scenes one after another. The copy rebases the indices inside it (a
-// node's childBase and triBase, a packed triangle's original index, an
-// emitter's triangle) by the scene's offsets, so a traversal that starts at
+// node's childBase and triBase by the scene's node and packed-triangle
+// offsets, a packed triangle's original index and an emitter's triangle by
+// its triangle offset), so a traversal that starts at
 // the scene's root node meets only that scene's nodes and triangles, and hit
 // indices address the shared shading arena. The offsets keep the order of
 // indices within a scene, so the reference's tie-break (smaller index at equal
@@ -319,8 +320,8 @@ struct BatchSceneData {
     int count = 0;
     BuiltBvh bvh;
     BuildResult build;
-    int builtWidth = 0;
-    unsigned triBase = 0, nodeBase = 0, lightBase = 0;
+    int builtWidth = 0, builtPieces = 0;
+    unsigned triBase = 0, nodeBase = 0, lightBase = 0, packedBase = 0;
 };
 struct BatchViewData {
     Camera cam;
@@ -355,7 +356,7 @@ struct Batch {
     int* dError = nullptr;
     WavefrontBuffers wave;
     // Tuning.
-    int block = 128, capacity = 0, refill = 24, width = 8, useGraph = 1;
+    int block = 128, capacity = 0, refill = 24, width = 8, useGraph = 1, pieces = 2;
     int environmentMode = 0;
     float3 environment = make_float3(0.0f, 0.0f, 0.0f);
     // Frame state.
@@ -424,13 +425,19 @@ bool ensureBase(Batch* b) {
     return true;
 }
 
+// Traversal tree of a scene at the batch's BVH width and pieces per triangle
+// (only the wide nodes and packed triangles are kept).
 bool buildScene(Batch* b, BatchSceneData& S) {
-    if (S.builtWidth == b->width) return true;
+    if (S.builtWidth == b->width && S.builtPieces == b->pieces) return true;
     freeBvh(S.bvh);
     const char* why = nullptr;
-    cudaError_t e = buildBvh(S.dTris, S.count, b->stream, S.bvh, S.build, &why, 3, b->width);
+    cudaError_t e = buildBvh(S.dTris, S.count, b->stream, S.bvh, S.build, &why, 3, b->width, b->pieces);
     if (e != cudaSuccess) { S.builtWidth = 0; return failB(b, e, why); }
+    void* unused[] = {S.bvh.binNodes, S.bvh.order, S.bvh.primLo, S.bvh.primHi};
+    for (void* q : unused) cudaFree(q);
+    S.bvh.binNodes = nullptr; S.bvh.order = nullptr; S.bvh.primLo = nullptr; S.bvh.primHi = nullptr;
     S.builtWidth = b->width;
+    S.builtPieces = b->pieces;
     return true;
 }
 
@@ -438,38 +445,43 @@ bool buildScene(Batch* b, BatchSceneData& S) {
 bool ensureArena(Batch* b) {
     if (b->arenaReady) return true;
     freeArena(b);
-    size_t tris = 0, nodes = 0, lights = 0;
+    size_t tris = 0, nodes = 0, lights = 0, packedCount = 0;
     for (BatchSceneData& S : b->scenes) {
         if (!buildScene(b, S)) return false;
         S.triBase = (unsigned)tris;
         S.nodeBase = (unsigned)nodes;
         S.lightBase = (unsigned)lights;
+        S.packedBase = (unsigned)packedCount;
         tris += (size_t)S.count;
         nodes += (size_t)S.build.wideNodes;
         lights += S.lights.size();
+        packedCount += (size_t)S.build.packedTriangles;
     }
-    if (tris > 0x7FFFFFFFull || nodes > 0x7FFFFFFFull) { b->error = "batch too large for 31-bit indices"; return false; }
+    if (tris > 0x7FFFFFFFull || nodes > 0x7FFFFFFFull || packedCount > 0x7FFFFFFFull) {
+        b->error = "batch too large for 31-bit indices";
+        return false;
+    }
     cudaError_t e;
     if ((e = cudaMalloc(&b->aTris, sizeof(SceneTri) * tris)) != cudaSuccess) return failB(b, e, "arena");
     if ((e = cudaMalloc(&b->aWide, sizeof(uint4) * 5 * nodes)) != cudaSuccess) return failB(b, e, "arena");
-    if ((e = cudaMalloc(&b->aPacked, sizeof(float4) * 3 * tris)) != cudaSuccess) return failB(b, e, "arena");
+    if ((e = cudaMalloc(&b->aPacked, sizeof(float4) * 3 * packedCount)) != cudaSuccess) return failB(b, e, "arena");
     if ((e = cudaMalloc(&b->aLights, sizeof(Light) * std::max<size_t>(lights, 1))) != cudaSuccess) return failB(b, e, "arena");
     if ((e = cudaMalloc(&b->dScenes, sizeof(BatchScene) * b->scenes.size())) != cudaSuccess) return failB(b, e, "arena");
     std::vector<BatchScene> table;
     std::vector<Light> allLights;
     allLights.reserve(lights);
     for (BatchSceneData& S : b->scenes) {
-        const size_t n = (size_t)S.count, w = (size_t)S.build.wideNodes;
+        const size_t n = (size_t)S.count, w = (size_t)S.build.wideNodes, np = (size_t)S.build.packedTriangles;
         if ((e = cudaMemcpyAsync(b->aTris + S.triBase, S.dTris, sizeof(SceneTri) * n, cudaMemcpyDeviceToDevice,
                                  b->stream)) != cudaSuccess) return failB(b, e);
         if ((e = cudaMemcpyAsync(b->aWide + (size_t)S.nodeBase * 5, S.bvh.wideNodes, sizeof(uint4) * 5 * w,
                                  cudaMemcpyDeviceToDevice, b->stream)) != cudaSuccess) return failB(b, e);
-        if ((e = cudaMemcpyAsync(b->aPacked + (size_t)S.triBase * 3, S.bvh.packedTris, sizeof(float4) * 3 * n,
+        if ((e = cudaMemcpyAsync(b->aPacked + (size_t)S.packedBase * 3, S.bvh.packedTris, sizeof(float4) * 3 * np,
                                  cudaMemcpyDeviceToDevice, b->stream)) != cudaSuccess) return failB(b, e);
         rebaseNodesKernel<<<blocksFor((long long)w, 256), 256, 0, b->stream>>>(b->aWide + (size_t)S.nodeBase * 5, (int)w,
-                                                                              S.nodeBase, S.triBase);
-        rebasePackedKernel<<<blocksFor((long long)n, 256), 256, 0, b->stream>>>(b->aPacked + (size_t)S.triBase * 3, (int)n,
-                                                                               S.triBase);
+                                                                              S.nodeBase, S.packedBase);
+        rebasePackedKernel<<<blocksFor((long long)np, 256), 256, 0, b->stream>>>(b->aPacked + (size_t)S.packedBase * 3,
+                                                                                (int)np, S.triBase);
         if ((e = cudaGetLastError()) != cudaSuccess) return failB(b, e);
         for (const Light& L : S.lights) allLights.push_back(Light{L.triangle + (int)S.triBase, L.cumulativeArea});
         SceneView view{b->aTris, b->aWide, b->aPacked, b->aLights + S.lightBase, (int)S.lights.size(), S.lightArea,
@@ -797,6 +809,10 @@ int RtxBatchSetTuning(void* p, int key, int value) {
         case RTX_BATCH_WIDTH:
             if (value != 4 && value != 8) break;
             if (value != b->width) { b->width = value; freeArena(b); }
+            return 1;
+        case RTX_BATCH_PIECES:
+            if (value < 1 || value > 8) break;
+            if (value != b->pieces) { b->pieces = value; freeArena(b); }
             return 1;
         default:
             break;

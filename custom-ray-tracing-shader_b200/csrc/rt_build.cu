@@ -39,6 +39,9 @@ constexpr int kLeafSize = 4;       // bvh.cuh:64
 constexpr int kScanBlock = 1024;   // elements per scan block
 constexpr int kBinBlock = 256;
 constexpr int kBinPer = 8;         // positions per thread in the binning pass
+// Tasks of at most kSmallTask primitives are binned by one warp each
+// (binSmallKernel); larger ones by position blocks (binKernel).
+constexpr int kSmallTask = 2048;
 
 struct Task {
     int node, first, count, depth;
@@ -105,14 +108,84 @@ __global__ void primBoxesKernel(const SceneTri* tris, int n, float4* plo, float4
     }
 }
 
+// Traversal-tree primitives: each triangle cut into `pieces` slabs along the
+// longest axis of its box; a piece's box bounds the part of the triangle in
+// its slab (vertices inside it and the edges' crossings of its planes), padded
+// like the reference pads triangle boxes (bvh.cuh:46-47). The padding exceeds
+// the rounding of the clipping, so every point of the triangle lies in the
+// padded box of a piece containing it, and the union of the pieces' boxes
+// covers the triangle's padded box's content that traversal can reach.
+__global__ void splitBoxesKernel(const SceneTri* tris, int n, int pieces, float4* plo, float4* phi, float4* cent,
+                                 Task* root) {
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    float v[12];
+    for (int k = 0; k < 3; k++) { v[k] = FLT_MAX; v[3 + k] = -FLT_MAX; v[6 + k] = FLT_MAX; v[9 + k] = -FLT_MAX; }
+    if (r < n * pieces) {
+        const int i = r / pieces, s = r % pieces;
+        const SceneTri& t = tris[i];
+        float3 P[3] = {t.origin, v3(t.origin.x + t.edge1.x, t.origin.y + t.edge1.y, t.origin.z + t.edge1.z),
+                       v3(t.origin.x + t.edge2.x, t.origin.y + t.edge2.y, t.origin.z + t.edge2.z)};
+        float tlo[3], thi[3];
+        for (int a = 0; a < 3; a++) {
+            tlo[a] = fminf(fminf(comp(P[0], a), comp(P[1], a)), comp(P[2], a));
+            thi[a] = fmaxf(fmaxf(comp(P[0], a), comp(P[1], a)), comp(P[2], a));
+        }
+        int ax = 0;
+        for (int a = 1; a < 3; a++) if (thi[a] - tlo[a] > thi[ax] - tlo[ax]) ax = a;
+        const float ext = thi[ax] - tlo[ax];
+        const float t0 = s == 0 ? tlo[ax] : tlo[ax] + ext * ((float)s / (float)pieces);
+        const float t1 = s == pieces - 1 ? thi[ax] : tlo[ax] + ext * ((float)(s + 1) / (float)pieces);
+        float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+        auto grow = [&](float3 q) {
+            for (int a = 0; a < 3; a++) { lo[a] = fminf(lo[a], comp(q, a)); hi[a] = fmaxf(hi[a], comp(q, a)); }
+        };
+        for (int e = 0; e < 3; e++) {
+            const float3 p = P[e], q = P[(e + 1) % 3];
+            const float pa = comp(p, ax), qa = comp(q, ax);
+            if (pa >= t0 && pa <= t1) grow(p);
+            for (int side = 0; side < 2; side++) {
+                const float plane = side ? t1 : t0;
+                if ((pa < plane && qa > plane) || (pa > plane && qa < plane)) {
+                    const float u = (plane - pa) / (qa - pa);
+                    float3 x = v3(p.x + u * (q.x - p.x), p.y + u * (q.y - p.y), p.z + u * (q.z - p.z));
+                    if (ax == 0) x.x = plane; else if (ax == 1) x.y = plane; else x.z = plane;
+                    grow(x);
+                }
+            }
+        }
+        float ce[3];
+        for (int a = 0; a < 3; a++) {
+            if (!(lo[a] <= hi[a])) { lo[a] = tlo[a]; hi[a] = thi[a]; }  // nothing collected: whole box
+            float pad = 1e-5f + 1e-6f * fmaxf(fabsf(tlo[a]), fabsf(thi[a]));
+            lo[a] -= pad; hi[a] += pad;
+            ce[a] = 0.5f * (lo[a] + hi[a]);
+        }
+        plo[r] = make_float4(lo[0], lo[1], lo[2], 0.0f);
+        phi[r] = make_float4(hi[0], hi[1], hi[2], 0.0f);
+        cent[r] = make_float4(ce[0], ce[1], ce[2], 0.0f);
+        for (int k = 0; k < 3; k++) { v[k] = lo[k]; v[3 + k] = hi[k]; v[6 + k] = ce[k]; v[9 + k] = ce[k]; }
+    }
+    for (int off = 16; off > 0; off >>= 1)
+        for (int k = 0; k < 12; k++) {
+            float o = __shfl_xor_sync(0xFFFFFFFFu, v[k], off);
+            v[k] = ((k / 3) & 1) ? fmaxf(v[k], o) : fminf(v[k], o);
+        }
+    if ((threadIdx.x & 31) == 0) {
+        for (int k = 0; k < 3; k++) {
+            atomicMinFloat(&root->lo[k], v[k]); atomicMaxFloat(&root->hi[k], v[3 + k]);
+            atomicMinFloat(&root->clo[k], v[6 + k]); atomicMaxFloat(&root->chi[k], v[9 + k]);
+        }
+    }
+}
+
 __global__ void iotaKernel(int* a, int n, int value0, int* b, int bValue) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) { a[i] = i + value0; if (b) b[i] = bValue; }
 }
 
-__global__ void clearBinsKernel(BinAcc* bins, int count) {
+__global__ void clearBinsKernel(BinAcc* bins, int count, const Task* tasks) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= count) return;
+    if (i >= count || tasks[i / (3 * kBins)].count <= kSmallTask) return;
     BinAcc& b = bins[i];
     b.count = 0;
     for (int a = 0; a < 3; a++) { b.lo[a] = FLT_MAX; b.hi[a] = -FLT_MAX; b.clo[a] = FLT_MAX; b.chi[a] = -FLT_MAX; }
@@ -147,9 +220,10 @@ __global__ void __launch_bounds__(kBinBlock) binKernel(const int* order, const i
         if (j >= nPos) break;
         int t = posTask[j];
         if (t < 0) continue;
+        const Task& T = tasks[t];
+        if (T.count <= kSmallTask) continue;  // binned by binSmallKernel
         int prim = order[j];
         float4 c = cent[prim], lo = plo[prim], hi = phi[prim];
-        const Task& T = tasks[t];
         for (int a = 0; a < 3; a++) {
             float extent = T.chi[a] - T.clo[a];
             if (extent <= 1e-12f) continue;
@@ -172,6 +246,44 @@ __global__ void __launch_bounds__(kBinBlock) binKernel(const int* order, const i
             }
         }
     }
+}
+
+// One warp per small task: warp-private bins in shared memory (atomics only
+// within the warp), written out with plain stores, so these bins need no
+// clearing and no global atomics. Bins hold a count and minima/maxima, so the
+// order of accumulation does not change them.
+__global__ void __launch_bounds__(256) binSmallKernel(const int* order, const float4* cent, const float4* plo,
+                                                      const float4* phi, const Task* tasks, int nTasks,
+                                                      BinAcc* bins) {
+    __shared__ BinAcc sb[8][3 * kBins];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int t = blockIdx.x * 8 + warp;
+    if (t >= nTasks) return;
+    const Task T = tasks[t];
+    if (T.count > kSmallTask) return;
+    BinAcc* my = sb[warp];
+    for (int i = lane; i < 3 * kBins; i += 32) {
+        BinAcc& b = my[i];
+        b.count = 0;
+        for (int a = 0; a < 3; a++) { b.lo[a] = FLT_MAX; b.hi[a] = -FLT_MAX; b.clo[a] = FLT_MAX; b.chi[a] = -FLT_MAX; }
+    }
+    __syncwarp();
+    float scale[3];
+    for (int a = 0; a < 3; a++) {
+        float extent = T.chi[a] - T.clo[a];
+        scale[a] = extent <= 1e-12f ? 0.0f : kBins / extent;
+    }
+    for (int j = T.first + lane; j < T.first + T.count; j += 32) {
+        const int prim = order[j];
+        const float4 c = cent[prim], lo = plo[prim], hi = phi[prim];
+        for (int a = 0; a < 3; a++) {
+            if (scale[a] == 0.0f) continue;
+            const float ca = a == 0 ? c.x : (a == 1 ? c.y : c.z);
+            accumulateBin(&my[a * kBins + binOf(ca, T.clo[a], scale[a])], lo, hi, c);
+        }
+    }
+    __syncwarp();
+    for (int i = lane; i < 3 * kBins; i += 32) bins[(size_t)t * 3 * kBins + i] = my[i];
 }
 
 // One thread per open task: the reference's SAH sweep, then node records.
@@ -248,6 +360,7 @@ __global__ void splitKernel(const Task* tasks, int nTasks, const BinAcc* bins, S
         } else {
             int k = atomicAdd(&counters[1], 1);
             if (k >= taskCapacity) { atomicExch(&counters[3], 2); continue; }
+            if (c.count > kSmallTask) atomicAdd(&counters[5], 1);
             nextTasks[k] = c;
             S.childTask[side] = k;
         }
@@ -276,13 +389,13 @@ __global__ void flagKernel(const int* order, const int* posTask, const float4* c
 }
 
 // Exclusive scan, phase 1: per-block scan in place, block totals out.
-__global__ void __launch_bounds__(256) scanBlocksKernel(unsigned* data, int n, unsigned* blockSums) {
+__global__ void __launch_bounds__(256) scanBlocksKernel(const unsigned* in, unsigned* data, int n, unsigned* blockSums) {
     __shared__ unsigned warpSums[8];
     int base = blockIdx.x * kScanBlock;
     unsigned v[4], local = 0;
     for (int k = 0; k < 4; k++) {
         int j = base + threadIdx.x * 4 + k;
-        v[k] = j < n ? data[j] : 0u;
+        v[k] = j < n ? in[j] : 0u;
         local += v[k];
     }
     unsigned incl = local;
@@ -396,11 +509,11 @@ __global__ void renumberKernel(const BinNode* nodes, int count, const int* newIn
 __global__ void collapseKernel(const BinNode* bn, const int* order, const float4* plo, const float4* phi,
                                const SceneTri* tris, const Job* jobs, int nJobs, Job* nextJobs, WideNode* wide,
                                float4* packed, int* counters, int wideCapacity, int jobCapacity, int triCapacity,
-                               int group, int width) {
+                               int group, int width, int pieces) {
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= nJobs) return;
     collapseJob(jobs[j], bn, order, plo, phi, tris, nextJobs, wide, packed, counters, wideCapacity, jobCapacity,
-                triCapacity, group, width);
+                triCapacity, group, width, pieces);
 }
 
 inline int blocksFor(long long n, int block) { return (int)((n + block - 1) / block); }
@@ -417,9 +530,14 @@ void freeBvh(BuiltBvh& b) {
     b = BuiltBvh{};
 }
 
-cudaError_t buildBvh(const SceneTri* tris, int n, cudaStream_t stream, BuiltBvh& out, BuildResult& result,
-                     const char** failure, int leafGroup, int width) {
+cudaError_t buildBvh(const SceneTri* tris, int triCount, cudaStream_t stream, BuiltBvh& out, BuildResult& result,
+                     const char** failure, int leafGroup, int width, int pieces) {
     if (width != 4 && width != 8) { *failure = "BVH width must be 4 or 8"; return cudaErrorInvalidValue; }
+    if (pieces < 1 || pieces > 8 || (long long)triCount * pieces > 0x3FFFFFFFll) {
+        *failure = "BVH pieces per triangle must be 1..8";
+        return cudaErrorInvalidValue;
+    }
+    const int n = triCount * pieces;  // primitives: triangles, or triangle pieces for a traversal tree
     *failure = nullptr;
     cudaError_t err = cudaSuccess;
     const int nodeCapacity = 2 * n + 2;
@@ -452,22 +570,31 @@ cudaError_t buildBvh(const SceneTri* tris, int n, cudaStream_t stream, BuiltBvh&
         RT_TRY(cudaMemcpyAsync(tasks, &root, sizeof(Task), cudaMemcpyHostToDevice, stream));
         int init[8] = {1, 0, 0, 0, 0, 0, 0, 0};
         RT_TRY(cudaMemcpyAsync(counters, init, sizeof(init), cudaMemcpyHostToDevice, stream));
-        primBoxesKernel<<<blocksFor(n, 256), 256, 0, stream>>>(tris, n, out.primLo, out.primHi, cent, tasks);
+        if (pieces == 1)
+            primBoxesKernel<<<blocksFor(n, 256), 256, 0, stream>>>(tris, n, out.primLo, out.primHi, cent, tasks);
+        else
+            splitBoxesKernel<<<blocksFor(n, 256), 256, 0, stream>>>(tris, triCount, pieces, out.primLo, out.primHi, cent,
+                                                                    tasks);
         iotaKernel<<<blocksFor(n, 256), 256, 0, stream>>>(out.order, n, 0, posTask, 0);
         RT_TRY(cudaGetLastError());
         int nTasks = 1;
         levelStart.push_back(0);  // depth 0 holds node 0
         levelStart.push_back(1);
+        int bigTasks = n > kSmallTask ? 1 : 0;
         while (nTasks > 0) {
-            clearBinsKernel<<<blocksFor((long long)nTasks * 3 * kBins, 256), 256, 0, stream>>>(bins, nTasks * 3 * kBins);
-            binKernel<<<blocksFor(n, kBinBlock * kBinPer), kBinBlock, 0, stream>>>(out.order, posTask, cent, out.primLo,
-                                                                                    out.primHi, tasks, n, bins);
+            if (bigTasks) {
+                clearBinsKernel<<<blocksFor((long long)nTasks * 3 * kBins, 256), 256, 0, stream>>>(bins, nTasks * 3 * kBins, tasks);
+                binKernel<<<blocksFor(n, kBinBlock * kBinPer), kBinBlock, 0, stream>>>(out.order, posTask, cent, out.primLo,
+                                                                                        out.primHi, tasks, n, bins);
+            }
+            binSmallKernel<<<blocksFor(nTasks, 8), 256, 0, stream>>>(out.order, cent, out.primLo, out.primHi, tasks, nTasks,
+                                                                     bins);
             RT_TRY(cudaMemsetAsync(counters + 1, 0, sizeof(int), stream));
+            RT_TRY(cudaMemsetAsync(counters + 5, 0, sizeof(int), stream));
             splitKernel<<<blocksFor(nTasks, 128), 128, 0, stream>>>(tasks, nTasks, bins, splits, rawNodes, counters,
                                                                     tasksB, nodeCapacity, taskCapacity);
             flagKernel<<<blocksFor(n, 256), 256, 0, stream>>>(out.order, posTask, cent, tasks, splits, n, flags);
-            RT_TRY(cudaMemcpyAsync(prefix, flags, sizeof(unsigned) * n, cudaMemcpyDeviceToDevice, stream));
-            scanBlocksKernel<<<nScanBlocks, 256, 0, stream>>>(prefix, n, blockSums);
+            scanBlocksKernel<<<nScanBlocks, 256, 0, stream>>>(flags, prefix, n, blockSums);
             scanTotalsKernel<<<1, 1024, 0, stream>>>(blockSums, nScanBlocks);
             scatterKernel<<<blocksFor(n, 256), 256, 0, stream>>>(out.order, posTask, tasks, splits, flags, prefix,
                                                                  blockSums, n, orderB, posTaskB, counters + 3);
@@ -478,6 +605,7 @@ cudaError_t buildBvh(const SceneTri* tris, int n, cudaStream_t stream, BuiltBvh&
             std::swap(out.order, orderB); std::swap(posTask, posTaskB); std::swap(tasks, tasksB);
             levelStart.push_back(hostCounters[0]);
             nTasks = hostCounters[1];
+            bigTasks = hostCounters[5];
             if ((int)levelStart.size() > kBinaryMaxDepth + 3) { *failure = "BVH build exceeded the depth limit"; err = cudaErrorUnknown; goto done; }
         }
         int nodeCount = hostCounters[0];
@@ -527,7 +655,7 @@ cudaError_t buildBvh(const SceneTri* tris, int n, cudaStream_t stream, BuiltBvh&
                                                                     jobs, nJobs, jobsB,
                                                                     reinterpret_cast<WideNode*>(out.wideNodes),
                                                                     out.packedTris, counters, wideCapacity, jobCapacity, n,
-                                                                    leafGroup, width);
+                                                                    leafGroup, width, pieces);
             RT_TRY(cudaGetLastError());
             RT_TRY(cudaMemcpyAsync(hostCounters, counters, 8 * sizeof(int), cudaMemcpyDeviceToHost, stream));
             RT_TRY(cudaStreamSynchronize(stream));
@@ -539,6 +667,7 @@ cudaError_t buildBvh(const SceneTri* tris, int n, cudaStream_t stream, BuiltBvh&
         RT_TRY(cudaEventSynchronize(e2));
         if (hostCounters[1] != n) { *failure = "wide BVH collapse lost triangles"; err = cudaErrorUnknown; goto done; }
         result.wideNodes = hostCounters[0];
+        result.packedTriangles = n;
         result.wideDepth = wideDepth;
         RT_TRY(cudaEventElapsedTime(&result.buildMs, e0, e1));
         RT_TRY(cudaEventElapsedTime(&result.collapseMs, e1, e2));

@@ -18,6 +18,7 @@ static_assert(sizeof(SceneTri) == 116, "Triangle layout");
 
 struct BuildResult {
     int binaryNodes = 0, binaryDepth = 0, wideNodes = 0, wideDepth = 0;
+    int packedTriangles = 0;  // entries of packedTris (triangles x pieces)
     float buildMs = 0, collapseMs = 0;
 };
 
@@ -35,9 +36,13 @@ struct BuiltBvh {
 // (cudaSuccess on success) and fills `out`/`result`. `scratchBytes` is the
 // peak temporary memory used, for reporting. Timing uses events on `stream`.
 // leafGroup (1..3): most triangles under one wide-node slot. width (4 or 8):
-// most children per wide node.
+// most children per wide node. pieces (1..8): with more than one, the tree is
+// built over triangle pieces (slabs along each triangle's longest axis, with
+// padded boxes of the part inside) for traversal only: packedTris then holds
+// each triangle once per leaf slot that reaches a piece of it, and the binary
+// nodes are not the reference's.
 cudaError_t buildBvh(const SceneTri* tris, int n, cudaStream_t stream, BuiltBvh& out, BuildResult& result,
-                     const char** failure, int leafGroup = 3, int width = 8);
+                     const char** failure, int leafGroup = 3, int width = 8, int pieces = 1);
 void freeBvh(BuiltBvh& bvh);
 
 }  // namespace rt

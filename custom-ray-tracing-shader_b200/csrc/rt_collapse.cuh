@@ -55,9 +55,11 @@ RT_HD int slotsOf(const BinNode& n, int group, int width) {
 // [2] next-level jobs, [3] error code. Host and device (atomics through
 // portableAdd), so the collapse can be checked on the CPU. width (4 or 8):
 // most children per node; the node format keeps eight slots either way.
+// pieces: primitives per triangle (primitive p belongs to triangle p / pieces).
 RT_HD void collapseJob(Job J, const BinNode* bn, const int* order, const float4* plo, const float4* phi,
                        const SceneTri* tris, Job* nextJobs, WideNode* wide, float4* packed, int* counters,
-                       int wideCapacity, int jobCapacity, int triCapacity, int group, int width = 8) {
+                       int wideCapacity, int jobCapacity, int triCapacity, int group, int width = 8,
+                       int pieces = 1) {
     if (J.kind == 0 && bn[J.node].count > 0) { J.kind = 1; J.first = bn[J.node].first; J.count = bn[J.node].count; }
     Kid kids[8];
     int nk = 0;
@@ -203,7 +205,7 @@ RT_HD void collapseJob(Job J, const BinNode* bn, const int* order, const float4*
         if (K.kind == 2) {
             W.meta[s] = (unsigned char)((((1u << K.count) - 1u) << 5) | (unsigned)triOffset);
             for (int i = 0; i < K.count; i++) {
-                int p = order[K.first + i];
+                int p = order[K.first + i] / pieces;  // the triangle of the primitive
                 const SceneTri& t = tris[p];
                 float4* dst = packed + (size_t)(triBase + triOffset + i) * 3;
                 dst[0] = make_float4(t.origin.x, t.origin.y, t.origin.z, t.edge1.x);

@@ -21,6 +21,9 @@ namespace rt {
 namespace {
 
 constexpr int kTileX = 16, kTileY = 8, kMegaBlock = kTileX * kTileY;
+// Resident blocks per SM the traversal kernels are compiled for: 7 caps them
+// at 72 registers (a few bytes of spills) for 7 instead of 6 blocks per SM.
+constexpr int kTraceMinBlocks = 7;
 
 __global__ void sobolTablesKernel(const unsigned* dirs, unsigned sample0, int rpp, unsigned seed, unsigned* passXor,
                                   unsigned* seedHash) {
@@ -98,7 +101,7 @@ struct ExtendIO {
         hits[queue[k]] = make_float4(h.distance, h.u, h.v, __int_as_float(h.index));
     }
 };
-__global__ void __launch_bounds__(kTraceBlock) extendKernel(const uint4* wide, const float4* packed, WavefrontBuffers B,
+__global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks) extendKernel(const uint4* wide, const float4* packed, WavefrontBuffers B,
                                                             int q, unsigned long long* counter, int* errorFlag,
                                                             int postponeBelow, int refill) {
     ExtendIO io{B.queue[q], B.pathA, B.pathB, B.hits};
@@ -179,7 +182,7 @@ struct ShadowIO {
         radiance[p] = make_float4(rad.x + c.x, rad.y + c.y, rad.z + c.z, rad.w);
     }
 };
-__global__ void __launch_bounds__(kTraceBlock) shadowKernel(const uint4* wide, const float4* packed, WavefrontBuffers B,
+__global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks) shadowKernel(const uint4* wide, const float4* packed, WavefrontBuffers B,
                                                             unsigned long long* counter, int* errorFlag,
                                                             int postponeBelow, int refill) {
     ShadowIO io{B.shadowRay, B.shadowDir, B.shadowContrib, B.radiance};

@@ -35,6 +35,10 @@ static_assert(sizeof(Triangle) == 116 && sizeof(CameraData) == 64 && sizeof(Rend
 static_assert(sizeof(PixelSum) == 40 && sizeof(BvhNode) == 32, "record sizes");
 static_assert(sizeof(RtxQuery) == 28 && sizeof(RtxHit) == 16, "query sizes");
 
+// Pieces per triangle of the traversal tree (RTX_TUNE_PIECES; 1: traverse the
+// collapse of the reference's tree).
+constexpr int kDefaultPieces = 2;
+
 // A denoising network with its last error message (RtxUnet* entry points).
 struct UnetHandle {
     rt::Unet net;
@@ -87,8 +91,11 @@ struct Session {
     unsigned long long* dCounters = nullptr;
     int* dError = nullptr;
     float4* dDenoise = nullptr;
-    BuiltBvh bvh;
+    BuiltBvh bvh;          // the reference's binary tree (RtBvhInfo, RtxExportBvh) and its wide collapse
     BuildResult build;
+    BuiltBvh pieceBvh;     // traversal tree over triangle pieces (when pieces > 1)
+    BuildResult pieceBuild;
+    int pieces = kDefaultPieces;
     WavefrontBuffers wave;
     // Host mirrors for the CPU backends (filled on first use).
     std::vector<Accum> hostSum;
@@ -112,8 +119,16 @@ bool fail(Session* s, cudaError_t e, const char* what = nullptr) {
     return false;
 }
 
+// The tree that traversal uses: over triangle pieces when built, else the
+// collapse of the reference's tree.
+const uint4* travWide(const Session* s) { return s->pieceBvh.wideNodes ? s->pieceBvh.wideNodes : s->bvh.wideNodes; }
+const float4* travPacked(const Session* s) { return s->pieceBvh.wideNodes ? s->pieceBvh.packedTris : s->bvh.packedTris; }
+const BuildResult& travBuild(const Session* s) { return s->pieceBvh.wideNodes ? s->pieceBuild : s->build; }
+
 void releaseScene(Session* s) {
     freeBvh(s->bvh);
+    freeBvh(s->pieceBvh);
+    s->pieceBuild = BuildResult{};
     freeWavefront(s->wave);
     void* owned[] = {s->dTris, s->dLights, s->dDirs, s->dPassXor, s->dSeedHash, s->dSum, s->dDepth, s->dPixels,
                      s->dCounters, s->dError, s->dDenoise};
@@ -151,8 +166,8 @@ bool validSettings(const RenderSettings* st) {
 }
 
 SceneView deviceView(Session* s) {
-    return SceneView{s->dTris, s->bvh.wideNodes, s->bvh.packedTris, s->dLights, s->lightCount, s->lightArea,
-                     s->build.wideDepth, s->environmentMode, s->environment};
+    return SceneView{s->dTris, travWide(s), travPacked(s), s->dLights, s->lightCount, s->lightArea,
+                     travBuild(s).wideDepth, s->environmentMode, s->environment};
 }
 
 bool ensureWave(Session* s) {
@@ -220,11 +235,11 @@ bool ensureHostScene(Session* s) {
 bool ensureHostBvh(Session* s) {
     if (!ensureHostScene(s)) return false;
     if (s->hostBvhReady) return true;
-    s->hostWide.resize((size_t)s->build.wideNodes * 5);
-    s->hostPacked.resize((size_t)s->triCount * 3);
-    cudaError_t e = cudaMemcpy(s->hostWide.data(), s->bvh.wideNodes, s->hostWide.size() * sizeof(uint4), cudaMemcpyDeviceToHost);
+    s->hostWide.resize((size_t)travBuild(s).wideNodes * 5);
+    s->hostPacked.resize((size_t)travBuild(s).packedTriangles * 3);
+    cudaError_t e = cudaMemcpy(s->hostWide.data(), travWide(s), s->hostWide.size() * sizeof(uint4), cudaMemcpyDeviceToHost);
     if (e == cudaSuccess)
-        e = cudaMemcpy(s->hostPacked.data(), s->bvh.packedTris, s->hostPacked.size() * sizeof(float4), cudaMemcpyDeviceToHost);
+        e = cudaMemcpy(s->hostPacked.data(), travPacked(s), s->hostPacked.size() * sizeof(float4), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return fail(s, e);
     s->hostBvhReady = true;
     return true;
@@ -248,7 +263,7 @@ bool renderHost(Session* s, const CameraData* camera, const RenderSettings* sett
     if (s->hostDepth.size() != (size_t)s->width * s->height) s->hostDepth.assign((size_t)s->width * s->height, 0.0f);
     float* depthSums = s->hostDepth.data();
     SceneView sc{s->tris.data(), s->hostWide.data(), s->hostPacked.data(), s->lights.data(), (int)s->lights.size(),
-                 s->lightArea, s->build.wideDepth, s->environmentMode, s->environment};
+                 s->lightArea, travBuild(s).wideDepth, s->environmentMode, s->environment};
     const int w = s->width, h = s->height;
     const unsigned sample0 = s->samples;
     Accum* sums = s->hostSum.data();
@@ -379,6 +394,17 @@ int RtInitialize(void* p, const Triangle* triangles, int count, int width, int h
     RT_CHECK(cudaMalloc(&s->dError, 2 * sizeof(int)));
     const char* why = nullptr;
     e = buildBvh(s->dTris, count, s->stream, s->bvh, s->build, &why);
+    if (e == cudaSuccess && s->pieces > 1) {
+        // Traversal tree over triangle pieces; the reference tree above stays
+        // for RtBvhInfo and RtxExportBvh.
+        e = buildBvh(s->dTris, count, s->stream, s->pieceBvh, s->pieceBuild, &why, 3, 8, s->pieces);
+        if (e == cudaSuccess) {
+            void* unused[] = {s->pieceBvh.binNodes, s->pieceBvh.order, s->pieceBvh.primLo, s->pieceBvh.primHi};
+            for (void* q : unused) cudaFree(q);
+            s->pieceBvh.binNodes = nullptr; s->pieceBvh.order = nullptr;
+            s->pieceBvh.primLo = nullptr; s->pieceBvh.primHi = nullptr;
+        }
+    }
     if (e != cudaSuccess) {
         fail(s, e, why);
         std::string keep = s->hostError;
@@ -482,8 +508,8 @@ int RtxQueryRays(void* p, const RtxQuery* queries, int count, int any, RtxHit* h
     if (e == cudaSuccess) e = cudaMalloc(&dh, sizeof(float4) * (size_t)count);
     if (e == cudaSuccess) e = cudaMemcpyAsync(dq, packed.data(), sizeof(float4) * packed.size(), cudaMemcpyHostToDevice, s->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(s->dError, 0, sizeof(int), s->stream);
-    if (e == cudaSuccess) e = launchQueries(s->bvh.wideNodes, s->bvh.packedTris, dq, count, any, dh, s->dError + 1, s->dError,
-                                            s->build.wideDepth, s->tuning, s->stream);
+    if (e == cudaSuccess) e = launchQueries(travWide(s), travPacked(s), dq, count, any, dh, s->dError + 1, s->dError,
+                                            travBuild(s).wideDepth, s->tuning, s->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(out.data(), dh, sizeof(float4) * (size_t)count, cudaMemcpyDeviceToHost, s->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&overflow, s->dError, sizeof(int), cudaMemcpyDeviceToHost, s->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
@@ -556,8 +582,8 @@ int RtxBvhStatsGet(void* p, RtxBvhStats* out) {
     }
     out->binaryNodes = s->build.binaryNodes;
     out->binaryDepth = s->build.binaryDepth;
-    out->wideNodes = s->build.wideNodes;
-    out->wideDepth = s->build.wideDepth;
+    out->wideNodes = travBuild(s).wideNodes;
+    out->wideDepth = travBuild(s).wideDepth;
     out->buildMs = s->build.buildMs;
     out->collapseMs = s->build.collapseMs;
     out->sahCost = s->sahCost;
@@ -565,6 +591,8 @@ int RtxBvhStatsGet(void* p, RtxBvhStats* out) {
     out->distinctColours = s->upload.distinctColours;
     out->lightCount = s->lightCount;
     out->lightArea = s->lightArea;
+    out->pieces = s->pieceBvh.wideNodes ? s->pieces : 1;
+    out->pieceBuildMs = s->pieceBvh.wideNodes ? s->pieceBuild.buildMs + s->pieceBuild.collapseMs : 0.0f;
     return 1;
 }
 
@@ -743,6 +771,10 @@ int RtxSetTuning(void* p, int key, int value) {
             if (value < 1 || value > 32) return 0;
             s->tuning.refill = value;
             return 1;
+        case RTX_TUNE_PIECES:
+            if (value < 1 || value > 8) return 0;
+            s->pieces = value;  // used by the next RtInitialize
+            return 1;
         default:
             return 0;
     }
@@ -835,8 +867,8 @@ extern "C" int RtxQueryRaysStatic(void* p, const RtxQuery* queries, int count, i
     // The array keeps the previous call's contents: clear the counters.
     if (e == cudaSuccess) e = cudaMemsetAsync(counters, 0, 2 * sizeof(int), s->stream);
     if (e == cudaSuccess)
-        e = launchQueries(s->bvh.wideNodes, s->bvh.packedTris, packed, count, any, deviceHits, counters, counters + 1,
-                          s->build.wideDepth, s->tuning, s->stream);
+        e = launchQueries(travWide(s), travPacked(s), packed, count, any, deviceHits, counters, counters + 1,
+                          travBuild(s).wideDepth, s->tuning, s->stream);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(hits, deviceHits, sizeof(RtxHit) * (size_t)count, cudaMemcpyDeviceToHost, s->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&overflow, counters + 1, sizeof(int), cudaMemcpyDeviceToHost, s->stream);

@@ -64,7 +64,7 @@ class RtxBvhStats(c.Structure):
     _fields_ = [('binaryNodes', c.c_int), ('binaryDepth', c.c_int), ('wideNodes', c.c_int),
                 ('wideDepth', c.c_int), ('buildMs', c.c_float), ('collapseMs', c.c_float),
                 ('sahCost', c.c_double), ('uploadMs', c.c_float), ('distinctColours', c.c_int),
-                ('lightCount', c.c_int), ('lightArea', c.c_float)]
+                ('lightCount', c.c_int), ('lightArea', c.c_float), ('pieces', c.c_int), ('pieceBuildMs', c.c_float)]
 
 
 class RtxBatchTune(c.Structure):
@@ -298,11 +298,12 @@ class Session:
     def set_integrator(self, mode):
         self.check(self.lib.RtxSetIntegrator(self.handle, mode))
 
-    TUNE_PATHS_IN_FLIGHT, TUNE_POSTPONE, TUNE_REFILL = 1, 2, 3
+    TUNE_PATHS_IN_FLIGHT, TUNE_POSTPONE, TUNE_REFILL, TUNE_PIECES = 1, 2, 3, 4
 
-    def set_tuning(self, paths_in_flight=None, postpone=None, refill=None):
+    def set_tuning(self, paths_in_flight=None, postpone=None, refill=None, pieces=None):
+        """pieces applies from the next initialize()."""
         for key, value in ((self.TUNE_PATHS_IN_FLIGHT, paths_in_flight), (self.TUNE_POSTPONE, postpone),
-                           (self.TUNE_REFILL, refill)):
+                           (self.TUNE_REFILL, refill), (self.TUNE_PIECES, pieces)):
             if value is not None:
                 self.check(self.lib.RtxSetTuning(self.handle, key, int(value)))
 
@@ -416,7 +417,7 @@ class Unet:
 class Batch:
     """Many views of many scenes rendered together (RtxBatch* entry points)."""
 
-    BLOCK, CAPACITY, REFILL, GRAPH, WIDTH = 1, 2, 3, 4, 5
+    BLOCK, CAPACITY, REFILL, GRAPH, WIDTH, PIECES = 1, 2, 3, 4, 5, 6
 
     def __init__(self, lib=None):
         self.lib = lib or load_library()
@@ -483,9 +484,9 @@ class Batch:
         self.check(self.lib.RtxBatchReadAccumulation(self.handle, view, out.ctypes.data, out.size))
         return out
 
-    def set_tuning(self, block=None, capacity=None, refill=None, graph=None, width=None):
+    def set_tuning(self, block=None, capacity=None, refill=None, graph=None, width=None, pieces=None):
         for key, value in ((self.BLOCK, block), (self.CAPACITY, capacity), (self.REFILL, refill),
-                           (self.GRAPH, graph), (self.WIDTH, width)):
+                           (self.GRAPH, graph), (self.WIDTH, width), (self.PIECES, pieces)):
             if value is not None:
                 self.check(self.lib.RtxBatchSetTuning(self.handle, key, int(value)))
 

@@ -94,7 +94,7 @@ typedef struct RtxBvhStats {
     int binaryNodes;        /* reference-layout nodes (same count as Native/bvh.cuh) */
     int binaryDepth;        /* deepest binary node (the reference's maxDepth) */
     int wideNodes;          /* 8-wide compressed nodes used for traversal */
-    int wideDepth;          /* deepest wide node */
+    int wideDepth;          /* deepest wide node of the traversal tree */
     float buildMs;          /* device time of the binned-SAH build (CUDA events) */
     float collapseMs;       /* device time of the wide collapse and triangle packing */
     double sahCost;         /* SAH cost of the binary tree, normalised by the root area */
@@ -102,6 +102,8 @@ typedef struct RtxBvhStats {
     int distinctColours;    /* colour values decoded through the host's powf (the rest on the device) */
     int lightCount;         /* emitting triangles */
     float lightArea;        /* their total area */
+    int pieces;             /* pieces per triangle of the traversal tree (1: the reference's tree) */
+    float pieceBuildMs;     /* device time of the traversal tree's build and collapse (0 with 1 piece) */
 } RtxBvhStats;
 
 /* ---- the reference's thirteen exports ---- */
@@ -175,10 +177,20 @@ int RtxSetIntegrator(void* session, int mode);
  *   RTX_TUNE_POSTPONE         1 = postpone triangle tests in sparse warps,
  *                             0 = off (default)
  *   RTX_TUNE_REFILL           refill a warp's idle lanes when fewer than this
- *                             many lanes are busy (1..32, default 24) */
+ *                             many lanes are busy (1..32, default 24)
+ *   RTX_TUNE_PIECES           pieces per triangle of the traversal tree (1..8,
+ *                             default 2; applies from the next RtInitialize):
+ *                             each triangle is cut into slabs along the longest
+ *                             axis of its box and the traversal tree is built
+ *                             over the pieces' padded boxes, which overlap less
+ *                             than whole triangles' boxes; the reference's tree
+ *                             is still built for RtBvhInfo and RtxExportBvh,
+ *                             and hits do not depend on the tree
+ */
 #define RTX_TUNE_PATHS_IN_FLIGHT 1
 #define RTX_TUNE_POSTPONE 2
 #define RTX_TUNE_REFILL 3
+#define RTX_TUNE_PIECES 4
 int RtxSetTuning(void* session, int key, int value);
 /* Light arriving from outside the scene on rays that leave it after the first
  * bounce (primary misses stay black, as in the reference). mode 0: the
@@ -247,6 +259,7 @@ int RtxReadAovs(void* session, float* aovs, int count);
 #define RTX_BATCH_REFILL 3    /* refill threshold of the persistent traversal (1..32) */
 #define RTX_BATCH_GRAPH 4     /* 1: replay frames from a CUDA graph (default), 0: launch kernels */
 #define RTX_BATCH_WIDTH 5     /* BVH node width: 4 or 8 (default 8); rebuilds every scene */
+#define RTX_BATCH_PIECES 6    /* pieces per triangle of the traversal trees (1..8, default 2; see RTX_TUNE_PIECES) */
 typedef struct RtxBatchTune {
     int block, capacity, refill, width;
     float frameMs;  /* device time of one frame of one path per pixel */

@@ -56,9 +56,14 @@ def test_gpu_bvh_equals_reference(session, oracle, name):
     assert stats['wideDepth'] <= 48
 
 
+@pytest.mark.parametrize('pieces', (1, 2, 3, 8))
 @pytest.mark.parametrize('name', SETS)
-def test_gpu_queries_equal_reference(session, name):
+def test_gpu_queries_equal_reference(session, name, pieces):
+    """Bit-exact against the reference's traversal whatever tree traversal
+    uses: the reference's own (1 piece per triangle) or trees over 2, 3 or 8
+    padded pieces per triangle (2 is the default)."""
     g = golden(f'bvh_{name}.npz')
+    session.set_tuning(pieces=pieces)
     session.initialize(GEOMETRY[name], 8, 8)
     closest = session.query(RAYS, any_hit=False)
     assert closest.tobytes() == g['closest'].tobytes()
@@ -261,3 +266,19 @@ def test_gpu_upload_matches_host_preparation(session, oracle, reference):
         assert np.abs(cpu.astype(int) - gpu.astype(int)).max() <= 1
     finally:
         ref.close()
+
+
+def test_gpu_piece_trees_render_identically(session):
+    """Accumulations do not depend on the traversal tree: 1, 2 and 4 pieces
+    per triangle give the same bytes; the reference's tree is still what
+    RtBvhInfo reports and RtxExportBvh returns."""
+    tris, cam, st, _, _ = scenes.displaced_sphere_room(subdivisions=40, width=64, height=48)
+    cam.aspect = 64 / 48
+    out = {}
+    for pieces in (1, 2, 4):
+        session.set_tuning(pieces=pieces)
+        session.initialize(tris, 64, 48)
+        session.render(cam, st)
+        session.render(cam, st)
+        out[pieces] = (session.accumulation().tobytes(), session.bvh_info()[:2], session.export_bvh(len(tris))[0].tobytes())
+    assert out[1] == out[2] == out[4]
