@@ -64,11 +64,13 @@ def parse():
     p.add_argument('--no-batch', dest='batch', action='store_false',
                    help='skip batched multi-scene tracing (8 scenes, 64 views; 1 GPU runs it by default)')
     p.add_argument('--batch-frames', type=int, default=3)
+    p.add_argument('--no-denoiser', dest='denoiser', action='store_false',
+                   help='skip the learned-denoiser inference timing (1 GPU runs it by default)')
     p.add_argument('--pieces', type=int, default=None,
                    help='pieces per triangle of the traversal tree (RTX_TUNE_PIECES; default: the library default)')
     p.add_argument('--denoiser-only', action='store_true',
                    help='only time learned-denoiser inference at 1920x1080 (a small case for profiling)')
-    p.set_defaults(quality=True, batch=True)
+    p.set_defaults(quality=True, batch=True, denoiser=True)
     return p.parse_args()
 
 
@@ -684,7 +686,7 @@ def run_ours(args, rank, local_rank, world):
             'reference_cuda': ref_cuda,
             'time_to_35db': quality_run(lib, args) if (args.quality and world == 1) else None,
             'batch': batch_run(lib, args) if (args.batch and world == 1) else None,
-            'denoiser': denoiser_run(lib, args) if world == 1 else None,
+            'denoiser': denoiser_run(lib, args) if (args.denoiser and world == 1) else None,
         }
     s.close()
     dist.close()
