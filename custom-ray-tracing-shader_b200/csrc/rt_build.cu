@@ -665,9 +665,15 @@ cudaError_t buildBvh(const SceneTri* tris, int triCount, cudaStream_t stream, Bu
         }
         RT_TRY(cudaEventRecord(e2, stream));
         RT_TRY(cudaEventSynchronize(e2));
-        if (hostCounters[1] != n) { *failure = "wide BVH collapse lost triangles"; err = cudaErrorUnknown; goto done; }
+        // Every primitive is packed once, except pieces of a triangle that
+        // share a leaf group (packed once for the group).
+        if (pieces == 1 ? hostCounters[1] != n : (hostCounters[1] < triCount || hostCounters[1] > n)) {
+            *failure = "wide BVH collapse lost triangles";
+            err = cudaErrorUnknown;
+            goto done;
+        }
         result.wideNodes = hostCounters[0];
-        result.packedTriangles = n;
+        result.packedTriangles = hostCounters[1];
         result.wideDepth = wideDepth;
         RT_TRY(cudaEventElapsedTime(&result.buildMs, e0, e1));
         RT_TRY(cudaEventElapsedTime(&result.collapseMs, e1, e2));

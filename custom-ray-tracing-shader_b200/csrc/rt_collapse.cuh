@@ -161,8 +161,21 @@ RT_HD void collapseJob(Job J, const BinNode* bn, const int* order, const float4*
             kidUsed[bk] = true; slotKid[bs] = bk;
         }
     }
+    // Triangles of each triangle group, once each: pieces of one triangle in
+    // the same group would only repeat its test (the group's box covers them).
+    int groupTris[8][3], groupCount[8];
     int nInterior = 0, nTris = 0;
-    for (int k = 0; k < nk; k++) { if (kids[k].kind == 2) nTris += kids[k].count; else nInterior++; }
+    for (int k = 0; k < nk; k++) {
+        groupCount[k] = 0;
+        if (kids[k].kind != 2) { nInterior++; continue; }
+        for (int i = 0; i < kids[k].count; i++) {
+            const int tri = order[kids[k].first + i] / pieces;
+            bool seen = false;
+            for (int j = 0; j < groupCount[k]; j++) seen = seen || groupTris[k][j] == tri;
+            if (!seen) groupTris[k][groupCount[k]++] = tri;
+        }
+        nTris += groupCount[k];
+    }
     int childBase = nInterior ? portableAdd(&counters[0], nInterior) : 0;
     int triBase = nTris ? portableAdd(&counters[1], nTris) : 0;
     if (childBase + nInterior > wideCapacity || triBase + nTris > triCapacity) { portableSet(&counters[3], 3); return; }
@@ -203,16 +216,17 @@ RT_HD void collapseJob(Job J, const BinNode* bn, const int* order, const float4*
             W.qhi[a][s] = (unsigned char)qh;
         }
         if (K.kind == 2) {
-            W.meta[s] = (unsigned char)((((1u << K.count) - 1u) << 5) | (unsigned)triOffset);
-            for (int i = 0; i < K.count; i++) {
-                int p = order[K.first + i] / pieces;  // the triangle of the primitive
+            const int count = groupCount[k];
+            W.meta[s] = (unsigned char)((((1u << count) - 1u) << 5) | (unsigned)triOffset);
+            for (int i = 0; i < count; i++) {
+                const int p = groupTris[k][i];  // the triangle
                 const SceneTri& t = tris[p];
                 float4* dst = packed + (size_t)(triBase + triOffset + i) * 3;
                 dst[0] = make_float4(t.origin.x, t.origin.y, t.origin.z, t.edge1.x);
                 dst[1] = make_float4(t.edge1.y, t.edge1.z, t.edge2.x, t.edge2.y);
                 dst[2] = make_float4(t.edge2.z, bitsToFloat(t.oneSided != 0 ? 1u : 0u), bitsToFloat((unsigned)p), 0.0f);
             }
-            triOffset += K.count;
+            triOffset += count;
         } else {
             W.meta[s] = (unsigned char)(0x20u | (24u + (unsigned)s));
             W.imask |= (unsigned char)(1u << s);
