@@ -356,7 +356,7 @@ struct Batch {
     int* dError = nullptr;
     WavefrontBuffers wave;
     // Tuning.
-    int block = 128, capacity = 0, refill = 24, width = 8, useGraph = 1, pieces = 2;
+    int block = 128, capacity = 0, refill = 24, width = 8, useGraph = 1, pieces = 3;
     int environmentMode = 0;
     float3 environment = make_float3(0.0f, 0.0f, 0.0f);
     // Frame state.
@@ -839,13 +839,14 @@ int RtxBatchAutotune(void* p, const RenderSettings* settings, RtxBatchTune* resu
             if (!renderFrame(b, &probe, &ms)) return false;
             if (i > 0) best = std::min(best, ms);
         }
-        tried.push_back(RtxBatchTune{b->block, waveCapacity(b), b->refill, b->width, best});
+        tried.push_back(RtxBatchTune{b->block, waveCapacity(b), b->refill, b->width, best, b->pieces});
         return true;
     };
     auto trial = [&](int key, int value, float& ms) -> bool {
         return RtxBatchSetTuning(b, key, value) && measure(ms);
     };
-    // Coordinate search: BVH width, block size, queue capacity, refill.
+    // Coordinate search: pieces per triangle, BVH width, block size, queue
+    // capacity, refill.
     float bestMs = 0;
     if (!measure(bestMs)) return 0;
     struct Axis { int key; std::vector<int> values; int* current; };
@@ -853,7 +854,8 @@ int RtxBatchAutotune(void* p, const RenderSettings* settings, RtxBatchTune* resu
     for (long long c : {262144ll, 1048576ll, 4194304ll, 16777216ll})
         if (c < (long long)b->pixels || caps.empty()) caps.push_back((int)std::min<long long>(c, (long long)b->pixels));
     if ((long long)b->pixels <= 16777216ll && caps.back() != (int)b->pixels) caps.push_back((int)b->pixels);
-    Axis axes[] = {{RTX_BATCH_WIDTH, {8, 4}, &b->width},
+    Axis axes[] = {{RTX_BATCH_PIECES, {3, 1, 2}, &b->pieces},
+                   {RTX_BATCH_WIDTH, {8, 4}, &b->width},
                    {RTX_BATCH_BLOCK, {64, 128, 256}, &b->block},
                    {RTX_BATCH_CAPACITY, caps, &b->capacity},
                    {RTX_BATCH_REFILL, {8, 16, 24, 32}, &b->refill}};
@@ -885,6 +887,7 @@ int RtxBatchStatsGet(void* p, RtxBatchStats* stats) {
     b->stats.capacity = b->viewsReady ? waveCapacity(b) : b->capacity;
     b->stats.refill = b->refill;
     b->stats.width = b->width;
+    b->stats.pieces = b->pieces;
     *stats = b->stats;
     return 1;
 }

@@ -115,14 +115,49 @@ __global__ void primBoxesKernel(const SceneTri* tris, int n, float4* plo, float4
 // the rounding of the clipping, so every point of the triangle lies in the
 // padded box of a piece containing it, and the union of the pieces' boxes
 // covers the triangle's padded box's content that traversal can reach.
-__global__ void splitBoxesKernel(const SceneTri* tris, int n, int pieces, float4* plo, float4* phi, float4* cent,
-                                 Task* root) {
+// Pieces of one triangle: the half area of its box over its own area tells
+// how much empty space the box holds. Well-shaped triangles (ratio below 12;
+// all but a fraction of a percent of ordinary meshes' triangles) stay whole;
+// slivers get floor(ratio / 6) pieces, at most maxPieces.
+__device__ int piecesOf(const SceneTri& t, int maxPieces) {
+    const float3 e1 = t.edge1, e2 = t.edge2;
+    const float ex = fmaxf(fmaxf(0.0f, e1.x), e2.x) - fminf(fminf(0.0f, e1.x), e2.x);
+    const float ey = fmaxf(fmaxf(0.0f, e1.y), e2.y) - fminf(fminf(0.0f, e1.y), e2.y);
+    const float ez = fmaxf(fmaxf(0.0f, e1.z), e2.z) - fminf(fminf(0.0f, e1.z), e2.z);
+    const float boxArea = ex * ey + ey * ez + ex * ez;
+    const float3 c = cross(e1, e2);
+    const float triArea = 0.5f * sqrtf(dot(c, c));
+    if (!(triArea > 0.0f) || !(boxArea < FLT_MAX)) return 1;
+    const float k = boxArea / triArea / 6.0f;
+    return k >= (float)maxPieces ? maxPieces : (k >= 2.0f ? (int)k : 1);
+}
+__global__ void pieceCountKernel(const SceneTri* tris, int n, int maxPieces, unsigned* counts) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) counts[i] = (unsigned)piecesOf(tris[i], maxPieces);
+}
+// primTri[first piece of i + s] = i, from the exclusive scan of the counts
+// (block-local prefix plus the block's total).
+__global__ void pieceFillKernel(const unsigned* counts, const unsigned* prefix, const unsigned* blockSums, int n,
+                                int* primTri, int* total) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const unsigned first = prefix[i] + blockSums[i / kScanBlock];
+    if (primTri)
+        for (unsigned s = 0; s < counts[i]; s++) primTri[first + s] = i;
+    if (i == n - 1) *total = (int)(first + counts[i]);
+}
+
+__global__ void splitBoxesKernel(const SceneTri* tris, const int* primTri, int nPrims, int maxPieces, float4* plo,
+                                 float4* phi, float4* cent, Task* root) {
     int r = blockIdx.x * blockDim.x + threadIdx.x;
     float v[12];
     for (int k = 0; k < 3; k++) { v[k] = FLT_MAX; v[3 + k] = -FLT_MAX; v[6 + k] = FLT_MAX; v[9 + k] = -FLT_MAX; }
-    if (r < n * pieces) {
-        const int i = r / pieces, s = r % pieces;
+    if (r < nPrims) {
+        const int i = primTri[r];
         const SceneTri& t = tris[i];
+        const int pieces = piecesOf(t, maxPieces);
+        int s = 0;  // which piece: primitives of a triangle are consecutive
+        while (s < r && s < pieces - 1 && primTri[r - s - 1] == i) s++;
         float3 P[3] = {t.origin, v3(t.origin.x + t.edge1.x, t.origin.y + t.edge1.y, t.origin.z + t.edge1.z),
                        v3(t.origin.x + t.edge2.x, t.origin.y + t.edge2.y, t.origin.z + t.edge2.z)};
         float tlo[3], thi[3];
@@ -509,11 +544,11 @@ __global__ void renumberKernel(const BinNode* nodes, int count, const int* newIn
 __global__ void collapseKernel(const BinNode* bn, const int* order, const float4* plo, const float4* phi,
                                const SceneTri* tris, const Job* jobs, int nJobs, Job* nextJobs, WideNode* wide,
                                float4* packed, int* counters, int wideCapacity, int jobCapacity, int triCapacity,
-                               int group, int width, int pieces) {
+                               int group, int width, const int* primTri) {
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= nJobs) return;
     collapseJob(jobs[j], bn, order, plo, phi, tris, nextJobs, wide, packed, counters, wideCapacity, jobCapacity,
-                triCapacity, group, width, pieces);
+                triCapacity, group, width, primTri);
 }
 
 inline int blocksFor(long long n, int block) { return (int)((n + block - 1) / block); }
@@ -530,6 +565,38 @@ void freeBvh(BuiltBvh& b) {
     b = BuiltBvh{};
 }
 
+cudaError_t pieceMap(const SceneTri* tris, int triCount, int maxPieces, cudaStream_t stream, int** primTri, int* total) {
+    unsigned *counts = nullptr, *pfx = nullptr, *sums = nullptr;
+    int* dTotal = nullptr;
+    const int nb = blocksFor(triCount, kScanBlock);
+    int hostTotal = 0;
+    if (primTri) *primTri = nullptr;
+    cudaError_t err = alloc(counts, triCount);
+    if (err == cudaSuccess) err = alloc(pfx, triCount);
+    if (err == cudaSuccess) err = alloc(sums, nb);
+    if (err == cudaSuccess) err = alloc(dTotal, 1);
+    if (err == cudaSuccess) {
+        pieceCountKernel<<<blocksFor(triCount, 256), 256, 0, stream>>>(tris, triCount, maxPieces, counts);
+        scanBlocksKernel<<<nb, 256, 0, stream>>>(counts, pfx, triCount, sums);
+        scanTotalsKernel<<<1, 1024, 0, stream>>>(sums, nb);
+        err = cudaGetLastError();
+    }
+    int* map = nullptr;
+    if (err == cudaSuccess && primTri) err = alloc(map, (size_t)triCount * maxPieces);
+    if (err == cudaSuccess) {
+        pieceFillKernel<<<blocksFor(triCount, 256), 256, 0, stream>>>(counts, pfx, sums, triCount, map, dTotal);
+        err = cudaGetLastError();
+    }
+    if (err == cudaSuccess) err = cudaMemcpyAsync(&hostTotal, dTotal, sizeof(int), cudaMemcpyDeviceToHost, stream);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(stream);
+    cudaFree(counts); cudaFree(pfx); cudaFree(sums); cudaFree(dTotal);
+    if (err == cudaSuccess && (hostTotal < triCount || hostTotal > triCount * maxPieces)) err = cudaErrorUnknown;
+    if (err != cudaSuccess) { cudaFree(map); return err; }
+    if (primTri) *primTri = map;
+    *total = hostTotal;
+    return cudaSuccess;
+}
+
 cudaError_t buildBvh(const SceneTri* tris, int triCount, cudaStream_t stream, BuiltBvh& out, BuildResult& result,
                      const char** failure, int leafGroup, int width, int pieces) {
     if (width != 4 && width != 8) { *failure = "BVH width must be 4 or 8"; return cudaErrorInvalidValue; }
@@ -537,9 +604,24 @@ cudaError_t buildBvh(const SceneTri* tris, int triCount, cudaStream_t stream, Bu
         *failure = "BVH pieces per triangle must be 1..8";
         return cudaErrorInvalidValue;
     }
-    const int n = triCount * pieces;  // primitives: triangles, or triangle pieces for a traversal tree
     *failure = nullptr;
     cudaError_t err = cudaSuccess;
+    // Primitives: the triangles, or for a traversal tree their pieces
+    // (piecesOf each, consecutive, primTri[p] = triangle of primitive p).
+    int n = triCount;
+    int* primTri = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
+    if ((err = cudaEventCreate(&e0)) != cudaSuccess || (err = cudaEventRecord(e0, stream)) != cudaSuccess) return err;
+    if (pieces > 1) {
+        int total = 0;
+        err = pieceMap(tris, triCount, pieces, stream, &primTri, &total);
+        if (err != cudaSuccess) { cudaEventDestroy(e0); *failure = "triangle pieces"; return err; }
+        if (total == triCount) {  // no triangle is split: a tree over the triangles themselves
+            cudaFree(primTri);
+            primTri = nullptr;
+        }
+        n = total;
+    }
     const int nodeCapacity = 2 * n + 2;
     const int taskCapacity = n / (kLeafSize + 1) + 2;
     // Temporaries.
@@ -549,7 +631,6 @@ cudaError_t buildBvh(const SceneTri* tris, int triCount, cudaStream_t stream, Bu
     BinNode* rawNodes = nullptr; int* interior = nullptr; int* rank = nullptr; int* newIndex = nullptr;
     Job* jobs = nullptr; Job* jobsB = nullptr;
     int* hostCounters = nullptr;
-    cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
     std::vector<int> levelStart;
     int nScanBlocks = blocksFor(n, kScanBlock);
 
@@ -561,8 +642,7 @@ cudaError_t buildBvh(const SceneTri* tris, int triCount, cudaStream_t stream, Bu
     RT_TRY(alloc(flags, n)); RT_TRY(alloc(prefix, n)); RT_TRY(alloc(blockSums, nScanBlocks));
     RT_TRY(alloc(counters, 8)); RT_TRY(alloc(rawNodes, nodeCapacity));
     RT_TRY(cudaMallocHost(reinterpret_cast<void**>(&hostCounters), 8 * sizeof(int)));
-    RT_TRY(cudaEventCreate(&e0)); RT_TRY(cudaEventCreate(&e1)); RT_TRY(cudaEventCreate(&e2));
-    RT_TRY(cudaEventRecord(e0, stream));
+    RT_TRY(cudaEventCreate(&e1)); RT_TRY(cudaEventCreate(&e2));
     {
         Task root{};
         root.node = 0; root.first = 0; root.count = n; root.depth = 0;
@@ -570,11 +650,11 @@ cudaError_t buildBvh(const SceneTri* tris, int triCount, cudaStream_t stream, Bu
         RT_TRY(cudaMemcpyAsync(tasks, &root, sizeof(Task), cudaMemcpyHostToDevice, stream));
         int init[8] = {1, 0, 0, 0, 0, 0, 0, 0};
         RT_TRY(cudaMemcpyAsync(counters, init, sizeof(init), cudaMemcpyHostToDevice, stream));
-        if (pieces == 1)
+        if (!primTri)
             primBoxesKernel<<<blocksFor(n, 256), 256, 0, stream>>>(tris, n, out.primLo, out.primHi, cent, tasks);
         else
-            splitBoxesKernel<<<blocksFor(n, 256), 256, 0, stream>>>(tris, triCount, pieces, out.primLo, out.primHi, cent,
-                                                                    tasks);
+            splitBoxesKernel<<<blocksFor(n, 256), 256, 0, stream>>>(tris, primTri, n, pieces, out.primLo, out.primHi,
+                                                                    cent, tasks);
         iotaKernel<<<blocksFor(n, 256), 256, 0, stream>>>(out.order, n, 0, posTask, 0);
         RT_TRY(cudaGetLastError());
         int nTasks = 1;
@@ -655,7 +735,7 @@ cudaError_t buildBvh(const SceneTri* tris, int triCount, cudaStream_t stream, Bu
                                                                     jobs, nJobs, jobsB,
                                                                     reinterpret_cast<WideNode*>(out.wideNodes),
                                                                     out.packedTris, counters, wideCapacity, jobCapacity, n,
-                                                                    leafGroup, width, pieces);
+                                                                    leafGroup, width, primTri);
             RT_TRY(cudaGetLastError());
             RT_TRY(cudaMemcpyAsync(hostCounters, counters, 8 * sizeof(int), cudaMemcpyDeviceToHost, stream));
             RT_TRY(cudaStreamSynchronize(stream));
@@ -667,7 +747,7 @@ cudaError_t buildBvh(const SceneTri* tris, int triCount, cudaStream_t stream, Bu
         RT_TRY(cudaEventSynchronize(e2));
         // Every primitive is packed once, except pieces of a triangle that
         // share a leaf group (packed once for the group).
-        if (pieces == 1 ? hostCounters[1] != n : (hostCounters[1] < triCount || hostCounters[1] > n)) {
+        if (!primTri ? hostCounters[1] != n : (hostCounters[1] < triCount || hostCounters[1] > n)) {
             *failure = "wide BVH collapse lost triangles";
             err = cudaErrorUnknown;
             goto done;
@@ -683,6 +763,7 @@ done:
     cudaFree(cent); cudaFree(orderB); cudaFree(posTask); cudaFree(posTaskB); cudaFree(tasks); cudaFree(tasksB);
     cudaFree(bins); cudaFree(splits); cudaFree(flags); cudaFree(prefix); cudaFree(blockSums); cudaFree(counters);
     cudaFree(rawNodes); cudaFree(interior); cudaFree(rank); cudaFree(newIndex); cudaFree(jobs); cudaFree(jobsB);
+    cudaFree(primTri);
     if (hostCounters) cudaFreeHost(hostCounters);
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);

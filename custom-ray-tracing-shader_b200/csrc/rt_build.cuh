@@ -37,12 +37,17 @@ struct BuiltBvh {
 // peak temporary memory used, for reporting. Timing uses events on `stream`.
 // leafGroup (1..3): most triangles under one wide-node slot. width (4 or 8):
 // most children per wide node. pieces (1..8): with more than one, the tree is
-// built over triangle pieces (slabs along each triangle's longest axis, with
-// padded boxes of the part inside) for traversal only: packedTris then holds
-// each triangle once per leaf slot that reaches a piece of it, and the binary
-// nodes are not the reference's.
+// built over triangle pieces for traversal only: triangles whose box holds
+// much empty space (box half area over triangle area of 12 or more) are cut
+// into up to `pieces` slabs along their box's longest axis, each with the
+// padded box of its part; packedTris then holds a triangle once per leaf slot
+// that reaches a piece of it, and the binary nodes are not the reference's.
 cudaError_t buildBvh(const SceneTri* tris, int n, cudaStream_t stream, BuiltBvh& out, BuildResult& result,
                      const char** failure, int leafGroup = 3, int width = 8, int pieces = 1);
 void freeBvh(BuiltBvh& bvh);
+// Pieces of a traversal tree over n triangles with at most maxPieces per
+// triangle: *total primitives and, when primTri is not null, a device array
+// (allocated here, cudaFree it) of each primitive's triangle. Synchronises.
+cudaError_t pieceMap(const SceneTri* tris, int n, int maxPieces, cudaStream_t stream, int** primTri, int* total);
 
 }  // namespace rt

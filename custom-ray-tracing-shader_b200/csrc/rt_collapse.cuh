@@ -55,11 +55,12 @@ RT_HD int slotsOf(const BinNode& n, int group, int width) {
 // [2] next-level jobs, [3] error code. Host and device (atomics through
 // portableAdd), so the collapse can be checked on the CPU. width (4 or 8):
 // most children per node; the node format keeps eight slots either way.
-// pieces: primitives per triangle (primitive p belongs to triangle p / pieces).
+// primTri: the triangle of each primitive when primitives are triangle pieces
+// (null: primitive p is triangle p).
 RT_HD void collapseJob(Job J, const BinNode* bn, const int* order, const float4* plo, const float4* phi,
                        const SceneTri* tris, Job* nextJobs, WideNode* wide, float4* packed, int* counters,
                        int wideCapacity, int jobCapacity, int triCapacity, int group, int width = 8,
-                       int pieces = 1) {
+                       const int* primTri = nullptr) {
     if (J.kind == 0 && bn[J.node].count > 0) { J.kind = 1; J.first = bn[J.node].first; J.count = bn[J.node].count; }
     Kid kids[8];
     int nk = 0;
@@ -169,7 +170,8 @@ RT_HD void collapseJob(Job J, const BinNode* bn, const int* order, const float4*
         groupCount[k] = 0;
         if (kids[k].kind != 2) { nInterior++; continue; }
         for (int i = 0; i < kids[k].count; i++) {
-            const int tri = order[kids[k].first + i] / pieces;
+            const int prim = order[kids[k].first + i];
+            const int tri = primTri ? primTri[prim] : prim;
             bool seen = false;
             for (int j = 0; j < groupCount[k]; j++) seen = seen || groupTris[k][j] == tri;
             if (!seen) groupTris[k][groupCount[k]++] = tri;

@@ -37,7 +37,7 @@ static_assert(sizeof(RtxQuery) == 28 && sizeof(RtxHit) == 16, "query sizes");
 
 // Pieces per triangle of the traversal tree (RTX_TUNE_PIECES; 1: traverse the
 // collapse of the reference's tree).
-constexpr int kDefaultPieces = 2;
+constexpr int kDefaultPieces = 3;
 
 // A denoising network with its last error message (RtxUnet* entry points).
 struct UnetHandle {
@@ -394,7 +394,9 @@ int RtInitialize(void* p, const Triangle* triangles, int count, int width, int h
     RT_CHECK(cudaMalloc(&s->dError, 2 * sizeof(int)));
     const char* why = nullptr;
     e = buildBvh(s->dTris, count, s->stream, s->bvh, s->build, &why);
-    if (e == cudaSuccess && s->pieces > 1) {
+    int pieceTotal = count;
+    if (e == cudaSuccess && s->pieces > 1) e = pieceMap(s->dTris, count, s->pieces, s->stream, nullptr, &pieceTotal);
+    if (e == cudaSuccess && pieceTotal > count) {
         // Traversal tree over triangle pieces; the reference tree above stays
         // for RtBvhInfo and RtxExportBvh.
         e = buildBvh(s->dTris, count, s->stream, s->pieceBvh, s->pieceBuild, &why, 3, 8, s->pieces);

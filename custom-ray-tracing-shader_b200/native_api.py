@@ -69,7 +69,7 @@ class RtxBvhStats(c.Structure):
 
 class RtxBatchTune(c.Structure):
     _fields_ = [('block', c.c_int), ('capacity', c.c_int), ('refill', c.c_int), ('width', c.c_int),
-                ('frameMs', c.c_float)]
+                ('frameMs', c.c_float), ('pieces', c.c_int)]
 
 
 class RtxBatchStats(c.Structure):
@@ -77,11 +77,11 @@ class RtxBatchStats(c.Structure):
                 ('paths', c.c_ulonglong), ('frameMs', c.c_float), ('buildMs', c.c_float),
                 ('triangles', c.c_longlong), ('pixels', c.c_longlong), ('scenes', c.c_int), ('views', c.c_int),
                 ('kernelLaunches', c.c_int), ('graph', c.c_int), ('block', c.c_int), ('capacity', c.c_int),
-                ('refill', c.c_int), ('width', c.c_int)]
+                ('refill', c.c_int), ('width', c.c_int), ('pieces', c.c_int)]
 
 
 assert (c.sizeof(Triangle), c.sizeof(Camera), c.sizeof(Settings)) == (116, 64, 28)
-assert (c.sizeof(RtxBatchTune), c.sizeof(RtxBatchStats)) == (20, 88)
+assert (c.sizeof(RtxBatchTune), c.sizeof(RtxBatchStats)) == (24, 96)
 assert (c.sizeof(PixelSum), c.sizeof(BvhNode), c.sizeof(RtxQuery), c.sizeof(RtxHit)) == (40, 32, 28, 16)
 
 # numpy views of the same records, for scenes of millions of triangles.

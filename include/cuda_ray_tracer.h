@@ -178,14 +178,18 @@ int RtxSetIntegrator(void* session, int mode);
  *                             0 = off (default)
  *   RTX_TUNE_REFILL           refill a warp's idle lanes when fewer than this
  *                             many lanes are busy (1..32, default 24)
- *   RTX_TUNE_PIECES           pieces per triangle of the traversal tree (1..8,
- *                             default 2; applies from the next RtInitialize):
- *                             each triangle is cut into slabs along the longest
- *                             axis of its box and the traversal tree is built
- *                             over the pieces' padded boxes, which overlap less
- *                             than whole triangles' boxes; the reference's tree
- *                             is still built for RtBvhInfo and RtxExportBvh,
- *                             and hits do not depend on the tree
+ *   RTX_TUNE_PIECES           most pieces per triangle of the traversal tree
+ *                             (1..8, default 3; applies from the next
+ *                             RtInitialize): triangles whose box holds much
+ *                             empty space (box half area at least 12 times the
+ *                             triangle's area) are cut into slabs along the
+ *                             longest axis of their box, and the traversal tree
+ *                             is built over the pieces' padded boxes, which
+ *                             overlap less than the whole triangles' boxes; with
+ *                             no such triangle, traversal uses the reference's
+ *                             tree. The reference's tree is always built for
+ *                             RtBvhInfo and RtxExportBvh; hits do not depend on
+ *                             the tree
  */
 #define RTX_TUNE_PATHS_IN_FLIGHT 1
 #define RTX_TUNE_POSTPONE 2
@@ -249,8 +253,8 @@ int RtxReadAovs(void* session, float* aovs, int count);
  *   RtxBatchReadImage / RtxBatchReadAccumulation  one view's RGBA8 image /
  *                      PixelSum records (bottom-up rows like RtRender)
  *   RtxBatchSetTuning  RTX_BATCH_* keys below
- *   RtxBatchAutotune   times candidate block sizes, queue capacities, refill
- *                      thresholds and BVH widths on this batch (frames of
+ *   RtxBatchAutotune   times candidate pieces per triangle, BVH widths, block
+ *                      sizes, queue capacities and refill thresholds on this batch (frames of
  *                      one path per pixel), keeps the fastest and writes
  *                      the candidates to results (up to maxResults)
  * Returns 1 on success and 0 on failure (RtxBatchLastError) unless noted. */
@@ -259,10 +263,11 @@ int RtxReadAovs(void* session, float* aovs, int count);
 #define RTX_BATCH_REFILL 3    /* refill threshold of the persistent traversal (1..32) */
 #define RTX_BATCH_GRAPH 4     /* 1: replay frames from a CUDA graph (default), 0: launch kernels */
 #define RTX_BATCH_WIDTH 5     /* BVH node width: 4 or 8 (default 8); rebuilds every scene */
-#define RTX_BATCH_PIECES 6    /* pieces per triangle of the traversal trees (1..8, default 2; see RTX_TUNE_PIECES) */
+#define RTX_BATCH_PIECES 6    /* most pieces per triangle of the traversal trees (1..8, default 3; see RTX_TUNE_PIECES) */
 typedef struct RtxBatchTune {
     int block, capacity, refill, width;
     float frameMs;  /* device time of one frame of one path per pixel */
+    int pieces;     /* pieces per triangle of the traversal trees */
 } RtxBatchTune;
 typedef struct RtxBatchStats {
     unsigned long long primaryRays, secondaryRays, shadowRays, paths;  /* of the last frame */
@@ -273,6 +278,7 @@ typedef struct RtxBatchStats {
     int kernelLaunches;            /* kernels in one frame (graph nodes when replayed) */
     int graph;                     /* 1 if the last frame was a graph launch */
     int block, capacity, refill, width;  /* tuning in use */
+    int pieces;
 } RtxBatchStats;
 void* RtxBatchCreate(void);
 void RtxBatchDestroy(void* batch);

@@ -73,6 +73,8 @@ def make_batch(lib, scene_list, views):
     {'block': 256, 'refill': 32, 'capacity': 3000},
     {'width': 4},
     {'width': 4, 'graph': 0, 'capacity': 2048},
+    {'pieces': 1},
+    {'pieces': 4, 'width': 4},
 ])
 def test_batch_equals_single_view_renders(lib, reference, tuning):
     scene_list, views, expect = reference
@@ -114,12 +116,14 @@ def test_autotune_keeps_results(lib, reference):
     scene_list, views, expect = reference
     with make_batch(lib, scene_list, views) as b:
         tried = b.autotune(SETTINGS)
-        assert len(tried) >= 7  # the current tuning, width 4, blocks 64 and 256, three refills
+        assert len(tried) >= 9  # the current tuning, pieces 1 and 3, width 4, blocks 64 and 256, three refills
         assert {t['width'] for t in tried} == {4, 8} and {t['block'] for t in tried} >= {64, 128, 256}
         assert all(t['frameMs'] > 0 for t in tried)
         best = min(tried, key=lambda t: t['frameMs'])
         st = b.stats()
-        assert (st['block'], st['refill'], st['width']) == (best['block'], best['refill'], best['width'])
+        assert (st['block'], st['refill'], st['width'], st['pieces']) == \
+            (best['block'], best['refill'], best['width'], best['pieces'])
+        assert {t['pieces'] for t in tried} == {1, 2, 3}
         assert b.sample_count() == 0
         b.render(SETTINGS)
         b.render(SETTINGS)
