@@ -68,6 +68,8 @@ def parse():
                    help='skip the learned-denoiser inference timing (1 GPU runs it by default)')
     p.add_argument('--pieces', type=int, default=None,
                    help='pieces per triangle of the traversal tree (RTX_TUNE_PIECES; default: the library default)')
+    p.add_argument('--leaf', type=int, default=None,
+                   help='leaf size of the traversal tree (RTX_TUNE_LEAF; default: the library default)')
     p.add_argument('--denoiser-only', action='store_true',
                    help='only time learned-denoiser inference at 1920x1080 (a small case for profiling)')
     p.set_defaults(quality=True, batch=True, denoiser=True)
@@ -536,11 +538,15 @@ def run_ours(args, rank, local_rank, world):
     import scenes
     with Session(lib) as warm:
         small = scenes.cornell_sphere(width=32, height=32)
-        warm.initialize(small[0], 32, 32)
+        # Two diagonal slivers: the warm-up also builds a tree over triangle pieces.
+        slivers = scenes.records([(0, 0, 0), (0, 0, 0)], [(1, 1, 1), (0.5, 0.3, 1.2)], [(1.01, 1, 1), (0.5, 0.31, 1.2)])
+        warm.initialize(np.concatenate([small[0], slivers]), 32, 32)
         warm.render(small[1], small[2])
     s = Session(lib)
     if args.pieces is not None:
         s.set_tuning(pieces=args.pieces)
+    if args.leaf is not None:
+        s.set_tuning(leaf=args.leaf)
     t_init = time.perf_counter()
     s.initialize(tris, w, h)
     init_wall_ms = (time.perf_counter() - t_init) * 1e3

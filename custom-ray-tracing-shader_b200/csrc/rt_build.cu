@@ -324,7 +324,7 @@ __global__ void __launch_bounds__(256) binSmallKernel(const int* order, const fl
 // One thread per open task: the reference's SAH sweep, then node records.
 __global__ void splitKernel(const Task* tasks, int nTasks, const BinAcc* bins, Split* splits, BinNode* nodes,
                             int* counters /*0 nodes,1 next tasks,2 max depth,3 error*/, Task* nextTasks,
-                            int nodeCapacity, int taskCapacity) {
+                            int nodeCapacity, int taskCapacity, int leafSize) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nTasks) return;
     const Task T = tasks[t];
@@ -332,7 +332,7 @@ __global__ void splitKernel(const Task* tasks, int nTasks, const BinAcc* bins, S
     int bestAxis = -1, bestBin = -1;
     float nodeArea = halfArea(T.lo, T.hi);
     float bestCost = nodeArea * T.count;
-    if (T.count > kLeafSize && T.depth != kBinaryMaxDepth) {
+    if (T.count > leafSize && T.depth != kBinaryMaxDepth) {
         for (int a = 0; a < 3; a++) {
             float extent = T.chi[a] - T.clo[a];
             if (extent <= 1e-12f) continue;
@@ -390,7 +390,7 @@ __global__ void splitKernel(const Task* tasks, int nTasks, const BinAcc* bins, S
         c.node = child + side;
         c.depth = T.depth + 1;
         atomicMax(&counters[2], c.depth);
-        if (c.count <= kLeafSize || c.depth == kBinaryMaxDepth) {
+        if (c.count <= leafSize || c.depth == kBinaryMaxDepth) {
             nodes[c.node] = BinNode{v3(c.lo[0], c.lo[1], c.lo[2]), c.first, v3(c.hi[0], c.hi[1], c.hi[2]), c.count};
         } else {
             int k = atomicAdd(&counters[1], 1);
@@ -598,8 +598,9 @@ cudaError_t pieceMap(const SceneTri* tris, int triCount, int maxPieces, cudaStre
 }
 
 cudaError_t buildBvh(const SceneTri* tris, int triCount, cudaStream_t stream, BuiltBvh& out, BuildResult& result,
-                     const char** failure, int leafGroup, int width, int pieces) {
+                     const char** failure, int leafGroup, int width, int pieces, int leafSize) {
     if (width != 4 && width != 8) { *failure = "BVH width must be 4 or 8"; return cudaErrorInvalidValue; }
+    if (leafSize < 1 || leafSize > 8) { *failure = "BVH leaf size must be 1..8"; return cudaErrorInvalidValue; }
     if (pieces < 1 || pieces > 8 || (long long)triCount * pieces > 0x3FFFFFFFll) {
         *failure = "BVH pieces per triangle must be 1..8";
         return cudaErrorInvalidValue;
@@ -623,7 +624,7 @@ cudaError_t buildBvh(const SceneTri* tris, int triCount, cudaStream_t stream, Bu
         n = total;
     }
     const int nodeCapacity = 2 * n + 2;
-    const int taskCapacity = n / (kLeafSize + 1) + 2;
+    const int taskCapacity = n / (leafSize + 1) + 2;
     // Temporaries.
     float4* cent = nullptr; int* orderB = nullptr; int* posTask = nullptr; int* posTaskB = nullptr;
     Task* tasks = nullptr; Task* tasksB = nullptr; BinAcc* bins = nullptr; Split* splits = nullptr;
@@ -672,7 +673,7 @@ cudaError_t buildBvh(const SceneTri* tris, int triCount, cudaStream_t stream, Bu
             RT_TRY(cudaMemsetAsync(counters + 1, 0, sizeof(int), stream));
             RT_TRY(cudaMemsetAsync(counters + 5, 0, sizeof(int), stream));
             splitKernel<<<blocksFor(nTasks, 128), 128, 0, stream>>>(tasks, nTasks, bins, splits, rawNodes, counters,
-                                                                    tasksB, nodeCapacity, taskCapacity);
+                                                                    tasksB, nodeCapacity, taskCapacity, leafSize);
             flagKernel<<<blocksFor(n, 256), 256, 0, stream>>>(out.order, posTask, cent, tasks, splits, n, flags);
             scanBlocksKernel<<<nScanBlocks, 256, 0, stream>>>(flags, prefix, n, blockSums);
             scanTotalsKernel<<<1, 1024, 0, stream>>>(blockSums, nScanBlocks);

@@ -42,8 +42,10 @@ struct BuiltBvh {
 // into up to `pieces` slabs along their box's longest axis, each with the
 // padded box of its part; packedTris then holds a triangle once per leaf slot
 // that reaches a piece of it, and the binary nodes are not the reference's.
+// leafSize (1..8): binary nodes of at most this many primitives become leaves
+// (4 is the reference's rule, bvh.cuh:64).
 cudaError_t buildBvh(const SceneTri* tris, int n, cudaStream_t stream, BuiltBvh& out, BuildResult& result,
-                     const char** failure, int leafGroup = 3, int width = 8, int pieces = 1);
+                     const char** failure, int leafGroup = 3, int width = 8, int pieces = 1, int leafSize = 4);
 void freeBvh(BuiltBvh& bvh);
 // Pieces of a traversal tree over n triangles with at most maxPieces per
 // triangle: *total primitives and, when primTri is not null, a device array

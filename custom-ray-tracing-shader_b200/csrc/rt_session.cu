@@ -38,6 +38,11 @@ static_assert(sizeof(RtxQuery) == 28 && sizeof(RtxHit) == 16, "query sizes");
 // Pieces per triangle of the traversal tree (RTX_TUNE_PIECES; 1: traverse the
 // collapse of the reference's tree).
 constexpr int kDefaultPieces = 3;
+// Leaf size of the traversal tree over pieces (RTX_TUNE_LEAF; the reference's
+// tree keeps its own rule of 4). Measured on the 1M-triangle room at most 3
+// pieces: leaves of 1, 2, 3, 4, 6, 8 gave 2,108, 2,114, 2,094, 2,078, 2,031,
+// 1,987 Mrays/s.
+constexpr int kDefaultTraversalLeaf = 2;
 
 // A denoising network with its last error message (RtxUnet* entry points).
 struct UnetHandle {
@@ -96,6 +101,7 @@ struct Session {
     BuiltBvh pieceBvh;     // traversal tree over triangle pieces (when pieces > 1)
     BuildResult pieceBuild;
     int pieces = kDefaultPieces;
+    int traversalLeaf = kDefaultTraversalLeaf;
     WavefrontBuffers wave;
     // Host mirrors for the CPU backends (filled on first use).
     std::vector<Accum> hostSum;
@@ -399,7 +405,7 @@ int RtInitialize(void* p, const Triangle* triangles, int count, int width, int h
     if (e == cudaSuccess && pieceTotal > count) {
         // Traversal tree over triangle pieces; the reference tree above stays
         // for RtBvhInfo and RtxExportBvh.
-        e = buildBvh(s->dTris, count, s->stream, s->pieceBvh, s->pieceBuild, &why, 3, 8, s->pieces);
+        e = buildBvh(s->dTris, count, s->stream, s->pieceBvh, s->pieceBuild, &why, 3, 8, s->pieces, s->traversalLeaf);
         if (e == cudaSuccess) {
             void* unused[] = {s->pieceBvh.binNodes, s->pieceBvh.order, s->pieceBvh.primLo, s->pieceBvh.primHi};
             for (void* q : unused) cudaFree(q);
@@ -776,6 +782,10 @@ int RtxSetTuning(void* p, int key, int value) {
         case RTX_TUNE_PIECES:
             if (value < 1 || value > 8) return 0;
             s->pieces = value;  // used by the next RtInitialize
+            return 1;
+        case RTX_TUNE_LEAF:
+            if (value < 1 || value > 8) return 0;
+            s->traversalLeaf = value;  // used by the next RtInitialize
             return 1;
         default:
             return 0;

@@ -190,11 +190,15 @@ int RtxSetIntegrator(void* session, int mode);
  *                             tree. The reference's tree is always built for
  *                             RtBvhInfo and RtxExportBvh; hits do not depend on
  *                             the tree
+ *   RTX_TUNE_LEAF             leaf size of that traversal tree (1..8, default 2;
+ *                             the reference tree keeps 4; applies from the next
+ *                             RtInitialize)
  */
 #define RTX_TUNE_PATHS_IN_FLIGHT 1
 #define RTX_TUNE_POSTPONE 2
 #define RTX_TUNE_REFILL 3
 #define RTX_TUNE_PIECES 4
+#define RTX_TUNE_LEAF 5
 int RtxSetTuning(void* session, int key, int value);
 /* Light arriving from outside the scene on rays that leave it after the first
  * bounce (primary misses stay black, as in the reference). mode 0: the
