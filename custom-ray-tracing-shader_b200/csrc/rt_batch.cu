@@ -320,7 +320,7 @@ struct BatchSceneData {
     int count = 0;
     BuiltBvh bvh;
     BuildResult build;
-    int builtWidth = 0, builtPieces = 0;
+    int builtWidth = 0, builtPieces = 0, builtLeaf = 0;
     unsigned triBase = 0, nodeBase = 0, lightBase = 0, packedBase = 0;
 };
 struct BatchViewData {
@@ -356,7 +356,7 @@ struct Batch {
     int* dError = nullptr;
     WavefrontBuffers wave;
     // Tuning.
-    int block = 128, capacity = 0, refill = 24, width = 8, useGraph = 1, pieces = 3;
+    int block = 128, capacity = 0, refill = 24, width = 8, useGraph = 1, pieces = 3, leaf = 2;
     int environmentMode = 0;
     float3 environment = make_float3(0.0f, 0.0f, 0.0f);
     // Frame state.
@@ -428,16 +428,17 @@ bool ensureBase(Batch* b) {
 // Traversal tree of a scene at the batch's BVH width and pieces per triangle
 // (only the wide nodes and packed triangles are kept).
 bool buildScene(Batch* b, BatchSceneData& S) {
-    if (S.builtWidth == b->width && S.builtPieces == b->pieces) return true;
+    if (S.builtWidth == b->width && S.builtPieces == b->pieces && S.builtLeaf == b->leaf) return true;
     freeBvh(S.bvh);
     const char* why = nullptr;
-    cudaError_t e = buildBvh(S.dTris, S.count, b->stream, S.bvh, S.build, &why, 3, b->width, b->pieces);
+    cudaError_t e = buildBvh(S.dTris, S.count, b->stream, S.bvh, S.build, &why, 3, b->width, b->pieces, b->leaf);
     if (e != cudaSuccess) { S.builtWidth = 0; return failB(b, e, why); }
     void* unused[] = {S.bvh.binNodes, S.bvh.order, S.bvh.primLo, S.bvh.primHi};
     for (void* q : unused) cudaFree(q);
     S.bvh.binNodes = nullptr; S.bvh.order = nullptr; S.bvh.primLo = nullptr; S.bvh.primHi = nullptr;
     S.builtWidth = b->width;
     S.builtPieces = b->pieces;
+    S.builtLeaf = b->leaf;
     return true;
 }
 
@@ -813,6 +814,10 @@ int RtxBatchSetTuning(void* p, int key, int value) {
         case RTX_BATCH_PIECES:
             if (value < 1 || value > 8) break;
             if (value != b->pieces) { b->pieces = value; freeArena(b); }
+            return 1;
+        case RTX_BATCH_LEAF:
+            if (value < 1 || value > 8) break;
+            if (value != b->leaf) { b->leaf = value; freeArena(b); }
             return 1;
         default:
             break;

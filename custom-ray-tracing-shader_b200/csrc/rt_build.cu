@@ -565,30 +565,38 @@ void freeBvh(BuiltBvh& b) {
     b = BuiltBvh{};
 }
 
-cudaError_t pieceMap(const SceneTri* tris, int triCount, int maxPieces, cudaStream_t stream, int** primTri, int* total) {
+cudaError_t pieceMap(const SceneTri* tris, int triCount, int maxPieces, cudaStream_t stream, int** primTri, int* total,
+                     float* ms) {
     unsigned *counts = nullptr, *pfx = nullptr, *sums = nullptr;
     int* dTotal = nullptr;
+    int* map = nullptr;
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
     const int nb = blocksFor(triCount, kScanBlock);
     int hostTotal = 0;
     if (primTri) *primTri = nullptr;
+    if (ms) *ms = 0.0f;
+    // Every allocation before the first kernel, so the timed span is the kernels'.
     cudaError_t err = alloc(counts, triCount);
     if (err == cudaSuccess) err = alloc(pfx, triCount);
     if (err == cudaSuccess) err = alloc(sums, nb);
     if (err == cudaSuccess) err = alloc(dTotal, 1);
+    if (err == cudaSuccess && primTri) err = alloc(map, (size_t)triCount * maxPieces);
+    if (err == cudaSuccess) err = cudaEventCreate(&t0);
+    if (err == cudaSuccess) err = cudaEventCreate(&t1);
+    if (err == cudaSuccess) err = cudaEventRecord(t0, stream);
     if (err == cudaSuccess) {
         pieceCountKernel<<<blocksFor(triCount, 256), 256, 0, stream>>>(tris, triCount, maxPieces, counts);
         scanBlocksKernel<<<nb, 256, 0, stream>>>(counts, pfx, triCount, sums);
         scanTotalsKernel<<<1, 1024, 0, stream>>>(sums, nb);
-        err = cudaGetLastError();
-    }
-    int* map = nullptr;
-    if (err == cudaSuccess && primTri) err = alloc(map, (size_t)triCount * maxPieces);
-    if (err == cudaSuccess) {
         pieceFillKernel<<<blocksFor(triCount, 256), 256, 0, stream>>>(counts, pfx, sums, triCount, map, dTotal);
         err = cudaGetLastError();
     }
+    if (err == cudaSuccess) err = cudaEventRecord(t1, stream);
     if (err == cudaSuccess) err = cudaMemcpyAsync(&hostTotal, dTotal, sizeof(int), cudaMemcpyDeviceToHost, stream);
     if (err == cudaSuccess) err = cudaStreamSynchronize(stream);
+    if (err == cudaSuccess && ms) err = cudaEventElapsedTime(ms, t0, t1);
+    if (t0) cudaEventDestroy(t0);
+    if (t1) cudaEventDestroy(t1);
     cudaFree(counts); cudaFree(pfx); cudaFree(sums); cudaFree(dTotal);
     if (err == cudaSuccess && (hostTotal < triCount || hostTotal > triCount * maxPieces)) err = cudaErrorUnknown;
     if (err != cudaSuccess) { cudaFree(map); return err; }
@@ -612,10 +620,11 @@ cudaError_t buildBvh(const SceneTri* tris, int triCount, cudaStream_t stream, Bu
     int n = triCount;
     int* primTri = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
-    if ((err = cudaEventCreate(&e0)) != cudaSuccess || (err = cudaEventRecord(e0, stream)) != cudaSuccess) return err;
+    float pieceMs = 0.0f;
+    if ((err = cudaEventCreate(&e0)) != cudaSuccess) return err;
     if (pieces > 1) {
         int total = 0;
-        err = pieceMap(tris, triCount, pieces, stream, &primTri, &total);
+        err = pieceMap(tris, triCount, pieces, stream, &primTri, &total, &pieceMs);
         if (err != cudaSuccess) { cudaEventDestroy(e0); *failure = "triangle pieces"; return err; }
         if (total == triCount) {  // no triangle is split: a tree over the triangles themselves
             cudaFree(primTri);
@@ -625,6 +634,7 @@ cudaError_t buildBvh(const SceneTri* tris, int triCount, cudaStream_t stream, Bu
     }
     const int nodeCapacity = 2 * n + 2;
     const int taskCapacity = n / (leafSize + 1) + 2;
+    const int wideCapacity = 2 * n + 8;
     // Temporaries.
     float4* cent = nullptr; int* orderB = nullptr; int* posTask = nullptr; int* posTaskB = nullptr;
     Task* tasks = nullptr; Task* tasksB = nullptr; BinAcc* bins = nullptr; Split* splits = nullptr;
@@ -643,7 +653,16 @@ cudaError_t buildBvh(const SceneTri* tris, int triCount, cudaStream_t stream, Bu
     RT_TRY(alloc(flags, n)); RT_TRY(alloc(prefix, n)); RT_TRY(alloc(blockSums, nScanBlocks));
     RT_TRY(alloc(counters, 8)); RT_TRY(alloc(rawNodes, nodeCapacity));
     RT_TRY(cudaMallocHost(reinterpret_cast<void**>(&hostCounters), 8 * sizeof(int)));
+    // Renumbering and collapse buffers at their upper bounds (node count <=
+    // nodeCapacity, wide nodes and jobs <= 2n + 8), so no allocation falls
+    // inside the timed spans.
+    RT_TRY(alloc(interior, nodeCapacity)); RT_TRY(alloc(rank, nodeCapacity)); RT_TRY(alloc(newIndex, nodeCapacity));
+    RT_TRY(alloc(out.binNodes, nodeCapacity));
+    RT_TRY(alloc(out.wideNodes, (size_t)wideCapacity * 5));
+    RT_TRY(alloc(out.packedTris, (size_t)n * 3));
+    RT_TRY(alloc(jobs, wideCapacity)); RT_TRY(alloc(jobsB, wideCapacity));
     RT_TRY(cudaEventCreate(&e1)); RT_TRY(cudaEventCreate(&e2));
+    RT_TRY(cudaEventRecord(e0, stream));  // build time: the kernels, not the allocations before them
     {
         Task root{};
         root.node = 0; root.first = 0; root.count = n; root.depth = 0;
@@ -695,8 +714,6 @@ cudaError_t buildBvh(const SceneTri* tris, int triCount, cudaStream_t stream, Bu
         // levelStart[d] .. levelStart[d+1] are the nodes of depth d.
         while (levelStart.size() > 2 && levelStart.back() == levelStart[levelStart.size() - 2]) levelStart.pop_back();
         int depths = (int)levelStart.size() - 1;
-        RT_TRY(alloc(interior, nodeCount)); RT_TRY(alloc(rank, nodeCount)); RT_TRY(alloc(newIndex, nodeCount));
-        RT_TRY(alloc(out.binNodes, nodeCount));
         for (int d = depths - 1; d >= 0; d--) {
             int b = levelStart[d], e = levelStart[d + 1];
             subtreeInteriorKernel<<<blocksFor(e - b, 256), 256, 0, stream>>>(rawNodes, b, e, interior);
@@ -719,10 +736,7 @@ cudaError_t buildBvh(const SceneTri* tris, int triCount, cudaStream_t stream, Bu
         RT_TRY(cudaEventRecord(e1, stream));
 
         // Collapse.
-        int wideCapacity = 2 * n + 8, jobCapacity = 2 * n + 8;
-        RT_TRY(alloc(out.wideNodes, (size_t)wideCapacity * 5));
-        RT_TRY(alloc(out.packedTris, (size_t)n * 3));
-        RT_TRY(alloc(jobs, jobCapacity)); RT_TRY(alloc(jobsB, jobCapacity));
+        const int jobCapacity = wideCapacity;
         Job rootJob{0, 0, 0, 0, 0};
         RT_TRY(cudaMemcpyAsync(jobs, &rootJob, sizeof(Job), cudaMemcpyHostToDevice, stream));
         int cinit[8] = {1, 0, 0, 0, 0, 0, 0, 0};
@@ -757,6 +771,7 @@ cudaError_t buildBvh(const SceneTri* tris, int triCount, cudaStream_t stream, Bu
         result.packedTriangles = hostCounters[1];
         result.wideDepth = wideDepth;
         RT_TRY(cudaEventElapsedTime(&result.buildMs, e0, e1));
+        result.buildMs += pieceMs;
         RT_TRY(cudaEventElapsedTime(&result.collapseMs, e1, e2));
     }
 done:

@@ -49,7 +49,9 @@ cudaError_t buildBvh(const SceneTri* tris, int n, cudaStream_t stream, BuiltBvh&
 void freeBvh(BuiltBvh& bvh);
 // Pieces of a traversal tree over n triangles with at most maxPieces per
 // triangle: *total primitives and, when primTri is not null, a device array
-// (allocated here, cudaFree it) of each primitive's triangle. Synchronises.
-cudaError_t pieceMap(const SceneTri* tris, int n, int maxPieces, cudaStream_t stream, int** primTri, int* total);
+// (allocated here, cudaFree it) of each primitive's triangle; *ms, when not
+// null, the device time of its kernels. Synchronises.
+cudaError_t pieceMap(const SceneTri* tris, int n, int maxPieces, cudaStream_t stream, int** primTri, int* total,
+                     float* ms = nullptr);
 
 }  // namespace rt

@@ -417,7 +417,7 @@ class Unet:
 class Batch:
     """Many views of many scenes rendered together (RtxBatch* entry points)."""
 
-    BLOCK, CAPACITY, REFILL, GRAPH, WIDTH, PIECES = 1, 2, 3, 4, 5, 6
+    BLOCK, CAPACITY, REFILL, GRAPH, WIDTH, PIECES, LEAF = 1, 2, 3, 4, 5, 6, 7
 
     def __init__(self, lib=None):
         self.lib = lib or load_library()
@@ -484,9 +484,9 @@ class Batch:
         self.check(self.lib.RtxBatchReadAccumulation(self.handle, view, out.ctypes.data, out.size))
         return out
 
-    def set_tuning(self, block=None, capacity=None, refill=None, graph=None, width=None, pieces=None):
+    def set_tuning(self, block=None, capacity=None, refill=None, graph=None, width=None, pieces=None, leaf=None):
         for key, value in ((self.BLOCK, block), (self.CAPACITY, capacity), (self.REFILL, refill),
-                           (self.GRAPH, graph), (self.WIDTH, width), (self.PIECES, pieces)):
+                           (self.GRAPH, graph), (self.WIDTH, width), (self.PIECES, pieces), (self.LEAF, leaf)):
             if value is not None:
                 self.check(self.lib.RtxBatchSetTuning(self.handle, key, int(value)))
 

@@ -268,6 +268,7 @@ int RtxReadAovs(void* session, float* aovs, int count);
 #define RTX_BATCH_GRAPH 4     /* 1: replay frames from a CUDA graph (default), 0: launch kernels */
 #define RTX_BATCH_WIDTH 5     /* BVH node width: 4 or 8 (default 8); rebuilds every scene */
 #define RTX_BATCH_PIECES 6    /* most pieces per triangle of the traversal trees (1..8, default 3; see RTX_TUNE_PIECES) */
+#define RTX_BATCH_LEAF 7      /* leaf size of the traversal trees (1..8, default 2) */
 typedef struct RtxBatchTune {
     int block, capacity, refill, width;
     float frameMs;  /* device time of one frame of one path per pixel */

@@ -75,6 +75,8 @@ def make_batch(lib, scene_list, views):
     {'width': 4, 'graph': 0, 'capacity': 2048},
     {'pieces': 1},
     {'pieces': 4, 'width': 4},
+    {'leaf': 4},
+    {'leaf': 1, 'pieces': 2},
 ])
 def test_batch_equals_single_view_renders(lib, reference, tuning):
     scene_list, views, expect = reference
