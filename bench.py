@@ -512,6 +512,19 @@ def denoiser_run(lib, args, repeats=10):
                                                    '8 MB read-back) against bf16 dense peak'}}
 
 
+def kernel_rates(integrator, per_kind, primary_ms, extend_ms, shadow_ms):
+    """Mrays/s of each traversal kind over its own kernels' device time:
+    primary (closest-hit at bounce 0), secondary (closest-hit at later
+    bounces) and shadow (any-hit) queries. Wavefront integrator only; the
+    megakernel interleaves all three in one launch."""
+    if integrator != 'wavefront' or extend_ms <= 0:
+        return None
+    rate = lambda rays, ms: rays / ms / 1e3 if ms > 0 else None
+    return {'primary': rate(per_kind['primaryRays'], primary_ms),
+            'secondary': rate(per_kind['secondaryRays'], extend_ms - primary_ms),
+            'shadow': rate(per_kind['shadowRays'], shadow_ms)}
+
+
 def l2_flusher():
     try:
         import torch
@@ -576,7 +589,7 @@ def run_ours(args, rank, local_rank, world):
         gpu_index = int(os.environ['CUDA_VISIBLE_DEVICES'].split(',')[0])
     clocks = Clocks(gpu_index)
     rays = launches = 0
-    device_ms = extend_ms = shadow_ms = 0.0
+    device_ms = extend_ms = shadow_ms = primary_ms = 0.0
     per_kind = {'primaryRays': 0, 'secondaryRays': 0, 'shadowRays': 0}
     dist.barrier()
     clocks.start()
@@ -591,6 +604,7 @@ def run_ours(args, rank, local_rank, world):
         launches += st['kernelLaunches']
         extend_ms += st['extendMs']
         shadow_ms += st['shadowMs']
+        primary_ms += st['primaryMs']
     wall = time.perf_counter() - wall0
     clock_info = clocks.stop()
     dist.barrier()
@@ -679,6 +693,7 @@ def run_ours(args, rank, local_rank, world):
             'roofline': roofline,
             'cpu_baseline': cpu,
             'rays': {k: v // args.steps for k, v in per_kind.items()},
+            'traversal_mrays_per_s': kernel_rates(best, per_kind, primary_ms, extend_ms, shadow_ms),
             'wall_ms_per_step': wall * 1e3 / args.steps,
             'build': {'ms': bvh['buildMs'] + bvh['collapseMs'], 'binned_sah_ms': bvh['buildMs'],
                       'collapse_ms': bvh['collapseMs'],

@@ -414,12 +414,15 @@ bool ensureBase(Batch* b) {
     if ((e = cudaEventCreate(&b->start)) != cudaSuccess) return failB(b, e);
     if ((e = cudaEventCreate(&b->stop)) != cudaSuccess) return failB(b, e);
     if ((e = cudaMalloc(&b->dDirs, sizeof(unsigned) * kSobolDims * 32)) != cudaSuccess) return failB(b, e);
-    if ((e = cudaMemcpy(b->dDirs, dirs, sizeof(unsigned) * kSobolDims * 32, cudaMemcpyHostToDevice)) != cudaSuccess)
+    // Copies and fills on b->stream: a non-blocking stream is not ordered
+    // after the legacy default stream.
+    if ((e = cudaMemcpyAsync(b->dDirs, dirs, sizeof(unsigned) * kSobolDims * 32, cudaMemcpyHostToDevice, b->stream)) !=
+        cudaSuccess)
         return failB(b, e);
     if ((e = cudaMalloc(&b->dPassXor, sizeof(unsigned) * 16 * kSobolDims)) != cudaSuccess) return failB(b, e);
     if ((e = cudaMalloc(&b->dSeedHash, sizeof(unsigned) * kSobolDims)) != cudaSuccess) return failB(b, e);
     if ((e = cudaMalloc(&b->dSample, sizeof(unsigned))) != cudaSuccess) return failB(b, e);
-    if ((e = cudaMemset(b->dSample, 0, sizeof(unsigned))) != cudaSuccess) return failB(b, e);
+    if ((e = cudaMemsetAsync(b->dSample, 0, sizeof(unsigned), b->stream)) != cudaSuccess) return failB(b, e);
     if ((e = cudaMalloc(&b->dCounters, 4 * sizeof(unsigned long long))) != cudaSuccess) return failB(b, e);
     if ((e = cudaMalloc(&b->dError, 2 * sizeof(int))) != cudaSuccess) return failB(b, e);
     return true;
@@ -516,7 +519,8 @@ bool ensureViews(Batch* b) {
     if ((e = cudaMalloc(&b->dSum, sizeof(Accum) * pixels)) != cudaSuccess) return failB(b, e, "accumulation");
     if ((e = cudaMalloc(&b->dDepth, sizeof(float) * pixels)) != cudaSuccess) return failB(b, e, "accumulation");
     if ((e = cudaMalloc(&b->dPixels, sizeof(uchar4) * pixels)) != cudaSuccess) return failB(b, e, "accumulation");
-    if ((e = cudaMemcpy(b->dViews, table.data(), sizeof(BatchView) * table.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
+    if ((e = cudaMemcpyAsync(b->dViews, table.data(), sizeof(BatchView) * table.size(), cudaMemcpyHostToDevice,
+                             b->stream)) != cudaSuccess)
         return failB(b, e);
     b->pixels = pixels;
     b->viewsReady = true;

@@ -381,7 +381,7 @@ cudaError_t launchMegakernel(const RenderLaunch& L, cudaStream_t stream, int* la
 }
 
 cudaError_t launchWavefront(const RenderLaunch& L, WavefrontBuffers& B, const TraceTuning& tuning, cudaStream_t stream,
-                            int* launches, float* extendMs, float* shadowMs, bool timing) {
+                            int* launches, float* extendMs, float* shadowMs, bool timing, float* primaryMs) {
     static int extendBlocks = 0, shadowBlocks = 0;
     if (!extendBlocks) {
         extendBlocks = traceBlocks(extendKernel, kTraceSmem);
@@ -394,7 +394,7 @@ cudaError_t launchWavefront(const RenderLaunch& L, WavefrontBuffers& B, const Tr
     int pixels = L.w * L.h;
     int n = 0;
     static thread_local std::vector<cudaEvent_t> pool;
-    struct Mark { cudaEvent_t a, b; bool shadow; };
+    struct Mark { cudaEvent_t a, b; int kind; };  // 0 primary closest-hit, 1 secondary, 2 shadow
     std::vector<Mark> marks;
     auto event = [&](size_t k) -> cudaEvent_t {
         while (pool.size() <= k) { cudaEvent_t e; cudaEventCreate(&e); pool.push_back(e); }
@@ -409,14 +409,14 @@ cudaError_t launchWavefront(const RenderLaunch& L, WavefrontBuffers& B, const Tr
             int q = 0;
             for (int bounce = 0; bounce < L.set.maxBounces; bounce++) {
                 resetQueuesKernel<<<1, 32, 0, stream>>>(B, q);
-                Mark m{nullptr, nullptr, false};
+                Mark m{nullptr, nullptr, bounce == 0 ? 0 : 1};
                 if (timing) { m.a = event(ev++); m.b = event(ev++); cudaEventRecord(m.a, stream); }
                 extendKernel<<<extendBlocks, kTraceBlock, smem, stream>>>(L.scene.wide, L.scene.packed, B, q,
                                                                           &L.counters[bounce == 0 ? 0 : 1], L.errorFlag,
                                                                           postponeBelow, refill);
                 if (timing) { cudaEventRecord(m.b, stream); marks.push_back(m); }
                 shadeKernel<<<shadeBlocks, 256, 0, stream>>>(A, B, q, bounce);
-                Mark s{nullptr, nullptr, true};
+                Mark s{nullptr, nullptr, 2};
                 if (timing) { s.a = event(ev++); s.b = event(ev++); cudaEventRecord(s.a, stream); }
                 shadowKernel<<<shadowBlocks, kTraceBlock, smem, stream>>>(L.scene.wide, L.scene.packed, B, &L.counters[2],
                                                                           L.errorFlag, postponeBelow, refill);
@@ -432,14 +432,15 @@ cudaError_t launchWavefront(const RenderLaunch& L, WavefrontBuffers& B, const Tr
     if (launches) *launches = n;
     if (timing && e == cudaSuccess) {
         e = cudaStreamSynchronize(stream);
-        float ext = 0, sh = 0;
+        float kindMs[3] = {0, 0, 0};
         for (const Mark& m : marks) {
             float ms = 0;
             cudaEventElapsedTime(&ms, m.a, m.b);
-            (m.shadow ? sh : ext) += ms;
+            kindMs[m.kind] += ms;
         }
-        if (extendMs) *extendMs = ext;
-        if (shadowMs) *shadowMs = sh;
+        if (extendMs) *extendMs = kindMs[0] + kindMs[1];
+        if (shadowMs) *shadowMs = kindMs[2];
+        if (primaryMs) *primaryMs = kindMs[0];
     }
     return e;
 }

@@ -57,7 +57,8 @@ cudaError_t launchMegakernel(const RenderLaunch& L, cudaStream_t stream, int* la
 // Wavefront: generate -> (extend -> shade -> shadow)* per wave. Timing of the
 // traversal kernels is accumulated into extendMs/shadowMs when timing != 0.
 cudaError_t launchWavefront(const RenderLaunch& L, WavefrontBuffers& b, const TraceTuning& tuning, cudaStream_t stream,
-                            int* launches, float* extendMs, float* shadowMs, bool timing);
+                            int* launches, float* extendMs, float* shadowMs, bool timing,
+                            float* primaryMs = nullptr);
 
 // fetch: one device int of scratch (the work counter of the persistent kernel).
 cudaError_t launchQueries(const uint4* wide, const float4* packed, const float4* queries /*2 per query*/, int count,

@@ -197,13 +197,13 @@ bool renderDevice(Session* s, const CameraData* camera, const RenderSettings* se
     RenderLaunch L{deviceView(s), cam, set, s->width, s->height, s->samples, s->dPassXor, s->dSeedHash,
                    s->dSum, s->dDepth, s->dPixels, s->dCounters, s->dError};
     int launches = 0;
-    float extendMs = 0, shadowMs = 0;
+    float extendMs = 0, shadowMs = 0, primaryMs = 0;
     if ((e = cudaEventRecord(s->start, s->stream)) != cudaSuccess) return fail(s, e);
     if (s->integrator == 1) {
         e = launchMegakernel(L, s->stream, &launches);
     } else {
         if (!ensureWave(s)) return false;
-        e = launchWavefront(L, s->wave, s->tuning, s->stream, &launches, &extendMs, &shadowMs, timing);
+        e = launchWavefront(L, s->wave, s->tuning, s->stream, &launches, &extendMs, &shadowMs, timing, &primaryMs);
     }
     if (e != cudaSuccess) return fail(s, e);
     if ((e = cudaEventRecord(s->stop, s->stream)) != cudaSuccess) return fail(s, e);
@@ -221,6 +221,7 @@ bool renderDevice(Session* s, const CameraData* camera, const RenderSettings* se
     s->stats.renderMs = *computeMs;
     s->stats.extendMs = extendMs;
     s->stats.shadowMs = shadowMs;
+    s->stats.primaryMs = primaryMs;
     s->stats.kernelLaunches = launches + 1;  // + the sampler-table kernel
     return true;
 }
@@ -390,7 +391,7 @@ int RtInitialize(void* p, const Triangle* triangles, int count, int width, int h
     s->lightCount = s->upload.lightCount;
     s->lightArea = s->upload.lightArea;
     RT_CHECK(cudaMalloc(&s->dDirs, sizeof(unsigned) * kSobolDims * 32));
-    RT_CHECK(cudaMemcpy(s->dDirs, dirs, sizeof(unsigned) * kSobolDims * 32, cudaMemcpyHostToDevice));
+    RT_CHECK(cudaMemcpyAsync(s->dDirs, dirs, sizeof(unsigned) * kSobolDims * 32, cudaMemcpyHostToDevice, s->stream));
     RT_CHECK(cudaMalloc(&s->dPassXor, sizeof(unsigned) * 16 * kSobolDims));
     RT_CHECK(cudaMalloc(&s->dSeedHash, sizeof(unsigned) * kSobolDims));
     RT_CHECK(cudaMalloc(&s->dSum, sizeof(Accum) * (size_t)width * height));
@@ -469,10 +470,10 @@ int RtDenoise(void* p, unsigned char* output, int outputBytes, float* millisecon
     cudaError_t e;
     if (!s->dDenoise && (e = cudaMalloc(&s->dDenoise, sizeof(float4) * 4 * count)) != cudaSuccess) { fail(s, e); return 0; }
     if (s->lastBackend != 2) {
-        if ((e = cudaMemcpy(s->dSum, s->hostSum.data(), count * sizeof(Accum), cudaMemcpyHostToDevice)) != cudaSuccess) { fail(s, e); return 0; }
+        if ((e = cudaMemcpyAsync(s->dSum, s->hostSum.data(), count * sizeof(Accum), cudaMemcpyHostToDevice, s->stream)) != cudaSuccess) { fail(s, e); return 0; }
     }
     if (s->lastBackend != 2 && s->hostDepth.size() == count) {
-        if ((e = cudaMemcpy(s->dDepth, s->hostDepth.data(), count * sizeof(float), cudaMemcpyHostToDevice)) != cudaSuccess) { fail(s, e); return 0; }
+        if ((e = cudaMemcpyAsync(s->dDepth, s->hostDepth.data(), count * sizeof(float), cudaMemcpyHostToDevice, s->stream)) != cudaSuccess) { fail(s, e); return 0; }
     }
     if (s->denoiser) {
         // Learned denoiser: AOVs -> U-Net -> display, all on the session stream.
@@ -735,9 +736,9 @@ int RtxReadAovs(void* p, float* out, int count) {
     cudaError_t e;
     if (!s->dDenoise && (e = cudaMalloc(&s->dDenoise, sizeof(float4) * 4 * need)) != cudaSuccess) { fail(s, e); return 0; }
     if (s->lastBackend != 2) {
-        if ((e = cudaMemcpy(s->dSum, s->hostSum.data(), need * sizeof(Accum), cudaMemcpyHostToDevice)) != cudaSuccess) { fail(s, e); return 0; }
+        if ((e = cudaMemcpyAsync(s->dSum, s->hostSum.data(), need * sizeof(Accum), cudaMemcpyHostToDevice, s->stream)) != cudaSuccess) { fail(s, e); return 0; }
         if (s->hostDepth.size() == need &&
-            (e = cudaMemcpy(s->dDepth, s->hostDepth.data(), need * sizeof(float), cudaMemcpyHostToDevice)) != cudaSuccess) { fail(s, e); return 0; }
+            (e = cudaMemcpyAsync(s->dDepth, s->hostDepth.data(), need * sizeof(float), cudaMemcpyHostToDevice, s->stream)) != cudaSuccess) { fail(s, e); return 0; }
     }
     float* aov = reinterpret_cast<float*>(s->dDenoise);
     if ((e = launchAovs(s->dSum, s->dDepth, s->samples, (int)need, aov, s->stream)) != cudaSuccess) { fail(s, e); return 0; }

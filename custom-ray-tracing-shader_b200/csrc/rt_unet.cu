@@ -396,11 +396,13 @@ Unet::Unet(unsigned seed) {
     cudaMalloc(&wbf_, sizeof(bf16) * params_);
     cudaMalloc(&wT_, sizeof(bf16) * params_);
     cudaMalloc(&convError_, sizeof(int));
-    cudaMemset(convError_, 0, sizeof(int));
+    // Every copy and fill goes through stream_: it is non-blocking, so it is
+    // not ordered after work on the legacy default stream.
     cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking);
-    cudaMemcpy(master_, host.data(), sizeof(float) * params_, cudaMemcpyHostToDevice);
-    cudaMemset(adamM_, 0, sizeof(float) * params_);
-    cudaMemset(adamV_, 0, sizeof(float) * params_);
+    cudaMemsetAsync(convError_, 0, sizeof(int), stream_);
+    cudaMemcpyAsync(master_, host.data(), sizeof(float) * params_, cudaMemcpyHostToDevice, stream_);
+    cudaMemsetAsync(adamM_, 0, sizeof(float) * params_, stream_);
+    cudaMemsetAsync(adamV_, 0, sizeof(float) * params_, stream_);
     syncWeights(stream_);
     cudaStreamSynchronize(stream_);
 }
@@ -425,16 +427,19 @@ cudaError_t Unet::checkConvolutions(std::string& error) {
     cudaError_t e = cudaMemcpy(&flag, convError_, sizeof(int), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return e;
     if (!flag) return cudaSuccess;
-    cudaMemset(convError_, 0, sizeof(int));
+    e = cudaMemsetAsync(convError_, 0, sizeof(int), stream_);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+    if (e != cudaSuccess) return e;
     error = "tensor-core convolution stopped: a wait on the tensor cores ran past its limit";
     return cudaErrorLaunchTimeout;
 }
 
 cudaError_t Unet::getParams(float* host) const {
-    return cudaMemcpy(host, master_, sizeof(float) * params_, cudaMemcpyDeviceToHost);
+    cudaError_t e = cudaMemcpyAsync(host, master_, sizeof(float) * params_, cudaMemcpyDeviceToHost, stream_);
+    return e == cudaSuccess ? cudaStreamSynchronize(stream_) : e;
 }
 cudaError_t Unet::setParams(const float* host) {
-    cudaError_t e = cudaMemcpy(master_, host, sizeof(float) * params_, cudaMemcpyHostToDevice);
+    cudaError_t e = cudaMemcpyAsync(master_, host, sizeof(float) * params_, cudaMemcpyHostToDevice, stream_);
     if (e != cudaSuccess) return e;
     e = syncWeights(stream_);
     if (e != cudaSuccess) return e;
@@ -663,11 +668,14 @@ cudaError_t Unet::inferDevice(const float* aovs, int h, int w, float* radiance, 
 // state flag (u64), FP32 parameters, then Adam m and v when the flag is set.
 cudaError_t Unet::save(const char* path, bool optimizerState, std::string& error) const {
     std::vector<float> host(params_ * (optimizerState ? 3 : 1));
-    cudaError_t e = cudaMemcpy(host.data(), master_, sizeof(float) * params_, cudaMemcpyDeviceToHost);
+    cudaError_t e = cudaMemcpyAsync(host.data(), master_, sizeof(float) * params_, cudaMemcpyDeviceToHost, stream_);
     if (optimizerState) {
-        if (e == cudaSuccess) e = cudaMemcpy(host.data() + params_, adamM_, sizeof(float) * params_, cudaMemcpyDeviceToHost);
-        if (e == cudaSuccess) e = cudaMemcpy(host.data() + 2 * params_, adamV_, sizeof(float) * params_, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(host.data() + params_, adamM_, sizeof(float) * params_, cudaMemcpyDeviceToHost, stream_);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(host.data() + 2 * params_, adamV_, sizeof(float) * params_, cudaMemcpyDeviceToHost, stream_);
     }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
     if (e != cudaSuccess) return e;
     FILE* f = std::fopen(path, "wb");
     if (!f) { error = std::string("cannot write ") + path; return cudaErrorInvalidValue; }
@@ -697,13 +705,15 @@ cudaError_t Unet::load(const char* path, std::string& error) {
     std::fclose(f);
     if (!ok) { error = std::string("not a denoiser checkpoint of this network: ") + path; return cudaErrorInvalidValue; }
     adamStep_ = state ? step : 0;
-    cudaError_t e = cudaMemcpy(master_, host.data(), sizeof(float) * params_, cudaMemcpyHostToDevice);
+    cudaError_t e = cudaMemcpyAsync(master_, host.data(), sizeof(float) * params_, cudaMemcpyHostToDevice, stream_);
     if (state) {
-        if (e == cudaSuccess) e = cudaMemcpy(adamM_, host.data() + params_, sizeof(float) * params_, cudaMemcpyHostToDevice);
-        if (e == cudaSuccess) e = cudaMemcpy(adamV_, host.data() + 2 * params_, sizeof(float) * params_, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(adamM_, host.data() + params_, sizeof(float) * params_, cudaMemcpyHostToDevice, stream_);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(adamV_, host.data() + 2 * params_, sizeof(float) * params_, cudaMemcpyHostToDevice, stream_);
     } else {
-        if (e == cudaSuccess) e = cudaMemset(adamM_, 0, sizeof(float) * params_);
-        if (e == cudaSuccess) e = cudaMemset(adamV_, 0, sizeof(float) * params_);
+        if (e == cudaSuccess) e = cudaMemsetAsync(adamM_, 0, sizeof(float) * params_, stream_);
+        if (e == cudaSuccess) e = cudaMemsetAsync(adamV_, 0, sizeof(float) * params_, stream_);
     }
     if (e == cudaSuccess) e = syncWeights(stream_);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);

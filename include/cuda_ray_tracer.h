@@ -87,6 +87,7 @@ typedef struct RtxRenderStats {
     float extendMs;                   /* part of renderMs spent in closest-hit traversal kernels */
     float shadowMs;                   /* part of renderMs spent in any-hit traversal kernels */
     int kernelLaunches;               /* kernels launched by the render */
+    float primaryMs;                  /* part of extendMs spent on bounce 0 (wavefront integrator) */
 } RtxRenderStats;
 
 /* Summary of the acceleration structure built at RtInitialize. */
