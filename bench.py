@@ -48,7 +48,7 @@ SPP_PER_STEP = 16
 def parse():
     p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     p.add_argument('--gpus', type=int, default=1)
-    p.add_argument('--steps', type=int, default=10)
+    p.add_argument('--steps', type=int, default=20)
     p.add_argument('--warmup', type=int, default=3)
     p.add_argument('--impl', choices=('ours', 'reference'), default='ours')
     p.add_argument('--integrator', choices=('auto', 'wavefront', 'megakernel'), default='auto')
@@ -70,6 +70,8 @@ def parse():
                    help='pieces per triangle of the traversal tree (RTX_TUNE_PIECES; default: the library default)')
     p.add_argument('--leaf', type=int, default=None,
                    help='leaf size of the traversal tree (RTX_TUNE_LEAF; default: the library default)')
+    p.add_argument('--lanes', type=int, default=None,
+                   help='waves in flight, 1 or 2 (RTX_TUNE_LANES; default: the library default)')
     p.add_argument('--denoiser-only', action='store_true',
                    help='only time learned-denoiser inference at 1920x1080 (a small case for profiling)')
     p.set_defaults(quality=True, batch=True, denoiser=True)
@@ -131,15 +133,28 @@ class Clocks:
     def __init__(self, gpu_index):
         self.gpu_index = gpu_index
         self.proc = None
+        self.skip = 0
         self.path = Path(os.environ.get('TMPDIR', '/tmp')) / f'bench_clocks_{os.getpid()}.csv'
 
     def start(self):
+        """Starts sampling every 100 ms and returns once nvidia-smi writes
+        samples (its start-up takes a while), so that the timed region that
+        follows is covered; samples from before it are dropped."""
+        self.skip = 0
         try:
             self.proc = subprocess.Popen(['nvidia-smi', '-i', str(self.gpu_index), f'--query-gpu={self.FIELDS}',
-                                          '--format=csv,noheader,nounits', '-lms', '200'],
+                                          '--format=csv,noheader,nounits', '-lms', '100'],
                                          stdout=open(self.path, 'w'), stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
+            return
+        t0 = time.perf_counter()
+        while time.perf_counter() - t0 < 5.0 and self.proc.poll() is None:
+            lines = self.path.read_text().count('\n')
+            if lines:
+                self.skip = lines
+                return
+            time.sleep(0.02)
 
     def stop(self):
         if not self.proc:
@@ -151,7 +166,7 @@ class Clocks:
             self.proc.kill()
         sm, sm_max, power, reasons = [], None, [], set()
         names = ('hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap')
-        for line in self.path.read_text().splitlines():
+        for line in self.path.read_text().splitlines()[self.skip:]:
             parts = [p.strip() for p in line.split(',')]
             if len(parts) < 9:
                 continue
@@ -512,17 +527,19 @@ def denoiser_run(lib, args, repeats=10):
                                                    '8 MB read-back) against bf16 dense peak'}}
 
 
-def kernel_rates(integrator, per_kind, primary_ms, extend_ms, shadow_ms):
+def kernel_rates(integrator, per_kind, primary_ms, extend_ms, shadow_ms, lanes):
     """Mrays/s of each traversal kind over its own kernels' device time:
     primary (closest-hit at bounce 0), secondary (closest-hit at later
     bounces) and shadow (any-hit) queries. Wavefront integrator only; the
-    megakernel interleaves all three in one launch."""
+    megakernel interleaves all three in one launch. With two lanes of waves
+    the launches overlap and these rates are lower bounds."""
     if integrator != 'wavefront' or extend_ms <= 0:
         return None
     rate = lambda rays, ms: rays / ms / 1e3 if ms > 0 else None
     return {'primary': rate(per_kind['primaryRays'], primary_ms),
             'secondary': rate(per_kind['secondaryRays'], extend_ms - primary_ms),
-            'shadow': rate(per_kind['shadowRays'], shadow_ms)}
+            'shadow': rate(per_kind['shadowRays'], shadow_ms),
+            'lanes': lanes, 'bound': 'lower' if lanes > 1 else 'isolated'}
 
 
 def l2_flusher():
@@ -560,6 +577,9 @@ def run_ours(args, rank, local_rank, world):
         s.set_tuning(pieces=args.pieces)
     if args.leaf is not None:
         s.set_tuning(leaf=args.leaf)
+    if args.lanes is not None:
+        s.set_tuning(lanes=args.lanes)
+    lanes = args.lanes if args.lanes is not None else 2  # RTX_TUNE_LANES default
     t_init = time.perf_counter()
     s.initialize(tris, w, h)
     init_wall_ms = (time.perf_counter() - t_init) * 1e3
@@ -667,6 +687,9 @@ def run_ours(args, rank, local_rank, world):
                                    'fallback 6.65 TB/s',
                     'bytes_per_closest_query': alg['closest'], 'bytes_per_shadow_query': alg['shadow'],
                     'model': '64 B per interior node + 44 B per triangle the reference traversal visits',
+                    'launch_timing': ('CUDA events around each launch; two lanes of waves overlap, so a launch '
+                                      'shares the GPU with the other lane for part of its duration and achieved is '
+                                      'a lower bound' if lanes > 1 else 'CUDA events around each launch, one lane'),
                     'sample_pixels': alg['sample_pixels']}
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
@@ -693,7 +716,7 @@ def run_ours(args, rank, local_rank, world):
             'roofline': roofline,
             'cpu_baseline': cpu,
             'rays': {k: v // args.steps for k, v in per_kind.items()},
-            'traversal_mrays_per_s': kernel_rates(best, per_kind, primary_ms, extend_ms, shadow_ms),
+            'traversal_mrays_per_s': kernel_rates(best, per_kind, primary_ms, extend_ms, shadow_ms, lanes),
             'wall_ms_per_step': wall * 1e3 / args.steps,
             'build': {'ms': bvh['buildMs'] + bvh['collapseMs'], 'binned_sah_ms': bvh['buildMs'],
                       'collapse_ms': bvh['collapseMs'],

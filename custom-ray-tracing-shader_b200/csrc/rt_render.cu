@@ -381,7 +381,8 @@ cudaError_t launchMegakernel(const RenderLaunch& L, cudaStream_t stream, int* la
 }
 
 cudaError_t launchWavefront(const RenderLaunch& L, WavefrontBuffers& B, const TraceTuning& tuning, cudaStream_t stream,
-                            int* launches, float* extendMs, float* shadowMs, bool timing, float* primaryMs) {
+                            int* launches, float* extendMs, float* shadowMs, bool timing, float* primaryMs,
+                            const WaveOverlap* overlap) {
     static int extendBlocks = 0, shadowBlocks = 0;
     if (!extendBlocks) {
         extendBlocks = traceBlocks(extendKernel, kTraceSmem);
@@ -401,32 +402,50 @@ cudaError_t launchWavefront(const RenderLaunch& L, WavefrontBuffers& B, const Tr
         return pool[k];
     };
     size_t ev = 0;
+    const bool two = overlap && overlap->buffers && overlap->stream && overlap->buffers->capacity == B.capacity;
+    WavefrontBuffers* lanes[2] = {&B, two ? overlap->buffers : &B};
+    cudaStream_t laneStream[2] = {stream, two ? overlap->stream : stream};
+    if (two) {
+        cudaEventRecord(overlap->fork, stream);  // the second lane starts after the work queued so far
+        cudaStreamWaitEvent(overlap->stream, overlap->fork, 0);
+    }
+    int wave = 0;
     for (int r = 0; r < L.set.raysPerPixel; r++) {
-        for (int start = 0; start < pixels; start += B.capacity) {
+        for (int start = 0; start < pixels; start += B.capacity, wave++) {
+            WavefrontBuffers& W = *lanes[two ? wave & 1 : 0];
+            cudaStream_t ws = laneStream[two ? wave & 1 : 0];
             WaveArgs A{L, r, start, pixels - start < B.capacity ? pixels - start : B.capacity};
-            generateKernel<<<blocks(A.n, 256), 256, 0, stream>>>(A, B);
+            generateKernel<<<blocks(A.n, 256), 256, 0, ws>>>(A, W);
             n++;
             int q = 0;
             for (int bounce = 0; bounce < L.set.maxBounces; bounce++) {
-                resetQueuesKernel<<<1, 32, 0, stream>>>(B, q);
+                resetQueuesKernel<<<1, 32, 0, ws>>>(W, q);
                 Mark m{nullptr, nullptr, bounce == 0 ? 0 : 1};
-                if (timing) { m.a = event(ev++); m.b = event(ev++); cudaEventRecord(m.a, stream); }
-                extendKernel<<<extendBlocks, kTraceBlock, smem, stream>>>(L.scene.wide, L.scene.packed, B, q,
-                                                                          &L.counters[bounce == 0 ? 0 : 1], L.errorFlag,
-                                                                          postponeBelow, refill);
-                if (timing) { cudaEventRecord(m.b, stream); marks.push_back(m); }
-                shadeKernel<<<shadeBlocks, 256, 0, stream>>>(A, B, q, bounce);
+                if (timing) { m.a = event(ev++); m.b = event(ev++); cudaEventRecord(m.a, ws); }
+                extendKernel<<<extendBlocks, kTraceBlock, smem, ws>>>(L.scene.wide, L.scene.packed, W, q,
+                                                                      &L.counters[bounce == 0 ? 0 : 1], L.errorFlag,
+                                                                      postponeBelow, refill);
+                if (timing) { cudaEventRecord(m.b, ws); marks.push_back(m); }
+                shadeKernel<<<shadeBlocks, 256, 0, ws>>>(A, W, q, bounce);
                 Mark s{nullptr, nullptr, 2};
-                if (timing) { s.a = event(ev++); s.b = event(ev++); cudaEventRecord(s.a, stream); }
-                shadowKernel<<<shadowBlocks, kTraceBlock, smem, stream>>>(L.scene.wide, L.scene.packed, B, &L.counters[2],
-                                                                          L.errorFlag, postponeBelow, refill);
-                if (timing) { cudaEventRecord(s.b, stream); marks.push_back(s); }
+                if (timing) { s.a = event(ev++); s.b = event(ev++); cudaEventRecord(s.a, ws); }
+                shadowKernel<<<shadowBlocks, kTraceBlock, smem, ws>>>(L.scene.wide, L.scene.packed, W, &L.counters[2],
+                                                                      L.errorFlag, postponeBelow, refill);
+                if (timing) { cudaEventRecord(s.b, ws); marks.push_back(s); }
                 n += 4;
                 q ^= 1;
             }
-            accumulateKernel<<<blocks(A.n, 256), 256, 0, stream>>>(A, B);
+            // Samples of a pixel are added in sample order: after the
+            // previous wave's accumulation, whichever lane ran it.
+            if (two && wave > 0) cudaStreamWaitEvent(ws, overlap->accumulated, 0);
+            accumulateKernel<<<blocks(A.n, 256), 256, 0, ws>>>(A, W);
+            if (two) cudaEventRecord(overlap->accumulated, ws);
             n++;
         }
+    }
+    if (two) {
+        cudaEventRecord(overlap->join, overlap->stream);
+        cudaStreamWaitEvent(stream, overlap->join, 0);
     }
     cudaError_t e = cudaGetLastError();
     if (launches) *launches = n;

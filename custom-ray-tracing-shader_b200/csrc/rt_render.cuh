@@ -45,6 +45,18 @@ struct WavefrontBuffers {
 struct TraceTuning {
     int postpone = 0;  // postpone triangle tests in sparse warps (measured neutral on B200)
     int refill = 24;   // refill idle lanes when fewer lanes than this are busy
+    int lanes = 2;     // waves in flight (1 or 2, see WaveOverlap)
+};
+
+// Second lane of waves: odd waves run on `stream` with their own buffers, so
+// the kernels of one wave fill the SMs while those of the other drain (every
+// persistent traversal launch ends in a tail of a few slow warps). Only the
+// accumulation is ordered across lanes (`accumulated`), which keeps each
+// pixel's samples added in sample order.
+struct WaveOverlap {
+    WavefrontBuffers* buffers = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr, accumulated = nullptr;
 };
 
 cudaError_t allocWavefront(WavefrontBuffers& b, int capacity);
@@ -58,7 +70,7 @@ cudaError_t launchMegakernel(const RenderLaunch& L, cudaStream_t stream, int* la
 // traversal kernels is accumulated into extendMs/shadowMs when timing != 0.
 cudaError_t launchWavefront(const RenderLaunch& L, WavefrontBuffers& b, const TraceTuning& tuning, cudaStream_t stream,
                             int* launches, float* extendMs, float* shadowMs, bool timing,
-                            float* primaryMs = nullptr);
+                            float* primaryMs = nullptr, const WaveOverlap* overlap = nullptr);
 
 // fetch: one device int of scratch (the work counter of the persistent kernel).
 cudaError_t launchQueries(const uint4* wide, const float4* packed, const float4* queries /*2 per query*/, int count,

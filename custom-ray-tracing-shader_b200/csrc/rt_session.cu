@@ -103,6 +103,8 @@ struct Session {
     int pieces = kDefaultPieces;
     int traversalLeaf = kDefaultTraversalLeaf;
     WavefrontBuffers wave;
+    WavefrontBuffers wave2;  // second lane of waves (tuning.lanes == 2)
+    WaveOverlap overlap;
     // Host mirrors for the CPU backends (filled on first use).
     std::vector<Accum> hostSum;
     std::vector<float> hostDepth;
@@ -131,11 +133,21 @@ const uint4* travWide(const Session* s) { return s->pieceBvh.wideNodes ? s->piec
 const float4* travPacked(const Session* s) { return s->pieceBvh.wideNodes ? s->pieceBvh.packedTris : s->bvh.packedTris; }
 const BuildResult& travBuild(const Session* s) { return s->pieceBvh.wideNodes ? s->pieceBuild : s->build; }
 
+void releaseOverlap(Session* s) {
+    freeWavefront(s->wave2);
+    if (s->overlap.stream) cudaStreamDestroy(s->overlap.stream);
+    cudaEvent_t events[] = {s->overlap.fork, s->overlap.join, s->overlap.accumulated};
+    for (cudaEvent_t e : events)
+        if (e) cudaEventDestroy(e);
+    s->overlap = WaveOverlap{};
+}
+
 void releaseScene(Session* s) {
     freeBvh(s->bvh);
     freeBvh(s->pieceBvh);
     s->pieceBuild = BuildResult{};
     freeWavefront(s->wave);
+    releaseOverlap(s);
     void* owned[] = {s->dTris, s->dLights, s->dDirs, s->dPassXor, s->dSeedHash, s->dSum, s->dDepth, s->dPixels,
                      s->dCounters, s->dError, s->dDenoise};
     for (void* p : owned)
@@ -179,9 +191,28 @@ SceneView deviceView(Session* s) {
 bool ensureWave(Session* s) {
     int pixels = s->width * s->height;
     int cap = s->pathsInFlight > 0 ? std::min(s->pathsInFlight, pixels) : pixels;
-    if (s->wave.capacity == cap) return true;
-    cudaError_t e = allocWavefront(s->wave, cap);
-    if (e != cudaSuccess) return fail(s, e, "could not allocate wavefront buffers");
+    cudaError_t e;
+    if (s->wave.capacity != cap && (e = allocWavefront(s->wave, cap)) != cudaSuccess)
+        return fail(s, e, "could not allocate wavefront buffers");
+    if (s->tuning.lanes < 2) {
+        if (s->overlap.stream) releaseOverlap(s);
+        return true;
+    }
+    if (s->wave2.capacity != cap && (e = allocWavefront(s->wave2, cap)) != cudaSuccess) {
+        releaseOverlap(s);
+        return fail(s, e, "could not allocate wavefront buffers");
+    }
+    if (!s->overlap.stream) {
+        WaveOverlap& o = s->overlap;
+        if ((e = cudaStreamCreateWithFlags(&o.stream, cudaStreamNonBlocking)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&o.fork, cudaEventDisableTiming)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&o.join, cudaEventDisableTiming)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&o.accumulated, cudaEventDisableTiming)) != cudaSuccess) {
+            releaseOverlap(s);
+            return fail(s, e, "could not create the second wave stream");
+        }
+    }
+    s->overlap.buffers = &s->wave2;
     return true;
 }
 
@@ -203,7 +234,8 @@ bool renderDevice(Session* s, const CameraData* camera, const RenderSettings* se
         e = launchMegakernel(L, s->stream, &launches);
     } else {
         if (!ensureWave(s)) return false;
-        e = launchWavefront(L, s->wave, s->tuning, s->stream, &launches, &extendMs, &shadowMs, timing, &primaryMs);
+        e = launchWavefront(L, s->wave, s->tuning, s->stream, &launches, &extendMs, &shadowMs, timing, &primaryMs,
+                            s->tuning.lanes > 1 ? &s->overlap : nullptr);
     }
     if (e != cudaSuccess) return fail(s, e);
     if ((e = cudaEventRecord(s->stop, s->stream)) != cudaSuccess) return fail(s, e);
@@ -787,6 +819,10 @@ int RtxSetTuning(void* p, int key, int value) {
         case RTX_TUNE_LEAF:
             if (value < 1 || value > 8) return 0;
             s->traversalLeaf = value;  // used by the next RtInitialize
+            return 1;
+        case RTX_TUNE_LANES:
+            if (value != 1 && value != 2) return 0;
+            s->tuning.lanes = value;
             return 1;
         default:
             return 0;

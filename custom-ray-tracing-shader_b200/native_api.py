@@ -298,12 +298,13 @@ class Session:
     def set_integrator(self, mode):
         self.check(self.lib.RtxSetIntegrator(self.handle, mode))
 
-    TUNE_PATHS_IN_FLIGHT, TUNE_POSTPONE, TUNE_REFILL, TUNE_PIECES, TUNE_LEAF = 1, 2, 3, 4, 5
+    TUNE_PATHS_IN_FLIGHT, TUNE_POSTPONE, TUNE_REFILL, TUNE_PIECES, TUNE_LEAF, TUNE_LANES = 1, 2, 3, 4, 5, 6
 
-    def set_tuning(self, paths_in_flight=None, postpone=None, refill=None, pieces=None, leaf=None):
+    def set_tuning(self, paths_in_flight=None, postpone=None, refill=None, pieces=None, leaf=None, lanes=None):
         """pieces and leaf apply from the next initialize()."""
         for key, value in ((self.TUNE_PATHS_IN_FLIGHT, paths_in_flight), (self.TUNE_POSTPONE, postpone),
-                           (self.TUNE_REFILL, refill), (self.TUNE_PIECES, pieces), (self.TUNE_LEAF, leaf)):
+                           (self.TUNE_REFILL, refill), (self.TUNE_PIECES, pieces), (self.TUNE_LEAF, leaf),
+                           (self.TUNE_LANES, lanes)):
             if value is not None:
                 self.check(self.lib.RtxSetTuning(self.handle, key, int(value)))
 

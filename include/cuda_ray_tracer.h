@@ -194,12 +194,18 @@ int RtxSetIntegrator(void* session, int mode);
  *   RTX_TUNE_LEAF             leaf size of that traversal tree (1..8, default 2;
  *                             the reference tree keeps 4; applies from the next
  *                             RtInitialize)
+ *   RTX_TUNE_LANES            waves in flight (1 or 2, default 2): with 2, odd
+ *                             waves run on a second stream with their own
+ *                             path buffers, overlapping the end of one wave's
+ *                             kernels with the other's; samples are still
+ *                             added to each pixel in sample order
  */
 #define RTX_TUNE_PATHS_IN_FLIGHT 1
 #define RTX_TUNE_POSTPONE 2
 #define RTX_TUNE_REFILL 3
 #define RTX_TUNE_PIECES 4
 #define RTX_TUNE_LEAF 5
+#define RTX_TUNE_LANES 6
 int RtxSetTuning(void* session, int key, int value);
 /* Light arriving from outside the scene on rays that leave it after the first
  * bounce (primary misses stay black, as in the reference). mode 0: the

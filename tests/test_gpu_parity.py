@@ -127,22 +127,28 @@ def test_gpu_render_bit_exact_vs_reference_cuda(session, reference, integrator):
 
 
 def test_gpu_integrators_bit_identical(session):
+    """Megakernel and wavefront, one or several waves per pass, one or two
+    waves in flight (RTX_TUNE_LANES): the same bytes."""
     tris, cam, st, w, h = scenes.cornell_sphere()
     st.raysPerPixel = 4
     session.initialize(tris, w, h)
     out = []
-    for integrator, paths in ((0, 0), (1, 0), (0, 5000)):
-        session.set_integrator(integrator)
-        if paths:
-            session.set_tuning(paths_in_flight=paths)  # several waves per pass
-        session.lib.RtReset(session.handle)
-        for _ in range(2):
-            rgba, _ = session.render(cam, st)
-        out.append((rgba.tobytes(), session.accumulation().tobytes(), session.render_stats()))
-    assert out[0][0] == out[1][0] == out[2][0]
-    assert out[0][1] == out[1][1] == out[2][1]
-    for k in ('primaryRays', 'secondaryRays', 'shadowRays'):
-        assert out[0][2][k] == out[1][2][k] == out[2][2][k]
+    try:
+        for integrator, paths, lanes in ((0, 0, 2), (1, 0, 2), (0, 5000, 2), (0, 5000, 1), (0, 0, 1)):
+            session.set_integrator(integrator)
+            session.set_tuning(lanes=lanes)
+            if paths:
+                session.set_tuning(paths_in_flight=paths)  # several waves per pass (5000 does not divide w*h)
+            session.lib.RtReset(session.handle)
+            for _ in range(2):
+                rgba, _ = session.render(cam, st)
+            out.append((rgba.tobytes(), session.accumulation().tobytes(), session.render_stats()))
+    finally:
+        session.set_tuning(lanes=2)
+    for o in out[1:]:
+        assert o[0] == out[0][0] and o[1] == out[0][1]
+        for k in ('primaryRays', 'secondaryRays', 'shadowRays'):
+            assert o[2][k] == out[0][2][k]
     assert out[0][2]['primaryRays'] == w * h * 4
 
 
