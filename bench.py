@@ -71,7 +71,7 @@ def parse():
     p.add_argument('--leaf', type=int, default=None,
                    help='leaf size of the traversal tree (RTX_TUNE_LEAF; default: the library default)')
     p.add_argument('--lanes', type=int, default=None,
-                   help='waves in flight, 1 or 2 (RTX_TUNE_LANES; default: the library default)')
+                   help="waves in flight, 1..4 (RTX_TUNE_LANES; default: the library default)")
     p.add_argument('--denoiser-only', action='store_true',
                    help='only time learned-denoiser inference at 1920x1080 (a small case for profiling)')
     p.set_defaults(quality=True, batch=True, denoiser=True)
@@ -579,7 +579,7 @@ def run_ours(args, rank, local_rank, world):
         s.set_tuning(leaf=args.leaf)
     if args.lanes is not None:
         s.set_tuning(lanes=args.lanes)
-    lanes = args.lanes if args.lanes is not None else 2  # RTX_TUNE_LANES default
+    lanes = args.lanes if args.lanes is not None else 4  # RTX_TUNE_LANES default
     t_init = time.perf_counter()
     s.initialize(tris, w, h)
     init_wall_ms = (time.perf_counter() - t_init) * 1e3

@@ -402,18 +402,26 @@ cudaError_t launchWavefront(const RenderLaunch& L, WavefrontBuffers& B, const Tr
         return pool[k];
     };
     size_t ev = 0;
-    const bool two = overlap && overlap->buffers && overlap->stream && overlap->buffers->capacity == B.capacity;
-    WavefrontBuffers* lanes[2] = {&B, two ? overlap->buffers : &B};
-    cudaStream_t laneStream[2] = {stream, two ? overlap->stream : stream};
+    int nLanes = overlap ? std::max(1, std::min(overlap->lanes, kMaxLanes)) : 1;
+    for (int k = 1; k < nLanes; k++)
+        if (!overlap->buffers[k - 1] || !overlap->streams[k - 1] || overlap->buffers[k - 1]->capacity != B.capacity)
+            nLanes = 1;
+    const bool two = nLanes > 1;
+    WavefrontBuffers* lanes[kMaxLanes] = {&B};
+    cudaStream_t laneStream[kMaxLanes] = {stream};
+    for (int k = 1; k < nLanes; k++) {
+        lanes[k] = overlap->buffers[k - 1];
+        laneStream[k] = overlap->streams[k - 1];
+    }
     if (two) {
-        cudaEventRecord(overlap->fork, stream);  // the second lane starts after the work queued so far
-        cudaStreamWaitEvent(overlap->stream, overlap->fork, 0);
+        cudaEventRecord(overlap->fork, stream);  // the other lanes start after the work queued so far
+        for (int k = 1; k < nLanes; k++) cudaStreamWaitEvent(laneStream[k], overlap->fork, 0);
     }
     int wave = 0;
     for (int r = 0; r < L.set.raysPerPixel; r++) {
         for (int start = 0; start < pixels; start += B.capacity, wave++) {
-            WavefrontBuffers& W = *lanes[two ? wave & 1 : 0];
-            cudaStream_t ws = laneStream[two ? wave & 1 : 0];
+            WavefrontBuffers& W = *lanes[wave % nLanes];
+            cudaStream_t ws = laneStream[wave % nLanes];
             WaveArgs A{L, r, start, pixels - start < B.capacity ? pixels - start : B.capacity};
             generateKernel<<<blocks(A.n, 256), 256, 0, ws>>>(A, W);
             n++;
@@ -443,9 +451,9 @@ cudaError_t launchWavefront(const RenderLaunch& L, WavefrontBuffers& B, const Tr
             n++;
         }
     }
-    if (two) {
-        cudaEventRecord(overlap->join, overlap->stream);
-        cudaStreamWaitEvent(stream, overlap->join, 0);
+    for (int k = 1; k < nLanes; k++) {
+        cudaEventRecord(overlap->joins[k - 1], laneStream[k]);
+        cudaStreamWaitEvent(stream, overlap->joins[k - 1], 0);
     }
     cudaError_t e = cudaGetLastError();
     if (launches) *launches = n;

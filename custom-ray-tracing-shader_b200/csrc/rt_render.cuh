@@ -45,18 +45,23 @@ struct WavefrontBuffers {
 struct TraceTuning {
     int postpone = 0;  // postpone triangle tests in sparse warps (measured neutral on B200)
     int refill = 24;   // refill idle lanes when fewer lanes than this are busy
-    int lanes = 2;     // waves in flight (1 or 2, see WaveOverlap)
+    int lanes = 4;     // waves in flight (1..kMaxLanes, see WaveOverlap)
 };
 
-// Second lane of waves: odd waves run on `stream` with their own buffers, so
-// the kernels of one wave fill the SMs while those of the other drain (every
-// persistent traversal launch ends in a tail of a few slow warps). Only the
-// accumulation is ordered across lanes (`accumulated`), which keeps each
-// pixel's samples added in sample order.
+// Lanes of waves: wave j runs on lane j % lanes, lane 0 on the caller's
+// stream and buffers, lane k > 0 on streams[k - 1] with buffers[k - 1], so
+// the kernels of one wave fill the SMs while those of another drain (every
+// persistent traversal launch ends in a tail of a few slow warps, and shading
+// is memory-bound where traversal is not). Only the accumulation is ordered
+// across lanes (`accumulated`), which keeps each pixel's samples added in
+// sample order.
+constexpr int kMaxLanes = 4;
 struct WaveOverlap {
-    WavefrontBuffers* buffers = nullptr;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t fork = nullptr, join = nullptr, accumulated = nullptr;
+    int lanes = 1;
+    WavefrontBuffers* buffers[kMaxLanes - 1] = {};
+    cudaStream_t streams[kMaxLanes - 1] = {};
+    cudaEvent_t joins[kMaxLanes - 1] = {};
+    cudaEvent_t fork = nullptr, accumulated = nullptr;
 };
 
 cudaError_t allocWavefront(WavefrontBuffers& b, int capacity);

@@ -103,7 +103,7 @@ struct Session {
     int pieces = kDefaultPieces;
     int traversalLeaf = kDefaultTraversalLeaf;
     WavefrontBuffers wave;
-    WavefrontBuffers wave2;  // second lane of waves (tuning.lanes == 2)
+    WavefrontBuffers laneWaves[kMaxLanes - 1];  // buffers of lanes 1.. (tuning.lanes > 1)
     WaveOverlap overlap;
     // Host mirrors for the CPU backends (filled on first use).
     std::vector<Accum> hostSum;
@@ -134,12 +134,15 @@ const float4* travPacked(const Session* s) { return s->pieceBvh.wideNodes ? s->p
 const BuildResult& travBuild(const Session* s) { return s->pieceBvh.wideNodes ? s->pieceBuild : s->build; }
 
 void releaseOverlap(Session* s) {
-    freeWavefront(s->wave2);
-    if (s->overlap.stream) cudaStreamDestroy(s->overlap.stream);
-    cudaEvent_t events[] = {s->overlap.fork, s->overlap.join, s->overlap.accumulated};
-    for (cudaEvent_t e : events)
-        if (e) cudaEventDestroy(e);
-    s->overlap = WaveOverlap{};
+    WaveOverlap& o = s->overlap;
+    for (int k = 0; k < kMaxLanes - 1; k++) {
+        freeWavefront(s->laneWaves[k]);
+        if (o.streams[k]) cudaStreamDestroy(o.streams[k]);
+        if (o.joins[k]) cudaEventDestroy(o.joins[k]);
+    }
+    if (o.fork) cudaEventDestroy(o.fork);
+    if (o.accumulated) cudaEventDestroy(o.accumulated);
+    o = WaveOverlap{};
 }
 
 void releaseScene(Session* s) {
@@ -194,25 +197,25 @@ bool ensureWave(Session* s) {
     cudaError_t e;
     if (s->wave.capacity != cap && (e = allocWavefront(s->wave, cap)) != cudaSuccess)
         return fail(s, e, "could not allocate wavefront buffers");
-    if (s->tuning.lanes < 2) {
-        if (s->overlap.stream) releaseOverlap(s);
-        return true;
-    }
-    if (s->wave2.capacity != cap && (e = allocWavefront(s->wave2, cap)) != cudaSuccess) {
+    const int lanes = s->tuning.lanes;
+    WaveOverlap& o = s->overlap;
+    if (lanes < o.lanes) releaseOverlap(s);  // fewer lanes: drop the extra ones
+    if (lanes < 2) return true;
+    if (!o.fork && ((e = cudaEventCreateWithFlags(&o.fork, cudaEventDisableTiming)) != cudaSuccess ||
+                    (e = cudaEventCreateWithFlags(&o.accumulated, cudaEventDisableTiming)) != cudaSuccess)) {
         releaseOverlap(s);
-        return fail(s, e, "could not allocate wavefront buffers");
+        return fail(s, e, "could not create the wave lane events");
     }
-    if (!s->overlap.stream) {
-        WaveOverlap& o = s->overlap;
-        if ((e = cudaStreamCreateWithFlags(&o.stream, cudaStreamNonBlocking)) != cudaSuccess ||
-            (e = cudaEventCreateWithFlags(&o.fork, cudaEventDisableTiming)) != cudaSuccess ||
-            (e = cudaEventCreateWithFlags(&o.join, cudaEventDisableTiming)) != cudaSuccess ||
-            (e = cudaEventCreateWithFlags(&o.accumulated, cudaEventDisableTiming)) != cudaSuccess) {
+    for (int k = 0; k < lanes - 1; k++) {
+        if ((s->laneWaves[k].capacity != cap && (e = allocWavefront(s->laneWaves[k], cap)) != cudaSuccess) ||
+            (!o.streams[k] && (e = cudaStreamCreateWithFlags(&o.streams[k], cudaStreamNonBlocking)) != cudaSuccess) ||
+            (!o.joins[k] && (e = cudaEventCreateWithFlags(&o.joins[k], cudaEventDisableTiming)) != cudaSuccess)) {
             releaseOverlap(s);
-            return fail(s, e, "could not create the second wave stream");
+            return fail(s, e, "could not allocate a wave lane");
         }
+        o.buffers[k] = &s->laneWaves[k];
     }
-    s->overlap.buffers = &s->wave2;
+    o.lanes = lanes;
     return true;
 }
 
@@ -821,7 +824,7 @@ int RtxSetTuning(void* p, int key, int value) {
             s->traversalLeaf = value;  // used by the next RtInitialize
             return 1;
         case RTX_TUNE_LANES:
-            if (value != 1 && value != 2) return 0;
+            if (value < 1 || value > kMaxLanes) return 0;
             s->tuning.lanes = value;
             return 1;
         default:

@@ -194,10 +194,10 @@ int RtxSetIntegrator(void* session, int mode);
  *   RTX_TUNE_LEAF             leaf size of that traversal tree (1..8, default 2;
  *                             the reference tree keeps 4; applies from the next
  *                             RtInitialize)
- *   RTX_TUNE_LANES            waves in flight (1 or 2, default 2): with 2, odd
- *                             waves run on a second stream with their own
- *                             path buffers, overlapping the end of one wave's
- *                             kernels with the other's; samples are still
+ *   RTX_TUNE_LANES            waves in flight (1..4, default 4): wave j runs
+ *                             on lane j % lanes, each lane a stream with its
+ *                             own path buffers, so the end of one wave's
+ *                             kernels overlaps another's; samples are still
  *                             added to each pixel in sample order
  */
 #define RTX_TUNE_PATHS_IN_FLIGHT 1

@@ -127,14 +127,14 @@ def test_gpu_render_bit_exact_vs_reference_cuda(session, reference, integrator):
 
 
 def test_gpu_integrators_bit_identical(session):
-    """Megakernel and wavefront, one or several waves per pass, one or two
+    """Megakernel and wavefront, one or several waves per pass, one to four
     waves in flight (RTX_TUNE_LANES): the same bytes."""
     tris, cam, st, w, h = scenes.cornell_sphere()
     st.raysPerPixel = 4
     session.initialize(tris, w, h)
     out = []
     try:
-        for integrator, paths, lanes in ((0, 0, 2), (1, 0, 2), (0, 5000, 2), (0, 5000, 1), (0, 0, 1)):
+        for integrator, paths, lanes in ((0, 0, 2), (1, 0, 2), (0, 5000, 2), (0, 5000, 1), (0, 0, 1), (0, 5000, 3), (0, 0, 4)):
             session.set_integrator(integrator)
             session.set_tuning(lanes=lanes)
             if paths:
@@ -144,7 +144,7 @@ def test_gpu_integrators_bit_identical(session):
                 rgba, _ = session.render(cam, st)
             out.append((rgba.tobytes(), session.accumulation().tobytes(), session.render_stats()))
     finally:
-        session.set_tuning(lanes=2)
+        session.set_tuning(lanes=4)
     for o in out[1:]:
         assert o[0] == out[0][0] and o[1] == out[0][1]
         for k in ('primaryRays', 'secondaryRays', 'shadowRays'):
