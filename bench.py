@@ -467,7 +467,7 @@ def batch_run(lib, args):
         'spp_per_frame': st.raysPerPixel, 'max_depth': st.maxBounces,
         'build_ms': built['buildMs'], 'build_mtris_per_s': built['triangles'] / built['buildMs'] / 1e3,
         'generate_s': gen_s, 'autotune_s': tune_s, 'autotune': tried,
-        'tuned': {k: tuned[k] for k in ('block', 'capacity', 'refill', 'width', 'pieces')},
+        'tuned': {k: tuned[k] for k in ('block', 'capacity', 'refill', 'width', 'pieces', 'lanes')},
         'batched_graph': graph, 'batched_launches': launches, 'per_view_launches': per_view,
         'speedup_vs_per_view': per_view['frame_ms'] / graph['frame_ms'],
         'same_rays': graph['rays_per_frame'] == per_view_rays,

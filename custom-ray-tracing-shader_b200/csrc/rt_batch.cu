@@ -355,8 +355,14 @@ struct Batch {
     unsigned long long* dCounters = nullptr;
     int* dError = nullptr;
     WavefrontBuffers wave;
+    // Lanes of waves beyond the first (wave j on lane j % lanes; WaveOverlap).
+    WavefrontBuffers laneWaves[kMaxLanes - 1];
+    cudaStream_t laneStreams[kMaxLanes - 1] = {};
+    cudaEvent_t laneJoins[kMaxLanes - 1] = {};
+    cudaEvent_t fork = nullptr, accumulated = nullptr;
+    int lanesReady = 1;
     // Tuning.
-    int block = 128, capacity = 0, refill = 24, width = 8, useGraph = 1, pieces = 3, leaf = 2;
+    int block = 128, capacity = 0, refill = 24, width = 8, useGraph = 1, pieces = 3, leaf = 2, lanes = 4;
     int environmentMode = 0;
     float3 environment = make_float3(0.0f, 0.0f, 0.0f);
     // Frame state.
@@ -533,19 +539,63 @@ int waveCapacity(const Batch* b) {
     return (int)std::min<long long>(want, (long long)b->pixels);
 }
 
+void freeLanes(Batch* b) {
+    for (int k = 0; k < kMaxLanes - 1; k++) {
+        freeWavefront(b->laneWaves[k]);
+        if (b->laneStreams[k]) cudaStreamDestroy(b->laneStreams[k]);
+        if (b->laneJoins[k]) cudaEventDestroy(b->laneJoins[k]);
+        b->laneStreams[k] = nullptr;
+        b->laneJoins[k] = nullptr;
+    }
+    if (b->fork) cudaEventDestroy(b->fork);
+    if (b->accumulated) cudaEventDestroy(b->accumulated);
+    b->fork = b->accumulated = nullptr;
+    b->lanesReady = 1;
+}
+
 bool ensureWave(Batch* b) {
     const int cap = waveCapacity(b);
-    if (b->wave.capacity == cap) return true;
-    dropGraph(b);
-    cudaError_t e = allocWavefront(b->wave, cap);
-    if (e != cudaSuccess) return failB(b, e, "wavefront buffers");
+    cudaError_t e;
+    if (b->wave.capacity != cap) {
+        dropGraph(b);
+        if ((e = allocWavefront(b->wave, cap)) != cudaSuccess) return failB(b, e, "wavefront buffers");
+    }
+    if (b->lanes < b->lanesReady) { dropGraph(b); freeLanes(b); }
+    if (b->lanes < 2) return true;
+    if (!b->fork && ((e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming)) != cudaSuccess ||
+                     (e = cudaEventCreateWithFlags(&b->accumulated, cudaEventDisableTiming)) != cudaSuccess)) {
+        freeLanes(b);
+        return failB(b, e, "wave lane events");
+    }
+    for (int k = 0; k < b->lanes - 1; k++) {
+        if (b->laneWaves[k].capacity != cap) {
+            dropGraph(b);
+            if ((e = allocWavefront(b->laneWaves[k], cap)) != cudaSuccess) { freeLanes(b); return failB(b, e, "wavefront buffers"); }
+        }
+        if ((!b->laneStreams[k] && (e = cudaStreamCreateWithFlags(&b->laneStreams[k], cudaStreamNonBlocking)) != cudaSuccess) ||
+            (!b->laneJoins[k] && (e = cudaEventCreateWithFlags(&b->laneJoins[k], cudaEventDisableTiming)) != cudaSuccess)) {
+            freeLanes(b);
+            return failB(b, e, "wave lanes");
+        }
+    }
+    if (b->lanesReady != b->lanes) dropGraph(b);
+    b->lanesReady = b->lanes;
     return true;
 }
 
-// The kernels of one frame, in order, on b->stream (captured or launched).
+// The kernels of one frame on b->stream and the lane streams forked from it
+// (captured or launched).
 cudaError_t enqueueFrame(Batch* b, const Settings& set, int* launches) {
-    cudaStream_t s = b->stream;
+    cudaStream_t main = b->stream;
     int n = 0;
+    const int nLanes = b->lanesReady;
+    WavefrontBuffers* laneWave[kMaxLanes] = {&b->wave};
+    cudaStream_t laneStream[kMaxLanes] = {main};
+    for (int k = 1; k < nLanes; k++) {
+        laneWave[k] = &b->laneWaves[k - 1];
+        laneStream[k] = b->laneStreams[k - 1];
+    }
+    cudaStream_t s = main;
     cudaError_t e;
     if ((e = cudaMemsetAsync(b->dCounters, 0, 4 * sizeof(unsigned long long), s)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(b->dError, 0, sizeof(int), s)) != cudaSuccess) return e;
@@ -557,34 +607,51 @@ cudaError_t enqueueFrame(Batch* b, const Settings& set, int* launches) {
                  b->dSum, b->dDepth, b->dPixels, b->dCounters, b->dError};
     const int cap = b->wave.capacity;
     const int shadeBlocks = deviceSms() * (2048 / 256);
+    if (nLanes > 1) {
+        if ((e = cudaEventRecord(b->fork, main)) != cudaSuccess) return e;
+        for (int k = 1; k < nLanes; k++)
+            if ((e = cudaStreamWaitEvent(laneStream[k], b->fork, 0)) != cudaSuccess) return e;
+    }
+    int wave = 0;
     for (int r = 0; r < set.raysPerPixel; r++) {
-        for (size_t start = 0; start < b->pixels; start += (size_t)cap) {
+        for (size_t start = 0; start < b->pixels; start += (size_t)cap, wave++) {
+            s = laneStream[wave % nLanes];
+            WavefrontBuffers& W = *laneWave[wave % nLanes];
             BatchWave A{F, r, (unsigned)start, (int)std::min<size_t>((size_t)cap, b->pixels - start)};
-            batchGenerateKernel<<<blocksFor(A.n, 256), 256, 0, s>>>(A, b->wave);
+            batchGenerateKernel<<<blocksFor(A.n, 256), 256, 0, s>>>(A, W);
             n++;
             int q = 0;
             for (int bounce = 0; bounce < set.maxBounces; bounce++) {
-                batchResetQueuesKernel<<<1, 32, 0, s>>>(b->wave, q);
+                batchResetQueuesKernel<<<1, 32, 0, s>>>(W, q);
                 unsigned long long* rays = &b->dCounters[bounce == 0 ? 0 : 1];
                 switch (b->block) {
-                    case 64: launchTraversal<64>(false, b->aWide, b->aPacked, b->wave, q, b->dViews, b->dScenes, rays, b->dError, b->refill, s); break;
-                    case 256: launchTraversal<256>(false, b->aWide, b->aPacked, b->wave, q, b->dViews, b->dScenes, rays, b->dError, b->refill, s); break;
-                    default: launchTraversal<128>(false, b->aWide, b->aPacked, b->wave, q, b->dViews, b->dScenes, rays, b->dError, b->refill, s); break;
+                    case 64: launchTraversal<64>(false, b->aWide, b->aPacked, W, q, b->dViews, b->dScenes, rays, b->dError, b->refill, s); break;
+                    case 256: launchTraversal<256>(false, b->aWide, b->aPacked, W, q, b->dViews, b->dScenes, rays, b->dError, b->refill, s); break;
+                    default: launchTraversal<128>(false, b->aWide, b->aPacked, W, q, b->dViews, b->dScenes, rays, b->dError, b->refill, s); break;
                 }
-                batchShadeKernel<<<shadeBlocks, 256, 0, s>>>(A, b->wave, q, bounce);
+                batchShadeKernel<<<shadeBlocks, 256, 0, s>>>(A, W, q, bounce);
                 unsigned long long* shadowRays = &b->dCounters[2];
                 switch (b->block) {
-                    case 64: launchTraversal<64>(true, b->aWide, b->aPacked, b->wave, q, b->dViews, b->dScenes, shadowRays, b->dError, b->refill, s); break;
-                    case 256: launchTraversal<256>(true, b->aWide, b->aPacked, b->wave, q, b->dViews, b->dScenes, shadowRays, b->dError, b->refill, s); break;
-                    default: launchTraversal<128>(true, b->aWide, b->aPacked, b->wave, q, b->dViews, b->dScenes, shadowRays, b->dError, b->refill, s); break;
+                    case 64: launchTraversal<64>(true, b->aWide, b->aPacked, W, q, b->dViews, b->dScenes, shadowRays, b->dError, b->refill, s); break;
+                    case 256: launchTraversal<256>(true, b->aWide, b->aPacked, W, q, b->dViews, b->dScenes, shadowRays, b->dError, b->refill, s); break;
+                    default: launchTraversal<128>(true, b->aWide, b->aPacked, W, q, b->dViews, b->dScenes, shadowRays, b->dError, b->refill, s); break;
                 }
                 n += 4;
                 q ^= 1;
             }
-            batchAccumulateKernel<<<blocksFor(A.n, 256), 256, 0, s>>>(A, b->wave);
+            // Samples of a pixel are added in sample order, whichever lane
+            // ran the previous wave.
+            if (nLanes > 1 && wave > 0 && (e = cudaStreamWaitEvent(s, b->accumulated, 0)) != cudaSuccess) return e;
+            batchAccumulateKernel<<<blocksFor(A.n, 256), 256, 0, s>>>(A, W);
+            if (nLanes > 1 && (e = cudaEventRecord(b->accumulated, s)) != cudaSuccess) return e;
             n++;
         }
     }
+    for (int k = 1; k < nLanes; k++) {
+        if ((e = cudaEventRecord(b->laneJoins[k - 1], laneStream[k])) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(main, b->laneJoins[k - 1], 0)) != cudaSuccess) return e;
+    }
+    s = main;
     batchAdvanceKernel<<<1, 32, 0, s>>>(b->dSample, set.raysPerPixel);
     n++;
     if (launches) *launches = n;
@@ -666,6 +733,7 @@ void RtxBatchDestroy(void* p) {
     freeArena(b);
     freeViews(b);
     freeWavefront(b->wave);
+    freeLanes(b);
     for (BatchSceneData& S : b->scenes) {
         freeBvh(S.bvh);
         if (S.dTris) cudaFree(S.dTris);
@@ -823,6 +891,10 @@ int RtxBatchSetTuning(void* p, int key, int value) {
             if (value < 1 || value > 8) break;
             if (value != b->leaf) { b->leaf = value; freeArena(b); }
             return 1;
+        case RTX_BATCH_LANES:
+            if (value < 1 || value > kMaxLanes) break;
+            if (value != b->lanes) { b->lanes = value; dropGraph(b); }
+            return 1;
         default:
             break;
     }
@@ -848,14 +920,14 @@ int RtxBatchAutotune(void* p, const RenderSettings* settings, RtxBatchTune* resu
             if (!renderFrame(b, &probe, &ms)) return false;
             if (i > 0) best = std::min(best, ms);
         }
-        tried.push_back(RtxBatchTune{b->block, waveCapacity(b), b->refill, b->width, best, b->pieces});
+        tried.push_back(RtxBatchTune{b->block, waveCapacity(b), b->refill, b->width, best, b->pieces, b->lanes});
         return true;
     };
     auto trial = [&](int key, int value, float& ms) -> bool {
         return RtxBatchSetTuning(b, key, value) && measure(ms);
     };
     // Coordinate search: pieces per triangle, BVH width, block size, queue
-    // capacity, refill.
+    // capacity, refill, lanes of waves.
     float bestMs = 0;
     if (!measure(bestMs)) return 0;
     struct Axis { int key; std::vector<int> values; int* current; };
@@ -867,7 +939,8 @@ int RtxBatchAutotune(void* p, const RenderSettings* settings, RtxBatchTune* resu
                    {RTX_BATCH_WIDTH, {8, 4}, &b->width},
                    {RTX_BATCH_BLOCK, {64, 128, 256}, &b->block},
                    {RTX_BATCH_CAPACITY, caps, &b->capacity},
-                   {RTX_BATCH_REFILL, {8, 16, 24, 32}, &b->refill}};
+                   {RTX_BATCH_REFILL, {8, 16, 24, 32}, &b->refill},
+                   {RTX_BATCH_LANES, {4, 2, 1}, &b->lanes}};
     if (b->capacity <= 0) b->capacity = waveCapacity(b);
     for (Axis& a : axes) {
         int bestValue = *a.current;
@@ -897,6 +970,7 @@ int RtxBatchStatsGet(void* p, RtxBatchStats* stats) {
     b->stats.refill = b->refill;
     b->stats.width = b->width;
     b->stats.pieces = b->pieces;
+    b->stats.lanes = b->lanes;
     *stats = b->stats;
     return 1;
 }

@@ -69,7 +69,7 @@ class RtxBvhStats(c.Structure):
 
 class RtxBatchTune(c.Structure):
     _fields_ = [('block', c.c_int), ('capacity', c.c_int), ('refill', c.c_int), ('width', c.c_int),
-                ('frameMs', c.c_float), ('pieces', c.c_int)]
+                ('frameMs', c.c_float), ('pieces', c.c_int), ('lanes', c.c_int)]
 
 
 class RtxBatchStats(c.Structure):
@@ -77,11 +77,11 @@ class RtxBatchStats(c.Structure):
                 ('paths', c.c_ulonglong), ('frameMs', c.c_float), ('buildMs', c.c_float),
                 ('triangles', c.c_longlong), ('pixels', c.c_longlong), ('scenes', c.c_int), ('views', c.c_int),
                 ('kernelLaunches', c.c_int), ('graph', c.c_int), ('block', c.c_int), ('capacity', c.c_int),
-                ('refill', c.c_int), ('width', c.c_int), ('pieces', c.c_int)]
+                ('refill', c.c_int), ('width', c.c_int), ('pieces', c.c_int), ('lanes', c.c_int)]
 
 
 assert (c.sizeof(Triangle), c.sizeof(Camera), c.sizeof(Settings)) == (116, 64, 28)
-assert (c.sizeof(RtxBatchTune), c.sizeof(RtxBatchStats)) == (24, 96)
+assert (c.sizeof(RtxBatchTune), c.sizeof(RtxBatchStats)) == (28, 96)
 assert (c.sizeof(PixelSum), c.sizeof(BvhNode), c.sizeof(RtxQuery), c.sizeof(RtxHit)) == (40, 32, 28, 16)
 
 # numpy views of the same records, for scenes of millions of triangles.
@@ -418,7 +418,7 @@ class Unet:
 class Batch:
     """Many views of many scenes rendered together (RtxBatch* entry points)."""
 
-    BLOCK, CAPACITY, REFILL, GRAPH, WIDTH, PIECES, LEAF = 1, 2, 3, 4, 5, 6, 7
+    BLOCK, CAPACITY, REFILL, GRAPH, WIDTH, PIECES, LEAF, LANES = 1, 2, 3, 4, 5, 6, 7, 8
 
     def __init__(self, lib=None):
         self.lib = lib or load_library()
@@ -485,9 +485,11 @@ class Batch:
         self.check(self.lib.RtxBatchReadAccumulation(self.handle, view, out.ctypes.data, out.size))
         return out
 
-    def set_tuning(self, block=None, capacity=None, refill=None, graph=None, width=None, pieces=None, leaf=None):
+    def set_tuning(self, block=None, capacity=None, refill=None, graph=None, width=None, pieces=None, leaf=None,
+                   lanes=None):
         for key, value in ((self.BLOCK, block), (self.CAPACITY, capacity), (self.REFILL, refill),
-                           (self.GRAPH, graph), (self.WIDTH, width), (self.PIECES, pieces), (self.LEAF, leaf)):
+                           (self.GRAPH, graph), (self.WIDTH, width), (self.PIECES, pieces), (self.LEAF, leaf),
+                           (self.LANES, lanes)):
             if value is not None:
                 self.check(self.lib.RtxBatchSetTuning(self.handle, key, int(value)))
 

@@ -265,7 +265,8 @@ int RtxReadAovs(void* session, float* aovs, int count);
  *                      PixelSum records (bottom-up rows like RtRender)
  *   RtxBatchSetTuning  RTX_BATCH_* keys below
  *   RtxBatchAutotune   times candidate pieces per triangle, BVH widths, block
- *                      sizes, queue capacities and refill thresholds on this batch (frames of
+ *                      sizes, queue capacities, refill thresholds and lanes
+ *                      of waves on this batch (frames of
  *                      one path per pixel), keeps the fastest and writes
  *                      the candidates to results (up to maxResults)
  * Returns 1 on success and 0 on failure (RtxBatchLastError) unless noted. */
@@ -276,10 +277,12 @@ int RtxReadAovs(void* session, float* aovs, int count);
 #define RTX_BATCH_WIDTH 5     /* BVH node width: 4 or 8 (default 8); rebuilds every scene */
 #define RTX_BATCH_PIECES 6    /* most pieces per triangle of the traversal trees (1..8, default 3; see RTX_TUNE_PIECES) */
 #define RTX_BATCH_LEAF 7      /* leaf size of the traversal trees (1..8, default 2) */
+#define RTX_BATCH_LANES 8     /* waves in flight (1..4, default 4; see RTX_TUNE_LANES) */
 typedef struct RtxBatchTune {
     int block, capacity, refill, width;
     float frameMs;  /* device time of one frame of one path per pixel */
     int pieces;     /* pieces per triangle of the traversal trees */
+    int lanes;      /* waves in flight */
 } RtxBatchTune;
 typedef struct RtxBatchStats {
     unsigned long long primaryRays, secondaryRays, shadowRays, paths;  /* of the last frame */
@@ -290,7 +293,7 @@ typedef struct RtxBatchStats {
     int kernelLaunches;            /* kernels in one frame (graph nodes when replayed) */
     int graph;                     /* 1 if the last frame was a graph launch */
     int block, capacity, refill, width;  /* tuning in use */
-    int pieces;
+    int pieces, lanes;
 } RtxBatchStats;
 void* RtxBatchCreate(void);
 void RtxBatchDestroy(void* batch);

@@ -77,6 +77,9 @@ def make_batch(lib, scene_list, views):
     {'pieces': 4, 'width': 4},
     {'leaf': 4},
     {'leaf': 1, 'pieces': 2},
+    {'lanes': 1},
+    {'lanes': 2, 'capacity': 1024},       # two lanes, waves spanning views
+    {'lanes': 3, 'capacity': 3000, 'graph': 0},
 ])
 def test_batch_equals_single_view_renders(lib, reference, tuning):
     scene_list, views, expect = reference
@@ -94,6 +97,7 @@ def test_batch_equals_single_view_renders(lib, reference, tuning):
         assert st['pixels'] == sum(w * h for _, _, w, h in views)
         assert st['paths'] == st['pixels'] * 4 and st['primaryRays'] == st['paths']
         assert st['width'] == tuning.get('width', 8) and st['block'] == tuning.get('block', 128)
+        assert st['lanes'] == tuning.get('lanes', 4)
         assert st['kernelLaunches'] > 0
 
 
@@ -123,9 +127,9 @@ def test_autotune_keeps_results(lib, reference):
         assert all(t['frameMs'] > 0 for t in tried)
         best = min(tried, key=lambda t: t['frameMs'])
         st = b.stats()
-        assert (st['block'], st['refill'], st['width'], st['pieces']) == \
-            (best['block'], best['refill'], best['width'], best['pieces'])
-        assert {t['pieces'] for t in tried} == {1, 2, 3}
+        assert (st['block'], st['refill'], st['width'], st['pieces'], st['lanes']) == \
+            (best['block'], best['refill'], best['width'], best['pieces'], best['lanes'])
+        assert {t['pieces'] for t in tried} == {1, 2, 3} and {t['lanes'] for t in tried} == {1, 2, 4}
         assert b.sample_count() == 0
         b.render(SETTINGS)
         b.render(SETTINGS)
@@ -148,7 +152,7 @@ def test_batch_errors(lib):
         b.add_view(k, cam, 16, 16)
         with pytest.raises(Exception, match='render first'):
             b.image(0)
-        for key, value in (('block', 96), ('capacity', 10), ('refill', 0), ('graph', 2), ('width', 6)):
+        for key, value in (('block', 96), ('capacity', 10), ('refill', 0), ('graph', 2), ('width', 6), ('lanes', 5)):
             with pytest.raises(Exception, match='out of range'):
                 b.set_tuning(**{key: value})
         bad = Settings(4, 1.0, 0.0, 1.0, 0.5, 42, 17)
