@@ -654,6 +654,21 @@ def run_ours(args, rank, local_rank, world):
         e2e_rays += st['primaryRays'] + st['secondaryRays'] + st['shadowRays']
     e2e_s = dist.max(time.perf_counter() - e0)
     e2e_value = dist.sum(e2e_rays) / e2e_s / 1e6
+    # The dominant kernel alone: with one lane of waves no launch shares the
+    # GPU, so its CUDA-event durations are the kernel's own (after the timed
+    # region; every rank takes the same steps).
+    isolated = None
+    if best == 'wavefront' and lanes > 1:
+        s.set_tuning(lanes=1)
+        iso_ms, iso_rays = 0.0, 0
+        for _ in range(min(args.steps, 5)):
+            flush()
+            s.render_device(cam, settings)
+            st = s.render_stats()
+            iso_ms += st['extendMs']
+            iso_rays += st['primaryRays'] + st['secondaryRays']
+        s.set_tuning(lanes=lanes)
+        isolated = (iso_ms, iso_rays)
     peak, peak_kind = measured_peaks()
     result = None
     if rank == 0:
@@ -681,6 +696,11 @@ def run_ours(args, rank, local_rank, world):
             tdata = json.loads(tfile.read_text()).get(best)
             if tdata:
                 traffic = tdata['dram_bytes_per_ray'] * rays_per_launch
+        iso = None
+        if isolated and isolated[0] > 0:
+            iso_achieved = isolated[1] * alg['closest'] / (isolated[0] / 1e3) / 1e9
+            iso = {'achieved': iso_achieved, 'frac': iso_achieved / peak, 'lanes': 1,
+                   'note': 'extendKernel timed with one lane of waves (no overlap), outside the timed region'}
         roofline = {'bound': 'hbm', 'kernel': kernel, 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
                     'frac': (achieved / peak) if achieved else None, 'traffic': traffic,
                     'peak_source': f'{peak_kind} hbm_gbs (MEASURED_PEAKS.json)' if peak_kind == 'measured' else
@@ -690,6 +710,7 @@ def run_ours(args, rank, local_rank, world):
                     'launch_timing': ('CUDA events around each launch; two lanes of waves overlap, so a launch '
                                       'shares the GPU with the other lane for part of its duration and achieved is '
                                       'a lower bound' if lanes > 1 else 'CUDA events around each launch, one lane'),
+                    'isolated': iso,
                     'sample_pixels': alg['sample_pixels']}
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
