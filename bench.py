@@ -70,6 +70,10 @@ def parse():
                    help='pieces per triangle of the traversal tree (RTX_TUNE_PIECES; default: the library default)')
     p.add_argument('--leaf', type=int, default=None,
                    help='leaf size of the traversal tree (RTX_TUNE_LEAF; default: the library default)')
+    p.add_argument('--refill', type=int, default=None,
+                   help='refill threshold of the persistent traversal (RTX_TUNE_REFILL; default: the library default)')
+    p.add_argument('--paths', type=int, default=None,
+                   help='paths per wave (RTX_TUNE_PATHS_IN_FLIGHT; default: all pixels)')
     p.add_argument('--lanes', type=int, default=None,
                    help="waves in flight, 1..4 (RTX_TUNE_LANES; default: the library default)")
     p.add_argument('--denoiser-only', action='store_true',
@@ -366,6 +370,7 @@ def quality_run(lib, args, target_db=35.0):
             arm['at_8spp'] = trials[0]
             return arm
 
+        s.denoise()  # the first call allocates the filter's buffers and loads its kernels
         denoised = denoised_arm('guided a-trous wavelet filter (RtDenoise without a network)')
         learned = None
         if DENOISER_WEIGHTS.exists():
@@ -579,7 +584,11 @@ def run_ours(args, rank, local_rank, world):
         s.set_tuning(leaf=args.leaf)
     if args.lanes is not None:
         s.set_tuning(lanes=args.lanes)
-    lanes = args.lanes if args.lanes is not None else 4  # RTX_TUNE_LANES default
+    if args.refill is not None:
+        s.set_tuning(refill=args.refill)
+    if args.paths is not None:
+        s.set_tuning(paths_in_flight=args.paths)
+    lanes = args.lanes if args.lanes is not None else 2  # RTX_TUNE_LANES default
     t_init = time.perf_counter()
     s.initialize(tris, w, h)
     init_wall_ms = (time.perf_counter() - t_init) * 1e3

@@ -64,18 +64,21 @@ __global__ void __launch_bounds__(kMegaBlock) megakernel(RenderLaunch L) {
 }
 
 // ---- wavefront stages ----
+// A wave is the paths [start, start + n) of a pass, path k being sample row
+// k / (w * h) of pixel k % (w * h); a wave may span several sample rows.
 struct WaveArgs {
     RenderLaunch L;
-    int r;            // raysPerPixel row of this wave
-    int pixStart, n;  // pixels [pixStart, pixStart + n)
+    int start, n;
 };
+__device__ __forceinline__ int waveRow(const WaveArgs& A, int p) { return (A.start + p) / (A.L.w * A.L.h); }
+__device__ __forceinline__ int wavePixel(const WaveArgs& A, int p) { return (A.start + p) % (A.L.w * A.L.h); }
 
 __global__ void generateKernel(WaveArgs A, WavefrontBuffers B) {
     int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= A.n) return;
-    int pix = A.pixStart + p;
+    int pix = wavePixel(A, p);
     int x = pix % A.L.w, y = pix / A.L.w;
-    Sampler rng{A.L.passXor + A.r * kSobolDims, A.L.seedHash, (unsigned)pix, 0u};
+    Sampler rng{A.L.passXor + waveRow(A, p) * kSobolDims, A.L.seedHash, (unsigned)pix, 0u};
     PathState st = startPath(A.L.cam, A.L.set, x, y, A.L.w, A.L.h, rng);
     B.pathA[p] = make_float4(st.origin.x, st.origin.y, st.origin.z, 0.0f);
     B.pathB[p] = make_float4(st.dir.x, st.dir.y, st.dir.z, 0.0f);
@@ -142,7 +145,8 @@ __global__ void shadeKernel(WaveArgs A, WavefrontBuffers B, int q, int bounce) {
             st.albedo = v3(al.x, al.y, al.z); st.normal = v3(no.x, no.y, no.z);
             st.depth = al.w;
             Hit h{__float_as_int(hv.w), hv.x, hv.y, hv.z};
-            Sampler rng{A.L.passXor + A.r * kSobolDims, A.L.seedHash, (unsigned)(A.pixStart + p), 4u + 8u * (unsigned)bounce};
+            Sampler rng{A.L.passXor + waveRow(A, p) * kSobolDims, A.L.seedHash, (unsigned)wavePixel(A, p),
+                        4u + 8u * (unsigned)bounce};
             unsigned f = shadeBounce(A.L.scene, A.L.set, bounce, st, h, rng, req);
             cont = (f & kContinue) != 0;
             shadow = (f & kShadow) != 0;
@@ -193,11 +197,15 @@ __global__ void resetQueuesKernel(WavefrontBuffers B, int q) {
     if (threadIdx.x == 0) { B.counts[q ^ 1] = 0; B.counts[2] = 0; B.counts[3] = 0; B.counts[4] = 0; }
 }
 
-__global__ void accumulateKernel(WaveArgs A, WavefrontBuffers B) {
-    int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= A.n) return;
-    size_t i = (size_t)(A.pixStart + p);
-    const bool first = A.r == 0 && A.L.sample0 == 0;
+// Adds paths [first, first + count) of the wave (all of one sample row) to
+// their pixels' sums; the rows of a wave are added by successive launches, so
+// each pixel's samples are added in sample order.
+__global__ void accumulateKernel(WaveArgs A, WavefrontBuffers B, int firstPath, int count) {
+    int p = firstPath + blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= firstPath + count) return;
+    size_t i = (size_t)wavePixel(A, p);
+    const int row = waveRow(A, p);
+    const bool first = row == 0 && A.L.sample0 == 0;
     Accum total = first ? Accum{v3(0, 0, 0), v3(0, 0, 0), v3(0, 0, 0), 0u} : A.L.sums[i];
     float depthTotal = first ? 0.0f : A.L.depthSums[i];
     float4 rad = B.radiance[p], al = B.albedo[p], no = B.normal[p];
@@ -207,7 +215,7 @@ __global__ void accumulateKernel(WaveArgs A, WavefrontBuffers B) {
     addPath(total, st);
     A.L.sums[i] = total;
     A.L.depthSums[i] = depthTotal + al.w;
-    if (A.r == A.L.set.raysPerPixel - 1)
+    if (row == A.L.set.raysPerPixel - 1)
         A.L.pixels[i] = displayPixel(total, A.L.sample0 + (unsigned)A.L.set.raysPerPixel, A.L.set.exposure);
 }
 
@@ -418,11 +426,12 @@ cudaError_t launchWavefront(const RenderLaunch& L, WavefrontBuffers& B, const Tr
         for (int k = 1; k < nLanes; k++) cudaStreamWaitEvent(laneStream[k], overlap->fork, 0);
     }
     int wave = 0;
-    for (int r = 0; r < L.set.raysPerPixel; r++) {
-        for (int start = 0; start < pixels; start += B.capacity, wave++) {
+    const int total = pixels * L.set.raysPerPixel;  // paths of the pass (at most 4096^2 * 16 < 2^31)
+    {
+        for (int start = 0; start < total; start += B.capacity, wave++) {
             WavefrontBuffers& W = *lanes[wave % nLanes];
             cudaStream_t ws = laneStream[wave % nLanes];
-            WaveArgs A{L, r, start, pixels - start < B.capacity ? pixels - start : B.capacity};
+            WaveArgs A{L, start, total - start < B.capacity ? total - start : B.capacity};
             generateKernel<<<blocks(A.n, 256), 256, 0, ws>>>(A, W);
             n++;
             int q = 0;
@@ -445,10 +454,16 @@ cudaError_t launchWavefront(const RenderLaunch& L, WavefrontBuffers& B, const Tr
             }
             // Samples of a pixel are added in sample order: after the
             // previous wave's accumulation, whichever lane ran it.
+            // Within the wave, one launch per sample row it covers.
             if (two && wave > 0) cudaStreamWaitEvent(ws, overlap->accumulated, 0);
-            accumulateKernel<<<blocks(A.n, 256), 256, 0, ws>>>(A, W);
+            for (int first = 0; first < A.n;) {
+                const int rowEnd = ((A.start + first) / pixels + 1) * pixels - A.start;
+                const int count = (rowEnd < A.n ? rowEnd : A.n) - first;
+                accumulateKernel<<<blocks(count, 256), 256, 0, ws>>>(A, W, first, count);
+                first += count;
+                n++;
+            }
             if (two) cudaEventRecord(overlap->accumulated, ws);
-            n++;
         }
     }
     for (int k = 1; k < nLanes; k++) {

@@ -45,7 +45,7 @@ struct WavefrontBuffers {
 struct TraceTuning {
     int postpone = 0;  // postpone triangle tests in sparse warps (measured neutral on B200)
     int refill = 24;   // refill idle lanes when fewer lanes than this are busy
-    int lanes = 4;     // waves in flight (1..kMaxLanes, see WaveOverlap)
+    int lanes = 2;     // waves in flight (1..kMaxLanes, see WaveOverlap)
 };
 
 // Lanes of waves: wave j runs on lane j % lanes, lane 0 on the caller's

@@ -191,9 +191,17 @@ SceneView deviceView(Session* s) {
                      travBuild(s).wideDepth, s->environmentMode, s->environment};
 }
 
-bool ensureWave(Session* s) {
-    int pixels = s->width * s->height;
-    int cap = s->pathsInFlight > 0 ? std::min(s->pathsInFlight, pixels) : pixels;
+// Paths per wave: RTX_TUNE_PATHS_IN_FLIGHT (default kDefaultPathsInFlight),
+// at most the paths of a pass of raysPerPixel rows. Large waves make few,
+// long traversal launches, so the drain at the end of each launch weighs
+// little: on the 1920x1080, 16-path workload waves of one row (2.07M paths)
+// gave 2,567 Mrays/s, of 2^24 paths 2,960 (168 B of path state per path and
+// lane: 2.8 GB per lane).
+constexpr int kDefaultPathsInFlight = 1 << 24;
+bool ensureWave(Session* s, int raysPerPixel) {
+    const long long pixels = (long long)s->width * s->height;
+    const int cap = (int)std::min<long long>(s->pathsInFlight > 0 ? s->pathsInFlight : kDefaultPathsInFlight,
+                                             pixels * raysPerPixel);
     cudaError_t e;
     if (s->wave.capacity != cap && (e = allocWavefront(s->wave, cap)) != cudaSuccess)
         return fail(s, e, "could not allocate wavefront buffers");
@@ -236,7 +244,7 @@ bool renderDevice(Session* s, const CameraData* camera, const RenderSettings* se
     if (s->integrator == 1) {
         e = launchMegakernel(L, s->stream, &launches);
     } else {
-        if (!ensureWave(s)) return false;
+        if (!ensureWave(s, set.raysPerPixel)) return false;
         e = launchWavefront(L, s->wave, s->tuning, s->stream, &launches, &extendMs, &shadowMs, timing, &primaryMs,
                             s->tuning.lanes > 1 ? &s->overlap : nullptr);
     }

@@ -174,7 +174,11 @@ int RtxSetIntegrator(void* session, int mode);
 /* Tunables of the wavefront integrator, one key at a time. Results do not
  * depend on them, only speed does. Returns 0 for an unknown key or a value
  * out of range.
- *   RTX_TUNE_PATHS_IN_FLIGHT  paths per wave (>= 1024; default: all pixels)
+ *   RTX_TUNE_PATHS_IN_FLIGHT  paths per wave (>= 1024; default 16,777,216,
+ *                             at most width * height * raysPerPixel); a wave
+ *                             may span several of a pass's raysPerPixel rows.
+ *                             Path state takes 168 bytes per path and lane
+ *                             (2.8 GB per lane at the default)
  *   RTX_TUNE_POSTPONE         1 = postpone triangle tests in sparse warps,
  *                             0 = off (default)
  *   RTX_TUNE_REFILL           refill a warp's idle lanes when fewer than this
@@ -194,7 +198,7 @@ int RtxSetIntegrator(void* session, int mode);
  *   RTX_TUNE_LEAF             leaf size of that traversal tree (1..8, default 2;
  *                             the reference tree keeps 4; applies from the next
  *                             RtInitialize)
- *   RTX_TUNE_LANES            waves in flight (1..4, default 4): wave j runs
+ *   RTX_TUNE_LANES            waves in flight (1..4, default 2): wave j runs
  *                             on lane j % lanes, each lane a stream with its
  *                             own path buffers, so the end of one wave's
  *                             kernels overlaps another's; samples are still

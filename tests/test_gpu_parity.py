@@ -134,17 +134,20 @@ def test_gpu_integrators_bit_identical(session):
     session.initialize(tris, w, h)
     out = []
     try:
-        for integrator, paths, lanes in ((0, 0, 2), (1, 0, 2), (0, 5000, 2), (0, 5000, 1), (0, 0, 1), (0, 5000, 3), (0, 0, 4)):
+        # Waves of 5,000 paths straddle sample rows; waves of 150,000 span
+        # two to three rows of the 65,536-pixel image; 262,144 is the pass.
+        cases = ((0, 0, 2), (1, 0, 2), (0, 5000, 2), (0, 5000, 1), (0, 0, 1), (0, 5000, 3), (0, 0, 4),
+                 (0, 150000, 4), (0, 150000, 1), (0, 262144, 2))
+        for integrator, paths, lanes in cases:
             session.set_integrator(integrator)
             session.set_tuning(lanes=lanes)
-            if paths:
-                session.set_tuning(paths_in_flight=paths)  # several waves per pass (5000 does not divide w*h)
+            session.set_tuning(paths_in_flight=paths or w * h)
             session.lib.RtReset(session.handle)
             for _ in range(2):
                 rgba, _ = session.render(cam, st)
             out.append((rgba.tobytes(), session.accumulation().tobytes(), session.render_stats()))
     finally:
-        session.set_tuning(lanes=4)
+        session.set_tuning(lanes=2)
     for o in out[1:]:
         assert o[0] == out[0][0] and o[1] == out[0][1]
         for k in ('primaryRays', 'secondaryRays', 'shadowRays'):
