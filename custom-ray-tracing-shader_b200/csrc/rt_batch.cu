@@ -51,12 +51,18 @@ struct BatchFrame {
     unsigned long long* counters;  // [0] primary, [1] secondary, [2] shadow rays
     int* errorFlag;
 };
+// A wave is the paths [start, start + n) of a frame, path k being sample
+// row k / pixels of global pixel k % pixels; a wave may span several rows.
 struct BatchWave {
     BatchFrame F;
-    int r;           // raysPerPixel row of this wave
-    unsigned start;  // first global pixel
-    int n;           // paths in the wave
+    unsigned long long start;  // first path
+    unsigned pixels;           // pixels of all views
+    int n;                     // paths in the wave
 };
+__device__ __forceinline__ int batchRow(const BatchWave& A, int p) { return (int)((A.start + (unsigned)p) / A.pixels); }
+__device__ __forceinline__ unsigned batchPixel(const BatchWave& A, int p) {
+    return (unsigned)((A.start + (unsigned)p) % A.pixels);
+}
 
 // View holding global pixel g: the last view whose first pixel is <= g.
 __device__ __forceinline__ int findView(const BatchView* views, int count, unsigned g) {
@@ -86,12 +92,12 @@ __global__ void batchSobolKernel(const unsigned* dirs, const unsigned* sample, i
 __global__ void batchGenerateKernel(BatchWave A, WavefrontBuffers B) {
     int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= A.n) return;
-    const unsigned g = A.start + (unsigned)p;
+    const unsigned g = batchPixel(A, p);
     const int v = findView(A.F.views, A.F.viewCount, g);
     const BatchView& V = A.F.views[v];
     const unsigned local = g - V.pixelStart;
     const int x = (int)(local % (unsigned)V.w), y = (int)(local / (unsigned)V.w);
-    Sampler rng{A.F.passXor + A.r * kSobolDims, A.F.seedHash, local, 0u};
+    Sampler rng{A.F.passXor + batchRow(A, p) * kSobolDims, A.F.seedHash, local, 0u};
     PathState st = startPath(V.cam, A.F.set, x, y, V.w, V.h, rng);
     B.pathA[p] = make_float4(st.origin.x, st.origin.y, st.origin.z, 0.0f);
     B.pathB[p] = make_float4(st.dir.x, st.dir.y, st.dir.z, __int_as_float(v));
@@ -168,8 +174,8 @@ __global__ void batchShadeKernel(BatchWave A, WavefrontBuffers B, int q, int bou
             st.albedo = v3(al.x, al.y, al.z); st.normal = v3(no.x, no.y, no.z);
             st.depth = al.w;
             Hit h{__float_as_int(hv.w), hv.x, hv.y, hv.z};
-            const unsigned local = A.start + (unsigned)p - V.pixelStart;
-            Sampler rng{A.F.passXor + A.r * kSobolDims, A.F.seedHash, local, 4u + 8u * (unsigned)bounce};
+            const unsigned local = batchPixel(A, p) - V.pixelStart;
+            Sampler rng{A.F.passXor + batchRow(A, p) * kSobolDims, A.F.seedHash, local, 4u + 8u * (unsigned)bounce};
             unsigned f = shadeBounce(S.view, A.F.set, bounce, st, h, rng, req);
             cont = (f & kContinue) != 0;
             shadow = (f & kShadow) != 0;
@@ -222,12 +228,15 @@ __global__ void batchResetQueuesKernel(WavefrontBuffers B, int q) {
     if (threadIdx.x == 0) { B.counts[q ^ 1] = 0; B.counts[2] = 0; B.counts[3] = 0; B.counts[4] = 0; }
 }
 
-__global__ void batchAccumulateKernel(BatchWave A, WavefrontBuffers B) {
-    int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= A.n) return;
-    const size_t i = (size_t)A.start + (size_t)p;
+// Adds paths [firstPath, firstPath + count) of the wave (all of one sample
+// row) to their pixels; the rows of a wave are added by successive launches.
+__global__ void batchAccumulateKernel(BatchWave A, WavefrontBuffers B, int firstPath, int count) {
+    int p = firstPath + blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= firstPath + count) return;
+    const size_t i = batchPixel(A, p);
+    const int row = batchRow(A, p);
     const unsigned sample0 = *A.F.sample;
-    const bool first = A.r == 0 && sample0 == 0;
+    const bool first = row == 0 && sample0 == 0;
     Accum total = first ? Accum{v3(0, 0, 0), v3(0, 0, 0), v3(0, 0, 0), 0u} : A.F.sums[i];
     float depthTotal = first ? 0.0f : A.F.depthSums[i];
     float4 rad = B.radiance[p], al = B.albedo[p], no = B.normal[p];
@@ -237,7 +246,7 @@ __global__ void batchAccumulateKernel(BatchWave A, WavefrontBuffers B) {
     addPath(total, st);
     A.F.sums[i] = total;
     A.F.depthSums[i] = depthTotal + al.w;
-    if (A.r == A.F.set.raysPerPixel - 1)
+    if (row == A.F.set.raysPerPixel - 1)
         A.F.pixels[i] = displayPixel(total, sample0 + (unsigned)A.F.set.raysPerPixel, A.F.set.exposure);
 }
 
@@ -362,7 +371,7 @@ struct Batch {
     cudaEvent_t fork = nullptr, accumulated = nullptr;
     int lanesReady = 1;
     // Tuning.
-    int block = 128, capacity = 0, refill = 24, width = 8, useGraph = 1, pieces = 3, leaf = 2, lanes = 4;
+    int block = 128, capacity = 0, refill = 24, width = 8, useGraph = 1, pieces = 3, leaf = 2, lanes = 2;
     int environmentMode = 0;
     float3 environment = make_float3(0.0f, 0.0f, 0.0f);
     // Frame state.
@@ -534,9 +543,11 @@ bool ensureViews(Batch* b) {
     return true;
 }
 
-int waveCapacity(const Batch* b) {
-    const long long want = b->capacity > 0 ? b->capacity : (4ll << 20);
-    return (int)std::min<long long>(want, (long long)b->pixels);
+// Paths per wave: RTX_BATCH_CAPACITY (default 2^24), at most the paths of a
+// frame of raysPerPixel rows.
+int waveCapacity(const Batch* b, int raysPerPixel) {
+    const long long want = b->capacity > 0 ? b->capacity : (1ll << 24);
+    return (int)std::min<long long>(want, (long long)b->pixels * raysPerPixel);
 }
 
 void freeLanes(Batch* b) {
@@ -553,8 +564,8 @@ void freeLanes(Batch* b) {
     b->lanesReady = 1;
 }
 
-bool ensureWave(Batch* b) {
-    const int cap = waveCapacity(b);
+bool ensureWave(Batch* b, int raysPerPixel) {
+    const int cap = waveCapacity(b, raysPerPixel);
     cudaError_t e;
     if (b->wave.capacity != cap) {
         dropGraph(b);
@@ -613,11 +624,12 @@ cudaError_t enqueueFrame(Batch* b, const Settings& set, int* launches) {
             if ((e = cudaStreamWaitEvent(laneStream[k], b->fork, 0)) != cudaSuccess) return e;
     }
     int wave = 0;
-    for (int r = 0; r < set.raysPerPixel; r++) {
-        for (size_t start = 0; start < b->pixels; start += (size_t)cap, wave++) {
+    const unsigned long long total = (unsigned long long)b->pixels * (unsigned long long)set.raysPerPixel;
+    {
+        for (unsigned long long start = 0; start < total; start += (unsigned long long)cap, wave++) {
             s = laneStream[wave % nLanes];
             WavefrontBuffers& W = *laneWave[wave % nLanes];
-            BatchWave A{F, r, (unsigned)start, (int)std::min<size_t>((size_t)cap, b->pixels - start)};
+            BatchWave A{F, start, (unsigned)b->pixels, (int)std::min<unsigned long long>((unsigned long long)cap, total - start)};
             batchGenerateKernel<<<blocksFor(A.n, 256), 256, 0, s>>>(A, W);
             n++;
             int q = 0;
@@ -642,9 +654,15 @@ cudaError_t enqueueFrame(Batch* b, const Settings& set, int* launches) {
             // Samples of a pixel are added in sample order, whichever lane
             // ran the previous wave.
             if (nLanes > 1 && wave > 0 && (e = cudaStreamWaitEvent(s, b->accumulated, 0)) != cudaSuccess) return e;
-            batchAccumulateKernel<<<blocksFor(A.n, 256), 256, 0, s>>>(A, W);
+            for (int first = 0; first < A.n;) {
+                const long long rowEnd = (long long)((A.start + (unsigned)first) / b->pixels + 1) * (long long)b->pixels -
+                                         (long long)A.start;
+                const int count = (int)std::min<long long>(rowEnd, A.n) - first;
+                batchAccumulateKernel<<<blocksFor(count, 256), 256, 0, s>>>(A, W, first, count);
+                first += count;
+                n++;
+            }
             if (nLanes > 1 && (e = cudaEventRecord(b->accumulated, s)) != cudaSuccess) return e;
-            n++;
         }
     }
     for (int k = 1; k < nLanes; k++) {
@@ -667,7 +685,7 @@ bool renderFrame(Batch* b, const RenderSettings* settings, float* ms) {
     if (b->scenes.empty() || b->views.empty()) { b->error = "RtxBatchRender: add a scene and a view first"; return false; }
     if (!validBatchSettings(settings)) { b->error = "RtxBatchRender: invalid settings"; return false; }
     cudaSetDevice(b->device);
-    if (!ensureArena(b) || !ensureViews(b) || !ensureWave(b)) return false;
+    if (!ensureArena(b) || !ensureViews(b) || !ensureWave(b, settings->raysPerPixel)) return false;
     if (!b->haveLast || std::memcmp(settings, &b->last, sizeof(RenderSettings))) {
         resetSamples(b);
         dropGraph(b);
@@ -920,7 +938,8 @@ int RtxBatchAutotune(void* p, const RenderSettings* settings, RtxBatchTune* resu
             if (!renderFrame(b, &probe, &ms)) return false;
             if (i > 0) best = std::min(best, ms);
         }
-        tried.push_back(RtxBatchTune{b->block, waveCapacity(b), b->refill, b->width, best, b->pieces, b->lanes});
+        tried.push_back(RtxBatchTune{b->block, waveCapacity(b, probe.raysPerPixel), b->refill, b->width, best, b->pieces,
+                                     b->lanes});
         return true;
     };
     auto trial = [&](int key, int value, float& ms) -> bool {
@@ -941,7 +960,7 @@ int RtxBatchAutotune(void* p, const RenderSettings* settings, RtxBatchTune* resu
                    {RTX_BATCH_CAPACITY, caps, &b->capacity},
                    {RTX_BATCH_REFILL, {8, 16, 24, 32}, &b->refill},
                    {RTX_BATCH_LANES, {4, 2, 1}, &b->lanes}};
-    if (b->capacity <= 0) b->capacity = waveCapacity(b);
+    if (b->capacity <= 0) b->capacity = waveCapacity(b, probe.raysPerPixel);
     for (Axis& a : axes) {
         int bestValue = *a.current;
         for (int v : a.values) {
@@ -966,7 +985,7 @@ int RtxBatchStatsGet(void* p, RtxBatchStats* stats) {
     Batch* b = static_cast<Batch*>(p);
     if (!b || !stats) return 0;
     b->stats.block = b->block;
-    b->stats.capacity = b->viewsReady ? waveCapacity(b) : b->capacity;
+    b->stats.capacity = b->viewsReady ? waveCapacity(b, b->haveLast ? b->last.raysPerPixel : 1) : b->capacity;
     b->stats.refill = b->refill;
     b->stats.width = b->width;
     b->stats.pieces = b->pieces;

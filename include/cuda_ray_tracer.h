@@ -275,13 +275,13 @@ int RtxReadAovs(void* session, float* aovs, int count);
  *                      the candidates to results (up to maxResults)
  * Returns 1 on success and 0 on failure (RtxBatchLastError) unless noted. */
 #define RTX_BATCH_BLOCK 1     /* threads per block of the traversal kernels: 64, 128 or 256 */
-#define RTX_BATCH_CAPACITY 2  /* paths in flight per wave (>= 1024) */
+#define RTX_BATCH_CAPACITY 2  /* paths per wave (>= 1024, default 16,777,216); a wave may span sample rows */
 #define RTX_BATCH_REFILL 3    /* refill threshold of the persistent traversal (1..32) */
 #define RTX_BATCH_GRAPH 4     /* 1: replay frames from a CUDA graph (default), 0: launch kernels */
 #define RTX_BATCH_WIDTH 5     /* BVH node width: 4 or 8 (default 8); rebuilds every scene */
 #define RTX_BATCH_PIECES 6    /* most pieces per triangle of the traversal trees (1..8, default 3; see RTX_TUNE_PIECES) */
 #define RTX_BATCH_LEAF 7      /* leaf size of the traversal trees (1..8, default 2) */
-#define RTX_BATCH_LANES 8     /* waves in flight (1..4, default 4; see RTX_TUNE_LANES) */
+#define RTX_BATCH_LANES 8     /* waves in flight (1..4, default 2; see RTX_TUNE_LANES) */
 typedef struct RtxBatchTune {
     int block, capacity, refill, width;
     float frameMs;  /* device time of one frame of one path per pixel */

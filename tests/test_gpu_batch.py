@@ -80,6 +80,8 @@ def make_batch(lib, scene_list, views):
     {'lanes': 1},
     {'lanes': 2, 'capacity': 1024},       # two lanes, waves spanning views
     {'lanes': 3, 'capacity': 3000, 'graph': 0},
+    {'lanes': 3, 'capacity': 10000},       # waves cross sample rows as well as views
+    {'lanes': 1, 'capacity': 20000},
 ])
 def test_batch_equals_single_view_renders(lib, reference, tuning):
     scene_list, views, expect = reference
@@ -97,7 +99,7 @@ def test_batch_equals_single_view_renders(lib, reference, tuning):
         assert st['pixels'] == sum(w * h for _, _, w, h in views)
         assert st['paths'] == st['pixels'] * 4 and st['primaryRays'] == st['paths']
         assert st['width'] == tuning.get('width', 8) and st['block'] == tuning.get('block', 128)
-        assert st['lanes'] == tuning.get('lanes', 4)
+        assert st['lanes'] == tuning.get('lanes', 2)
         assert st['kernelLaunches'] > 0
 
 
