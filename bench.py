@@ -695,7 +695,9 @@ def run_ours(args, rank, local_rank, world):
         # the rays of one launch here.
         closest_step = (per_kind['primaryRays'] + per_kind['secondaryRays']) / args.steps
         if best == 'wavefront':
-            launches_step = settings.raysPerPixel * settings.maxBounces  # one wave per sample row
+            paths = w * h * settings.raysPerPixel
+            waves = -(-paths // min(args.paths or (1 << 24), paths))  # RTX_TUNE_PATHS_IN_FLIGHT default 2^24
+            launches_step = waves * settings.maxBounces  # one closest-hit launch per bounce of a wave
             rays_per_launch = closest_step / launches_step
         else:
             rays_per_launch = sum(per_kind.values()) / args.steps

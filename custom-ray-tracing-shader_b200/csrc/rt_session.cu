@@ -198,10 +198,15 @@ SceneView deviceView(Session* s) {
 // gave 2,567 Mrays/s, of 2^24 paths 2,960 (168 B of path state per path and
 // lane: 2.8 GB per lane).
 constexpr int kDefaultPathsInFlight = 1 << 24;
+// Buffers only grow while they fit the limit (the setting, or 16 rows of the
+// image), so passes of different sizes do not reallocate them; a wave is at
+// most the buffers' capacity.
 bool ensureWave(Session* s, int raysPerPixel) {
     const long long pixels = (long long)s->width * s->height;
-    const int cap = (int)std::min<long long>(s->pathsInFlight > 0 ? s->pathsInFlight : kDefaultPathsInFlight,
-                                             pixels * raysPerPixel);
+    const long long setting = s->pathsInFlight > 0 ? s->pathsInFlight : kDefaultPathsInFlight;
+    const int need = (int)std::min<long long>(setting, pixels * raysPerPixel);
+    const int limit = (int)std::min<long long>(setting, pixels * 16);
+    const int cap = (s->wave.capacity >= need && s->wave.capacity <= limit) ? s->wave.capacity : need;
     cudaError_t e;
     if (s->wave.capacity != cap && (e = allocWavefront(s->wave, cap)) != cudaSuccess)
         return fail(s, e, "could not allocate wavefront buffers");
@@ -240,11 +245,12 @@ bool renderDevice(Session* s, const CameraData* camera, const RenderSettings* se
                    s->dSum, s->dDepth, s->dPixels, s->dCounters, s->dError};
     int launches = 0;
     float extendMs = 0, shadowMs = 0, primaryMs = 0;
+    // Path buffers are (re)allocated before the timed span.
+    if (s->integrator != 1 && !ensureWave(s, set.raysPerPixel)) return false;
     if ((e = cudaEventRecord(s->start, s->stream)) != cudaSuccess) return fail(s, e);
     if (s->integrator == 1) {
         e = launchMegakernel(L, s->stream, &launches);
     } else {
-        if (!ensureWave(s, set.raysPerPixel)) return false;
         e = launchWavefront(L, s->wave, s->tuning, s->stream, &launches, &extendMs, &shadowMs, timing, &primaryMs,
                             s->tuning.lanes > 1 ? &s->overlap : nullptr);
     }
