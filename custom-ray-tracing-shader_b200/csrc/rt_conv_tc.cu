@@ -279,17 +279,20 @@ __global__ void __launch_bounds__(kThreads, 1) convTcKernel(ConvTcArgs a) {
                     __syncthreads();
                     if (tid == 0) {
                         tcFenceAfter();
-                        const uint32_t rbase = smemAddress(hbuf), wbase = smemAddress(wbuf);
+                        // Descriptors as base + offset in 16-byte units: the
+                        // start address is the low 14-bit field and every
+                        // operand lies in shared memory (< 256 KB), so the
+                        // sum never carries into the other fields.
+                        const uint64_t aBase = ummaSmemDesc(smemAddress(hbuf), ringPlane, 128u);
+                        const uint64_t bBase = ummaSmemDesc(smemAddress(wbuf), (uint32_t)a.cout * 16u, 128u);
                         const uint32_t acc = tmem + (uint32_t)(y & 1) * a.accCols;
+                        const uint32_t kStepA = 2u * 4u * kHaloW, kStepB = 2u * (uint32_t)a.cout;
                         for (int t = 0; t < 9; t++) {
                             const int dy = t / 3, dx = t % 3, slot = (y + dy - 1) & 3;
-                            for (int k = 0; k < a.kc / 16; k++) {
-                                const uint32_t aAddr = rbase + ((uint32_t)((2 * k * 4 + slot) * kHaloW + dx)) * 16u;
-                                const uint32_t bAddr = wbase + ((uint32_t)(t * groups + 2 * k) * (uint32_t)a.cout) * 16u;
-                                mmaBf16(acc, ummaSmemDesc(aAddr, ringPlane, 128u),
-                                        ummaSmemDesc(bAddr, (uint32_t)a.cout * 16u, 128u), idesc,
-                                        (t > 0 || k > 0) ? 1u : 0u);
-                            }
+                            uint64_t aDesc = aBase + (uint32_t)(slot * kHaloW + dx);
+                            uint64_t bDesc = bBase + (uint32_t)(t * groups) * (uint32_t)a.cout;
+                            for (int k = 0; k < a.kc / 16; k++, aDesc += kStepA, bDesc += kStepB)
+                                mmaBf16(acc, aDesc, bDesc, idesc, (t > 0 || k > 0) ? 1u : 0u);
                         }
                         mmaCommit((y & 1) ? bar1 : bar0);
                     }
@@ -339,17 +342,19 @@ __global__ void __launch_bounds__(kThreads, 1) convTcKernel(ConvTcArgs a) {
             __syncthreads();
             if (tid == 0) {
                 tcFenceAfter();
-                const uint32_t hbase = smemAddress(hbuf + (size_t)stage * a.haloBytes);
-                const uint32_t wbase = smemAddress(a.resident ? wbuf + (size_t)c * stageW : wbuf + (size_t)stage * stageW);
+                // Descriptors as base + offset in 16-byte units (see the
+                // ring loop above).
+                const uint64_t aBase = ummaSmemDesc(smemAddress(hbuf + (size_t)stage * a.haloBytes), haloPlane, 128u);
+                const uint64_t bBase = ummaSmemDesc(
+                    smemAddress(a.resident ? wbuf + (size_t)c * stageW : wbuf + (size_t)stage * stageW),
+                    (uint32_t)a.cout * 16u, 128u);
+                const uint32_t kStepA = 2u * 3u * kHaloW, kStepB = 2u * (uint32_t)a.cout;
                 for (int t = 0; t < 9; t++) {
                     const int dy = t / 3, dx = t % 3;
-                    for (int k = 0; k < a.kc / 16; k++) {
-                        const uint32_t aAddr = hbase + ((uint32_t)((2 * k * 3 + dy) * kHaloW + dx)) * 16u;
-                        const uint32_t bAddr = wbase + ((uint32_t)(t * groups + 2 * k) * (uint32_t)a.cout) * 16u;
-                        mmaBf16(tmem, ummaSmemDesc(aAddr, haloPlane, 128u),
-                                ummaSmemDesc(bAddr, (uint32_t)a.cout * 16u, 128u), idesc,
-                                (c > 0 || t > 0 || k > 0) ? 1u : 0u);
-                    }
+                    uint64_t aDesc = aBase + (uint32_t)(dy * kHaloW + dx);
+                    uint64_t bDesc = bBase + (uint32_t)(t * groups) * (uint32_t)a.cout;
+                    for (int k = 0; k < a.kc / 16; k++, aDesc += kStepA, bDesc += kStepB)
+                        mmaBf16(tmem, aDesc, bDesc, idesc, (c > 0 || t > 0 || k > 0) ? 1u : 0u);
                 }
                 mmaCommit(stage ? bar1 : bar0);
             }
