@@ -524,6 +524,7 @@ int RtDenoise(void* p, unsigned char* output, int outputBytes, float* millisecon
     if (s->lastBackend != 2 && s->hostDepth.size() == count) {
         if ((e = cudaMemcpyAsync(s->dDepth, s->hostDepth.data(), count * sizeof(float), cudaMemcpyHostToDevice, s->stream)) != cudaSuccess) { fail(s, e); return 0; }
     }
+    if ((e = cudaEventRecord(s->start, s->stream)) != cudaSuccess) { fail(s, e); return 0; }
     if (s->denoiser) {
         // Learned denoiser: AOVs -> U-Net -> display, all on the session stream.
         float* aov = reinterpret_cast<float*>(s->dDenoise);
@@ -533,7 +534,9 @@ int RtDenoise(void* p, unsigned char* output, int outputBytes, float* millisecon
         if ((e = s->denoiser->net.inferDevice(aov, s->height, s->width, radiance, s->stream, why)) != cudaSuccess) { fail(s, e, why.empty() ? nullptr : why.c_str()); return 0; }
         if ((e = launchPresentRadiance(s->dSum, radiance, (int)count, s->lastSettings.exposure, s->dPixels, s->stream)) != cudaSuccess) { fail(s, e); return 0; }
     } else if ((e = launchDenoise(s->dSum, s->samples, s->width, s->height, s->lastSettings.exposure, s->dDenoise, s->dPixels, s->stream)) != cudaSuccess) { fail(s, e); return 0; }
+    if ((e = cudaEventRecord(s->stop, s->stream)) != cudaSuccess) { fail(s, e); return 0; }
     if ((e = cudaStreamSynchronize(s->stream)) != cudaSuccess) { fail(s, e); return 0; }
+    if ((e = cudaEventElapsedTime(&s->stats.denoiseMs, s->start, s->stop)) != cudaSuccess) { fail(s, e); return 0; }
     if (s->denoiser) {
         std::string why;
         if ((e = s->denoiser->net.checkConvolutions(why)) != cudaSuccess) { fail(s, e, why.c_str()); return 0; }

@@ -57,7 +57,8 @@ class RtxHit(c.Structure):
 class RtxRenderStats(c.Structure):
     _fields_ = [('primaryRays', c.c_ulonglong), ('secondaryRays', c.c_ulonglong), ('shadowRays', c.c_ulonglong),
                 ('paths', c.c_ulonglong), ('renderMs', c.c_float), ('extendMs', c.c_float),
-                ('shadowMs', c.c_float), ('kernelLaunches', c.c_int), ('primaryMs', c.c_float)]
+                ('shadowMs', c.c_float), ('kernelLaunches', c.c_int), ('primaryMs', c.c_float),
+                ('denoiseMs', c.c_float)]
 
 
 class RtxBvhStats(c.Structure):

@@ -88,6 +88,8 @@ typedef struct RtxRenderStats {
     float shadowMs;                   /* part of renderMs spent in any-hit traversal kernels */
     int kernelLaunches;               /* kernels launched by the render */
     float primaryMs;                  /* part of extendMs spent on bounce 0 (wavefront integrator) */
+    float denoiseMs;                  /* device time of the last RtDenoise's kernels (AOVs, network or
+                                         filter, display), without its read-back */
 } RtxRenderStats;
 
 /* Summary of the acceleration structure built at RtInitialize. */

@@ -231,7 +231,7 @@ def test_session_aovs_and_learned_denoise(lib, session, net):
     plain, _ = session.denoise()
     session.set_denoiser(net)
     learned, ms = session.denoise()
-    assert ms > 0
+    assert ms > 0 and 0 < session.render_stats()['denoiseMs'] <= ms  # device time of the kernels, within the call
     radiance = net.infer(aovs)
     c = 1 - np.exp(-np.maximum(radiance, 0) * np.float32(settings.exposure))
     c = np.where(c <= 0.0031308, 12.92 * c, 1.055 * np.power(c, 1 / 2.4) - 0.055)
