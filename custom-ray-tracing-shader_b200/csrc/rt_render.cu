@@ -21,9 +21,11 @@ namespace rt {
 namespace {
 
 constexpr int kTileX = 16, kTileY = 8, kMegaBlock = kTileX * kTileY;
-// Resident blocks per SM the traversal kernels are compiled for: 7 caps them
-// at 72 registers (a few bytes of spills) for 7 instead of 6 blocks per SM.
-constexpr int kTraceMinBlocks = 7;
+// Resident blocks per SM the traversal kernels are compiled for: 8 caps them
+// at 64 registers (16-40 bytes of spills) for 32 resident warps. Measured on
+// the 1M-triangle workload with waves of 2^24 paths: 6 blocks (77-79
+// registers) 2,841 Mrays/s, 7 (72) 2,972, 8 (64) 3,003.
+constexpr int kTraceMinBlocks = 8;
 
 __global__ void sobolTablesKernel(const unsigned* dirs, unsigned sample0, int rpp, unsigned seed, unsigned* passXor,
                                   unsigned* seedHash) {
