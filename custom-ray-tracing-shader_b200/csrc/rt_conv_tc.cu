@@ -1,15 +1,16 @@
 // tcgen05 implicit-GEMM 3x3 convolution (see rt_conv_tc.cuh).
 //
-// One persistent block of 128 threads per SM (or more when shared and tensor
+// One persistent block of 256 threads per SM (or more when shared and tensor
 // memory allow) walks over tiles of 128 output pixels. For every tile the
 // input channels are taken in chunks of 16 or 32: all threads stage the
 // chunk's halo (and, when the weights do not fit in shared memory for the
 // whole kernel, the chunk's weights) with cp.async into one of two stages;
 // thread 0 issues the chunk's 9 taps x (chunk / 16) MMAs of 128 x N x 16 and
 // commits them to the stage's mbarrier, while the threads go on to stage
-// the next chunk into the other stage. After a tile's last chunk the four
-// warps read the accumulators back from tensor memory (each warp its 32
-// lanes = 32 pixels), add the bias, apply ReLU and store.
+// the next chunk into the other stage. After a tile's last chunk the eight
+// warps read the accumulators back from tensor memory (each warp 32 lanes =
+// 32 pixels and half of the channel groups), add the bias, apply ReLU and
+// store.
 //
 // Every wait on an mbarrier is bounded; past the bound the kernel stops its
 // work, waits for its own copies, frees its tensor memory, sets *errorFlag
@@ -24,7 +25,10 @@ namespace {
 using bf16 = __nv_bfloat16;
 constexpr int kTileM = 128;             // output pixels per tile (the MMA's M)
 constexpr int kHaloW = kTileM + 2;      // halo pixels per row
-constexpr int kThreads = 128;
+// Eight warps: staging is shared by all of them, and in the epilogue warp w
+// reads tensor-memory lanes 32 * (w % 4) .. + 31 (the lanes a warp may
+// access) and every other group of 16 accumulator columns from 16 * (w / 4).
+constexpr int kThreads = 256;
 constexpr uint32_t kHeaderBytes = 128;  // mbarriers and the tensor-memory address
 constexpr uint32_t kMaxSmem = 227 * 1024;
 constexpr long long kSpinLimit = 1ll << 24;  // about a second of polling
@@ -202,12 +206,13 @@ __global__ void __launch_bounds__(kThreads, 1) convTcKernel(ConvTcArgs a) {
     // accumulators from tensor memory, bias, ReLU, store.
     auto epilogue = [&](int rowIdx, int x0, uint32_t column) {
         tcFenceAfter();
-        const int x = x0 + warp * 32 + lane;
+        const int quarter = warp & 3, half = warp >> 2;
+        const int x = x0 + quarter * 32 + lane;
         const bool inside = x < a.w;
         const size_t pix = (size_t)rowIdx * a.w + (size_t)x;
-        for (int cb = 0; cb < a.cout; cb += 16) {
+        for (int cb = 16 * half; cb < a.cout; cb += 32) {
             uint32_t r[16];
-            tmemLoad16(tmem + ((uint32_t)(warp * 32) << 16) + column + (uint32_t)cb, r);
+            tmemLoad16(tmem + ((uint32_t)(quarter * 32) << 16) + column + (uint32_t)cb, r);
             if (!inside) continue;
             float v[16];
 #pragma unroll
