@@ -126,8 +126,10 @@ struct BatchExtendIO {
         hits[queue[k]] = make_float4(h.distance, h.u, h.v, __int_as_float(h.index));
     }
 };
+// Traversal kernels are compiled for 1,024 resident threads per SM (64
+// registers), as the single-scene ones.
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) batchExtendKernel(const uint4* wide, const float4* packed,
+__global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) batchExtendKernel(const uint4* wide, const float4* packed,
                                                            WavefrontBuffers B, int q, const BatchView* views,
                                                            const BatchScene* scenes, unsigned long long* counter,
                                                            int* errorFlag, int refill) {
@@ -217,7 +219,7 @@ struct BatchShadowIO {
     }
 };
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) batchShadowKernel(const uint4* wide, const float4* packed,
+__global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) batchShadowKernel(const uint4* wide, const float4* packed,
                                                            WavefrontBuffers B, unsigned long long* counter,
                                                            int* errorFlag, int refill) {
     BatchShadowIO io{B.shadowRay, B.shadowDir, B.shadowContrib, B.radiance};
