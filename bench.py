@@ -675,14 +675,20 @@ def run_ours(args, rank, local_rank, world):
     if best == 'wavefront' and lanes > 1:
         s.set_tuning(lanes=1)
         iso_ms, iso_rays = 0.0, 0
+        iso_kind = {'primaryRays': 0, 'secondaryRays': 0, 'shadowRays': 0}
+        iso_primary = iso_shadow = 0.0
         for _ in range(min(args.steps, 5)):
             flush()
             s.render_device(cam, settings)
             st = s.render_stats()
             iso_ms += st['extendMs']
+            iso_primary += st['primaryMs']
+            iso_shadow += st['shadowMs']
             iso_rays += st['primaryRays'] + st['secondaryRays']
+            for k in iso_kind:
+                iso_kind[k] += st[k]
         s.set_tuning(lanes=lanes)
-        isolated = (iso_ms, iso_rays)
+        isolated = (iso_ms, iso_rays, kernel_rates(best, iso_kind, iso_primary, iso_ms, iso_shadow, 1))
     peak, peak_kind = measured_peaks()
     result = None
     if rank == 0:
@@ -753,7 +759,8 @@ def run_ours(args, rank, local_rank, world):
             'roofline': roofline,
             'cpu_baseline': cpu,
             'rays': {k: v // args.steps for k, v in per_kind.items()},
-            'traversal_mrays_per_s': kernel_rates(best, per_kind, primary_ms, extend_ms, shadow_ms, lanes),
+            'traversal_mrays_per_s': dict(kernel_rates(best, per_kind, primary_ms, extend_ms, shadow_ms, lanes) or {},
+                                          isolated=isolated[2] if isolated else None),
             'wall_ms_per_step': wall * 1e3 / args.steps,
             'build': {'ms': bvh['buildMs'] + bvh['collapseMs'], 'binned_sah_ms': bvh['buildMs'],
                       'collapse_ms': bvh['collapseMs'],
