@@ -185,6 +185,31 @@ def test_gpu_full_size_scene(session, oracle):
     assert session.accumulation().tobytes() == a.tobytes()
 
 
+def test_gpu_full_size_pass_schedules_identical(session):
+    """The bench's pass on the 1,003,532-triangle workload (1920x1080, 16
+    paths per pixel, depth 3): the default schedule (two waves of up to 2^24
+    paths that straddle sample rows, on two lanes) accumulates the same bytes
+    as waves of one sample row on one lane and as the one-kernel integrator,
+    over two passes."""
+    tris, cam, st, w, h = scenes.displaced_sphere_room()
+    st.raysPerPixel = 16
+    session.initialize(tris, w, h)
+    out = []
+    for integrator, paths, lanes in ((0, 0, 2), (0, w * h, 1), (1, 0, 2)):
+        session.set_integrator(integrator)
+        session.set_tuning(lanes=lanes)
+        if paths:
+            session.set_tuning(paths_in_flight=paths)
+        session.lib.RtReset(session.handle)
+        for _ in range(2):
+            session.render_device(cam, st)
+        out.append((session.accumulation().tobytes(), session.render_stats()))
+    assert out[0][0] == out[1][0] == out[2][0]
+    for k in ('primaryRays', 'secondaryRays', 'shadowRays'):
+        assert out[0][1][k] == out[1][1][k] == out[2][1][k]
+    assert out[0][1]['primaryRays'] == w * h * 16
+
+
 def test_gpu_reference_snapshot(session, reference):
     """The reference's own 982-triangle Suzanne room (its Unity snapshot, via
     scene_io and the committed fixture): the GPU builder reproduces the
