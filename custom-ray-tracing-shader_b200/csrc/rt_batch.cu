@@ -288,6 +288,10 @@ struct TraceLaunch {
     static void configure() {
         if (extendBlocks) return;
         const size_t smem = traceSharedBytes(BLOCK);
+        // Blocks of 256 threads take more than the 48 KB of dynamic shared
+        // memory a kernel gets without opting in.
+        cudaFuncSetAttribute(batchExtendKernel<BLOCK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(batchShadowKernel<BLOCK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         int perSm = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, batchExtendKernel<BLOCK>, BLOCK, smem) != cudaSuccess ||
             perSm <= 0)
