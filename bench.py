@@ -73,7 +73,7 @@ def parse():
     p.add_argument('--refill', type=int, default=None,
                    help='refill threshold of the persistent traversal (RTX_TUNE_REFILL; default: the library default)')
     p.add_argument('--paths', type=int, default=None,
-                   help='paths per wave (RTX_TUNE_PATHS_IN_FLIGHT; default: all pixels)')
+                   help='paths per wave (RTX_TUNE_PATHS_IN_FLIGHT; default: the library default, 2^24)')
     p.add_argument('--lanes', type=int, default=None,
                    help="waves in flight, 1..4 (RTX_TUNE_LANES; default: the library default)")
     p.add_argument('--denoiser-only', action='store_true',
