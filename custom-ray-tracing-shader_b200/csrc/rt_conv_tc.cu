@@ -25,10 +25,15 @@ namespace {
 using bf16 = __nv_bfloat16;
 constexpr int kTileM = 128;             // output pixels per tile (the MMA's M)
 constexpr int kHaloW = kTileM + 2;      // halo pixels per row
-// Eight warps: staging is shared by all of them, and in the epilogue warp w
+// Nine warps: staging is shared by all of them; in the epilogue warp w < 8
 // reads tensor-memory lanes 32 * (w % 4) .. + 31 (the lanes a warp may
-// access) and every other group of 16 accumulator columns from 16 * (w / 4).
-constexpr int kThreads = 256;
+// access) and every other group of 16 accumulator columns from 16 * (w / 4);
+// warp 8 issues the MMAs and takes no part in the epilogue, so issuing a
+// tile's MMAs overlaps the drain of the previous tile instead of delaying it
+// (a block barrier waits for the slowest warp).
+constexpr int kDrainWarps = 8;
+constexpr int kThreads = 32 * (kDrainWarps + 1);
+constexpr int kIssuer = 32 * kDrainWarps;  // thread that issues the MMAs
 constexpr uint32_t kHeaderBytes = 128;  // mbarriers and the tensor-memory address
 constexpr uint32_t kMaxSmem = 227 * 1024;
 constexpr long long kSpinLimit = 1ll << 24;  // about a second of polling
@@ -206,6 +211,11 @@ __global__ void __launch_bounds__(kThreads, 1) convTcKernel(ConvTcArgs a) {
     // accumulators from tensor memory, bias, ReLU, store.
     auto epilogue = [&](int rowIdx, int x0, uint32_t column) {
         tcFenceAfter();
+        if (warp >= kDrainWarps) {  // the issuing warp: only the barrier below
+            tcFenceBefore();
+            __syncthreads();
+            return;
+        }
         const int quarter = warp & 3, half = warp >> 2;
         const int x = x0 + quarter * 32 + lane;
         const bool inside = x < a.w;
@@ -282,7 +292,7 @@ __global__ void __launch_bounds__(kThreads, 1) convTcKernel(ConvTcArgs a) {
                     cpAsyncWait<1>();
                     fenceProxyAsync();
                     __syncthreads();
-                    if (tid == 0) {
+                    if (tid == kIssuer) {
                         tcFenceAfter();
                         // Descriptors as base + offset in 16-byte units: the
                         // start address is the low 14-bit field and every
@@ -345,7 +355,7 @@ __global__ void __launch_bounds__(kThreads, 1) convTcKernel(ConvTcArgs a) {
             }
             fenceProxyAsync();
             __syncthreads();
-            if (tid == 0) {
+            if (tid == kIssuer) {
                 tcFenceAfter();
                 // Descriptors as base + offset in 16-byte units (see the
                 // ring loop above).
@@ -458,7 +468,7 @@ cudaError_t convTc(const bf16* in, const bf16* low, int lowChannels, int n, int 
     // Blocks per SM: shared memory (228 KB per SM, 1 KB reserved per block)
     // and the 512 columns of tensor memory.
     int perSm = (int)((228u * 1024u) / (smemBytes + 1024u));
-    perSm = std::max(1, std::min({perSm, (int)(512u / a.tmemCols), 8}));
+    perSm = std::max(1, std::min({perSm, (int)(512u / a.tmemCols), 2048 / kThreads}));
     int units = a.tiles;
     if (a.ring) {
         // Strips long enough to reuse rows, short enough for two units per block.
