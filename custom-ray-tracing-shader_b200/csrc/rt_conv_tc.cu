@@ -1,16 +1,17 @@
 // tcgen05 implicit-GEMM 3x3 convolution (see rt_conv_tc.cuh).
 //
-// One persistent block of 256 threads per SM (or more when shared and tensor
-// memory allow) walks over tiles of 128 output pixels. For every tile the
+// Persistent blocks (one per SM, or more when shared and tensor memory
+// allow; 4 warps, or 8 + 1 for layers with fewer than 4 blocks per SM, see
+// WarpLayout) walk over tiles of 128 output pixels. For every tile the
 // input channels are taken in chunks of 16 or 32: all threads stage the
 // chunk's halo (and, when the weights do not fit in shared memory for the
 // whole kernel, the chunk's weights) with cp.async into one of two stages;
-// thread 0 issues the chunk's 9 taps x (chunk / 16) MMAs of 128 x N x 16 and
+// one thread issues the chunk's 9 taps x (chunk / 16) MMAs of 128 x N x 16 and
 // commits them to the stage's mbarrier, while the threads go on to stage
-// the next chunk into the other stage. After a tile's last chunk the eight
-// warps read the accumulators back from tensor memory (each warp 32 lanes =
-// 32 pixels and half of the channel groups), add the bias, apply ReLU and
-// store.
+// the next chunk into the other stage. After a tile's last chunk the
+// draining warps read the accumulators back from tensor memory (each warp 32
+// lanes = 32 pixels and its share of the channel groups), add the bias,
+// apply ReLU and store.
 //
 // Every wait on an mbarrier is bounded; past the bound the kernel stops its
 // work, waits for its own copies, frees its tensor memory, sets *errorFlag
@@ -25,15 +26,22 @@ namespace {
 using bf16 = __nv_bfloat16;
 constexpr int kTileM = 128;             // output pixels per tile (the MMA's M)
 constexpr int kHaloW = kTileM + 2;      // halo pixels per row
-// Nine warps: staging is shared by all of them; in the epilogue warp w < 8
-// reads tensor-memory lanes 32 * (w % 4) .. + 31 (the lanes a warp may
-// access) and every other group of 16 accumulator columns from 16 * (w / 4);
-// warp 8 issues the MMAs and takes no part in the epilogue, so issuing a
+// Warp layouts (template parameters of the kernel): DRAIN warps stage and
+// drain; in the epilogue warp w < DRAIN reads tensor-memory lanes
+// 32 * (w % 4) .. + 31 (the lanes a warp may access) and every DRAIN / 4-th
+// group of 16 accumulator columns from 16 * (w / 4). With ISSUER = 1 an
+// extra warp issues the MMAs and takes no part in the epilogue, so issuing a
 // tile's MMAs overlaps the drain of the previous tile instead of delaying it
-// (a block barrier waits for the slowest warp).
-constexpr int kDrainWarps = 8;
-constexpr int kThreads = 32 * (kDrainWarps + 1);
-constexpr int kIssuer = 32 * kDrainWarps;  // thread that issues the MMAs
+// (a block barrier waits for the slowest warp); with ISSUER = 0 thread 0
+// issues. Layers that fit 4 or more blocks per SM use 4 warps (more blocks,
+// less per-block overhead), the others 8 + 1.
+template <int DRAIN, int ISSUER>
+struct WarpLayout {
+    static constexpr int kThreads = 32 * (DRAIN + ISSUER);
+    static constexpr int kIssuer = ISSUER ? 32 * DRAIN : 0;
+    static constexpr int kDrainWarps = DRAIN;
+    static constexpr int kColumnStep = 16 * (DRAIN / 4);
+};
 constexpr uint32_t kHeaderBytes = 128;  // mbarriers and the tensor-memory address
 constexpr uint32_t kMaxSmem = 227 * 1024;
 constexpr long long kSpinLimit = 1ll << 24;  // about a second of polling
@@ -120,7 +128,10 @@ __device__ __forceinline__ void tmemLoad16(uint32_t taddr, uint32_t (&r)[16]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 }
 
-__global__ void __launch_bounds__(kThreads, 1) convTcKernel(ConvTcArgs a) {
+template <int DRAIN, int ISSUER>
+__global__ void __launch_bounds__(WarpLayout<DRAIN, ISSUER>::kThreads, 1) convTcKernel(ConvTcArgs a) {
+    using Layout = WarpLayout<DRAIN, ISSUER>;
+    constexpr int kThreads = Layout::kThreads, kIssuer = Layout::kIssuer, kDrainWarps = Layout::kDrainWarps;
     extern __shared__ __align__(1024) unsigned char smem[];
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem);          // two mbarriers
     uint32_t* tmemSlot = reinterpret_cast<uint32_t*>(smem + 16);  // tensor-memory address
@@ -220,7 +231,7 @@ __global__ void __launch_bounds__(kThreads, 1) convTcKernel(ConvTcArgs a) {
         const int x = x0 + quarter * 32 + lane;
         const bool inside = x < a.w;
         const size_t pix = (size_t)rowIdx * a.w + (size_t)x;
-        for (int cb = 16 * half; cb < a.cout; cb += 32) {
+        for (int cb = 16 * half; cb < a.cout; cb += Layout::kColumnStep) {
             uint32_t r[16];
             tmemLoad16(tmem + ((uint32_t)(quarter * 32) << 16) + column + (uint32_t)cb, r);
             if (!inside) continue;
@@ -415,10 +426,12 @@ cudaError_t convTc(const bf16* in, const bf16* low, int lowChannels, int n, int 
         return cudaErrorInvalidValue;
     static bool configured = false;
     if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(convTcKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(convTcKernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-        if (e != cudaSuccess) return e;
+        void (*kernels[2])(ConvTcArgs) = {convTcKernel<4, 0>, convTcKernel<8, 1>};
+        for (auto k : kernels) {
+            cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem);
+            if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+            if (e != cudaSuccess) return e;
+        }
         configured = true;
     }
     ConvTcArgs a{};
@@ -467,8 +480,13 @@ cudaError_t convTc(const bf16* in, const bf16* low, int lowChannels, int n, int 
     a.tmemCols = a.ring ? 2u * a.accCols : a.accCols;  // ring mode: two accumulators
     // Blocks per SM: shared memory (228 KB per SM, 1 KB reserved per block)
     // and the 512 columns of tensor memory.
+    // Layers that fit 4 or more blocks of 4 warps per SM keep 4 warps; the
+    // others run 8 draining warps and an issuing warp (measured per layer:
+    // 16->32 at full resolution 102 against 122 us, 80->32 578 against 480).
     int perSm = (int)((228u * 1024u) / (smemBytes + 1024u));
-    perSm = std::max(1, std::min({perSm, (int)(512u / a.tmemCols), 2048 / kThreads}));
+    perSm = std::max(1, std::min({perSm, (int)(512u / a.tmemCols), 8}));
+    const bool wide = perSm < 4;
+    if (wide) perSm = std::min(perSm, 2048 / WarpLayout<8, 1>::kThreads);
     int units = a.tiles;
     if (a.ring) {
         // Strips long enough to reuse rows, short enough for two units per block.
@@ -477,7 +495,10 @@ cudaError_t convTc(const bf16* in, const bf16* low, int lowChannels, int n, int 
         units = n * a.tilesPerRow * ((h + a.stripRows - 1) / a.stripRows);
     }
     const int grid = std::min(units, deviceSms() * perSm);
-    convTcKernel<<<grid, kThreads, smemBytes, stream>>>(a);
+    if (wide)
+        convTcKernel<8, 1><<<grid, WarpLayout<8, 1>::kThreads, smemBytes, stream>>>(a);
+    else
+        convTcKernel<4, 0><<<grid, WarpLayout<4, 0>::kThreads, smemBytes, stream>>>(a);
     return cudaGetLastError();
 }
 
