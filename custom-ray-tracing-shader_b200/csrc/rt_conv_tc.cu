@@ -44,7 +44,6 @@ struct WarpLayout {
 };
 constexpr uint32_t kHeaderBytes = 128;  // mbarriers and the tensor-memory address
 constexpr uint32_t kMaxSmem = 227 * 1024;
-constexpr long long kSpinLimit = 1ll << 24;  // about a second of polling
 
 static_assert(ummaInstrDescBf16(128, 64) == 0x08100490u, "instruction descriptor layout");
 
@@ -84,21 +83,21 @@ __device__ __forceinline__ void cpAsyncWait() { asm volatile("cp.async.wait_grou
 __device__ __forceinline__ void mbarInit(uint32_t bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
 }
-__device__ __forceinline__ bool mbarTest(uint32_t bar, uint32_t phase) {
+// mbarrier.try_wait suspends the thread until the phase completes or the
+// hint (1 us) passes, so a completion wakes the waiters at once; 2^20 tries
+// bound the wait to about a second.
+__device__ __forceinline__ bool mbarTryWait(uint32_t bar, uint32_t phase) {
     uint32_t done;
     asm volatile(
-        "{\n.reg .pred p;\nmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
+        "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\nselp.u32 %0, 1, 0, p;\n}\n"
         : "=r"(done)
-        : "r"(bar), "r"(phase)
+        : "r"(bar), "r"(phase), "r"(1000u)
         : "memory");
     return done != 0;
 }
-// Waits for the completion of the barrier's phase with the given parity.
 __device__ bool mbarWait(uint32_t bar, uint32_t phase) {
-    for (long long i = 0; i < kSpinLimit; i++) {
-        if (mbarTest(bar, phase)) return true;
-        __nanosleep(32);
-    }
+    for (int i = 0; i < (1 << 20); i++)
+        if (mbarTryWait(bar, phase)) return true;
     return false;
 }
 
