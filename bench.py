@@ -270,8 +270,11 @@ def cpu_baseline(tris, cam, settings, w, h, budget_s):
     }
 
 
-def reference_cuda(tris, cam, settings, w, h, rays_per_step, steps=3):
-    """The reference's own CUDA renderer (oracle/_ref, built for sm_100a)."""
+def reference_cuda(tris, cam, settings, w, h, rays_per_step, first_pass, steps=3):
+    """The reference's own CUDA renderer (oracle/_ref, built for sm_100a).
+    first_pass = (PixelSum records, RGBA8 image) of this library's first pass
+    on the same session settings; parity is true when the reference's first
+    pass accumulates the same bytes and shows the same image."""
     from oracle_api import Reference, ReferenceSession, reference_available
     if not reference_available():
         return None
@@ -279,12 +282,18 @@ def reference_cuda(tris, cam, settings, w, h, rays_per_step, steps=3):
     try:
         ref.initialize(tris, w, h)
         times = []
-        for _ in range(steps + 1):
-            _, ms = ref.render(cam, settings)
+        parity = None
+        for k in range(steps + 1):
+            rgba, ms = ref.render(cam, settings)
             times.append(ms)
+            if k == 0:
+                parity = (ref.sums().tobytes() == first_pass[0].tobytes() and
+                          rgba.tobytes() == first_pass[1].tobytes())
         ms = statistics.median(times[1:])
-        return {'value': rays_per_step / ms / 1e3, 'unit': METRIC, 'ms_per_step': ms,
-                'note': 'Native/renderer.cu renderKernel built for sm_100a, same scene, settings and ray count'}
+        return {'value': rays_per_step / ms / 1e3, 'unit': METRIC, 'ms_per_step': ms, 'parity': parity,
+                'note': 'Native/renderer.cu renderKernel built for sm_100a, same scene, settings and ray count; '
+                        'parity: its first pass accumulates the same PixelSum bytes and RGBA8 image as this '
+                        "library's"}
     finally:
         ref.close()
 
@@ -298,13 +307,70 @@ def psnr8(image, reference):
     return (float('inf') if mse == 0 else float(20.0 * np.log10(255.0 / np.sqrt(mse)))), float(np.sqrt(mse))
 
 
+def display_float(radiance, exposure):
+    """The reference's display transform (Native/renderer.cu:86-90) before its
+    8-bit quantisation: 1 - exp(-max(c, 0) * exposure), the sRGB curve,
+    clamped to 1; float64."""
+    import numpy as np
+    c = 1.0 - np.exp(-np.maximum(np.asarray(radiance, np.float64), 0.0) * exposure)
+    c = np.where(c <= 0.0031308, 12.92 * c, 1.055 * np.power(c, 1.0 / 2.4) - 0.055)
+    return np.minimum(c, 1.0)
+
+
+class QualityReference:
+    """The 4096-path FP32 render of a scene: linear radiance per pixel
+    (sum / samples) and its display values as floats."""
+
+    def __init__(self, radiance, exposure, rgba):
+        import numpy as np
+        self.linear = np.asarray(radiance, np.float64)
+        self.display = display_float(self.linear, exposure)
+        self.exposure = exposure
+        self.rgba = rgba
+
+    def score(self, radiance, rgba=None):
+        """PSNR (dB) of float display values, RMSE of linear HDR radiance and,
+        given the RGBA8 image, the 8-bit PSNR of the reference's own quality
+        tool (Tools/verify_quality.py:53-54)."""
+        import numpy as np
+        lin = np.asarray(radiance, np.float64)
+        d = display_float(lin, self.exposure) - self.display
+        rmse = float(np.sqrt(np.mean(d * d)))
+        out = {'psnr_float_db': float('inf') if rmse == 0 else float(20.0 * np.log10(1.0 / rmse)),
+               'rmse_display': rmse,
+               'rmse_linear': float(np.sqrt(np.mean((lin - self.linear) ** 2)))}
+        if rgba is not None:
+            out['psnr_8bit_db'], out['rmse_8bit'] = psnr8(rgba, self.rgba)
+        return out
+
+
+def accumulated_radiance(session):
+    import numpy as np
+    acc = session.accumulation()
+    samples = session.sample_count()
+    return np.stack([acc['radiance'][k] for k in 'xyz'], 1).astype(np.float64) / samples
+
+
 def quality_run(lib, args, target_db=35.0):
-    """Time to reach target_db PSNR against a high-spp render of the
-    end-to-end scene (2M triangles, depth 5, constant 0.1 environment):
-    plain progressive accumulation vs 8 spp followed by RtDenoise. PSNR is
-    taken on the 8-bit display images (the reference's own quality tool
-    compares 8-bit RGB, Tools/verify_quality.py:53-54); the high-spp render
-    uses a different sampler seed than the arms."""
+    """Time to reach target_db PSNR against a 4096-path FP32 render of the
+    end-to-end scene (2M triangles, 1920x1080, depth 5, constant 0.1
+    environment): plain progressive accumulation against 8 (or more) paths
+    per pixel followed by RtDenoise, with the learned U-Net and with the
+    guided filter.
+
+    Quality: PSNR of the display values as floats (the reference's display
+    transform before 8-bit quantisation) and RMSE of the linear HDR radiance,
+    both against the FP32 accumulation of the 4096-path render (another
+    sampler seed than the arms'); the 8-bit PSNR that the reference's own
+    tool uses (Tools/verify_quality.py:53-54, against 2048 paths there) is
+    reported beside them. The denoised arms are scored on RtxReadDenoised's
+    linear radiance, the plain arm on its running sums.
+
+    Time: each arm is re-run from a reset once its path count is known and
+    timed on the host wall clock through the public calls (RtRender per pass,
+    with its RGBA8 read-back, then RtDenoise with its read-back), after the
+    buffers were allocated by earlier calls; the device time of the same calls
+    (CUDA events) is reported beside it."""
     import numpy as np
     import scenes
     from native_api import DENOISER_WEIGHTS, Session, Settings, Unet
@@ -322,47 +388,82 @@ def quality_run(lib, args, target_db=35.0):
         passes = max(1, args.oracle_spp // 16)
         for _ in range(passes - 1):
             oracle_ms += s.render_device(cam, oracle_settings)
-        oracle, ms = s.render(cam, oracle_settings)
+        oracle_rgba, ms = s.render(cam, oracle_settings)
         oracle_ms += ms
-        oracle = oracle.copy()
-        # Plain progressive accumulation: PSNR after every pass of 4 paths per
-        # pixel (one pass size throughout: RtRender restarts the accumulation
-        # when any setting changes, renderer.cu:388-389).
-        spp, device_ms, wall0 = 0, 0.0, time.perf_counter()
-        curve = []
-        reached = None
+        ref = QualityReference(accumulated_radiance(s), st.exposure, oracle_rgba.copy())
+        out = np.zeros(w * h * 4, np.uint8)
+
+        def replay(spp, per_pass, denoise):
+            """Wall and device time of spp paths per pixel from a reset through
+            RtRender passes of per_pass, then RtDenoise when asked."""
+            st.raysPerPixel = per_pass
+            s.lib.RtReset(s.handle)
+            device = 0.0
+            t0 = time.perf_counter()
+            while s.sample_count() < spp:
+                _, ms = s.render(cam, st, output=out)
+                device += ms
+            if denoise:
+                s.denoise(output=out)
+            wall = (time.perf_counter() - t0) * 1e3
+            if denoise:
+                device += s.render_stats()['denoiseMs']
+            return wall, device
+
+        # Plain progressive accumulation, 4 paths per pixel per pass (one pass
+        # size throughout: RtRender restarts when a setting changes,
+        # renderer.cu:388-389): the first pass count that reaches the target,
+        # found by scoring every 8th pass, then every pass of the last stretch
+        # rendered again from a reset (the same paths: results are
+        # deterministic).
         st.raysPerPixel = 4
+        coarse = 8
         s.lib.RtReset(s.handle)
-        while spp < args.oracle_spp // 2:
-            img, ms = s.render(cam, st)
-            device_ms += ms
+        s.render(cam, st, output=out)  # allocations of this pass size
+        s.lib.RtReset(s.handle)
+        curve, reached, upper = [], None, None
+        while s.sample_count() < args.oracle_spp // 2:
+            img, _ = s.render(cam, st, output=out)
             spp = s.sample_count()
-            db, rmse = psnr8(img, oracle)
-            curve.append([spp, round(device_ms, 2), round(db, 3)])
-            if db >= target_db:
-                reached = {'spp': spp, 'device_ms': device_ms, 'psnr_db': db, 'rmse_8bit': rmse}
-                break
-        plain_wall_ms = (time.perf_counter() - wall0) * 1e3
+            if spp % (4 * coarse) == 0 or spp >= args.oracle_spp // 2:
+                q = ref.score(accumulated_radiance(s), img)
+                curve.append([spp, round(q['psnr_float_db'], 3), round(q['psnr_8bit_db'], 3)])
+                if q['psnr_float_db'] >= target_db:
+                    upper = spp
+                    break
+        if upper is not None:
+            s.lib.RtReset(s.handle)
+            while s.sample_count() < max(0, upper - 4 * coarse):
+                s.render(cam, st, output=out)
+            while s.sample_count() < upper:
+                img, _ = s.render(cam, st, output=out)
+                q = ref.score(accumulated_radiance(s), img)
+                if q['psnr_float_db'] >= target_db:
+                    reached = dict(q, spp=s.sample_count())
+                    break
+        plain = dict(reached or {'spp': s.sample_count(), 'psnr_float_db': curve[-1][1] if curve else None},
+                     reaches_target=reached is not None)
+        if reached:
+            plain['wall_ms'], plain['device_ms'] = replay(reached['spp'], 4, False)
+
         def denoised_arm(name):
-            """8 spp, then more paths per pixel until the denoised image
-            reaches the target (each budget rendered from scratch; a budget
-            above 16 spp is several passes of 16 with one setting)."""
+            """8 paths per pixel, then more until the denoised image reaches
+            the target (each budget rendered from a reset; above 16 paths a
+            budget is several passes of 16)."""
             trials, arm = [], None
             for budget in (8, 16, 32, 64, 128, 256):
                 per = min(16, budget)
                 st.raysPerPixel = per
                 s.lib.RtReset(s.handle)
-                render_ms = 0.0
                 while s.sample_count() < budget:
-                    img, ms = s.render(cam, st)
-                    render_ms += ms
-                raw_db, _ = psnr8(img, oracle)
-                den, denoise_ms = s.denoise()
-                den_db, den_rmse = psnr8(den, oracle)
-                trial = {'spp': budget, 'render_ms': render_ms, 'denoise_ms': denoise_ms, 'psnr_db': den_db,
-                         'rmse_8bit': den_rmse, 'raw_psnr_db': raw_db}
+                    img, _ = s.render(cam, st, output=out)
+                raw = ref.score(accumulated_radiance(s), img)
+                den, _ = s.denoise()
+                q = ref.score(s.denoised_radiance(), den)
+                trial = dict(q, spp=budget, raw_psnr_float_db=raw['psnr_float_db'])
+                trial['wall_ms'], trial['device_ms'] = replay(budget, per, True)
                 trials.append(trial)
-                if den_db >= target_db:
+                if q['psnr_float_db'] >= target_db:
                     arm = dict(trial, reaches_target=True)
                     break
             arm = arm or dict(trials[-1], reaches_target=False)
@@ -370,16 +471,18 @@ def quality_run(lib, args, target_db=35.0):
             arm['at_8spp'] = trials[0]
             return arm
 
+        st.raysPerPixel = 8
+        s.lib.RtReset(s.handle)
+        s.render(cam, st, output=out)
         s.denoise()  # the first call allocates the filter's buffers and loads its kernels
-        denoised = denoised_arm('guided a-trous wavelet filter (RtDenoise without a network)')
+        filtered = denoised_arm('guided a-trous wavelet filter (RtDenoise without a network)')
         learned = None
         if DENOISER_WEIGHTS.exists():
             net = Unet(lib)
             try:
                 net.load(DENOISER_WEIGHTS)
                 s.set_denoiser(net)
-                # The first inference at this size allocates the activations.
-                s.denoise()
+                s.denoise()  # the first inference at this size allocates the activations
                 learned = denoised_arm(f'learned U-Net ({net.param_count:,} parameters, BF16 tensor cores; '
                                        f'RtDenoise with RtxSetDenoiser)')
             finally:
@@ -389,17 +492,18 @@ def quality_run(lib, args, target_db=35.0):
             'workload': 'end_to_end_room', 'triangles': len(tris), 'width': w, 'height': h,
             'max_depth': st.maxBounces, 'environment': 0.1, 'exposure': st.exposure, 'target_db': target_db,
             'oracle_spp': passes * 16, 'oracle_device_ms': oracle_ms,
-            'plain': dict(reached or {'spp': spp, 'device_ms': device_ms, 'psnr_db': curve[-1][2] if curve else None},
-                          reaches_target=reached is not None, wall_ms=plain_wall_ms),
-            'denoised': denoised,
-            'learned': learned,
-            'psnr_metric': '20 log10(255 / RMSE) over 8-bit RGB display values',
+            'psnr_metric': ('20 log10(1 / RMSE) of display values as floats (Native/renderer.cu:86-90 before '
+                            '8-bit quantisation) against the FP32 4096-path accumulation; rmse_linear on linear '
+                            'HDR radiance; psnr_8bit_db is the reference tool\'s 8-bit metric'),
+            'timing': 'wall_ms: host wall clock through RtRender passes (RGBA8 read-back each) and RtDenoise '
+                      '(RGBA8 read-back), after allocation; device_ms: CUDA events of the same calls',
+            'plain': plain, 'filter': filtered, 'learned': learned,
             'curve_every_4spp': curve[:: max(1, len(curve) // 32)],
         }
-        if reached and denoised['reaches_target']:
-            result['speedup_denoised_vs_plain'] = reached['device_ms'] / (denoised['render_ms'] + denoised['denoise_ms'])
-        if reached and learned and learned['reaches_target']:
-            result['speedup_learned_vs_plain'] = reached['device_ms'] / (learned['render_ms'] + learned['denoise_ms'])
+        for key, arm in (('filter', filtered), ('learned', learned)):
+            if plain.get('reaches_target') and arm and arm['reaches_target']:
+                result[f'speedup_{key}_vs_plain_wall'] = plain['wall_ms'] / arm['wall_ms']
+                result[f'speedup_{key}_vs_plain_device'] = plain['device_ms'] / arm['device_ms']
         return result
     finally:
         s.close()
@@ -741,8 +845,12 @@ def run_ours(args, rank, local_rank, world):
             cpu.pop('rays', None)
         ref_cuda = None
         if world == 1 and not args.no_reference_cuda:
+            # This library's first pass of the same settings, for the parity check.
+            s.lib.RtReset(s.handle)
+            first_rgba, _ = s.render(cam, settings)
+            first_pass = (s.accumulation(), first_rgba.copy())
             try:
-                ref_cuda = reference_cuda(tris, cam, settings, w, h, rays / args.steps)
+                ref_cuda = reference_cuda(tris, cam, settings, w, h, rays / args.steps, first_pass)
             except Exception as exc:
                 ref_cuda = {'unavailable': str(exc)}
         result = {
@@ -845,6 +953,9 @@ def main():
         result = run_ours(args, rank, local_rank, world)
     if rank == 0 and result is not None:
         print(json.dumps(result), flush=True)
+        ref_cuda = result.get('reference_cuda') or {}
+        if ref_cuda.get('parity') is False:
+            sys.exit('parity failure: the reference CUDA renderer accumulated different bytes on the bench workload')
 
 
 if __name__ == '__main__':

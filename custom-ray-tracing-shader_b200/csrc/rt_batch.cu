@@ -434,18 +434,18 @@ bool ensureBase(Batch* b) {
     if ((e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) != cudaSuccess) return failB(b, e);
     if ((e = cudaEventCreate(&b->start)) != cudaSuccess) return failB(b, e);
     if ((e = cudaEventCreate(&b->stop)) != cudaSuccess) return failB(b, e);
-    if ((e = cudaMalloc(&b->dDirs, sizeof(unsigned) * kSobolDims * 32)) != cudaSuccess) return failB(b, e);
+    if ((e = rt::deviceAlloc(&b->dDirs, sizeof(unsigned) * kSobolDims * 32)) != cudaSuccess) return failB(b, e);
     // Copies and fills on b->stream: a non-blocking stream is not ordered
     // after the legacy default stream.
     if ((e = cudaMemcpyAsync(b->dDirs, dirs, sizeof(unsigned) * kSobolDims * 32, cudaMemcpyHostToDevice, b->stream)) !=
         cudaSuccess)
         return failB(b, e);
-    if ((e = cudaMalloc(&b->dPassXor, sizeof(unsigned) * 16 * kSobolDims)) != cudaSuccess) return failB(b, e);
-    if ((e = cudaMalloc(&b->dSeedHash, sizeof(unsigned) * kSobolDims)) != cudaSuccess) return failB(b, e);
-    if ((e = cudaMalloc(&b->dSample, sizeof(unsigned))) != cudaSuccess) return failB(b, e);
+    if ((e = rt::deviceAlloc(&b->dPassXor, sizeof(unsigned) * 16 * kSobolDims)) != cudaSuccess) return failB(b, e);
+    if ((e = rt::deviceAlloc(&b->dSeedHash, sizeof(unsigned) * kSobolDims)) != cudaSuccess) return failB(b, e);
+    if ((e = rt::deviceAlloc(&b->dSample, sizeof(unsigned))) != cudaSuccess) return failB(b, e);
     if ((e = cudaMemsetAsync(b->dSample, 0, sizeof(unsigned), b->stream)) != cudaSuccess) return failB(b, e);
-    if ((e = cudaMalloc(&b->dCounters, 4 * sizeof(unsigned long long))) != cudaSuccess) return failB(b, e);
-    if ((e = cudaMalloc(&b->dError, 2 * sizeof(int))) != cudaSuccess) return failB(b, e);
+    if ((e = rt::deviceAlloc(&b->dCounters, 4 * sizeof(unsigned long long))) != cudaSuccess) return failB(b, e);
+    if ((e = rt::deviceAlloc(&b->dError, 2 * sizeof(int))) != cudaSuccess) return failB(b, e);
     return true;
 }
 
@@ -487,11 +487,11 @@ bool ensureArena(Batch* b) {
         return false;
     }
     cudaError_t e;
-    if ((e = cudaMalloc(&b->aTris, sizeof(SceneTri) * tris)) != cudaSuccess) return failB(b, e, "arena");
-    if ((e = cudaMalloc(&b->aWide, sizeof(uint4) * 5 * nodes)) != cudaSuccess) return failB(b, e, "arena");
-    if ((e = cudaMalloc(&b->aPacked, sizeof(float4) * 3 * packedCount)) != cudaSuccess) return failB(b, e, "arena");
-    if ((e = cudaMalloc(&b->aLights, sizeof(Light) * std::max<size_t>(lights, 1))) != cudaSuccess) return failB(b, e, "arena");
-    if ((e = cudaMalloc(&b->dScenes, sizeof(BatchScene) * b->scenes.size())) != cudaSuccess) return failB(b, e, "arena");
+    if ((e = rt::deviceAlloc(&b->aTris, sizeof(SceneTri) * tris)) != cudaSuccess) return failB(b, e, "arena");
+    if ((e = rt::deviceAlloc(&b->aWide, sizeof(uint4) * 5 * nodes)) != cudaSuccess) return failB(b, e, "arena");
+    if ((e = rt::deviceAlloc(&b->aPacked, sizeof(float4) * 3 * packedCount)) != cudaSuccess) return failB(b, e, "arena");
+    if ((e = rt::deviceAlloc(&b->aLights, sizeof(Light) * std::max<size_t>(lights, 1))) != cudaSuccess) return failB(b, e, "arena");
+    if ((e = rt::deviceAlloc(&b->dScenes, sizeof(BatchScene) * b->scenes.size())) != cudaSuccess) return failB(b, e, "arena");
     std::vector<BatchScene> table;
     std::vector<Light> allLights;
     allLights.reserve(lights);
@@ -536,10 +536,10 @@ bool ensureViews(Batch* b) {
     }
     if (pixels > 0x7FFFFFFFull) { b->error = "batch has more than 2^31 pixels"; return false; }
     cudaError_t e;
-    if ((e = cudaMalloc(&b->dViews, sizeof(BatchView) * table.size())) != cudaSuccess) return failB(b, e);
-    if ((e = cudaMalloc(&b->dSum, sizeof(Accum) * pixels)) != cudaSuccess) return failB(b, e, "accumulation");
-    if ((e = cudaMalloc(&b->dDepth, sizeof(float) * pixels)) != cudaSuccess) return failB(b, e, "accumulation");
-    if ((e = cudaMalloc(&b->dPixels, sizeof(uchar4) * pixels)) != cudaSuccess) return failB(b, e, "accumulation");
+    if ((e = rt::deviceAlloc(&b->dViews, sizeof(BatchView) * table.size())) != cudaSuccess) return failB(b, e);
+    if ((e = rt::deviceAlloc(&b->dSum, sizeof(Accum) * pixels)) != cudaSuccess) return failB(b, e, "accumulation");
+    if ((e = rt::deviceAlloc(&b->dDepth, sizeof(float) * pixels)) != cudaSuccess) return failB(b, e, "accumulation");
+    if ((e = rt::deviceAlloc(&b->dPixels, sizeof(uchar4) * pixels)) != cudaSuccess) return failB(b, e, "accumulation");
     if ((e = cudaMemcpyAsync(b->dViews, table.data(), sizeof(BatchView) * table.size(), cudaMemcpyHostToDevice,
                              b->stream)) != cudaSuccess)
         return failB(b, e);
@@ -690,7 +690,7 @@ bool validBatchSettings(const RenderSettings* st) {
 bool renderFrame(Batch* b, const RenderSettings* settings, float* ms) {
     if (b->scenes.empty() || b->views.empty()) { b->error = "RtxBatchRender: add a scene and a view first"; return false; }
     if (!validBatchSettings(settings)) { b->error = "RtxBatchRender: invalid settings"; return false; }
-    cudaSetDevice(b->device);
+    if (cudaSetDevice(b->device) != cudaSuccess) { b->error = "RtxBatchRender: could not make the batch's device current"; return false; }
     if (!ensureArena(b) || !ensureViews(b) || !ensureWave(b, settings->raysPerPixel)) return false;
     if (!b->haveLast || std::memcmp(settings, &b->last, sizeof(RenderSettings))) {
         resetSamples(b);
@@ -753,7 +753,7 @@ void* RtxBatchCreate(void) { return new Batch(); }
 void RtxBatchDestroy(void* p) {
     Batch* b = static_cast<Batch*>(p);
     if (!b) return;
-    if (b->device >= 0) cudaSetDevice(b->device);
+    if (b->device >= 0) (void)cudaSetDevice(b->device);  // freeing goes on regardless
     freeArena(b);
     freeViews(b);
     freeWavefront(b->wave);
@@ -778,7 +778,7 @@ int RtxBatchAddScene(void* p, const Triangle* triangles, int count) {
     if (!b) return -1;
     if (!triangles || count <= 0) { b->error = "RtxBatchAddScene: need triangles and count > 0"; return -1; }
     if (!ensureBase(b)) return -1;
-    cudaSetDevice(b->device);
+    if (cudaSetDevice(b->device) != cudaSuccess) { b->error = "RtxBatchAddScene: could not make the batch's device current"; return -1; }
     // Prepared on the device like RtInitialize's scenes (rt_upload.cuh); the
     // emitters come back to the host for the arena's emitter list.
     BatchSceneData S;

@@ -554,7 +554,7 @@ __global__ void collapseKernel(const BinNode* bn, const int* order, const float4
 inline int blocksFor(long long n, int block) { return (int)((n + block - 1) / block); }
 
 template <class T>
-cudaError_t alloc(T*& p, size_t count) { return cudaMalloc(reinterpret_cast<void**>(&p), sizeof(T) * (count ? count : 1)); }
+cudaError_t alloc(T*& p, size_t count) { return rt::deviceAlloc(reinterpret_cast<void**>(&p), sizeof(T) * (count ? count : 1)); }
 
 }  // namespace
 

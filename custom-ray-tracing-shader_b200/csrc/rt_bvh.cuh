@@ -174,11 +174,12 @@ struct TraversalCounters { unsigned nodes, tris; };
 // Closest (ANY = false) or any (ANY = true) hit against the wide BVH.
 // stack points at this ray's first stack entry; entries are stackStride apart
 // (shared-memory column on the device, contiguous on the host). On stack
-// overflow the query stops and sets *overflow (never happens for trees built
-// by this library: their depth is checked against kStackCapacity).
+// overflow (more than stackLimit <= kStackCapacity entries) the query stops
+// and sets *overflow (never happens at the default limit for trees built by
+// this library: their depth is checked against kStackCapacity).
 template <bool ANY>
 RT_HD Hit traverse(const uint4* nodes, const float4* tris, float3 o, float3 d, float limit, uint2* stack,
-                   int stackStride, int* overflow, TraversalCounters* counters) {
+                   int stackStride, int* overflow, TraversalCounters* counters, int stackLimit = kStackCapacity) {
     Hit hit{-1, limit, 0.0f, 0.0f};
     RaySetup r = setupRay(o, d);
     // Virtual root group: one interior child (node 0) in the highest slot.
@@ -194,7 +195,7 @@ RT_HD Hit traverse(const uint4* nodes, const float4* tris, float3 o, float3 d, f
             unsigned rel = popc(group.y & 0xFFu & ((1u << slot) - 1u));
             unsigned child = group.x + rel;
             if (group.y > 0x00FFFFFFu) {
-                if (top >= kStackCapacity) { if (overflow) *overflow = 1; break; }
+                if (top >= stackLimit) { if (overflow) *overflow = 1; break; }
                 stack[top * stackStride] = group;
                 top++;
             }

@@ -21,6 +21,16 @@ namespace rt {
 
 constexpr float kPi = 3.14159265358979323846f;
 
+// ---- device allocation ----
+// The renderer's device allocations go through deviceAlloc, so a test can
+// make the n-th next one fail on the host, as an out-of-memory cudaMalloc
+// would, without touching the GPU (RtxDebugFailAllocation).
+cudaError_t deviceAllocBytes(void** p, size_t bytes);
+template <class T>
+inline cudaError_t deviceAlloc(T** p, size_t bytes) {
+    return deviceAllocBytes(reinterpret_cast<void**>(p), bytes);
+}
+
 // ---- portable bit helpers (device intrinsics, host builtins) ----
 RT_HD unsigned popc(unsigned x) {
 #ifdef __CUDA_ARCH__

@@ -84,8 +84,9 @@ __device__ __forceinline__ void mbarInit(uint32_t bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
 }
 // mbarrier.try_wait suspends the thread until the phase completes or the
-// hint (1 us) passes, so a completion wakes the waiters at once; 2^20 tries
-// bound the wait to about a second.
+// hint (1 us) passes, so a completion wakes the waiters at once. A wait gives
+// up one second (of %globaltimer, not a count of tries: a suspension may end
+// early) after its first failed try.
 __device__ __forceinline__ bool mbarTryWait(uint32_t bar, uint32_t phase) {
     uint32_t done;
     asm volatile(
@@ -95,10 +96,18 @@ __device__ __forceinline__ bool mbarTryWait(uint32_t bar, uint32_t phase) {
         : "memory");
     return done != 0;
 }
+__device__ __forceinline__ uint64_t globalTimerNs() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+constexpr uint64_t kWaitLimitNs = 1000000000ull;
 __device__ bool mbarWait(uint32_t bar, uint32_t phase) {
-    for (int i = 0; i < (1 << 20); i++)
-        if (mbarTryWait(bar, phase)) return true;
-    return false;
+    if (mbarTryWait(bar, phase)) return true;
+    const uint64_t deadline = globalTimerNs() + kWaitLimitNs;
+    while (!mbarTryWait(bar, phase))
+        if (globalTimerNs() > deadline) return false;
+    return true;
 }
 
 __device__ __forceinline__ void fenceProxyAsync() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }

@@ -72,6 +72,7 @@ struct SceneView {
     int wideDepth;           // levels of the wide BVH (bounds the traversal stack)
     int environmentMode;     // 0: the reference's sky gradient x skyStrength; 1: constant radiance
     float3 environment;      // the constant radiance of mode 1
+    int stackLimit = kStackCapacity;  // traversal stack entries before the overflow error
 };
 
 // ---- BRDF and sky (renderer.cu:181-196) ----
@@ -262,12 +263,14 @@ RT_HD void renderPixel(const SceneView& sc, const Camera& cam, const Settings& s
         for (int bounce = 0; bounce < set.maxBounces; bounce++) {
             rng.base = 4u + 8u * (unsigned)bounce;
             if (bounce == 0) nPrimary++; else nSecondary++;
-            Hit hit = traverse<false>(sc.wide, sc.packed, st.origin, st.dir, 1e30f, stack, stackStride, overflow, nullptr);
+            Hit hit = traverse<false>(sc.wide, sc.packed, st.origin, st.dir, 1e30f, stack, stackStride, overflow, nullptr,
+                                     sc.stackLimit);
             ShadowRequest req;
             unsigned f = shadeBounce(sc, set, bounce, st, hit, rng, req);
             if (f & kShadow) {
                 nShadow++;
-                Hit sh = traverse<true>(sc.wide, sc.packed, req.origin, req.dir, req.limit, stack, stackStride, overflow, nullptr);
+                Hit sh = traverse<true>(sc.wide, sc.packed, req.origin, req.dir, req.limit, stack, stackStride, overflow,
+                                        nullptr, sc.stackLimit);
                 if (sh.index < 0) st.radiance = add(st.radiance, req.contribution);
             }
             if (!(f & kContinue)) break;

@@ -108,9 +108,9 @@ struct ExtendIO {
 };
 __global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks) extendKernel(const uint4* wide, const float4* packed, WavefrontBuffers B,
                                                             int q, unsigned long long* counter, int* errorFlag,
-                                                            int postponeBelow, int refill) {
+                                                            int stackLimit, int refill) {
     ExtendIO io{B.queue[q], B.pathA, B.pathB, B.hits};
-    persistentTrace<false>(io, B.counts[q], wide, packed, &B.counts[3], counter, errorFlag, postponeBelow, refill);
+    persistentTrace<false>(io, B.counts[q], wide, packed, &B.counts[3], counter, errorFlag, stackLimit, refill);
 }
 
 // Appends to a queue with one atomic per warp.
@@ -190,9 +190,9 @@ struct ShadowIO {
 };
 __global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks) shadowKernel(const uint4* wide, const float4* packed, WavefrontBuffers B,
                                                             unsigned long long* counter, int* errorFlag,
-                                                            int postponeBelow, int refill) {
+                                                            int stackLimit, int refill) {
     ShadowIO io{B.shadowRay, B.shadowDir, B.shadowContrib, B.radiance};
-    persistentTrace<true>(io, B.counts[2], wide, packed, &B.counts[4], counter, errorFlag, postponeBelow, refill);
+    persistentTrace<true>(io, B.counts[2], wide, packed, &B.counts[4], counter, errorFlag, stackLimit, refill);
 }
 
 __global__ void resetQueuesKernel(WavefrontBuffers B, int q) {
@@ -236,9 +236,9 @@ struct QueryIO {
 template <bool ANY>
 __global__ void __launch_bounds__(kTraceBlock) queryKernel(const uint4* wide, const float4* packed, const float4* q,
                                                            int count, float4* out, int* fetch, int* errorFlag,
-                                                           int postponeBelow, int refill) {
+                                                           int stackLimit, int refill) {
     QueryIO io{q, out};
-    persistentTrace<ANY>(io, count, wide, packed, fetch, nullptr, errorFlag, postponeBelow, refill);
+    persistentTrace<ANY>(io, count, wide, packed, fetch, nullptr, errorFlag, stackLimit, refill);
 }
 
 __global__ void sobolSamplesKernel(const unsigned* dirs, const unsigned* pixel, const unsigned* sample,
@@ -352,7 +352,7 @@ cudaError_t allocWavefront(WavefrontBuffers& b, int capacity) {
     freeWavefront(b);
     size_t n = (size_t)capacity;
     cudaError_t e;
-#define RT_ALLOC(p, count) if ((e = cudaMalloc(reinterpret_cast<void**>(&(p)), sizeof(*(p)) * (count))) != cudaSuccess) { freeWavefront(b); return e; }
+#define RT_ALLOC(p, count) if ((e = rt::deviceAlloc(reinterpret_cast<void**>(&(p)), sizeof(*(p)) * (count))) != cudaSuccess) { freeWavefront(b); return e; }
     RT_ALLOC(b.pathA, n); RT_ALLOC(b.pathB, n); RT_ALLOC(b.pathC, n);
     RT_ALLOC(b.radiance, n); RT_ALLOC(b.albedo, n); RT_ALLOC(b.normal, n); RT_ALLOC(b.hits, n);
     RT_ALLOC(b.queue[0], n); RT_ALLOC(b.queue[1], n);
@@ -399,7 +399,7 @@ cudaError_t launchWavefront(const RenderLaunch& L, WavefrontBuffers& B, const Tr
         shadowBlocks = traceBlocks(shadowKernel, kTraceSmem);
     }
     const size_t smem = kTraceSmem;
-    const int postponeBelow = tuning.postpone ? kStackCapacity - L.scene.wideDepth - 2 : 0;
+    const int stackLimit = tuning.stackLimit;
     const int refill = tuning.refill;
     int shadeBlocks = persistentBlocks(256);
     int pixels = L.w * L.h;
@@ -443,13 +443,13 @@ cudaError_t launchWavefront(const RenderLaunch& L, WavefrontBuffers& B, const Tr
                 if (timing) { m.a = event(ev++); m.b = event(ev++); cudaEventRecord(m.a, ws); }
                 extendKernel<<<extendBlocks, kTraceBlock, smem, ws>>>(L.scene.wide, L.scene.packed, W, q,
                                                                       &L.counters[bounce == 0 ? 0 : 1], L.errorFlag,
-                                                                      postponeBelow, refill);
+                                                                      stackLimit, refill);
                 if (timing) { cudaEventRecord(m.b, ws); marks.push_back(m); }
                 shadeKernel<<<shadeBlocks, 256, 0, ws>>>(A, W, q, bounce);
                 Mark s{nullptr, nullptr, 2};
                 if (timing) { s.a = event(ev++); s.b = event(ev++); cudaEventRecord(s.a, ws); }
                 shadowKernel<<<shadowBlocks, kTraceBlock, smem, ws>>>(L.scene.wide, L.scene.packed, W, &L.counters[2],
-                                                                      L.errorFlag, postponeBelow, refill);
+                                                                      L.errorFlag, stackLimit, refill);
                 if (timing) { cudaEventRecord(s.b, ws); marks.push_back(s); }
                 n += 4;
                 q ^= 1;
@@ -492,18 +492,19 @@ cudaError_t launchWavefront(const RenderLaunch& L, WavefrontBuffers& B, const Tr
 cudaError_t launchQueries(const uint4* wide, const float4* packed, const float4* queries, int count, int any,
                           float4* hits, int* fetch, int* errorFlag, int wideDepth, const TraceTuning& tuning,
                           cudaStream_t stream) {
-    const int postponeBelow = tuning.postpone ? kStackCapacity - wideDepth - 2 : 0;
+    (void)wideDepth;
+    const int stackLimit = tuning.stackLimit;
     const int refill = tuning.refill;
     cudaError_t e = cudaMemsetAsync(fetch, 0, sizeof(int), stream);
     if (e != cudaSuccess) return e;
     if (any) {
         static int blocks = traceBlocks(queryKernel<true>, kTraceSmem);
         queryKernel<true><<<blocks, kTraceBlock, kTraceSmem, stream>>>(wide, packed, queries, count, hits, fetch, errorFlag,
-                                                                      postponeBelow, refill);
+                                                                      stackLimit, refill);
     } else {
         static int blocks = traceBlocks(queryKernel<false>, kTraceSmem);
         queryKernel<false><<<blocks, kTraceBlock, kTraceSmem, stream>>>(wide, packed, queries, count, hits, fetch, errorFlag,
-                                                                       postponeBelow, refill);
+                                                                       stackLimit, refill);
     }
     return cudaGetLastError();
 }
@@ -515,6 +516,24 @@ cudaError_t launchSobolSamples(const unsigned* dirs, const unsigned* pixel, cons
     return cudaGetLastError();
 }
 
+// Denoised linear radiance as 3 floats per pixel (uncovered pixels 0, as the
+// display shows them): src holds srcStride floats per pixel.
+__global__ void denoisedRgbKernel(const Accum* sums, const float* src, int srcStride, int count, float* out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const float* r = src + (size_t)i * srcStride;
+    const bool covered = sums[i].covered != 0u;
+    out[3 * (size_t)i] = covered ? r[0] : 0.0f;
+    out[3 * (size_t)i + 1] = covered ? r[1] : 0.0f;
+    out[3 * (size_t)i + 2] = covered ? r[2] : 0.0f;
+}
+
+cudaError_t launchDenoisedRgb(const Accum* sums, const float* src, int srcStride, int count, float* out,
+                              cudaStream_t stream) {
+    denoisedRgbKernel<<<blocks(count, 256), 256, 0, stream>>>(sums, src, srcStride, count, out);
+    return cudaGetLastError();
+}
+
 cudaError_t launchDenoise(const Accum* sums, unsigned samples, int w, int h, float exposure, float4* work,
                           uchar4* pixels, cudaStream_t stream) {
     int count = w * h;
@@ -523,7 +542,7 @@ cudaError_t launchDenoise(const Accum* sums, unsigned samples, int w, int h, flo
     dim3 block(16, 16), grid((w + 15) / 16, (h + 15) / 16);
     float4 *src = color, *dst = tmp;
     float phi = 0.5f;
-    for (int it = 0; it < 5; it++) {
+    for (int it = 0; it < kAtrousPasses; it++) {
         atrousKernel<<<grid, block, 0, stream>>>(src, albedo, normal, dst, w, h, 1 << it, phi);
         float4* t = src; src = dst; dst = t;
         phi *= 0.5f;

@@ -43,9 +43,12 @@ struct WavefrontBuffers {
 
 // Speed-only knobs of the persistent traversal kernels.
 struct TraceTuning {
-    int postpone = 0;  // postpone triangle tests in sparse warps (measured neutral on B200)
     int refill = 24;   // refill idle lanes when fewer lanes than this are busy
     int lanes = 2;     // waves in flight (1..kMaxLanes, see WaveOverlap)
+    // Traversal stack entries a ray may use before the query stops with the
+    // overflow error (1..kStackCapacity). Trees built here never need more
+    // than kStackCapacity; a smaller limit forces the error path.
+    int stackLimit = kStackCapacity;
 };
 
 // Lanes of waves: wave j runs on lane j % lanes, lane 0 on the caller's
@@ -84,8 +87,15 @@ cudaError_t launchQueries(const uint4* wide, const float4* packed, const float4*
 cudaError_t launchSobolSamples(const unsigned* dirs, const unsigned* pixel, const unsigned* sample, const unsigned* seed,
                                int count, int ndim, float* out, cudaStream_t stream);
 // Denoise: prepare guides from the running sums, filter, tonemap into pixels.
+// work holds 4 float4 regions of w*h: colour, albedo, normal, ping-pong; after
+// the kAtrousPasses (odd) passes the filtered colour is in region 3.
+constexpr int kAtrousPasses = 5;
 cudaError_t launchDenoise(const Accum* sums, unsigned samples, int w, int h, float exposure, float4* work /*4*w*h*/,
                           uchar4* pixels, cudaStream_t stream);
+// The last denoise's linear radiance (srcStride floats per pixel at src) as 3
+// floats per pixel, uncovered pixels 0.
+cudaError_t launchDenoisedRgb(const Accum* sums, const float* src, int srcStride, int count, float* out,
+                              cudaStream_t stream);
 
 // Denoiser input: per pixel colour = radiance / samples, albedo / samples,
 // normalised normal sum (renderer.cu:422-428) and depth / samples (10 floats).

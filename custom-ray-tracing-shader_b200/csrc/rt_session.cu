@@ -17,6 +17,7 @@
 #include <omp.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstring>
 #include <curand.h>
@@ -52,6 +53,20 @@ struct UnetHandle {
 };
 
 namespace rt {
+// Countdown of RtxDebugFailAllocation: when it reaches the call that brings
+// it from 1 to 0, that allocation fails without calling cudaMalloc.
+static std::atomic<long long> g_failAllocationIn{0};
+cudaError_t deviceAllocBytes(void** p, size_t bytes) {
+    long long n = g_failAllocationIn.load();
+    while (n > 0 && !g_failAllocationIn.compare_exchange_weak(n, n - 1)) {
+    }
+    if (n == 1) {
+        *p = nullptr;
+        return cudaErrorMemoryAllocation;
+    }
+    return cudaMalloc(p, bytes);
+}
+
 // The sampler's direction numbers: cuRAND's JOEKUO6 table, fetched at run
 // time like the reference (sampling.cuh:10), 260 dimensions x 32 words.
 const unsigned* hostSobolDirections(std::string& error) {
@@ -119,12 +134,25 @@ struct Session {
     int environmentMode = 0;
     float3 environment = make_float3(0.0f, 0.0f, 0.0f);
     UnetHandle* denoiser = nullptr;  // learned denoiser used by RtDenoise (not owned)
+    // Where the last RtDenoise left its linear radiance inside dDenoise (float
+    // offset and floats per pixel), valid until the accumulation changes.
+    bool denoisedValid = false;
+    size_t denoisedOffset = 0;
+    int denoisedStride = 0;
 };
 
 bool fail(Session* s, cudaError_t e, const char* what = nullptr) {
     s->error = e;
     if (what) s->hostError = what;
     return false;
+}
+
+// Makes the session's device current; false (with the error recorded) when
+// the runtime refuses.
+bool useDevice(Session* s) {
+    cudaError_t e = cudaSetDevice(s->device);
+    if (e != cudaSuccess) return fail(s, e, "could not make the session's device current");
+    return true;
 }
 
 // The tree that traversal uses: over triangle pieces when built, else the
@@ -179,6 +207,7 @@ void releaseScene(Session* s) {
     s->build = BuildResult{};
     s->sahCost = -1.0;
     s->stats = RtxRenderStats{};
+    s->denoisedValid = false;
 }
 
 bool validSettings(const RenderSettings* st) {
@@ -188,7 +217,7 @@ bool validSettings(const RenderSettings* st) {
 
 SceneView deviceView(Session* s) {
     return SceneView{s->dTris, travWide(s), travPacked(s), s->dLights, s->lightCount, s->lightArea,
-                     travBuild(s).wideDepth, s->environmentMode, s->environment};
+                     travBuild(s).wideDepth, s->environmentMode, s->environment, s->tuning.stackLimit};
 }
 
 // Paths per wave: RTX_TUNE_PATHS_IN_FLIGHT (default kDefaultPathsInFlight),
@@ -238,6 +267,11 @@ bool renderDevice(Session* s, const CameraData* camera, const RenderSettings* se
     std::memcpy(&cam, camera, sizeof(cam));
     std::memcpy(&set, settings, sizeof(set));
     cudaError_t e;
+    // Path buffers are (re)allocated before the timed span; the span covers
+    // all of the pass's device work: sampler tables, counter resets, the
+    // integrator's kernels.
+    if (s->integrator != 1 && !ensureWave(s, set.raysPerPixel)) return false;
+    if ((e = cudaEventRecord(s->start, s->stream)) != cudaSuccess) return fail(s, e);
     if ((e = buildSobolTables(s->dDirs, s->samples, set.raysPerPixel, set.seed, s->dPassXor, s->dSeedHash, s->stream)) != cudaSuccess) return fail(s, e);
     if ((e = cudaMemsetAsync(s->dCounters, 0, 4 * sizeof(unsigned long long), s->stream)) != cudaSuccess) return fail(s, e);
     if ((e = cudaMemsetAsync(s->dError, 0, sizeof(int), s->stream)) != cudaSuccess) return fail(s, e);
@@ -245,9 +279,6 @@ bool renderDevice(Session* s, const CameraData* camera, const RenderSettings* se
                    s->dSum, s->dDepth, s->dPixels, s->dCounters, s->dError};
     int launches = 0;
     float extendMs = 0, shadowMs = 0, primaryMs = 0;
-    // Path buffers are (re)allocated before the timed span.
-    if (s->integrator != 1 && !ensureWave(s, set.raysPerPixel)) return false;
-    if ((e = cudaEventRecord(s->start, s->stream)) != cudaSuccess) return fail(s, e);
     if (s->integrator == 1) {
         e = launchMegakernel(L, s->stream, &launches);
     } else {
@@ -319,7 +350,7 @@ bool renderHost(Session* s, const CameraData* camera, const RenderSettings* sett
     if (s->hostDepth.size() != (size_t)s->width * s->height) s->hostDepth.assign((size_t)s->width * s->height, 0.0f);
     float* depthSums = s->hostDepth.data();
     SceneView sc{s->tris.data(), s->hostWide.data(), s->hostPacked.data(), s->lights.data(), (int)s->lights.size(),
-                 s->lightArea, travBuild(s).wideDepth, s->environmentMode, s->environment};
+                 s->lightArea, travBuild(s).wideDepth, s->environmentMode, s->environment, s->tuning.stackLimit};
     const int w = s->width, h = s->height;
     const unsigned sample0 = s->samples;
     Accum* sums = s->hostSum.data();
@@ -352,7 +383,8 @@ bool renderHost(Session* s, const CameraData* camera, const RenderSettings* sett
 
 // Shared front half of RtRender and RtxRenderDevice (renderer.cu:376-390).
 bool beginRender(Session* s, const CameraData* camera, const RenderSettings* settings, int backend) {
-    if (s->ready && s->device >= 0) cudaSetDevice(s->device);
+    s->denoisedValid = false;
+    if (s->ready && s->device >= 0 && !useDevice(s)) return false;
     if (backend == 3) {
         s->hostError = "Embree backend (3) is not available in this build";
         s->error = cudaErrorInvalidValue;
@@ -379,7 +411,7 @@ void* RtCreate(void) { return new Session(); }
 
 void RtReset(void* p) {
     Session* s = static_cast<Session*>(p);
-    if (s) { s->samples = 0; s->accumulationVersion++; }
+    if (s) { s->samples = 0; s->accumulationVersion++; s->denoisedValid = false; }
 }
 unsigned RtAccumulationVersion(void* p) { return p ? static_cast<Session*>(p)->accumulationVersion : 0u; }
 unsigned RtSampleCount(void* p) { return p ? static_cast<Session*>(p)->samples : 0u; }
@@ -399,7 +431,9 @@ const char* RtLastError(void* p) {
 void RtShutdown(void* p) {
     Session* s = static_cast<Session*>(p);
     if (!s) return;
-    if (s->device >= 0 && s->stream) cudaSetDevice(s->device);
+    // Releasing on another device than the scene's would free nothing; the
+    // attempt goes on regardless so the session is left empty.
+    if (s->device >= 0 && s->stream) (void)useDevice(s);
     releaseScene(s);
     s->hostError.clear();
 }
@@ -439,15 +473,15 @@ int RtInitialize(void* p, const Triangle* triangles, int count, int width, int h
     s->triCount = count;
     s->lightCount = s->upload.lightCount;
     s->lightArea = s->upload.lightArea;
-    RT_CHECK(cudaMalloc(&s->dDirs, sizeof(unsigned) * kSobolDims * 32));
+    RT_CHECK(rt::deviceAlloc(&s->dDirs, sizeof(unsigned) * kSobolDims * 32));
     RT_CHECK(cudaMemcpyAsync(s->dDirs, dirs, sizeof(unsigned) * kSobolDims * 32, cudaMemcpyHostToDevice, s->stream));
-    RT_CHECK(cudaMalloc(&s->dPassXor, sizeof(unsigned) * 16 * kSobolDims));
-    RT_CHECK(cudaMalloc(&s->dSeedHash, sizeof(unsigned) * kSobolDims));
-    RT_CHECK(cudaMalloc(&s->dSum, sizeof(Accum) * (size_t)width * height));
-    RT_CHECK(cudaMalloc(&s->dDepth, sizeof(float) * (size_t)width * height));
-    RT_CHECK(cudaMalloc(&s->dPixels, sizeof(uchar4) * (size_t)width * height));
-    RT_CHECK(cudaMalloc(&s->dCounters, 4 * sizeof(unsigned long long)));
-    RT_CHECK(cudaMalloc(&s->dError, 2 * sizeof(int)));
+    RT_CHECK(rt::deviceAlloc(&s->dPassXor, sizeof(unsigned) * 16 * kSobolDims));
+    RT_CHECK(rt::deviceAlloc(&s->dSeedHash, sizeof(unsigned) * kSobolDims));
+    RT_CHECK(rt::deviceAlloc(&s->dSum, sizeof(Accum) * (size_t)width * height));
+    RT_CHECK(rt::deviceAlloc(&s->dDepth, sizeof(float) * (size_t)width * height));
+    RT_CHECK(rt::deviceAlloc(&s->dPixels, sizeof(uchar4) * (size_t)width * height));
+    RT_CHECK(rt::deviceAlloc(&s->dCounters, 4 * sizeof(unsigned long long)));
+    RT_CHECK(rt::deviceAlloc(&s->dError, 2 * sizeof(int)));
     const char* why = nullptr;
     e = buildBvh(s->dTris, count, s->stream, s->bvh, s->build, &why);
     int pieceTotal = count;
@@ -512,12 +546,12 @@ int RtDenoise(void* p, unsigned char* output, int outputBytes, float* millisecon
                                    : "RtDenoise: invalid output buffer";
         return 0;
     }
-    cudaSetDevice(s->device);
+    if (!useDevice(s)) return 0;
     auto begin = std::chrono::steady_clock::now();
     s->hostError.clear();
     size_t count = (size_t)s->width * s->height;
     cudaError_t e;
-    if (!s->dDenoise && (e = cudaMalloc(&s->dDenoise, sizeof(float4) * 4 * count)) != cudaSuccess) { fail(s, e); return 0; }
+    if (!s->dDenoise && (e = rt::deviceAlloc(&s->dDenoise, sizeof(float4) * 4 * count)) != cudaSuccess) { fail(s, e); return 0; }
     if (s->lastBackend != 2) {
         if ((e = cudaMemcpyAsync(s->dSum, s->hostSum.data(), count * sizeof(Accum), cudaMemcpyHostToDevice, s->stream)) != cudaSuccess) { fail(s, e); return 0; }
     }
@@ -533,7 +567,13 @@ int RtDenoise(void* p, unsigned char* output, int outputBytes, float* millisecon
         if ((e = launchAovs(s->dSum, s->dDepth, s->samples, (int)count, aov, s->stream)) != cudaSuccess) { fail(s, e); return 0; }
         if ((e = s->denoiser->net.inferDevice(aov, s->height, s->width, radiance, s->stream, why)) != cudaSuccess) { fail(s, e, why.empty() ? nullptr : why.c_str()); return 0; }
         if ((e = launchPresentRadiance(s->dSum, radiance, (int)count, s->lastSettings.exposure, s->dPixels, s->stream)) != cudaSuccess) { fail(s, e); return 0; }
-    } else if ((e = launchDenoise(s->dSum, s->samples, s->width, s->height, s->lastSettings.exposure, s->dDenoise, s->dPixels, s->stream)) != cudaSuccess) { fail(s, e); return 0; }
+        s->denoisedOffset = 10 * count;
+        s->denoisedStride = 3;
+    } else {
+        if ((e = launchDenoise(s->dSum, s->samples, s->width, s->height, s->lastSettings.exposure, s->dDenoise, s->dPixels, s->stream)) != cudaSuccess) { fail(s, e); return 0; }
+        s->denoisedOffset = 4 * 3 * count;  // region 3 of the filter's work buffer
+        s->denoisedStride = 4;
+    }
     if ((e = cudaEventRecord(s->stop, s->stream)) != cudaSuccess) { fail(s, e); return 0; }
     if ((e = cudaStreamSynchronize(s->stream)) != cudaSuccess) { fail(s, e); return 0; }
     if ((e = cudaEventElapsedTime(&s->stats.denoiseMs, s->start, s->stop)) != cudaSuccess) { fail(s, e); return 0; }
@@ -544,6 +584,7 @@ int RtDenoise(void* p, unsigned char* output, int outputBytes, float* millisecon
     if ((e = cudaMemcpy(output, s->dPixels, count * 4, cudaMemcpyDeviceToHost)) != cudaSuccess) { fail(s, e); return 0; }
     *milliseconds = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - begin).count();
     if (!(*milliseconds > 0)) *milliseconds = 1e-6f;
+    s->denoisedValid = true;
     s->error = cudaSuccess;
     return 1;
 }
@@ -555,7 +596,7 @@ int RtxQueryRays(void* p, const RtxQuery* queries, int count, int any, RtxHit* h
     if (!s) return 0;
     if (!s->ready || !queries || !hits || count < 0) { s->error = cudaErrorInvalidValue; s->hostError = "RtxQueryRays: invalid arguments"; return 0; }
     if (count == 0) return 1;
-    cudaSetDevice(s->device);
+    if (!useDevice(s)) return 0;
     std::vector<float4> packed((size_t)count * 2);
     for (int i = 0; i < count; i++) {
         const RtxQuery& q = queries[i];
@@ -565,8 +606,8 @@ int RtxQueryRays(void* p, const RtxQuery* queries, int count, int any, RtxHit* h
     float4 *dq = nullptr, *dh = nullptr;
     std::vector<float4> out((size_t)count);
     int overflow = 0;
-    cudaError_t e = cudaMalloc(&dq, sizeof(float4) * packed.size());
-    if (e == cudaSuccess) e = cudaMalloc(&dh, sizeof(float4) * (size_t)count);
+    cudaError_t e = rt::deviceAlloc(&dq, sizeof(float4) * packed.size());
+    if (e == cudaSuccess) e = rt::deviceAlloc(&dh, sizeof(float4) * (size_t)count);
     if (e == cudaSuccess) e = cudaMemcpyAsync(dq, packed.data(), sizeof(float4) * packed.size(), cudaMemcpyHostToDevice, s->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(s->dError, 0, sizeof(int), s->stream);
     if (e == cudaSuccess) e = launchQueries(travWide(s), travPacked(s), dq, count, any, dh, s->dError + 1, s->dError,
@@ -594,11 +635,11 @@ int RtxSobolSamples(const unsigned* pixel, const unsigned* sample, const unsigne
     unsigned *dd = nullptr, *dp = nullptr, *ds = nullptr, *dseed = nullptr;
     float* dout = nullptr;
     size_t n = (size_t)count;
-    cudaError_t e = cudaMalloc(&dd, sizeof(unsigned) * kSobolDims * 32);
-    if (e == cudaSuccess) e = cudaMalloc(&dp, sizeof(unsigned) * n);
-    if (e == cudaSuccess) e = cudaMalloc(&ds, sizeof(unsigned) * n);
-    if (e == cudaSuccess) e = cudaMalloc(&dseed, sizeof(unsigned) * n);
-    if (e == cudaSuccess) e = cudaMalloc(&dout, sizeof(float) * n * ndim);
+    cudaError_t e = rt::deviceAlloc(&dd, sizeof(unsigned) * kSobolDims * 32);
+    if (e == cudaSuccess) e = rt::deviceAlloc(&dp, sizeof(unsigned) * n);
+    if (e == cudaSuccess) e = rt::deviceAlloc(&ds, sizeof(unsigned) * n);
+    if (e == cudaSuccess) e = rt::deviceAlloc(&dseed, sizeof(unsigned) * n);
+    if (e == cudaSuccess) e = rt::deviceAlloc(&dout, sizeof(float) * n * ndim);
     if (e == cudaSuccess) e = cudaMemcpy(dd, dirs, sizeof(unsigned) * kSobolDims * 32, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(dp, pixel, sizeof(unsigned) * n, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(ds, sample, sizeof(unsigned) * n, cudaMemcpyHostToDevice);
@@ -615,7 +656,7 @@ int RtxExportBvh(void* p, BvhNode* nodes, int nodeCapacity, int* order, int orde
     if (!s->ready || (nodes && nodeCapacity < s->build.binaryNodes) || (order && orderCapacity < s->triCount)) {
         s->error = cudaErrorInvalidValue; s->hostError = "RtxExportBvh: not initialised or buffers too small"; return 0;
     }
-    cudaSetDevice(s->device);
+    if (!useDevice(s)) return 0;
     cudaError_t e = cudaSuccess;
     if (nodes) e = cudaMemcpy(nodes, s->bvh.binNodes, sizeof(BvhNode) * (size_t)s->build.binaryNodes, cudaMemcpyDeviceToHost);
     if (e == cudaSuccess && order) e = cudaMemcpy(order, s->bvh.order, sizeof(int) * (size_t)s->triCount, cudaMemcpyDeviceToHost);
@@ -629,7 +670,7 @@ int RtxBvhStatsGet(void* p, RtxBvhStats* out) {
     if (!s->ready) { s->hostError = "RtxBvhStatsGet: session is not initialised"; return 0; }
     if (s->sahCost < 0) {
         std::vector<BvhNode> nodes((size_t)s->build.binaryNodes);
-        cudaSetDevice(s->device);
+        if (!useDevice(s)) return 0;
         cudaError_t e = cudaMemcpy(nodes.data(), s->bvh.binNodes, sizeof(BvhNode) * nodes.size(), cudaMemcpyDeviceToHost);
         if (e != cudaSuccess) { fail(s, e); return 0; }
         auto area = [](const BvhNode& n) {
@@ -669,7 +710,7 @@ int RtxReadAccumulation(void* p, PixelSum* out, int count) {
         std::memcpy(out, s->hostSum.data(), need * sizeof(PixelSum));
         return 1;
     }
-    cudaSetDevice(s->device);
+    if (!useDevice(s)) return 0;
     cudaError_t e = cudaMemcpy(out, s->dSum, need * sizeof(PixelSum), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) { fail(s, e); return 0; }
     return 1;
@@ -748,8 +789,8 @@ int RtxUnetInfer(void* p, const float* aovs, int h, int w, float* radiance) {
     float *dIn = nullptr, *dOut = nullptr;
     size_t px = (size_t)w * h;
     std::string why;
-    cudaError_t e = cudaMalloc(&dIn, sizeof(float) * px * 10);
-    if (e == cudaSuccess) e = cudaMalloc(&dOut, sizeof(float) * px * 3);
+    cudaError_t e = rt::deviceAlloc(&dIn, sizeof(float) * px * 10);
+    if (e == cudaSuccess) e = rt::deviceAlloc(&dOut, sizeof(float) * px * 3);
     if (e == cudaSuccess) e = cudaMemcpy(dIn, aovs, sizeof(float) * px * 10, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = u->net.inferDevice(dIn, h, w, dOut, 0, why);
     if (e == cudaSuccess) e = cudaMemcpy(radiance, dOut, sizeof(float) * px * 3, cudaMemcpyDeviceToHost);
@@ -784,9 +825,9 @@ int RtxReadAovs(void* p, float* out, int count) {
         s->hostError = "RtxReadAovs: render first, and pass room for width*height pixels";
         return 0;
     }
-    cudaSetDevice(s->device);
+    if (!useDevice(s)) return 0;
     cudaError_t e;
-    if (!s->dDenoise && (e = cudaMalloc(&s->dDenoise, sizeof(float4) * 4 * need)) != cudaSuccess) { fail(s, e); return 0; }
+    if (!s->dDenoise && (e = rt::deviceAlloc(&s->dDenoise, sizeof(float4) * 4 * need)) != cudaSuccess) { fail(s, e); return 0; }
     if (s->lastBackend != 2) {
         if ((e = cudaMemcpyAsync(s->dSum, s->hostSum.data(), need * sizeof(Accum), cudaMemcpyHostToDevice, s->stream)) != cudaSuccess) { fail(s, e); return 0; }
         if (s->hostDepth.size() == need &&
@@ -796,6 +837,28 @@ int RtxReadAovs(void* p, float* out, int count) {
     if ((e = launchAovs(s->dSum, s->dDepth, s->samples, (int)need, aov, s->stream)) != cudaSuccess) { fail(s, e); return 0; }
     if ((e = cudaStreamSynchronize(s->stream)) != cudaSuccess) { fail(s, e); return 0; }
     if ((e = cudaMemcpy(out, aov, need * 10 * sizeof(float), cudaMemcpyDeviceToHost)) != cudaSuccess) { fail(s, e); return 0; }
+    return 1;
+}
+
+int RtxReadDenoised(void* p, float* rgb, int count) {
+    Session* s = static_cast<Session*>(p);
+    if (!s) return 0;
+    const size_t need = (size_t)s->width * s->height;
+    if (!s->ready || !s->denoisedValid || !rgb || count < 0 || (size_t)count < need) {
+        s->error = cudaErrorInvalidValue;
+        s->hostError = "RtxReadDenoised: call RtDenoise after the last render, and pass room for width*height pixels";
+        return 0;
+    }
+    if (!useDevice(s)) return 0;
+    float* base = reinterpret_cast<float*>(s->dDenoise);
+    // Staged in floats [0, 3 * count), free once the denoise is done and below
+    // both result locations (10 * count for the network, 12 * count for the
+    // filter), so the result stays readable.
+    float* out = base;
+    cudaError_t e;
+    if ((e = launchDenoisedRgb(s->dSum, base + s->denoisedOffset, s->denoisedStride, (int)need, out, s->stream)) != cudaSuccess) { fail(s, e); return 0; }
+    if ((e = cudaMemcpyAsync(rgb, out, need * 3 * sizeof(float), cudaMemcpyDeviceToHost, s->stream)) != cudaSuccess) { fail(s, e); return 0; }
+    if ((e = cudaStreamSynchronize(s->stream)) != cudaSuccess) { fail(s, e); return 0; }
     return 1;
 }
 
@@ -816,6 +879,12 @@ int RtxSetEnvironment(void* p, int mode, float r, float g, float b) {
     return 1;
 }
 
+int RtxDebugFailAllocation(int n) {
+    if (n < 0) return 0;
+    rt::g_failAllocationIn.store(n);
+    return 1;
+}
+
 int RtxSetTuning(void* p, int key, int value) {
     Session* s = static_cast<Session*>(p);
     if (!s) return 0;
@@ -824,10 +893,8 @@ int RtxSetTuning(void* p, int key, int value) {
             if (value < 1024) return 0;
             s->pathsInFlight = value;
             return 1;
-        case RTX_TUNE_POSTPONE:
-            if (value != 0 && value != 1) return 0;
-            s->tuning.postpone = value;
-            return 1;
+        case RTX_TUNE_POSTPONE:  // no effect on this traversal schedule; accepted for compatibility
+            return value == 0 || value == 1;
         case RTX_TUNE_REFILL:
             if (value < 1 || value > 32) return 0;
             s->tuning.refill = value;
@@ -843,6 +910,10 @@ int RtxSetTuning(void* p, int key, int value) {
         case RTX_TUNE_LANES:
             if (value < 1 || value > kMaxLanes) return 0;
             s->tuning.lanes = value;
+            return 1;
+        case RTX_TUNE_STACK_LIMIT:
+            if (value < 1 || value > kStackCapacity) return 0;
+            s->tuning.stackLimit = value;
             return 1;
         default:
             return 0;
@@ -866,7 +937,7 @@ constexpr size_t kStaticPacked = 0;                                    // 2 floa
 constexpr size_t kStaticHits = 2 * (size_t)kStaticQueryRays;           // 1 float4 per ray, RtxHit layout
 constexpr size_t kStaticRaw = 3 * (size_t)kStaticQueryRays;            // caller's 28-byte RtxQuery records
 constexpr size_t kStaticCounters = kStaticRaw + (7 * (size_t)kStaticQueryRays + 3) / 4;  // work counter, error flag
-constexpr size_t kStaticFloat4s = kStaticCounters + 1;                 // 1.25 MiB in total
+constexpr size_t kStaticFloat4s = kStaticCounters + 1;                 // 1,245,200 bytes in total
 constexpr int kStaticMaxDevices = 64;
 
 // One copy per GPU that loads the library, held until the process exits.
@@ -877,7 +948,9 @@ std::mutex g_staticScratchLock;
 float4* g_staticScratchAddress[kStaticMaxDevices] = {};
 
 // Device address of g_staticQueryScratch on the current device, looked up
-// once per device (the host-side symbol is not a device address).
+// once per device (the host-side symbol is not a device address). The cached
+// address is valid while the device's primary context lives; a
+// cudaDeviceReset makes it stale.
 float4* staticQueryScratch(int device, std::string& error) {
     if (device < 0 || device >= kStaticMaxDevices) { error = "RtxQueryRaysStatic: device index out of range"; return nullptr; }
     std::lock_guard<std::mutex> guard(g_staticScratchLock);
@@ -918,8 +991,8 @@ extern "C" int RtxQueryRaysStatic(void* p, const RtxQuery* queries, int count, i
         return 0;
     }
     if (count == 0) return 1;
-    cudaError_t e = cudaSetDevice(s->device);
-    if (e != cudaSuccess) { fail(s, e); return 0; }
+    if (!useDevice(s)) return 0;
+    cudaError_t e;
     std::string why;
     float4* scratch = staticQueryScratch(s->device, why);
     if (!scratch) { s->hostError = why; return 0; }

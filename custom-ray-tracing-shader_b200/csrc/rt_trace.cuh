@@ -66,7 +66,7 @@ __device__ __forceinline__ bool triangleStep(LaneRay& L, const float4* tris) {
 // the current group has no interior children left, then visits one child
 // node (its eight child boxes). Returns true when the traversal is complete.
 __device__ __forceinline__ bool nodeStep(LaneRay& L, const uint4* nodes, uint2* sstack, int stride, uint2* lstack,
-                                         int& overflow) {
+                                         int& overflow, int stackLimit) {
     if (L.group.y <= 0x00FFFFFFu) {
         if (L.top == 0) return true;
         L.top--;
@@ -79,7 +79,7 @@ __device__ __forceinline__ bool nodeStep(LaneRay& L, const uint4* nodes, uint2* 
     unsigned slot = ((unsigned)bit - 24u) ^ L.r.octInv;
     unsigned child = L.group.x + __popc(L.group.y & 0xFFu & ((1u << slot) - 1u));
     if (L.group.y > 0x00FFFFFFu) {
-        if (L.top >= kStackCapacity) { overflow = 1; return true; }
+        if (L.top >= stackLimit) { overflow = 1; return true; }
         if (L.top < kSharedStack) sstack[L.top * stride] = L.group;
         else lstack[L.top - kSharedStack] = L.group;
         L.top++;
@@ -196,20 +196,18 @@ __device__ __forceinline__ bool warpTrianglePhase(LaneRay& L, bool busy, const f
 //   __device__ void load(int k, float3& o, float3& d, float& limit, unsigned& root);
 //   __device__ void store(int k, const Hit& h);
 // `fetch` must be zero at launch. Adds the number of finished queries to
-// *done and sets *errorFlag on stack overflow. Dynamic shared memory:
-// traceSharedBytes(blockDim.x).
+// *done and sets *errorFlag on stack overflow (more than stackLimit <=
+// kStackCapacity entries). Dynamic shared memory: traceSharedBytes(blockDim.x).
 //
 // Each round has a triangle phase, in which the warp tests all pending
 // triangles of its lanes cooperatively (warpTrianglePhase), and a node phase,
 // in which every busy lane takes one node step. The node step (eight box
 // tests) is the costly one, so running it in lockstep for all busy lanes
-// keeps the warp's lanes doing useful work. postponeBelow is unused by this
-// schedule and kept for the tuning interface.
+// keeps the warp's lanes doing useful work.
 template <bool ANY, class IO>
 __device__ __forceinline__ void persistentTrace(IO& io, int count, const uint4* nodes, const float4* tris, int* fetch,
-                                                unsigned long long* done, int* errorFlag, int postponeBelow,
+                                                unsigned long long* done, int* errorFlag, int stackLimit,
                                                 int refill) {
-    (void)postponeBelow;
     extern __shared__ uint2 smemStack[];
     uint2* sstack = smemStack + threadIdx.x;
     const int stride = blockDim.x;
@@ -258,7 +256,7 @@ __device__ __forceinline__ void persistentTrace(IO& io, int count, const uint4* 
                 k = -1;
                 finished++;
             }
-            if (k >= 0 && nodeStep(L, nodes, sstack, stride, lstack, overflow)) {
+            if (k >= 0 && nodeStep(L, nodes, sstack, stride, lstack, overflow, stackLimit)) {
                 io.store(k, L.hit);
                 k = -1;
                 finished++;

@@ -180,14 +180,14 @@ cudaError_t uploadScene(const void* triangles, int count, cudaStream_t stream, S
     float area = 0.0f;
     unsigned cap = 1u << 12;  // set slots; grows until the distinct values fit in half
 #define RT_TRY(x) do { if ((e = (x)) != cudaSuccess) goto done; } while (0)
-    RT_TRY(cudaMalloc(&dTris, sizeof(SceneTri) * (size_t)count));
+    RT_TRY(rt::deviceAlloc(&dTris, sizeof(SceneTri) * (size_t)count));
     RT_TRY(cudaMemcpyAsync(dTris, triangles, sizeof(SceneTri) * (size_t)count, cudaMemcpyHostToDevice, stream));
     // counters: [0] distinct values, [1] overflow, [2] missing, [3] emitters
-    RT_TRY(cudaMalloc(&counters, 4 * sizeof(unsigned)));
+    RT_TRY(rt::deviceAlloc(&counters, 4 * sizeof(unsigned)));
     for (;;) {
-        RT_TRY(cudaMalloc(&table, sizeof(unsigned long long) * cap));
-        RT_TRY(cudaMalloc(&slotIndex, sizeof(unsigned) * cap));
-        RT_TRY(cudaMalloc(&values, sizeof(unsigned) * (cap / 2)));
+        RT_TRY(rt::deviceAlloc(&table, sizeof(unsigned long long) * cap));
+        RT_TRY(rt::deviceAlloc(&slotIndex, sizeof(unsigned) * cap));
+        RT_TRY(rt::deviceAlloc(&values, sizeof(unsigned) * (cap / 2)));
         RT_TRY(cudaMemsetAsync(table, 0, sizeof(unsigned long long) * cap, stream));
         RT_TRY(cudaMemsetAsync(counters, 0, 4 * sizeof(unsigned), stream));
         collectColoursKernel<<<gridFor(components, kBlock), kBlock, 0, stream>>>(dTris, components, table, cap - 1,
@@ -212,14 +212,14 @@ cudaError_t uploadScene(const void* triangles, int count, cudaStream_t stream, S
             std::memcpy(&c, &hostValues[k], sizeof(c));
             hostDecoded[k] = srgbToLinear(c);  // the reference's host expression (renderer.cu:84-85,347)
         }
-        RT_TRY(cudaMalloc(&decoded, sizeof(float) * hostDecoded.size()));
+        RT_TRY(rt::deviceAlloc(&decoded, sizeof(float) * hostDecoded.size()));
         RT_TRY(cudaMemcpyAsync(decoded, hostDecoded.data(), sizeof(float) * hostDecoded.size(), cudaMemcpyHostToDevice, stream));
     }
     applyColoursKernel<<<gridFor(components, kBlock), kBlock, 0, stream>>>(dTris, components, table, cap - 1, slotIndex,
                                                                             decoded, reinterpret_cast<int*>(&counters[2]));
     RT_TRY(cudaGetLastError());
     // Emitters.
-    RT_TRY(cudaMalloc(&blockCounts, sizeof(unsigned) * (size_t)blocks));
+    RT_TRY(rt::deviceAlloc(&blockCounts, sizeof(unsigned) * (size_t)blocks));
     emitterCountKernel<<<blocks, kBlock, 0, stream>>>(dTris, count, blockCounts);
     scanCountsKernel<<<1, 1024, 0, stream>>>(blockCounts, blocks, &counters[3]);
     RT_TRY(cudaGetLastError());
@@ -228,9 +228,9 @@ cudaError_t uploadScene(const void* triangles, int count, cudaStream_t stream, S
     if (hostCounters[2]) { error = "colour decode table is missing a value"; e = cudaErrorUnknown; goto done; }
     R.lightCount = (int)hostCounters[3];
     if (R.lightCount > 0) {
-        RT_TRY(cudaMalloc(&emitterTri, sizeof(int) * (size_t)R.lightCount));
-        RT_TRY(cudaMalloc(&emitterArea, sizeof(float) * (size_t)R.lightCount + sizeof(float)));
-        RT_TRY(cudaMalloc(&dLights, sizeof(Light) * (size_t)R.lightCount));
+        RT_TRY(rt::deviceAlloc(&emitterTri, sizeof(int) * (size_t)R.lightCount));
+        RT_TRY(rt::deviceAlloc(&emitterArea, sizeof(float) * (size_t)R.lightCount + sizeof(float)));
+        RT_TRY(rt::deviceAlloc(&dLights, sizeof(Light) * (size_t)R.lightCount));
         emitterScatterKernel<<<blocks, kBlock, 0, stream>>>(dTris, count, blockCounts, emitterTri, emitterArea);
         cumulativeAreaKernel<<<1, 32, 0, stream>>>(emitterTri, emitterArea, R.lightCount, dLights,
                                                    emitterArea + R.lightCount);

@@ -107,9 +107,10 @@ EXPORTS = ('RtCreate', 'RtDestroy', 'RtShutdown', 'RtInitialize', 'RtRender', 'R
            'RtAccumulationVersion', 'RtSampleCount', 'RtEmbreeBuildMilliseconds', 'RtCpuThreadCount',
            'RtBvhInfo', 'RtLastError', 'RtxQueryRays', 'RtxSobolSamples', 'RtxExportBvh', 'RtxBvhStatsGet',
            'RtxReadAccumulation', 'RtxRenderStatsGet', 'RtxRenderDevice', 'RtxSetIntegrator', 'RtxSetTuning',
+           'RtxDebugFailAllocation',
            'RtxQueryRaysStatic', 'RtxSetEnvironment', 'RtxUnetCreate', 'RtxUnetDestroy', 'RtxUnetParamCount',
            'RtxUnetLastError', 'RtxUnetGetParams', 'RtxUnetSetParams', 'RtxUnetLossGrad', 'RtxUnetTrain',
-           'RtxUnetInfer', 'RtxUnetSave', 'RtxUnetLoad', 'RtxSetDenoiser', 'RtxReadAovs',
+           'RtxUnetInfer', 'RtxUnetSave', 'RtxUnetLoad', 'RtxSetDenoiser', 'RtxReadAovs', 'RtxReadDenoised',
            'RtxBatchCreate', 'RtxBatchDestroy', 'RtxBatchLastError', 'RtxBatchAddScene', 'RtxBatchAddView',
            'RtxBatchSetEnvironment', 'RtxBatchRender', 'RtxBatchReset', 'RtxBatchSampleCount', 'RtxBatchReadImage',
            'RtxBatchReadAccumulation', 'RtxBatchSetTuning', 'RtxBatchAutotune', 'RtxBatchStatsGet')
@@ -147,6 +148,7 @@ def load_library(path=None):
     lib.RtxRenderDevice.argtypes = [vp, c.POINTER(Camera), c.POINTER(Settings), c.POINTER(c.c_float)]
     lib.RtxSetIntegrator.argtypes = [vp, c.c_int]
     lib.RtxSetTuning.argtypes = [vp, c.c_int, c.c_int]
+    lib.RtxDebugFailAllocation.argtypes = [c.c_int]
     lib.RtxQueryRaysStatic.argtypes = [vp, c.c_void_p, c.c_int, c.c_int, c.c_void_p]
     lib.RtxSetEnvironment.argtypes = [vp, c.c_int, c.c_float, c.c_float, c.c_float]
     lib.RtxUnetCreate.restype = vp
@@ -165,6 +167,7 @@ def load_library(path=None):
     lib.RtxUnetLoad.argtypes = [vp, c.c_char_p]
     lib.RtxSetDenoiser.argtypes = [vp, vp]
     lib.RtxReadAovs.argtypes = [vp, c.c_void_p, c.c_int]
+    lib.RtxReadDenoised.argtypes = [vp, c.c_void_p, c.c_int]
     lib.RtxBatchCreate.restype = vp
     lib.RtxBatchCreate.argtypes = []
     lib.RtxBatchDestroy.argtypes = [vp]
@@ -300,12 +303,15 @@ class Session:
         self.check(self.lib.RtxSetIntegrator(self.handle, mode))
 
     TUNE_PATHS_IN_FLIGHT, TUNE_POSTPONE, TUNE_REFILL, TUNE_PIECES, TUNE_LEAF, TUNE_LANES = 1, 2, 3, 4, 5, 6
+    TUNE_STACK_LIMIT = 7
 
-    def set_tuning(self, paths_in_flight=None, postpone=None, refill=None, pieces=None, leaf=None, lanes=None):
-        """pieces and leaf apply from the next initialize()."""
+    def set_tuning(self, paths_in_flight=None, postpone=None, refill=None, pieces=None, leaf=None, lanes=None,
+                   stack_limit=None):
+        """pieces and leaf apply from the next initialize(); stack_limit below
+        48 makes traversal fail with a stack overflow (the failure path)."""
         for key, value in ((self.TUNE_PATHS_IN_FLIGHT, paths_in_flight), (self.TUNE_POSTPONE, postpone),
                            (self.TUNE_REFILL, refill), (self.TUNE_PIECES, pieces), (self.TUNE_LEAF, leaf),
-                           (self.TUNE_LANES, lanes)):
+                           (self.TUNE_LANES, lanes), (self.TUNE_STACK_LIMIT, stack_limit)):
             if value is not None:
                 self.check(self.lib.RtxSetTuning(self.handle, key, int(value)))
 
@@ -321,6 +327,12 @@ class Session:
         """Denoiser inputs of the current accumulation, shape (height, width, 10)."""
         out = np.zeros((self.height, self.width, 10), np.float32)
         self.check(self.lib.RtxReadAovs(self.handle, out.ctypes.data, self.width * self.height))
+        return out
+
+    def denoised_radiance(self):
+        """Linear radiance of the last denoise(), (width*height, 3) float32."""
+        out = np.zeros((self.width * self.height, 3), np.float32)
+        self.check(self.lib.RtxReadDenoised(self.handle, out.ctypes.data, self.width * self.height))
         return out
 
     def set_denoiser(self, net):

@@ -174,15 +174,16 @@ int RtxRenderDevice(void* session, const CameraData* camera, const RenderSetting
  * 1 = one-kernel path tracer. Both give bit-identical accumulations. */
 int RtxSetIntegrator(void* session, int mode);
 /* Tunables of the wavefront integrator, one key at a time. Results do not
- * depend on them, only speed does. Returns 0 for an unknown key or a value
- * out of range.
+ * depend on them, only speed does (except RTX_TUNE_STACK_LIMIT below its
+ * default, which makes traversal fail). Returns 0 for an unknown key or a
+ * value out of range.
  *   RTX_TUNE_PATHS_IN_FLIGHT  paths per wave (>= 1024; default 16,777,216,
  *                             at most width * height * raysPerPixel); a wave
  *                             may span several of a pass's raysPerPixel rows.
  *                             Path state takes 168 bytes per path and lane
  *                             (2.8 GB per lane at the default)
- *   RTX_TUNE_POSTPONE         1 = postpone triangle tests in sparse warps,
- *                             0 = off (default)
+ *   RTX_TUNE_POSTPONE         0 or 1; no effect on the current traversal
+ *                             schedule (accepted for compatibility)
  *   RTX_TUNE_REFILL           refill a warp's idle lanes when fewer than this
  *                             many lanes are busy (1..32, default 24)
  *   RTX_TUNE_PIECES           most pieces per triangle of the traversal tree
@@ -205,6 +206,13 @@ int RtxSetIntegrator(void* session, int mode);
  *                             own path buffers, so the end of one wave's
  *                             kernels overlaps another's; samples are still
  *                             added to each pixel in sample order
+ *   RTX_TUNE_STACK_LIMIT      traversal stack entries a ray may use (1..48,
+ *                             default 48, which every tree built here fits):
+ *                             a query that needs more stops, and RtRender,
+ *                             RtxRenderDevice and RtxQueryRays return 0 with
+ *                             "BVH traversal stack overflow" (the accumulation
+ *                             of that pass is not valid; RtReset before the
+ *                             next one). For testing the failure path.
  */
 #define RTX_TUNE_PATHS_IN_FLIGHT 1
 #define RTX_TUNE_POSTPONE 2
@@ -212,7 +220,17 @@ int RtxSetIntegrator(void* session, int mode);
 #define RTX_TUNE_PIECES 4
 #define RTX_TUNE_LEAF 5
 #define RTX_TUNE_LANES 6
+#define RTX_TUNE_STACK_LIMIT 7
 int RtxSetTuning(void* session, int key, int value);
+
+/* Failure injection on the host, no counterpart in the reference: the n-th
+ * next device allocation made by the renderer (sessions, scene upload, BVH
+ * build, wave buffers, batches) fails with cudaErrorMemoryAllocation without
+ * calling cudaMalloc, as if the device were out of memory; n = 0 disarms it.
+ * Process-wide; for testing the error paths (each must return 0, report the
+ * error through RtLastError and leave the session usable). Returns 0 for
+ * n < 0. */
+int RtxDebugFailAllocation(int n);
 /* Light arriving from outside the scene on rays that leave it after the first
  * bounce (primary misses stay black, as in the reference). mode 0: the
  * reference's sky gradient times settings->skyStrength (Native/renderer.cu:
@@ -251,6 +269,13 @@ int RtxSetDenoiser(void* session, void* net);
  * (radiance / samples), albedo / samples, normalised normal sum, first-hit
  * distance / samples (the distance is an added AOV). */
 int RtxReadAovs(void* session, float* aovs, int count);
+/* The linear radiance of the last RtDenoise (learned network or filter), 3
+ * floats per pixel in the accumulation's order, uncovered pixels 0: what
+ * RtDenoise tonemaps into its RGBA8 image, before quantisation, so quality
+ * can be measured on float values. Fails unless RtDenoise succeeded after
+ * the last render or reset. count >= width * height. No counterpart in the
+ * reference (its OptiX pass returns only the RGBA8 image). */
+int RtxReadDenoised(void* session, float* rgb, int count);
 /* ---- Batched multi-scene rendering (no counterpart in the reference) ----
  * Many views of many scenes of uneven size, rendered together: every frame
  * traces the paths of all views in shared waves, so each traversal launch
@@ -321,12 +346,15 @@ int RtxBatchStatsGet(void* batch, RtxBatchStats* stats);
  * running beside a CUDA graph capture, latency-critical loops where
  * cudaMalloc/cudaFree would synchronise the device, hosts whose device memory
  * belongs to a pool). Rays and hits are staged in a file-scope device array
- * of 1.25 MiB that every GPU loading the library keeps until the process
- * exits; count may be at most 16384 per call (larger counts return 0 with a
- * message). The first call on each device looks up that array's device
- * address, so make it before any stream capture. All calls on a device share
- * the array: calls whose GPU work overlaps race and must be serialised by the
- * caller. Results equal RtxQueryRays. */
+ * of 1,245,200 bytes (about 1.19 MiB) that every GPU loading the library
+ * keeps until the process exits; count may be at most 16384 per call (larger
+ * counts return 0 with a message). The first call on each device looks up
+ * that array's device address, so make it before any stream capture; the
+ * address is cached per device and stays valid while the device's primary
+ * context lives (after cudaDeviceReset the cached address is stale, so do
+ * not call this entry point again in that process). All calls on a device
+ * share the array: calls whose GPU work overlaps race and must be serialised
+ * by the caller. Results equal RtxQueryRays. */
 int RtxQueryRaysStatic(void* session, const RtxQuery* queries, int count, int any, RtxHit* hits);
 
 #ifdef __cplusplus

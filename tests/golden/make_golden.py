@@ -10,6 +10,7 @@ oracle and the CUDA library against these files, so they also run where the
 reference is absent.
 """
 import hashlib
+import os
 import sys
 from pathlib import Path
 
@@ -23,6 +24,10 @@ import scenes  # noqa: E402
 from oracle_api import Reference  # noqa: E402
 
 OUT = Path(__file__).resolve().parent
+# Where the reference's sources lie (the REFERENCE_ROOT environment variable);
+# tests that read the reference's own files take it from here and skip when it
+# is absent.
+REFERENCE_ROOT = Path(os.environ.get('REFERENCE_ROOT', '/root/reference'))
 
 
 def sha(a):
@@ -93,7 +98,7 @@ def main():
     print('golden fixtures written to', OUT)
 
 
-def snapshot_fixture(reference_root=Path('/root/reference')):
+def snapshot_fixture(reference_root=REFERENCE_ROOT):
     """The reference's Suzanne-room snapshot (Benchmarks/embree/scene.json,
     982 triangles) as scene_io loads it, with the size, depth and node-array
     hash of the reference builder's BVH for it."""

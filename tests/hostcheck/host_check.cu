@@ -64,16 +64,19 @@ int hc_collapse(const BinNode* bn, const int* order, const SceneTri* tris, int n
 
 // Ray queries (28-byte origin/direction/limit records) against a wide BVH.
 // stats: [0] node visits, [1] triangle tests, [2] stack overflows.
+// stats: [0] node visits, [1] triangle tests, [2] queries that overflowed a
+// stack of stackLimit entries (0: the library's default, kStackCapacity).
 void hc_query(const uint4* wide, const float4* packed, const float* queries, int count, int any, Hit* out,
-              unsigned long long* stats, unsigned* perRay) {
+              unsigned long long* stats, unsigned* perRay, int stackLimit) {
     uint2 stack[kStackCapacity];
+    const int limit = stackLimit > 0 && stackLimit < kStackCapacity ? stackLimit : kStackCapacity;
     for (int i = 0; i < count; i++) {
         const float* q = queries + 7 * (size_t)i;
         int overflow = 0;
         TraversalCounters tc{0, 0};
         float3 o = v3(q[0], q[1], q[2]), d = v3(q[3], q[4], q[5]);
-        out[i] = any ? traverse<true>(wide, packed, o, d, q[6], stack, 1, &overflow, &tc)
-                     : traverse<false>(wide, packed, o, d, q[6], stack, 1, &overflow, &tc);
+        out[i] = any ? traverse<true>(wide, packed, o, d, q[6], stack, 1, &overflow, &tc, limit)
+                     : traverse<false>(wide, packed, o, d, q[6], stack, 1, &overflow, &tc, limit);
         stats[0] += tc.nodes; stats[1] += tc.tris; stats[2] += (unsigned)overflow;
         if (perRay) { perRay[2 * (size_t)i] = tc.nodes; perRay[2 * (size_t)i + 1] = tc.tris; }
     }

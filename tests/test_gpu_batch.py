@@ -1,10 +1,15 @@
 """Batched multi-scene rendering (RtxBatch*) on a GPU.
 
-A view rendered in a batch must accumulate exactly what RtRender (backend 2)
-accumulates for the same scene, camera and settings: every tuning (block
-size, queue capacity down to waves that span several views, refill, graph
-replay or direct launches, 4- or 8-wide BVH) only changes the schedule, so
-the PixelSum records are compared bit for bit."""
+A view rendered in a batch must accumulate exactly what the reference's own
+CUDA renderer (Native/renderer.cu renderKernel, built for sm_100a into
+oracle/_ref) accumulates for that scene, camera and settings alone: every
+tuning (block size, queue capacity down to waves that span several views,
+refill, graph replay or direct launches, 4- or 8-wide BVH) only changes the
+schedule, so the PixelSum records and images are compared bit for bit. Where
+oracle/_ref is absent the expectation is this library's RtRender (backend 2),
+itself bit-identical to the reference renderer in tests/test_gpu_parity.py.
+The constant environment is this library's addition, so its expectation is
+always RtRender."""
 import math
 
 import numpy as np
@@ -50,10 +55,29 @@ def session_reference(lib, tris, cam, w, h, frames, settings=SETTINGS, environme
         s.close()
 
 
+def reference_renderer(tris, cam, w, h, frames, settings=SETTINGS):
+    """The reference's CUDA renderer on one view (None where oracle/_ref is absent)."""
+    from oracle_api import Reference, ReferenceSession, reference_available
+    if not reference_available():
+        return None
+    ref = ReferenceSession(Reference())
+    try:
+        ref.initialize(tris, w, h)
+        for _ in range(frames):
+            image, _ = ref.render(cam, settings)
+        return ref.sums(), image.copy()
+    finally:
+        ref.close()
+
+
 @pytest.fixture(scope='module')
 def reference(lib):
     scene_list, views = views_of_two_scenes()
-    return scene_list, views, [session_reference(lib, scene_list[k], cam, w, h, 2) for k, cam, w, h in views]
+    expect = []
+    for k, cam, w, h in views:
+        expect.append(reference_renderer(scene_list[k], cam, w, h, 2) or
+                      session_reference(lib, scene_list[k], cam, w, h, 2))
+    return scene_list, views, expect
 
 
 def make_batch(lib, scene_list, views):

@@ -30,7 +30,7 @@ def hc():
     lib = c.CDLL(str(LIB))
     vp = c.c_void_p
     lib.hc_collapse.argtypes = [vp, vp, vp, c.c_int, vp, c.c_int, vp, vp, c.c_int, c.c_int]
-    lib.hc_query.argtypes = [vp, vp, vp, c.c_int, c.c_int, vp, vp, vp]
+    lib.hc_query.argtypes = [vp, vp, vp, c.c_int, c.c_int, vp, vp, vp, c.c_int]
     lib.hc_render.argtypes = [vp, vp, c.c_int, c.c_float, vp, vp, vp, vp, vp, c.c_int, c.c_int, c.c_uint, vp, vp, vp]
     return lib
 
@@ -62,7 +62,7 @@ def test_wide_traversal_matches_reference(hc, oracle, name, group, width):
         out = np.zeros(len(RAYS), HIT_DTYPE)
         stats = np.zeros(3, np.uint64)
         hc.hc_query(wide.ctypes.data, packed.ctypes.data, np.ascontiguousarray(RAYS).ctypes.data, len(RAYS), any_hit,
-                    out.ctypes.data, stats.ctypes.data, None)
+                    out.ctypes.data, stats.ctypes.data, None, 0)
         assert stats[2] == 0
         if any_hit:
             assert ((out['index'] >= 0) == (g['any_index'] >= 0)).all()

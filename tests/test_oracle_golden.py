@@ -1,6 +1,5 @@
 """The oracle against fixtures produced by the reference itself (tests/golden),
 and against the reference's own known answers. CPU only."""
-from pathlib import Path
 
 import numpy as np
 import pytest
@@ -162,7 +161,8 @@ def test_known_answers(oracle):
             assert (rgba[3::4] == 255).all()
 
 
-REFERENCE_SCENE = Path('/root/reference/Benchmarks/embree/scene.json')
+from make_golden import REFERENCE_ROOT  # noqa: E402
+REFERENCE_SCENE = REFERENCE_ROOT / 'Benchmarks/embree/scene.json'
 
 
 @pytest.mark.skipif(not REFERENCE_SCENE.exists(), reason='reference scene snapshots absent on this machine')

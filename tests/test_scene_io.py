@@ -3,7 +3,6 @@ Triangle records of an object, against the reference's own files where they
 exist (its two scene snapshots, the Suzanne mesh and the dragon OBJ) and
 against hand-made files everywhere."""
 import importlib.util
-from pathlib import Path
 
 import numpy as np
 import pytest
@@ -11,7 +10,7 @@ import pytest
 import scene_io
 import scenes
 
-REFERENCE = Path('/root/reference')
+from make_golden import REFERENCE_ROOT as REFERENCE  # noqa: E402
 ROOM_SNAPSHOT = REFERENCE / 'Benchmarks/embree/scene.json'           # 982 triangles: Suzanne room
 DRAGON_SNAPSHOT = REFERENCE / 'Benchmarks/quality/dragon/scene.json.gz'  # 87,165 triangles
 SUZANNE = REFERENCE / 'UnityRayTracer/Assets/RayTracing/Models/Suzanne.json'

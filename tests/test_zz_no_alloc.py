@@ -38,6 +38,11 @@ def test_static_queries_equal_allocating_queries():
                 got = s.query_static(rays, any_hit=any_hit)
                 assert got.tobytes() == expected.tobytes()
                 assert (got['index'] >= 0).any()
+        # Exactly the capacity: the caller's raw records then end where the
+        # array's counters begin.
+        full = scenes.random_rays(rng, Session.STATIC_QUERY_CAPACITY)
+        for any_hit in (False, True):
+            assert s.query_static(full, any_hit=any_hit).tobytes() == s.query(full, any_hit=any_hit).tobytes()
     finally:
         s.close()
 
