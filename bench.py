@@ -78,7 +78,11 @@ def parse():
                    help="waves in flight, 1..4 (RTX_TUNE_LANES; default: the library default)")
     p.add_argument('--denoiser-only', action='store_true',
                    help='only time learned-denoiser inference at 1920x1080 (a small case for profiling)')
-    p.set_defaults(quality=True, batch=True, denoiser=True)
+    p.add_argument('--no-train-step', dest='train_step', action='store_false',
+                   help='skip timing U-Net training steps (batch 32 of 128x128 crops; 1 GPU runs it by default)')
+    p.add_argument('--train-steps', type=int, default=20, help='timed training steps')
+    p.add_argument('--train-step-only', action='store_true', help='only time U-Net training steps (for profiling)')
+    p.set_defaults(quality=True, batch=True, denoiser=True, train_step=True)
     return p.parse_args()
 
 
@@ -641,6 +645,41 @@ def denoiser_run(lib, args, repeats=10):
                                  'display; CUDA events), against the bf16 dense GEMM peak'}}
 
 
+def train_step_run(lib, args, batch=32, size=128, crops=64, warmup=5):
+    """U-Net training steps as configured for the denoiser (batch 32 of
+    128x128 crops, Adam): forward, L1 loss on log radiance, backward (data
+    and weight gradients on the tensor cores), Adam and the BF16 weight
+    copies, driven by RtxUnetTrain on a seeded synthetic crop set resident on
+    the device. ms_per_step = host wall time of RtxUnetTrain over the timed
+    steps (it synchronises at its end) / steps."""
+    import numpy as np
+    from native_api import Unet
+    rng = np.random.default_rng(31)
+    yy, xx = np.mgrid[0:size, 0:size] / size
+    target = (rng.uniform(0.1, 2.0, (crops, 1, 1, 3)) * (0.5 + 0.5 * np.sin(3 * xx + 2 * yy))[None, ..., None])
+    aovs = np.empty((crops, size, size, 10), np.float32)
+    aovs[..., 0:3] = target * rng.exponential(1.0, (crops, size, size, 3))
+    aovs[..., 3:6] = rng.uniform(0, 1, (crops, 1, 1, 3))
+    nrm = rng.normal(size=(crops, size, size, 3))
+    aovs[..., 6:9] = nrm / np.linalg.norm(nrm, axis=-1, keepdims=True)
+    aovs[..., 9] = 1.0 + 4.0 * yy[None]
+    target = target.astype(np.float32)
+    net = Unet(lib, seed=3)
+    try:
+        net.train(aovs, target, steps=warmup, batch=batch, lr=1e-3, seed=1)
+        t0 = time.perf_counter()
+        losses = net.train(aovs, target, steps=args.train_steps, batch=batch, lr=1e-3, seed=2)
+        wall = time.perf_counter() - t0
+    finally:
+        net.close()
+    ms = wall * 1e3 / args.train_steps
+    flops = 3.0 * unet_flops_per_pixel() * batch * size * size  # forward, data gradient, weight gradient
+    return {'workload': f'U-Net training step, batch {batch} of {size}x{size} crops, Adam (RtxUnetTrain)',
+            'steps': args.train_steps, 'ms_per_step': ms, 'gflop_per_step': flops / 1e9,
+            'tflops': flops / (ms * 1e-3) / 1e12, 'loss_first': float(losses[0]), 'loss_last': float(losses[-1]),
+            'timing': 'host wall clock around RtxUnetTrain (synchronises at its end), after warm-up steps'}
+
+
 def kernel_rates(integrator, per_kind, primary_ms, extend_ms, shadow_ms, lanes):
     """Mrays/s of each traversal kind over its own kernels' device time:
     primary (closest-hit at bounce 0), secondary (closest-hit at later
@@ -883,6 +922,7 @@ def run_ours(args, rank, local_rank, world):
             'time_to_35db': quality_run(lib, args) if (args.quality and world == 1) else None,
             'batch': batch_run(lib, args) if (args.batch and world == 1) else None,
             'denoiser': denoiser_run(lib, args) if (args.denoiser and world == 1) else None,
+            'train_step': train_step_run(lib, args) if (args.train_step and world == 1) else None,
         }
     s.close()
     dist.close()
@@ -947,6 +987,9 @@ def main():
     if args.denoiser_only:
         from native_api import load_library
         result = denoiser_run(load_library(), args) if rank == 0 else None
+    elif args.train_step_only:
+        from native_api import load_library
+        result = train_step_run(load_library(), args) if rank == 0 else None
     elif args.impl == 'reference':
         result = run_reference(args, rank, world)
     else:

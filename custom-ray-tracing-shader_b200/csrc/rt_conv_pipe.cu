@@ -1,0 +1,653 @@
+// Warp-specialised 3x3 convolution on the fifth-generation tensor cores,
+// fed by TMA: the row-ring form of the denoiser's convolutions.
+//
+// Implicit GEMM as in rt_conv_tc.cuh: a tile is 128 consecutive output pixels
+// of one image row (the MMA's M) and all output channels (N); K runs over
+// the 9 taps and the input channels. A block owns strips of rows of one
+// 128-pixel column of an image and walks them top to bottom, so every input
+// row is staged once per strip and read by the three tiles that need it.
+//
+// Roles (6 warps):
+//   warp 0     producer: TMA loads of the weights (once per block) and of the
+//              input rows into a ring of R slots, each row as planes of 8
+//              channels x 130 pixels x 16 bytes (the no-swizzle K-major
+//              operand layout: core matrices of 8 pixels x 16 bytes, 128
+//              bytes apart along M, one plane apart along K). For the
+//              decoder's concatenated input [upsample2(low), skip] the skip
+//              planes come from one tensor map and the low-resolution row
+//              from another into a staging area, which the warp's lanes
+//              expand (each low pixel to two) into the slot's first planes.
+//   warp 1     MMA issuer (one thread) and tensor-memory owner: per tile 9
+//              taps x cin/16 tcgen05.mma into one of two accumulators; a
+//              commit tells the epilogue the accumulator is full and another
+//              frees the ring slot of the row no later tile reads.
+//   warps 2-5  epilogue: tcgen05.ld of the accumulator (warp w reads lanes
+//              32 (w % 4) ...), which is then handed back to the issuer,
+//              bias, ReLU and the store (BF16, or FP32 added to or written).
+// Hand-offs are mbarriers only: full/empty per ring slot, full/empty per
+// accumulator, one for the weights. Every wait is bounded by %globaltimer;
+// a wait that runs out sets the block's abort flag and the error flag, every
+// role leaves its loop, the producer waits (bounded) for its loads in
+// flight, the issuer for its MMAs, and the tensor memory is freed.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <mutex>
+#include <vector>
+
+#include "rt_conv_tc.cuh"
+
+namespace rt {
+namespace {
+
+using bf16 = __nv_bfloat16;
+
+constexpr int kM = 128;                  // output pixels per tile
+constexpr int kHalo = kM + 2;            // input pixels per staged row
+constexpr int kLowHalo = kM / 2 + 2;     // low-resolution pixels per staged row
+// Bytes of one 8-channel plane of a staged row (130 and 66 pixels x 16
+// bytes), padded to 128 bytes: every TMA destination starts on a 128-byte
+// boundary.
+constexpr uint32_t kPlane = (kHalo * 16 + 127) / 128 * 128;        // 2,176
+constexpr uint32_t kLowPlane = (kLowHalo * 16 + 127) / 128 * 128;  // 1,152
+constexpr int kThreads = 192;
+constexpr int kMinRing = 3;  // the rows a tile reads; 4 and more let the producer run ahead
+constexpr int kMaxRing = 8;
+constexpr uint32_t kHeader = 1024;       // barriers and flags
+
+struct PipeArgs {
+    int n, h, w, cin, cout, lowChannels;
+    int tilesPerRow, stripRows, strips, units, ring;
+    uint32_t weightBytes, slotBytes, lowSlotBytes, accCols, tmemCols;
+    const float* bias;
+    bf16* outB;
+    float* outF;
+    int relu, accumulate, reverseTaps;
+    int* errorFlag;
+    unsigned long long waitLimitNs;
+    int probe;  // 1: the issuer first waits on a barrier nothing completes (tests the abort path)
+};
+
+// Shared-memory header: barrier offsets (8 bytes each).
+struct Header {
+    static constexpr uint32_t full = 0;                    // kMaxRing
+    static constexpr uint32_t empty = 8 * kMaxRing;        // kMaxRing
+    static constexpr uint32_t lowFull = 16 * kMaxRing;     // kMaxRing
+    static constexpr uint32_t accFull = 24 * kMaxRing;     // 2
+    static constexpr uint32_t accEmpty = 24 * kMaxRing + 16;
+    static constexpr uint32_t weights = 24 * kMaxRing + 32;
+    static constexpr uint32_t probe = 24 * kMaxRing + 40;
+    static constexpr uint32_t drain = 24 * kMaxRing + 48;
+    static constexpr uint32_t tmemSlot = 24 * kMaxRing + 56;
+    static constexpr uint32_t abort = 24 * kMaxRing + 60;
+};
+static_assert(Header::abort + 4 <= kHeader, "header size");
+
+__device__ __forceinline__ uint32_t smemAddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ uint64_t nowNs() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ void barInit(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void barArrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void barExpectTx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool barTryWait(uint32_t bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\nselp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity), "r"(1000u)
+        : "memory");
+    return done != 0;
+}
+__device__ __forceinline__ bool barTestWait(uint32_t bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n.reg .pred p;\nmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+// Bounded wait for the phase of parity `parity` to complete. Gives up when
+// the block's abort flag is set or when limitNs pass (then sets the flag).
+__device__ bool waitPhase(uint32_t bar, uint32_t parity, volatile int* abortFlag, uint64_t limitNs) {
+    if (barTryWait(bar, parity)) return true;
+    const uint64_t deadline = nowNs() + limitNs;
+    for (;;) {
+        if (barTryWait(bar, parity)) return true;
+        if (*abortFlag) return false;
+        if (nowNs() > deadline) { *abortFlag = 1; return false; }
+    }
+}
+// The same for a whole warp: lane 0 waits and every lane gets its verdict,
+// so the warp's control flow stays uniform (tcgen05.ld and __syncwarp need
+// converged lanes).
+__device__ __forceinline__ bool waitPhaseWarp(uint32_t bar, uint32_t parity, volatile int* abortFlag,
+                                              uint64_t limitNs) {
+    bool ok = true;
+    if ((threadIdx.x & 31) == 0) ok = waitPhase(bar, parity, abortFlag, limitNs);
+    return __shfl_sync(0xFFFFFFFFu, ok ? 1 : 0, 0) != 0;
+}
+// Bounded poll that ignores the abort flag (the drains on the abort path).
+__device__ void pollPhase(uint32_t bar, uint32_t parity, uint64_t limitNs) {
+    const uint64_t deadline = nowNs() + limitNs;
+    while (!barTryWait(bar, parity) && nowNs() < deadline) {
+    }
+}
+
+// TMA loads (no multicast; the tensor maps cover this GPU's memory only).
+__device__ __forceinline__ void tmaLoad4(uint32_t dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
+                                         uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+        "[%6];\n" ::"r"(dst),
+        "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(bar)
+        : "memory");
+}
+__device__ __forceinline__ void tmaLoad3(uint32_t dst, const CUtensorMap* map, int c0, int c1, int c2, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];\n" ::"r"(dst),
+        "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(bar)
+        : "memory");
+}
+
+__device__ __forceinline__ void tcFenceBefore() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void tcFenceAfter() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void mma(uint32_t tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}\n" ::"r"(tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+        : "memory");
+}
+__device__ __forceinline__ void commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar)
+                 : "memory");
+}
+__device__ __forceinline__ void tmemLoad16(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+        "%14, %15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+}
+__device__ __forceinline__ void tmemWaitLoads() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
+
+// Unit u: image, column tile and strip of rows [y0, y1).
+struct Unit { int img, x0, y0, y1; };
+__device__ __forceinline__ Unit unitOf(const PipeArgs& a, int u) {
+    const int strip = u % a.strips, xt = (u / a.strips) % a.tilesPerRow, img = u / (a.strips * a.tilesPerRow);
+    const int y0 = strip * a.stripRows;
+    return Unit{img, xt * kM, y0, min(a.h, y0 + a.stripRows)};
+}
+
+template <int COUT>
+__device__ __forceinline__ void epilogueStore(const PipeArgs& a, const uint32_t (&acc)[COUT], size_t pix) {
+    float v[COUT];
+#pragma unroll
+    for (int j = 0; j < COUT; j++) {
+        const float s = __uint_as_float(acc[j]) + (a.bias ? __ldg(a.bias + j) : 0.0f);
+        v[j] = a.relu ? fmaxf(s, 0.0f) : s;
+    }
+    if (a.outF) {
+        float4* o = reinterpret_cast<float4*>(a.outF + pix * COUT);
+#pragma unroll
+        for (int q = 0; q < COUT / 4; q++) {
+            float4 x = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+            if (a.accumulate) {
+                const float4 old = o[q];
+                x = make_float4(old.x + x.x, old.y + x.y, old.z + x.z, old.w + x.w);
+            }
+            o[q] = x;
+        }
+    } else {
+        uint4* o = reinterpret_cast<uint4*>(a.outB + pix * COUT);
+#pragma unroll
+        for (int q = 0; q < COUT / 8; q++) {
+            uint32_t words[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                __nv_bfloat162 pair = __floats2bfloat162_rn(v[8 * q + 2 * j], v[8 * q + 2 * j + 1]);
+                words[j] = *reinterpret_cast<uint32_t*>(&pair);
+            }
+            o[q] = make_uint4(words[0], words[1], words[2], words[3]);
+        }
+    }
+}
+
+template <int COUT>
+__global__ void __launch_bounds__(kThreads) convPipeKernel(const __grid_constant__ CUtensorMap inMap,
+                                                          const __grid_constant__ CUtensorMap lowMap,
+                                                          const __grid_constant__ CUtensorMap wMap, PipeArgs a) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t base = smemAddr(smem);
+    volatile int* abortFlag = reinterpret_cast<volatile int*>(smem + Header::abort);
+    const uint32_t wAddr = base + kHeader;
+    const uint32_t ringAddr = wAddr + a.weightBytes;
+    const uint32_t lowAddr = ringAddr + (uint32_t)a.ring * a.slotBytes;  // 2 staging rows of the low input
+    unsigned char* lowPtr = smem + (lowAddr - base);
+    unsigned char* ringPtr = smem + (ringAddr - base);
+    const int G = a.cin / 8, Glow = a.lowChannels / 8, Gin = G - Glow;
+    const int R = a.ring;
+    const uint64_t limit = a.waitLimitNs;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < R; s++) {
+            barInit(base + Header::full + 8 * s, Glow ? 2 : 1);
+            barInit(base + Header::empty + 8 * s, 1);
+        }
+        for (int s = 0; s < 2; s++) barInit(base + Header::lowFull + 8 * s, 1);
+        for (int b = 0; b < 2; b++) {
+            barInit(base + Header::accFull + 8 * b, 1);
+            barInit(base + Header::accEmpty + 8 * b, 4);
+        }
+        barInit(base + Header::weights, 1);
+        barInit(base + Header::probe, 1);
+        barInit(base + Header::drain, 1);
+        *abortFlag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(base + Header::tmemSlot),
+                     "r"(a.tmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+    }
+    tcFenceBefore();
+    __syncthreads();
+    tcFenceAfter();
+    const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(smem + Header::tmemSlot);
+
+    if (warp == 0) {
+        // ---- producer ----
+        if (lane == 0) {
+            asm volatile("prefetch.tensormap [%0];\n" ::"l"(&inMap) : "memory");
+            if (Glow) asm volatile("prefetch.tensormap [%0];\n" ::"l"(&lowMap) : "memory");
+            asm volatile("prefetch.tensormap [%0];\n" ::"l"(&wMap) : "memory");
+            const uint32_t wb = base + Header::weights;
+            barExpectTx(wb, a.weightBytes);
+            for (int t = 0; t < 9; t++)
+                for (int g = 0; g < G; g++)
+                    tmaLoad3(wAddr + (uint32_t)((t * G + g) * COUT * 16), &wMap, g * 8, 0, a.reverseTaps ? 8 - t : t,
+                             wb);
+        }
+        // Rows are numbered in issue order q; row q sits in slot q % R, its
+        // low-resolution part (concatenated input) in staging buffer q % 2.
+        // A row is expanded at most one row behind the last one issued (the
+        // two staging buffers), and before the producer would block on a
+        // slot: a slot may be waiting for exactly that expansion.
+        long long q = 0, expanded = 0;
+        bool ok = true;
+        auto expand = [&](long long e) -> bool {
+            if (!waitPhaseWarp(base + Header::lowFull + 8 * (int)(e & 1), (uint32_t)((e >> 1) & 1), abortFlag, limit))
+                return false;
+            const uint4* src = reinterpret_cast<const uint4*>(lowPtr + (size_t)(e & 1) * a.lowSlotBytes);
+            uint4* dst = reinterpret_cast<uint4*>(ringPtr + (size_t)(e % R) * a.slotBytes);
+            // Staged pixel p is input x0 - 1 + p, whose low-resolution pixel
+            // floor((x0 - 1 + p) / 2) is staged at (p + 1) / 2 (x0 even).
+            for (int v = lane; v < Glow * kHalo; v += 32) {
+                const int g = v / kHalo, p = v % kHalo;
+                dst[g * (kPlane / 16) + p] = src[g * (kLowPlane / 16) + (p + 1) / 2];
+            }
+            asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+            __syncwarp();
+            if (lane == 0) barArrive(base + Header::full + 8 * (int)(e % R));
+            return true;
+        };
+        for (int u = blockIdx.x; u < a.units && ok; u += gridDim.x) {
+            const Unit U = unitOf(a, u);
+            for (int r = U.y0 - 1; r <= U.y1 && ok; r++) {
+                const int s = (int)(q % R);
+                const uint32_t emptyBar = base + Header::empty + 8 * s, emptyParity = (uint32_t)(((q / R) & 1) ^ 1);
+                if (Glow && expanded < q) {
+                    const bool freeNow = __shfl_sync(0xFFFFFFFFu, lane == 0 ? (barTestWait(emptyBar, emptyParity) ? 1 : 0) : 0, 0) != 0;
+                    if (!freeNow) {
+                        if (!expand(expanded)) { ok = false; break; }
+                        expanded++;
+                    }
+                }
+                if (!waitPhaseWarp(emptyBar, emptyParity, abortFlag, limit)) { ok = false; break; }
+                if (lane == 0) {
+                    const uint32_t fb = base + Header::full + 8 * s;
+                    const uint32_t slot = ringAddr + (uint32_t)s * a.slotBytes;
+                    barExpectTx(fb, (uint32_t)Gin * kHalo * 16u);  // the boxes' bytes (planes are padded)
+                    for (int g = 0; g < Gin; g++)
+                        tmaLoad4(slot + (uint32_t)(Glow + g) * kPlane, &inMap, g * 8, U.x0 - 1, r, U.img, fb);
+                    if (Glow) {
+                        const uint32_t lb = base + Header::lowFull + 8 * (int)(q & 1);
+                        const uint32_t ls = lowAddr + (uint32_t)(q & 1) * a.lowSlotBytes;
+                        barExpectTx(lb, (uint32_t)Glow * kLowHalo * 16u);
+                        for (int g = 0; g < Glow; g++)
+                            tmaLoad4(ls + (uint32_t)g * kLowPlane, &lowMap, g * 8, U.x0 / 2 - 1, r >> 1, U.img, lb);
+                    }
+                }
+                __syncwarp();
+                q++;
+                // Keep at most one row unexpanded (its staging buffer is
+                // the one the next row does not use).
+                if (Glow && expanded < q - 1) {
+                    if (!expand(expanded)) { ok = false; break; }
+                    expanded++;
+                }
+            }
+        }
+        while (ok && Glow && expanded < q) {
+            ok = expand(expanded);
+            if (ok) expanded++;
+        }
+        // Every load issued must land before the block exits, also when the
+        // issuer gave up before reading them: poll the phases of the weights,
+        // the two staging buffers and the last R slots (each the latest
+        // phase of its barrier, so the parities are unambiguous). After a
+        // failure, rows not expanded get their second arrival first so
+        // their slot's phase can complete.
+        if (!ok) *abortFlag = 1;
+        if (lane == 0) {
+            pollPhase(base + Header::weights, 0u, limit);
+            for (long long e = q > 2 ? q - 2 : 0; e < q && Glow; e++)
+                pollPhase(base + Header::lowFull + 8 * (int)(e & 1), (uint32_t)((e >> 1) & 1), limit);
+            for (long long e = q > R ? q - R : 0; e < q; e++) {
+                if (Glow && e >= expanded) barArrive(base + Header::full + 8 * (int)(e % R));
+                pollPhase(base + Header::full + 8 * (int)(e % R), (uint32_t)((e / R) & 1), limit);
+            }
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        // ---- MMA issuer ----
+        bool ok = true;
+        if (lane == 0) {
+            const uint32_t idesc = ummaInstrDescBf16(kM, COUT);
+            if (a.probe) ok = waitPhase(base + Header::probe, 0u, abortFlag, limit);
+            if (ok) ok = waitPhase(base + Header::weights, 0u, abortFlag, limit);
+            long long q = 0, tile = 0;
+            const uint32_t kStepA = (2u * kPlane) >> 4, kStepB = (2u * COUT * 16u) >> 4;
+            for (int u = blockIdx.x; u < a.units && ok; u += gridDim.x) {
+                const Unit U = unitOf(a, u);
+                const long long q0 = q;  // row U.y0 - 1
+                for (int y = U.y0; y < U.y1 && ok; y++, tile++) {
+                    const long long qr = q0 + (y - U.y0);  // row y - 1
+                    for (long long e = (y == U.y0 ? qr : qr + 2); e <= qr + 2 && ok; e++)
+                        ok = waitPhase(base + Header::full + 8 * (int)(e % R), (uint32_t)((e / R) & 1), abortFlag, limit);
+                    const int b = (int)(tile & 1);
+                    if (ok) ok = waitPhase(base + Header::accEmpty + 8 * b, (uint32_t)(((tile >> 1) & 1) ^ 1), abortFlag, limit);
+                    if (!ok) break;
+                    tcFenceAfter();
+                    const uint32_t acc = tmem + (uint32_t)b * a.accCols;
+                    for (int t = 0; t < 9; t++) {
+                        const int dy = t / 3, dx = t % 3;
+                        const uint32_t slot = ringAddr + (uint32_t)((qr + dy) % R) * a.slotBytes;
+                        uint64_t aDesc = ummaSmemDesc(slot + (uint32_t)dx * 16u, kPlane, 128u);
+                        uint64_t bDesc = ummaSmemDesc(wAddr + (uint32_t)(t * G * COUT * 16), COUT * 16u, 128u);
+                        for (int k = 0; k < G / 2; k++, aDesc += kStepA, bDesc += kStepB)
+                            mma(acc, aDesc, bDesc, idesc, (t > 0 || k > 0) ? 1u : 0u);
+                    }
+                    commit(base + Header::accFull + 8 * b);
+                    commit(base + Header::empty + 8 * (int)(qr % R));  // row y - 1: no later tile reads it
+                }
+                if (!ok) break;
+                // Rows y1 - 1 and y1 of the strip are read by no later tile.
+                const long long last = q0 + (U.y1 - U.y0);
+                commit(base + Header::empty + 8 * (int)(last % R));
+                commit(base + Header::empty + 8 * (int)((last + 1) % R));
+                q = last + 2;
+            }
+            if (ok) {
+                // The commits' arrivals land after the MMAs complete: wait for
+                // the last ones (the rows released last, the last two
+                // accumulators) before the block's shared memory goes away.
+                for (long long e = q > R ? q - R : 0; e < q; e++)
+                    pollPhase(base + Header::empty + 8 * (int)(e % R), (uint32_t)((e / R) & 1), limit);
+                for (long long t = tile > 2 ? tile - 2 : 0; t < tile; t++)
+                    pollPhase(base + Header::accFull + 8 * (int)(t & 1), (uint32_t)((t >> 1) & 1), limit);
+            } else {
+                *abortFlag = 1;
+                // Wait (bounded) for every MMA issued so far.
+                commit(base + Header::drain);
+                pollPhase(base + Header::drain, 0u, limit);
+            }
+        }
+        __syncwarp();
+    } else {
+        // ---- epilogue: warps 2-5, lanes 32 * (warp % 4) ... of the accumulator ----
+        const int quarter = warp & 3;
+        long long tile = 0;
+        bool ok = true;
+        for (int u = blockIdx.x; u < a.units && ok; u += gridDim.x) {
+            const Unit U = unitOf(a, u);
+            for (int y = U.y0; y < U.y1; y++, tile++) {
+                const int b = (int)(tile & 1);
+                if (!waitPhaseWarp(base + Header::accFull + 8 * b, (uint32_t)((tile >> 1) & 1), abortFlag, limit)) { ok = false; break; }
+                tcFenceAfter();
+                uint32_t acc[COUT];
+                const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)b * a.accCols;
+#pragma unroll
+                for (int c = 0; c < COUT / 16; c++) {
+                    uint32_t r[16];
+                    tmemLoad16(taddr + (uint32_t)(16 * c), r);
+#pragma unroll
+                    for (int j = 0; j < 16; j++) acc[16 * c + j] = r[j];
+                }
+                tmemWaitLoads();
+                tcFenceBefore();
+                __syncwarp();
+                if (lane == 0) barArrive(base + Header::accEmpty + 8 * b);
+                const int x = U.x0 + quarter * 32 + lane;
+                if (x < a.w) epilogueStore<COUT>(a, acc, ((size_t)U.img * a.h + y) * a.w + x);
+            }
+        }
+    }
+    tcFenceBefore();
+    __syncthreads();
+    if (threadIdx.x == 0 && *abortFlag) atomicExch(a.errorFlag, 1);
+    if (warp == 1) {
+        tcFenceAfter();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(a.tmemCols)
+                     : "memory");
+    }
+}
+
+// ---- host ----
+
+PFN_cuTensorMapEncodeTiled_v12000 encodeTiled() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+// Rank-4 or rank-3 BF16 tensor map, no swizzle, zero fill outside the tensor.
+bool makeMap(CUtensorMap* map, const void* ptr, int rank, const uint64_t* dims, const uint64_t* strides,
+             const uint32_t* box) {
+    auto fn = encodeTiled();
+    if (!fn) return false;
+    uint32_t elem[4] = {1, 1, 1, 1};
+    return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, (cuuint32_t)rank, const_cast<void*>(ptr), dims, strides, box,
+              elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+int deviceSmCount() {
+    int device = 0, sms = 0;
+    cudaGetDevice(&device);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    return sms > 0 ? sms : 1;
+}
+
+template <int COUT>
+cudaError_t launchPipe(const CUtensorMap& inMap, const CUtensorMap& lowMap, const CUtensorMap& wMap,
+                       const PipeArgs& a, int grid, uint32_t smemBytes, cudaStream_t stream) {
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(convPipeKernel<COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             227 * 1024);
+        if (e != cudaSuccess) return e;
+        configured = true;
+    }
+    convPipeKernel<COUT><<<grid, kThreads, smemBytes, stream>>>(inMap, lowMap, wMap, a);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+uint32_t convPipeSmemBytes(int cin, int cout, int lowChannels, int ring) {
+    const uint32_t weights = 9u * (uint32_t)cin * (uint32_t)cout * 2u;
+    const uint32_t slot = ((uint32_t)(cin / 8) * kPlane + 127u) & ~127u;
+    const uint32_t lowSlot = ((uint32_t)(lowChannels / 8) * kLowPlane + 127u) & ~127u;
+    return kHeader + weights + (uint32_t)ring * slot + 2u * lowSlot;
+}
+
+bool convPipeSupported(int cin, int cout, int lowChannels) {
+    static const int couts[] = {16, 32, 48, 64, 80, 96};
+    bool known = false;
+    for (int c : couts) known = known || c == cout;
+    return known && cin >= 16 && cin % 16 == 0 && lowChannels % 16 == 0 && lowChannels < cin &&
+           convPipeSmemBytes(cin, cout, lowChannels, kMinRing) <= 227u * 1024u;
+}
+
+cudaError_t convPipe(const bf16* in, const bf16* low, int lowChannels, int n, int h, int w, int cin,
+                     const bf16* weights, bool reverseTaps, const float* bias, int cout, bf16* outB, float* outF,
+                     bool relu, bool accumulate, int* errorFlag, cudaStream_t stream, const ConvPipeTest* test) {
+    if (!low) lowChannels = 0;
+    if (n < 1 || h < 1 || w < 1 || !convPipeSupported(cin, cout, lowChannels) || (!outB && !outF) || !errorFlag ||
+        (lowChannels && (h % 2 || w % 2)))
+        return cudaErrorNotSupported;
+    const int cinIn = cin - lowChannels;
+    CUtensorMap inMap{}, lowMap{}, wMap{};
+    {
+        const uint64_t dims[4] = {(uint64_t)cinIn, (uint64_t)w, (uint64_t)h, (uint64_t)n};
+        const uint64_t strides[3] = {(uint64_t)cinIn * 2, (uint64_t)w * cinIn * 2, (uint64_t)h * w * cinIn * 2};
+        const uint32_t box[4] = {8, kHalo, 1, 1};
+        if (!makeMap(&inMap, in, 4, dims, strides, box)) return cudaErrorNotSupported;
+    }
+    if (lowChannels) {
+        const uint64_t dims[4] = {(uint64_t)lowChannels, (uint64_t)(w / 2), (uint64_t)(h / 2), (uint64_t)n};
+        const uint64_t strides[3] = {(uint64_t)lowChannels * 2, (uint64_t)(w / 2) * lowChannels * 2,
+                                     (uint64_t)(h / 2) * (w / 2) * lowChannels * 2};
+        const uint32_t box[4] = {8, kLowHalo, 1, 1};
+        if (!makeMap(&lowMap, low, 4, dims, strides, box)) return cudaErrorNotSupported;
+    } else {
+        lowMap = inMap;
+    }
+    {
+        const uint64_t dims[3] = {(uint64_t)cin, (uint64_t)cout, 9};
+        const uint64_t strides[2] = {(uint64_t)cin * 2, (uint64_t)cout * cin * 2};
+        const uint32_t box[3] = {8, (uint32_t)cout, 1};
+        if (!makeMap(&wMap, weights, 3, dims, strides, box)) return cudaErrorNotSupported;
+    }
+    PipeArgs a{};
+    a.n = n; a.h = h; a.w = w; a.cin = cin; a.cout = cout; a.lowChannels = lowChannels;
+    a.tilesPerRow = (w + kM - 1) / kM;
+    a.weightBytes = 9u * (uint32_t)cin * (uint32_t)cout * 2u;
+    a.slotBytes = ((uint32_t)(cin / 8) * kPlane + 127u) & ~127u;
+    a.lowSlotBytes = ((uint32_t)(lowChannels / 8) * kLowPlane + 127u) & ~127u;
+    a.accCols = 32;
+    while (a.accCols < (uint32_t)cout) a.accCols <<= 1;
+    a.tmemCols = 2 * a.accCols;
+    a.bias = bias; a.outB = outB; a.outF = outF;
+    a.relu = relu ? 1 : 0; a.accumulate = accumulate ? 1 : 0; a.reverseTaps = reverseTaps ? 1 : 0;
+    a.errorFlag = errorFlag;
+    a.waitLimitNs = test && test->waitLimitNs ? test->waitLimitNs : 1000000000ull;
+    a.probe = test && test->probe ? 1 : 0;
+    // Blocks per SM from shared and tensor memory at a ring of 4 rows (3
+    // where 4 do not fit); then the largest ring (up to 8 rows) that keeps
+    // that many blocks per SM.
+    const int sms = deviceSmCount();
+    const uint32_t smemPerSm = 228u * 1024u;
+    a.ring = convPipeSmemBytes(cin, cout, lowChannels, 4) <= 227u * 1024u ? 4 : kMinRing;
+    int perSm = (int)(smemPerSm / (convPipeSmemBytes(cin, cout, lowChannels, a.ring) + 1024u));
+    perSm = std::max(1, std::min({perSm, (int)(512u / a.tmemCols), 2048 / kThreads}));
+    while (a.ring < kMaxRing && (uint32_t)perSm * (convPipeSmemBytes(cin, cout, lowChannels, a.ring + 1) + 1024u) <= smemPerSm &&
+           convPipeSmemBytes(cin, cout, lowChannels, a.ring + 1) <= 227u * 1024u)
+        a.ring++;
+    if (test && test->ring >= kMinRing && test->ring <= kMaxRing) a.ring = test->ring;
+    const uint32_t smemBytes = convPipeSmemBytes(cin, cout, lowChannels, a.ring);
+    if (smemBytes > 227u * 1024u) return cudaErrorNotSupported;
+    // Strips: long enough to reuse rows (each strip stages 2 extra rows),
+    // short enough to give every block about two units.
+    const long long columns = (long long)n * a.tilesPerRow;
+    const long long blocks = (long long)sms * perSm;
+    long long rows = std::max(1ll, columns * h / (2 * blocks));
+    a.stripRows = (int)std::max(4ll, std::min<long long>(32, rows));
+    if (test && test->stripRows > 0) a.stripRows = test->stripRows;
+    a.strips = (h + a.stripRows - 1) / a.stripRows;
+    a.units = (int)(columns * a.strips);
+    const int grid = (int)std::min<long long>(a.units, blocks);
+    switch (cout) {
+        case 16: return launchPipe<16>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
+        case 32: return launchPipe<32>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
+        case 48: return launchPipe<48>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
+        case 64: return launchPipe<64>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
+        case 80: return launchPipe<80>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
+        case 96: return launchPipe<96>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
+        default: return cudaErrorNotSupported;
+    }
+}
+
+int convPipeWaitProbe() {
+    // A 128 x 4 image of 16 channels, zero input and weights: the output is
+    // ReLU(bias). First launch: the issuer waits on a barrier nothing
+    // completes, with a 2 ms limit; the block must give up, report and free
+    // its tensor memory. Second launch: the normal path on the same buffers.
+    const int n = 1, h = 4, w = 128, cin = 16, cout = 32;
+    bf16 *in = nullptr, *weights = nullptr, *out = nullptr;
+    float* bias = nullptr;
+    int* flag = nullptr;
+    int ok = 0;
+    std::vector<float> hostBias(cout);
+    for (int c = 0; c < cout; c++) hostBias[c] = (float)(c % 7) - 2.5f;
+    std::vector<bf16> hostOut((size_t)n * h * w * cout);
+    int hostFlag = -1;
+    cudaError_t e = cudaMalloc(&in, sizeof(bf16) * n * h * w * cin);
+    if (e == cudaSuccess) e = cudaMalloc(&weights, sizeof(bf16) * 9 * cin * cout);
+    if (e == cudaSuccess) e = cudaMalloc(&out, sizeof(bf16) * hostOut.size());
+    if (e == cudaSuccess) e = cudaMalloc(&bias, sizeof(float) * cout);
+    if (e == cudaSuccess) e = cudaMalloc(&flag, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(in, 0, sizeof(bf16) * n * h * w * cin);
+    if (e == cudaSuccess) e = cudaMemset(weights, 0, sizeof(bf16) * 9 * cin * cout);
+    if (e == cudaSuccess) e = cudaMemset(out, 0, sizeof(bf16) * hostOut.size());
+    if (e == cudaSuccess) e = cudaMemset(flag, 0, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemcpy(bias, hostBias.data(), sizeof(float) * cout, cudaMemcpyHostToDevice);
+    ConvPipeTest probe{2000000ull, 1, 0, 0};
+    if (e == cudaSuccess)
+        e = convPipe(in, nullptr, 0, n, h, w, cin, weights, false, bias, cout, out, nullptr, true, false, flag, 0, &probe);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(&hostFlag, flag, sizeof(int), cudaMemcpyDeviceToHost);
+    const bool reported = e == cudaSuccess && hostFlag == 1;
+    if (e == cudaSuccess) e = cudaMemset(flag, 0, sizeof(int));
+    if (e == cudaSuccess)
+        e = convPipe(in, nullptr, 0, n, h, w, cin, weights, false, bias, cout, out, nullptr, true, false, flag, 0);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(&hostFlag, flag, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(hostOut.data(), out, sizeof(bf16) * hostOut.size(), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && reported && hostFlag == 0) {
+        ok = 1;
+        for (size_t i = 0; i < hostOut.size() && ok; i++)
+            if (__bfloat162float(hostOut[i]) != fmaxf(hostBias[i % cout], 0.0f)) ok = 0;
+    }
+    cudaFree(in); cudaFree(weights); cudaFree(out); cudaFree(bias); cudaFree(flag);
+    return e == cudaSuccess ? ok : 0;
+}
+
+}  // namespace rt

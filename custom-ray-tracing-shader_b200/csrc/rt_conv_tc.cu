@@ -18,6 +18,8 @@
 // and returns.
 #include <algorithm>
 
+#include <atomic>
+
 #include "rt_conv_tc.cuh"
 
 namespace rt {
@@ -425,9 +427,20 @@ int deviceSms() {
 
 }  // namespace
 
+static std::atomic<int> g_convPath{0};
+void setConvPath(int mode) { g_convPath.store(mode); }
+int convPath() { return g_convPath.load(); }
+
 cudaError_t convTc(const bf16* in, const bf16* low, int lowChannels, int n, int h, int w, int cin,
                    const bf16* weights, bool reverseTaps, const float* bias, int cout, bf16* outB, float* outF,
                    bool relu, bool accumulate, int* errorFlag, cudaStream_t stream) {
+    // The warp-specialised TMA form where its shared memory allows (see
+    // rt_conv_pipe.cu); this kernel for the layers with the largest weights.
+    if (g_convPath.load() == 0 && convPipeSupported(cin, cout, low ? lowChannels : 0)) {
+        cudaError_t e = convPipe(in, low, lowChannels, n, h, w, cin, weights, reverseTaps, bias, cout, outB, outF,
+                                 relu, accumulate, errorFlag, stream);
+        if (e != cudaErrorNotSupported) return e;
+    }
     if (n < 1 || h < 1 || w < 1 || cin < 16 || cin % 16 || cout < 16 || cout % 16 || cout > 256 ||
         (!outB && !outF) || !errorFlag || (low && (lowChannels < 16 || lowChannels % 16 || lowChannels >= cin ||
                                                    h % 2 || w % 2)))

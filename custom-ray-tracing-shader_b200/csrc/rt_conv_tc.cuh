@@ -50,4 +50,43 @@ cudaError_t convTc(const __nv_bfloat16* in, const __nv_bfloat16* low, int lowCha
                    const __nv_bfloat16* weights, bool reverseTaps, const float* bias, int cout, __nv_bfloat16* outB,
                    float* outF, bool relu, bool accumulate, int* errorFlag, cudaStream_t stream);
 
+// Which kernel convTc runs: 0 (default) the pipelined form wherever it
+// applies, 1 always the kernel above (process-wide; for comparisons).
+void setConvPath(int mode);
+int convPath();
+
+// Test hooks of the pipelined form (convPipe): zero values keep the defaults.
+struct ConvPipeTest {
+    unsigned long long waitLimitNs;  // bound of every wait (default one second)
+    int probe;                       // 1: the MMA issuer first waits on a barrier nothing completes
+    int ring;                        // ring rows (4..8)
+    int stripRows;                   // rows per strip
+};
+
+// The same convolution as convTc, warp-specialised and fed by TMA (input
+// rows in a ring of shared-memory slots, weights resident): for Cout in {16,
+// 32, 48, 64, 80, 96} when the weights and a ring of 4 rows fit in shared
+// memory. Returns cudaErrorNotSupported (before any launch) for other
+// shapes. Same arguments as convTc, plus optional test hooks.
+bool convPipeSupported(int cin, int cout, int lowChannels);
+uint32_t convPipeSmemBytes(int cin, int cout, int lowChannels, int ring);
+cudaError_t convPipe(const __nv_bfloat16* in, const __nv_bfloat16* low, int lowChannels, int n, int h, int w, int cin,
+                     const __nv_bfloat16* weights, bool reverseTaps, const float* bias, int cout,
+                     __nv_bfloat16* outB, float* outF, bool relu, bool accumulate, int* errorFlag,
+                     cudaStream_t stream, const ConvPipeTest* test = nullptr);
+
+// Weight gradient on tcgen05 (rt_wgrad_tc.cu): dw[tap][ci][co] += sum_p
+// x[p + off(tap)][ci] dy[p][co] over NHWC BF16 x (cin channels) and dy (cout
+// channels), dw FP32 [9][cin][cout]. cin, cout multiples of 16, cout <= 128,
+// cin <= 256. Returns cudaErrorNotSupported (before any launch) otherwise.
+bool wgradTcSupported(int cin, int cout);
+cudaError_t wgradTc(const __nv_bfloat16* x, const __nv_bfloat16* dy, int n, int h, int w, int cin, int cout, float* dw,
+                    int* errorFlag, cudaStream_t stream);
+
+// Runs the pipelined kernel once with a wait that must run out (2 ms limit
+// on a barrier nothing completes), then once normally: 1 when the first
+// launch reported the timeout through its error flag without a CUDA error
+// and the second produced the right output, else 0.
+int convPipeWaitProbe();
+
 }  // namespace rt

@@ -27,6 +27,7 @@
 
 #include "../../include/cuda_ray_tracer.h"
 #include "rt_render.cuh"
+#include "rt_conv_tc.cuh"
 #include "rt_unet.cuh"
 #include "rt_upload.cuh"
 
@@ -878,6 +879,14 @@ int RtxSetEnvironment(void* p, int mode, float r, float g, float b) {
     }
     return 1;
 }
+
+int RtxSetConvPath(int mode) {
+    if (mode != 0 && mode != 1) return 0;
+    rt::setConvPath(mode);
+    return 1;
+}
+
+int RtxDebugConvWaitProbe(void) { return rt::convPipeWaitProbe(); }
 
 int RtxDebugFailAllocation(int n) {
     if (n < 0) return 0;

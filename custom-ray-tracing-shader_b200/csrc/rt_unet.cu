@@ -6,8 +6,10 @@
 //                with K-major weights wT[tap][co][ci]
 //   data grad    convTc on dY with B[ci][co] = w[8 - tap][ci][co]: the forward
 //                weights read with the taps reversed
-//   weight grad  dw[tap][ci][co] = sum_p x[p + off(tap)][ci] dY[p][co] with
-//                16x16x16 warp-level MMA (wgradKernel)
+//   weight grad  dw[tap][ci][co] = sum_p x[p + off(tap)][ci] dY[p][co] on
+//                the tensor cores (wgradTc, rt_wgrad_tc.cu; the 16x16x16
+//                warp-level MMA kernel wgradKernel when the single-role
+//                convolution path is selected)
 #include <mma.h>
 
 #include <algorithm>
@@ -304,7 +306,15 @@ cudaError_t launchWgrad(const bf16* x, const bf16* dy, int N, int H, int W, int 
     wgradKernel<CT><<<grid, 128, 0, s>>>(x, dy, N, H, W, Cin, Cout, per, dw);
     return cudaGetLastError();
 }
-cudaError_t wgrad(const bf16* x, const bf16* dy, int N, int H, int W, int Cin, int Cout, float* dw, cudaStream_t s) {
+// Weight gradient: the tcgen05 kernel (rt_wgrad_tc.cu) unless the
+// single-role convolution path is selected (RtxSetConvPath(1)), then the
+// warp-level MMA kernel above.
+cudaError_t wgrad(const bf16* x, const bf16* dy, int N, int H, int W, int Cin, int Cout, float* dw, int* errorFlag,
+                  cudaStream_t s) {
+    if (convPath() == 0 && wgradTcSupported(Cin, Cout)) {
+        cudaError_t e = wgradTc(x, dy, N, H, W, Cin, Cout, dw, errorFlag, s);
+        if (e != cudaErrorNotSupported) return e;
+    }
     if (Cout % 64 == 0) return launchWgrad<64>(x, dy, N, H, W, Cin, Cout, dw, s);
     if (Cout % 48 == 0) return launchWgrad<48>(x, dy, N, H, W, Cin, Cout, dw, s);
     if (Cout % 32 == 0) return launchWgrad<32>(x, dy, N, H, W, Cin, Cout, dw, s);
@@ -545,7 +555,7 @@ cudaError_t Unet::backward(cudaStream_t s) {
         int per = std::max(1, 256 / L.cout);
         biasGradKernel<<<std::min<long long>(1024, blocksFor((long long)n * H * W, per)), per * L.cout, 0, s>>>(
             A.dPre, (long long)n * H * W, L.cout, grad_ + L.bOffset);
-        cudaError_t err = wgrad(input, A.dPre, n, H, W, L.cin, L.cout, grad_ + L.wOffset, s);
+        cudaError_t err = wgrad(input, A.dPre, n, H, W, L.cin, L.cout, grad_ + L.wOffset, convError_, s);
         if (err != cudaSuccess) return err;
         if (dIn) return convTc(A.dPre, nullptr, 0, n, H, W, L.cout, wbf_ + L.wOffset, true, nullptr, L.cin, nullptr, dIn, false, accumulate, convError_, s);
         return cudaSuccess;

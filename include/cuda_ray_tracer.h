@@ -223,6 +223,18 @@ int RtxSetIntegrator(void* session, int mode);
 #define RTX_TUNE_STACK_LIMIT 7
 int RtxSetTuning(void* session, int key, int value);
 
+/* Which tensor-core convolution kernel the learned denoiser runs, no
+ * counterpart in the reference: 0 (default) the warp-specialised TMA-fed
+ * kernel wherever its shared memory allows, 1 the single-role kernel for
+ * every layer. Process-wide; results agree to BF16 rounding. */
+int RtxSetConvPath(int mode);
+/* Failure path of the warp-specialised convolution, no counterpart in the
+ * reference: one launch whose wait on a barrier that nothing completes runs
+ * out (2 ms limit) must report it through its error flag and free its
+ * tensor memory without a CUDA error, and a normal launch after it must give
+ * the right output. Returns 1 when both hold. Runs on the current device. */
+int RtxDebugConvWaitProbe(void);
+
 /* Failure injection on the host, no counterpart in the reference: the n-th
  * next device allocation made by the renderer (sessions, scene upload, BVH
  * build, wave buffers, batches) fails with cudaErrorMemoryAllocation without

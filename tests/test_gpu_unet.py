@@ -272,3 +272,39 @@ def test_trained_network_gains_over_the_filter(lib):
         assert learned > guided + 2.0 and learned > raw + 6.0, gains
     finally:
         net.close()
+
+
+def test_conv_kernels_agree(lib, net):
+    """The warp-specialised, TMA-fed convolution (the default wherever its
+    shared memory allows) and the single-role kernel for every layer
+    (RtxSetConvPath(1)) give the same inference and training gradients to
+    BF16 rounding: at image sizes with partial 128-pixel column tiles, the
+    concatenated decoder inputs read in place, and tiny deep levels."""
+    rng = np.random.default_rng(12)
+    try:
+        for h, w in ((64, 256), (72, 136), (37, 23)):
+            aovs, _ = synthetic(rng, 1, h, w)
+            assert lib.RtxSetConvPath(1)
+            old = net.infer(aovs[0])
+            assert lib.RtxSetConvPath(0)
+            new = net.infer(aovs[0])
+            diff = np.abs(np.log1p(new) - np.log1p(old))
+            assert diff.max() < 5e-2 and diff.mean() < 2e-3, (h, w, diff.max(), diff.mean())
+        aovs, target = synthetic(rng, 2, 32, 160)
+        lib.RtxSetConvPath(1)
+        loss_old, grad_old = net.loss_grad(aovs, target)
+        lib.RtxSetConvPath(0)
+        loss_new, grad_new = net.loss_grad(aovs, target)
+        assert abs(loss_new - loss_old) <= 2e-3 * loss_old
+        g, e = grad_new.astype(np.float64), grad_old.astype(np.float64)
+        assert np.linalg.norm(g - e) <= 2e-2 * np.linalg.norm(e)
+    finally:
+        lib.RtxSetConvPath(0)
+
+
+def test_conv_wait_limit_reports_and_recovers(lib):
+    """A pipelined convolution whose tensor-core issuer waits on a barrier
+    that nothing completes gives up after its (2 ms) limit, reports through
+    the error flag, frees its tensor memory and loads, and the next launch
+    on the same device computes the right output."""
+    assert lib.RtxDebugConvWaitProbe() == 1
