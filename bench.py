@@ -680,6 +680,38 @@ def train_step_run(lib, args, batch=32, size=128, crops=64, warmup=5):
             'timing': 'host wall clock around RtxUnetTrain (synchronises at its end), after warm-up steps'}
 
 
+def build_report(tris, bvh, init_wall_ms, peak, peak_kind):
+    """GPU BVH build at RtInitialize. The traced tree (over triangle pieces
+    when some triangle is split, else the reference's tree) is what
+    RtInitialize builds; the reference's own tree is built on the first
+    RtBvhInfo / RtxExportBvh / RtxBvhStatsGet when it is not the traced one.
+    Roofline: algorithmic bytes per build triangle B_tri = (36 B of vertices
+    + 8 B of index read/write) per binned-SAH level, ceil(log2(N / 4))
+    levels, + 32 B per node of the reference's tree, against HBM bandwidth."""
+    import math
+    n = len(tris)
+    pieces = bvh['pieces']
+    reference_ms = bvh['buildMs'] + bvh['collapseMs']
+    traced_ms = bvh['pieceBuildMs'] if pieces > 1 else reference_ms
+    b_tri = 44.0 * math.ceil(math.log2(max(n / 4.0, 2.0))) + 32.0 * bvh['binaryNodes'] / n
+    achieved = n * b_tri / (traced_ms * 1e-3) / 1e9
+    return {
+        'traced_tree': {'ms': traced_ms, 'mtris_per_s': n / traced_ms / 1e3, 'pieces_per_triangle': pieces,
+                        'wide_nodes': bvh['wideNodes'], 'wide_depth': bvh['wideDepth'],
+                        'built': 'at RtInitialize'},
+        'reference_tree': {'ms': reference_ms, 'binned_sah_ms': bvh['buildMs'], 'collapse_ms': bvh['collapseMs'],
+                           'mtris_per_s': n / reference_ms / 1e3, 'binary_nodes': bvh['binaryNodes'],
+                           'binary_depth': bvh['binaryDepth'], 'sah_cost': bvh['sahCost'],
+                           'built': ('on first RtBvhInfo/RtxExportBvh/RtxBvhStatsGet' if pieces > 1
+                                     else 'at RtInitialize (it is the traced tree)')},
+        'mtris_per_s': n / traced_ms / 1e3,
+        'roofline': {'bound': 'hbm', 'bytes_per_triangle': b_tri, 'achieved': achieved, 'peak': peak,
+                     'unit': 'GB/s', 'frac': achieved / peak,
+                     'peak_source': f'{peak_kind} hbm_gbs', 'kernel': 'traced-tree build (all its kernels)'},
+        'initialize_wall_ms': init_wall_ms, 'upload_ms': bvh['uploadMs'], 'distinct_colours': bvh['distinctColours'],
+    }
+
+
 def kernel_rates(integrator, per_kind, primary_ms, extend_ms, shadow_ms, lanes):
     """Mrays/s of each traversal kind over its own kernels' device time:
     primary (closest-hit at bounce 0), secondary (closest-hit at later
@@ -909,15 +941,7 @@ def run_ours(args, rank, local_rank, world):
             'traversal_mrays_per_s': dict(kernel_rates(best, per_kind, primary_ms, extend_ms, shadow_ms, lanes) or {},
                                           isolated=isolated[2] if isolated else None),
             'wall_ms_per_step': wall * 1e3 / args.steps,
-            'build': {'ms': bvh['buildMs'] + bvh['collapseMs'], 'binned_sah_ms': bvh['buildMs'],
-                      'collapse_ms': bvh['collapseMs'],
-                      'mtris_per_s': len(tris) / (bvh['buildMs'] + bvh['collapseMs']) / 1e3,
-                      'binary_nodes': bvh['binaryNodes'], 'binary_depth': bvh['binaryDepth'],
-                      'sah_cost': bvh['sahCost'],
-                      'traversal_tree': {'pieces_per_triangle': bvh['pieces'], 'build_ms': bvh['pieceBuildMs'],
-                                         'wide_nodes': bvh['wideNodes'], 'wide_depth': bvh['wideDepth']},
-                      'initialize_wall_ms': init_wall_ms, 'upload_ms': bvh['uploadMs'],
-                      'distinct_colours': bvh['distinctColours']},
+            'build': build_report(tris, bvh, init_wall_ms, peak, peak_kind),
             'reference_cuda': ref_cuda,
             'time_to_35db': quality_run(lib, args) if (args.quality and world == 1) else None,
             'batch': batch_run(lib, args) if (args.batch and world == 1) else None,

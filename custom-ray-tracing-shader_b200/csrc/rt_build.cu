@@ -42,6 +42,8 @@ constexpr int kBinPer = 8;         // positions per thread in the binning pass
 // Tasks of at most kSmallTask primitives are binned by one warp each
 // (binSmallKernel); larger ones by position blocks (binKernel).
 constexpr int kSmallTask = 2048;
+// Levels (binned SAH, or wide collapse) queued per host read of the counts.
+constexpr int kLevelBatch = 8;
 
 struct Task {
     int node, first, count, depth;
@@ -218,12 +220,18 @@ __global__ void iotaKernel(int* a, int n, int value0, int* b, int bValue) {
     if (i < n) { a[i] = i + value0; if (b) b[i] = bValue; }
 }
 
-__global__ void clearBinsKernel(BinAcc* bins, int count, const Task* tasks) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= count || tasks[i / (3 * kBins)].count <= kSmallTask) return;
-    BinAcc& b = bins[i];
-    b.count = 0;
-    for (int a = 0; a < 3; a++) { b.lo[a] = FLT_MAX; b.hi[a] = -FLT_MAX; b.clo[a] = FLT_MAX; b.chi[a] = -FLT_MAX; }
+// Level counts (taskCount[0] open tasks, taskCount[1] of them larger than
+// kSmallTask) live on the device, so levels are queued without the host
+// reading them: per-task kernels loop over the device count.
+__global__ void clearBinsKernel(BinAcc* bins, const int* taskCount, const Task* tasks) {
+    if (!taskCount[1]) return;
+    const int count = taskCount[0] * 3 * kBins;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        if (tasks[i / (3 * kBins)].count <= kSmallTask) continue;
+        BinAcc& b = bins[i];
+        b.count = 0;
+        for (int a = 0; a < 3; a++) { b.lo[a] = FLT_MAX; b.hi[a] = -FLT_MAX; b.clo[a] = FLT_MAX; b.chi[a] = -FLT_MAX; }
+    }
 }
 
 __device__ __forceinline__ void accumulateBin(BinAcc* dst, float4 lo, float4 hi, float4 c) {
@@ -238,9 +246,10 @@ __device__ __forceinline__ void accumulateBin(BinAcc* dst, float4 lo, float4 hi,
 // of a block's chunk is aggregated in shared memory; others go to global bins.
 __global__ void __launch_bounds__(kBinBlock) binKernel(const int* order, const int* posTask, const float4* cent,
                                                        const float4* plo, const float4* phi, const Task* tasks,
-                                                       int nPos, BinAcc* bins) {
+                                                       int nPos, BinAcc* bins, const int* taskCount) {
     __shared__ BinAcc sb[3 * kBins];
     __shared__ int sTask;
+    if (!taskCount[1]) return;  // no task above kSmallTask at this level
     int base = blockIdx.x * kBinBlock * kBinPer;
     if (threadIdx.x == 0) sTask = base < nPos ? posTask[base] : -1;
     if (threadIdx.x < 3 * kBins) {
@@ -283,20 +292,9 @@ __global__ void __launch_bounds__(kBinBlock) binKernel(const int* order, const i
     }
 }
 
-// One warp per small task: warp-private bins in shared memory (atomics only
-// within the warp), written out with plain stores, so these bins need no
-// clearing and no global atomics. Bins hold a count and minima/maxima, so the
-// order of accumulation does not change them.
-__global__ void __launch_bounds__(256) binSmallKernel(const int* order, const float4* cent, const float4* plo,
-                                                      const float4* phi, const Task* tasks, int nTasks,
-                                                      BinAcc* bins) {
-    __shared__ BinAcc sb[8][3 * kBins];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int t = blockIdx.x * 8 + warp;
-    if (t >= nTasks) return;
-    const Task T = tasks[t];
+__device__ void binSmallTask(const int* order, const float4* cent, const float4* plo, const float4* phi,
+                             const Task T, int t, BinAcc* bins, BinAcc* my, int lane) {
     if (T.count > kSmallTask) return;
-    BinAcc* my = sb[warp];
     for (int i = lane; i < 3 * kBins; i += 32) {
         BinAcc& b = my[i];
         b.count = 0;
@@ -319,15 +317,39 @@ __global__ void __launch_bounds__(256) binSmallKernel(const int* order, const fl
     }
     __syncwarp();
     for (int i = lane; i < 3 * kBins; i += 32) bins[(size_t)t * 3 * kBins + i] = my[i];
+    __syncwarp();
+}
+
+// One warp per small task: warp-private bins in shared memory (atomics only
+// within the warp), written out with plain stores, so these bins need no
+// clearing and no global atomics. Bins hold a count and minima/maxima, so the
+// order of accumulation does not change them.
+__global__ void __launch_bounds__(256) binSmallKernel(const int* order, const float4* cent, const float4* plo,
+                                                      const float4* phi, const Task* tasks, const int* taskCount,
+                                                      BinAcc* bins) {
+    __shared__ BinAcc sb[8][3 * kBins];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nTasks = taskCount[0];
+    for (int t = blockIdx.x * 8 + warp; t < nTasks; t += gridDim.x * 8)
+        binSmallTask(order, cent, plo, phi, tasks[t], t, bins, sb[warp], lane);
 }
 
 // One thread per open task: the reference's SAH sweep, then node records.
-__global__ void splitKernel(const Task* tasks, int nTasks, const BinAcc* bins, Split* splits, BinNode* nodes,
-                            int* counters /*0 nodes,1 next tasks,2 max depth,3 error*/, Task* nextTasks,
+// taskCount: this level's counts; nextCount: the next level's (open tasks,
+// tasks above kSmallTask); levelStart: receives the node count once this
+// level's nodes are allocated (the first node of the next depth).
+__device__ void splitTask(const Task T, int t, const BinAcc* bins, Split* splits, BinNode* nodes, int* counters,
+                          int* nextCount, Task* nextTasks, int nodeCapacity, int taskCapacity, int leafSize);
+__global__ void splitKernel(const Task* tasks, const int* taskCount, const BinAcc* bins, Split* splits, BinNode* nodes,
+                            int* counters /*0 nodes,2 max depth,3 error*/, int* nextCount, Task* nextTasks,
                             int nodeCapacity, int taskCapacity, int leafSize) {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= nTasks) return;
-    const Task T = tasks[t];
+    const int nTasks = taskCount[0];
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nTasks; t += gridDim.x * blockDim.x)
+        splitTask(tasks[t], t, bins, splits, nodes, counters, nextCount, nextTasks, nodeCapacity, taskCapacity,
+                  leafSize);
+}
+__device__ void splitTask(const Task T, int t, const BinAcc* bins, Split* splits, BinNode* nodes, int* counters,
+                          int* nextCount, Task* nextTasks, int nodeCapacity, int taskCapacity, int leafSize) {
     atomicMax(&counters[2], T.depth);
     int bestAxis = -1, bestBin = -1;
     float nodeArea = halfArea(T.lo, T.hi);
@@ -393,9 +415,9 @@ __global__ void splitKernel(const Task* tasks, int nTasks, const BinAcc* bins, S
         if (c.count <= leafSize || c.depth == kBinaryMaxDepth) {
             nodes[c.node] = BinNode{v3(c.lo[0], c.lo[1], c.lo[2]), c.first, v3(c.hi[0], c.hi[1], c.hi[2]), c.count};
         } else {
-            int k = atomicAdd(&counters[1], 1);
+            int k = atomicAdd(&nextCount[0], 1);
             if (k >= taskCapacity) { atomicExch(&counters[3], 2); continue; }
-            if (c.count > kSmallTask) atomicAdd(&counters[5], 1);
+            if (c.count > kSmallTask) atomicAdd(&nextCount[1], 1);
             nextTasks[k] = c;
             S.childTask[side] = k;
         }
@@ -510,6 +532,9 @@ __global__ void scatterKernel(const int* order, const int* posTask, const Task* 
     posTaskNext[dst] = S.childTask[left ? 0 : 1];
 }
 
+// Node count after a level's splits: the first node of the next depth.
+__global__ void recordLevelKernel(const int* counters, int* levelStart) { *levelStart = counters[0]; }
+
 // ---- renumbering into the reference's depth-first numbering ----
 __global__ void subtreeInteriorKernel(const BinNode* nodes, int begin, int end, int* interior) {
     int i = begin + blockIdx.x * blockDim.x + threadIdx.x;
@@ -541,14 +566,15 @@ __global__ void renumberKernel(const BinNode* nodes, int count, const int* newIn
 }
 
 // ---- collapse into wide nodes (logic in rt_collapse.cuh) ----
+// jobCount: this wide level's jobs; nextCount receives the next level's.
 __global__ void collapseKernel(const BinNode* bn, const int* order, const float4* plo, const float4* phi,
-                               const SceneTri* tris, const Job* jobs, int nJobs, Job* nextJobs, WideNode* wide,
-                               float4* packed, int* counters, int wideCapacity, int jobCapacity, int triCapacity,
-                               int group, int width, const int* primTri) {
-    int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= nJobs) return;
-    collapseJob(jobs[j], bn, order, plo, phi, tris, nextJobs, wide, packed, counters, wideCapacity, jobCapacity,
-                triCapacity, group, width, primTri);
+                               const SceneTri* tris, const Job* jobs, const int* jobCount, Job* nextJobs,
+                               int* nextCount, WideNode* wide, float4* packed, int* counters, int wideCapacity,
+                               int jobCapacity, int triCapacity, int group, int width, const int* primTri) {
+    const int nJobs = *jobCount;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nJobs; j += gridDim.x * blockDim.x)
+        collapseJob(jobs[j], bn, order, plo, phi, tris, nextJobs, wide, packed, counters, wideCapacity, jobCapacity,
+                    triCapacity, group, width, primTri, nextCount);
 }
 
 inline int blocksFor(long long n, int block) { return (int)((n + block - 1) / block); }
@@ -642,6 +668,8 @@ cudaError_t buildBvh(const SceneTri* tris, int triCount, cudaStream_t stream, Bu
     BinNode* rawNodes = nullptr; int* interior = nullptr; int* rank = nullptr; int* newIndex = nullptr;
     Job* jobs = nullptr; Job* jobsB = nullptr;
     int* hostCounters = nullptr;
+    int* levelCounts = nullptr; int* levelStartDev = nullptr; int* jobCounts = nullptr;
+    int* hostLevels = nullptr; int* hostStarts = nullptr; int* hostJobs = nullptr;
     std::vector<int> levelStart;
     int nScanBlocks = blocksFor(n, kScanBlock);
 
@@ -653,6 +681,14 @@ cudaError_t buildBvh(const SceneTri* tris, int triCount, cudaStream_t stream, Bu
     RT_TRY(alloc(flags, n)); RT_TRY(alloc(prefix, n)); RT_TRY(alloc(blockSums, nScanBlocks));
     RT_TRY(alloc(counters, 8)); RT_TRY(alloc(rawNodes, nodeCapacity));
     RT_TRY(cudaMallocHost(reinterpret_cast<void**>(&hostCounters), 8 * sizeof(int)));
+    {
+        const int levelSlots = kBinaryMaxDepth + 2 + kLevelBatch, jobSlots = kStackCapacity + 2 + kLevelBatch;
+        RT_TRY(alloc(levelCounts, 2 * levelSlots)); RT_TRY(alloc(levelStartDev, levelSlots + 2));
+        RT_TRY(alloc(jobCounts, jobSlots));
+        RT_TRY(cudaMallocHost(reinterpret_cast<void**>(&hostLevels), sizeof(int) * 2 * levelSlots));
+        RT_TRY(cudaMallocHost(reinterpret_cast<void**>(&hostStarts), sizeof(int) * (levelSlots + 2)));
+        RT_TRY(cudaMallocHost(reinterpret_cast<void**>(&hostJobs), sizeof(int) * jobSlots));
+    }
     // Renumbering and collapse buffers at their upper bounds (node count <=
     // nodeCapacity, wide nodes and jobs <= 2n + 8), so no allocation falls
     // inside the timed spans.
@@ -677,37 +713,55 @@ cudaError_t buildBvh(const SceneTri* tris, int triCount, cudaStream_t stream, Bu
                                                                     cent, tasks);
         iotaKernel<<<blocksFor(n, 256), 256, 0, stream>>>(out.order, n, 0, posTask, 0);
         RT_TRY(cudaGetLastError());
-        int nTasks = 1;
-        levelStart.push_back(0);  // depth 0 holds node 0
-        levelStart.push_back(1);
-        int bigTasks = n > kSmallTask ? 1 : 0;
-        while (nTasks > 0) {
-            if (bigTasks) {
-                clearBinsKernel<<<blocksFor((long long)nTasks * 3 * kBins, 256), 256, 0, stream>>>(bins, nTasks * 3 * kBins, tasks);
+        // Binned SAH, level by level without the host in the loop: each
+        // level's counts (open tasks, tasks above kSmallTask) are written
+        // by the previous level's split kernel into levelCounts, and the
+        // per-task kernels loop over them, so the host queues a batch of
+        // levels and reads the counts once per batch. A level with no task
+        // only copies the order through. Depth is at most kBinaryMaxDepth,
+        // so at most kBinaryMaxDepth + 1 levels hold tasks.
+        const int levelSlots = kBinaryMaxDepth + 2 + kLevelBatch;
+        RT_TRY(cudaMemsetAsync(levelCounts, 0, sizeof(int) * 2 * levelSlots, stream));
+        RT_TRY(cudaMemsetAsync(levelStartDev, 0, sizeof(int) * (levelSlots + 2), stream));
+        {
+            int rootCounts[2] = {1, n > kSmallTask ? 1 : 0};
+            int starts[2] = {0, 1};  // depth 0 holds node 0
+            RT_TRY(cudaMemcpyAsync(levelCounts, rootCounts, sizeof(rootCounts), cudaMemcpyHostToDevice, stream));
+            RT_TRY(cudaMemcpyAsync(levelStartDev, starts, sizeof(starts), cudaMemcpyHostToDevice, stream));
+        }
+        const int perTaskBlocks = std::max(1, std::min(blocksFor(taskCapacity, 8), 1184));
+        const int splitBlocks = std::max(1, std::min(blocksFor(taskCapacity, 128), 592));
+        const int clearBlocks = std::max(1, std::min(blocksFor((long long)taskCapacity * 3 * kBins, 256), 1184));
+        int level = 0;
+        for (;;) {
+            for (int b = 0; b < kLevelBatch && level < levelSlots - 1; b++, level++) {
+                const int* tc = levelCounts + 2 * level;
+                int* nc = levelCounts + 2 * (level + 1);
+                clearBinsKernel<<<clearBlocks, 256, 0, stream>>>(bins, tc, tasks);
                 binKernel<<<blocksFor(n, kBinBlock * kBinPer), kBinBlock, 0, stream>>>(out.order, posTask, cent, out.primLo,
-                                                                                        out.primHi, tasks, n, bins);
+                                                                                        out.primHi, tasks, n, bins, tc);
+                binSmallKernel<<<perTaskBlocks, 256, 0, stream>>>(out.order, cent, out.primLo, out.primHi, tasks, tc, bins);
+                splitKernel<<<splitBlocks, 128, 0, stream>>>(tasks, tc, bins, splits, rawNodes, counters, nc, tasksB,
+                                                             nodeCapacity, taskCapacity, leafSize);
+                recordLevelKernel<<<1, 1, 0, stream>>>(counters, levelStartDev + level + 2);
+                flagKernel<<<blocksFor(n, 256), 256, 0, stream>>>(out.order, posTask, cent, tasks, splits, n, flags);
+                scanBlocksKernel<<<nScanBlocks, 256, 0, stream>>>(flags, prefix, n, blockSums);
+                scanTotalsKernel<<<1, 1024, 0, stream>>>(blockSums, nScanBlocks);
+                scatterKernel<<<blocksFor(n, 256), 256, 0, stream>>>(out.order, posTask, tasks, splits, flags, prefix,
+                                                                     blockSums, n, orderB, posTaskB, counters + 3);
+                std::swap(out.order, orderB); std::swap(posTask, posTaskB); std::swap(tasks, tasksB);
             }
-            binSmallKernel<<<blocksFor(nTasks, 8), 256, 0, stream>>>(out.order, cent, out.primLo, out.primHi, tasks, nTasks,
-                                                                     bins);
-            RT_TRY(cudaMemsetAsync(counters + 1, 0, sizeof(int), stream));
-            RT_TRY(cudaMemsetAsync(counters + 5, 0, sizeof(int), stream));
-            splitKernel<<<blocksFor(nTasks, 128), 128, 0, stream>>>(tasks, nTasks, bins, splits, rawNodes, counters,
-                                                                    tasksB, nodeCapacity, taskCapacity, leafSize);
-            flagKernel<<<blocksFor(n, 256), 256, 0, stream>>>(out.order, posTask, cent, tasks, splits, n, flags);
-            scanBlocksKernel<<<nScanBlocks, 256, 0, stream>>>(flags, prefix, n, blockSums);
-            scanTotalsKernel<<<1, 1024, 0, stream>>>(blockSums, nScanBlocks);
-            scatterKernel<<<blocksFor(n, 256), 256, 0, stream>>>(out.order, posTask, tasks, splits, flags, prefix,
-                                                                 blockSums, n, orderB, posTaskB, counters + 3);
             RT_TRY(cudaGetLastError());
             RT_TRY(cudaMemcpyAsync(hostCounters, counters, 8 * sizeof(int), cudaMemcpyDeviceToHost, stream));
+            RT_TRY(cudaMemcpyAsync(hostLevels, levelCounts, sizeof(int) * 2 * levelSlots, cudaMemcpyDeviceToHost, stream));
             RT_TRY(cudaStreamSynchronize(stream));
             if (hostCounters[3]) { *failure = "BVH build ran out of node or task capacity"; err = cudaErrorMemoryAllocation; goto done; }
-            std::swap(out.order, orderB); std::swap(posTask, posTaskB); std::swap(tasks, tasksB);
-            levelStart.push_back(hostCounters[0]);
-            nTasks = hostCounters[1];
-            bigTasks = hostCounters[5];
-            if ((int)levelStart.size() > kBinaryMaxDepth + 3) { *failure = "BVH build exceeded the depth limit"; err = cudaErrorUnknown; goto done; }
+            if (hostLevels[2 * level] == 0) break;  // the next level has no task
+            if (level >= levelSlots - 1) { *failure = "BVH build exceeded the depth limit"; err = cudaErrorUnknown; goto done; }
         }
+        RT_TRY(cudaMemcpyAsync(hostStarts, levelStartDev, sizeof(int) * (level + 2), cudaMemcpyDeviceToHost, stream));
+        RT_TRY(cudaStreamSynchronize(stream));
+        levelStart.assign(hostStarts, hostStarts + level + 2);
         int nodeCount = hostCounters[0];
         result.binaryNodes = nodeCount;
         result.binaryDepth = hostCounters[2];
@@ -730,34 +784,40 @@ cudaError_t buildBvh(const SceneTri* tris, int triCount, cudaStream_t stream, Bu
         renumberKernel<<<blocksFor(nodeCount, 256), 256, 0, stream>>>(rawNodes, nodeCount, newIndex, out.binNodes,
                                                                       counters + 3);
         RT_TRY(cudaGetLastError());
-        RT_TRY(cudaMemcpyAsync(hostCounters, counters, 8 * sizeof(int), cudaMemcpyDeviceToHost, stream));
-        RT_TRY(cudaStreamSynchronize(stream));
-        if (hostCounters[3]) { *failure = "BVH renumbering found an inconsistent tree"; err = cudaErrorUnknown; goto done; }
         RT_TRY(cudaEventRecord(e1, stream));
 
-        // Collapse.
+        // Collapse, one wide level per launch; job counts per level on the
+        // device (jobCounts), read once per batch of levels.
         const int jobCapacity = wideCapacity;
         Job rootJob{0, 0, 0, 0, 0};
         RT_TRY(cudaMemcpyAsync(jobs, &rootJob, sizeof(Job), cudaMemcpyHostToDevice, stream));
         int cinit[8] = {1, 0, 0, 0, 0, 0, 0, 0};
         RT_TRY(cudaMemcpyAsync(counters, cinit, sizeof(cinit), cudaMemcpyHostToDevice, stream));
-        int nJobs = 1, wideDepth = 0;
-        while (nJobs > 0) {
-            wideDepth++;
-            if (wideDepth > kStackCapacity) { *failure = "wide BVH deeper than the traversal stack"; err = cudaErrorUnknown; goto done; }
-            RT_TRY(cudaMemsetAsync(counters + 2, 0, sizeof(int), stream));
-            collapseKernel<<<blocksFor(nJobs, 64), 64, 0, stream>>>(out.binNodes, out.order, out.primLo, out.primHi, tris,
-                                                                    jobs, nJobs, jobsB,
-                                                                    reinterpret_cast<WideNode*>(out.wideNodes),
-                                                                    out.packedTris, counters, wideCapacity, jobCapacity, n,
-                                                                    leafGroup, width, primTri);
+        const int jobSlots = kStackCapacity + 2 + kLevelBatch;
+        RT_TRY(cudaMemsetAsync(jobCounts, 0, sizeof(int) * jobSlots, stream));
+        RT_TRY(cudaMemcpyAsync(jobCounts, cinit, sizeof(int), cudaMemcpyHostToDevice, stream));  // one root job
+        const int collapseBlocks = std::max(1, std::min(blocksFor(jobCapacity, 64), 2368));
+        int wideLevel = 0, wideDepth = 0;
+        for (;;) {
+            for (int b = 0; b < kLevelBatch && wideLevel < jobSlots - 1; b++, wideLevel++) {
+                collapseKernel<<<collapseBlocks, 64, 0, stream>>>(out.binNodes, out.order, out.primLo, out.primHi, tris,
+                                                                  jobs, jobCounts + wideLevel, jobsB,
+                                                                  jobCounts + wideLevel + 1,
+                                                                  reinterpret_cast<WideNode*>(out.wideNodes),
+                                                                  out.packedTris, counters, wideCapacity, jobCapacity, n,
+                                                                  leafGroup, width, primTri);
+                std::swap(jobs, jobsB);
+            }
             RT_TRY(cudaGetLastError());
             RT_TRY(cudaMemcpyAsync(hostCounters, counters, 8 * sizeof(int), cudaMemcpyDeviceToHost, stream));
+            RT_TRY(cudaMemcpyAsync(hostJobs, jobCounts, sizeof(int) * jobSlots, cudaMemcpyDeviceToHost, stream));
             RT_TRY(cudaStreamSynchronize(stream));
             if (hostCounters[3]) { *failure = "wide BVH collapse ran out of capacity"; err = cudaErrorMemoryAllocation; goto done; }
-            std::swap(jobs, jobsB);
-            nJobs = hostCounters[2];
+            if (hostJobs[wideLevel] == 0) break;
+            if (wideLevel >= jobSlots - 1) break;
         }
+        while (wideDepth < jobSlots && hostJobs[wideDepth] > 0) wideDepth++;
+        if (wideDepth > kStackCapacity) { *failure = "wide BVH deeper than the traversal stack"; err = cudaErrorUnknown; goto done; }
         RT_TRY(cudaEventRecord(e2, stream));
         RT_TRY(cudaEventSynchronize(e2));
         // Every primitive is packed once, except pieces of a triangle that
@@ -781,6 +841,10 @@ done:
     cudaFree(rawNodes); cudaFree(interior); cudaFree(rank); cudaFree(newIndex); cudaFree(jobs); cudaFree(jobsB);
     cudaFree(primTri);
     if (hostCounters) cudaFreeHost(hostCounters);
+    cudaFree(levelCounts); cudaFree(levelStartDev); cudaFree(jobCounts);
+    if (hostLevels) cudaFreeHost(hostLevels);
+    if (hostStarts) cudaFreeHost(hostStarts);
+    if (hostJobs) cudaFreeHost(hostJobs);
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     if (e2) cudaEventDestroy(e2);

@@ -56,11 +56,12 @@ RT_HD int slotsOf(const BinNode& n, int group, int width) {
 // portableAdd), so the collapse can be checked on the CPU. width (4 or 8):
 // most children per node; the node format keeps eight slots either way.
 // primTri: the triangle of each primitive when primitives are triangle pieces
-// (null: primitive p is triangle p).
+// (null: primitive p is triangle p). nextCount, when set, counts the
+// next-level jobs in place of counters[2].
 RT_HD void collapseJob(Job J, const BinNode* bn, const int* order, const float4* plo, const float4* phi,
                        const SceneTri* tris, Job* nextJobs, WideNode* wide, float4* packed, int* counters,
                        int wideCapacity, int jobCapacity, int triCapacity, int group, int width = 8,
-                       const int* primTri = nullptr) {
+                       const int* primTri = nullptr, int* nextCount = nullptr) {
     if (J.kind == 0 && bn[J.node].count > 0) { J.kind = 1; J.first = bn[J.node].first; J.count = bn[J.node].count; }
     Kid kids[8];
     int nk = 0;
@@ -232,7 +233,7 @@ RT_HD void collapseJob(Job J, const BinNode* bn, const int* order, const float4*
         } else {
             W.meta[s] = (unsigned char)(0x20u | (24u + (unsigned)s));
             W.imask |= (unsigned char)(1u << s);
-            int q = portableAdd(&counters[2], 1);
+            int q = portableAdd(nextCount ? nextCount : &counters[2], 1);
             if (q >= jobCapacity) { portableSet(&counters[3], 4); continue; }
             nextJobs[q] = Job{K.kind == 0 ? 0 : 1, K.node, K.first, K.count, childBase + interiorSeen};
             interiorSeen++;

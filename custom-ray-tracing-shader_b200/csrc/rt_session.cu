@@ -116,6 +116,7 @@ struct Session {
     BuildResult build;
     BuiltBvh pieceBvh;     // traversal tree over triangle pieces (when pieces > 1)
     BuildResult pieceBuild;
+    bool referenceTreeReady = false;  // bvh/build hold the reference's tree
     int pieces = kDefaultPieces;
     int traversalLeaf = kDefaultTraversalLeaf;
     WavefrontBuffers wave;
@@ -158,6 +159,19 @@ bool useDevice(Session* s) {
 
 // The tree that traversal uses: over triangle pieces when built, else the
 // collapse of the reference's tree.
+// The reference's tree, built on first use when the session traces a tree
+// over triangle pieces (RtInitialize builds only the traced tree).
+bool ensureReferenceTree(Session* s) {
+    if (s->referenceTreeReady) return true;
+    if (!s->ready) return false;
+    if (!useDevice(s)) return false;
+    const char* why = nullptr;
+    cudaError_t e = buildBvh(s->dTris, s->triCount, s->stream, s->bvh, s->build, &why);
+    if (e != cudaSuccess) return fail(s, e, why);
+    s->referenceTreeReady = true;
+    return true;
+}
+
 const uint4* travWide(const Session* s) { return s->pieceBvh.wideNodes ? s->pieceBvh.wideNodes : s->bvh.wideNodes; }
 const float4* travPacked(const Session* s) { return s->pieceBvh.wideNodes ? s->pieceBvh.packedTris : s->bvh.packedTris; }
 const BuildResult& travBuild(const Session* s) { return s->pieceBvh.wideNodes ? s->pieceBuild : s->build; }
@@ -206,6 +220,7 @@ void releaseScene(Session* s) {
     s->lightArea = 0;
     s->lastBackend = -1;
     s->build = BuildResult{};
+    s->referenceTreeReady = false;
     s->sahCost = -1.0;
     s->stats = RtxRenderStats{};
     s->denoisedValid = false;
@@ -420,6 +435,7 @@ float RtEmbreeBuildMilliseconds(void*) { return 0.0f; }
 int RtCpuThreadCount(void* p) { return p ? static_cast<Session*>(p)->cpuThreads : 0; }
 void RtBvhInfo(void* p, int* nodes, int* depth, float* buildMs) {
     Session* s = static_cast<Session*>(p);
+    if (s && s->ready && !ensureReferenceTree(s)) s = nullptr;  // zeros, and RtLastError says why
     if (nodes) *nodes = s ? s->build.binaryNodes : 0;
     if (depth) *depth = s ? s->build.binaryDepth : 0;
     if (buildMs) *buildMs = s ? s->build.buildMs : 0.0f;
@@ -484,12 +500,16 @@ int RtInitialize(void* p, const Triangle* triangles, int count, int width, int h
     RT_CHECK(rt::deviceAlloc(&s->dCounters, 4 * sizeof(unsigned long long)));
     RT_CHECK(rt::deviceAlloc(&s->dError, 2 * sizeof(int)));
     const char* why = nullptr;
-    e = buildBvh(s->dTris, count, s->stream, s->bvh, s->build, &why);
+    // The tree that is traced is built here: over triangle pieces when some
+    // triangle is split, else the reference's own tree. The reference's tree
+    // (RtBvhInfo, RtxExportBvh, RtxBvhStatsGet) is then built on its first
+    // use (ensureReferenceTree), so RtInitialize pays for the traced tree
+    // only.
     int pieceTotal = count;
-    if (e == cudaSuccess && s->pieces > 1) e = pieceMap(s->dTris, count, s->pieces, s->stream, nullptr, &pieceTotal);
+    s->referenceTreeReady = false;
+    e = cudaSuccess;
+    if (s->pieces > 1) e = pieceMap(s->dTris, count, s->pieces, s->stream, nullptr, &pieceTotal);
     if (e == cudaSuccess && pieceTotal > count) {
-        // Traversal tree over triangle pieces; the reference tree above stays
-        // for RtBvhInfo and RtxExportBvh.
         e = buildBvh(s->dTris, count, s->stream, s->pieceBvh, s->pieceBuild, &why, 3, 8, s->pieces, s->traversalLeaf);
         if (e == cudaSuccess) {
             void* unused[] = {s->pieceBvh.binNodes, s->pieceBvh.order, s->pieceBvh.primLo, s->pieceBvh.primHi};
@@ -497,6 +517,9 @@ int RtInitialize(void* p, const Triangle* triangles, int count, int width, int h
             s->pieceBvh.binNodes = nullptr; s->pieceBvh.order = nullptr;
             s->pieceBvh.primLo = nullptr; s->pieceBvh.primHi = nullptr;
         }
+    } else if (e == cudaSuccess) {
+        e = buildBvh(s->dTris, count, s->stream, s->bvh, s->build, &why);
+        s->referenceTreeReady = e == cudaSuccess;
     }
     if (e != cudaSuccess) {
         fail(s, e, why);
@@ -654,6 +677,7 @@ int RtxSobolSamples(const unsigned* pixel, const unsigned* sample, const unsigne
 int RtxExportBvh(void* p, BvhNode* nodes, int nodeCapacity, int* order, int orderCapacity) {
     Session* s = static_cast<Session*>(p);
     if (!s) return 0;
+    if (s->ready && !ensureReferenceTree(s)) return 0;
     if (!s->ready || (nodes && nodeCapacity < s->build.binaryNodes) || (order && orderCapacity < s->triCount)) {
         s->error = cudaErrorInvalidValue; s->hostError = "RtxExportBvh: not initialised or buffers too small"; return 0;
     }
@@ -669,6 +693,7 @@ int RtxBvhStatsGet(void* p, RtxBvhStats* out) {
     Session* s = static_cast<Session*>(p);
     if (!s || !out) return 0;
     if (!s->ready) { s->hostError = "RtxBvhStatsGet: session is not initialised"; return 0; }
+    if (!ensureReferenceTree(s)) return 0;
     if (s->sahCost < 0) {
         std::vector<BvhNode> nodes((size_t)s->build.binaryNodes);
         if (!useDevice(s)) return 0;

@@ -235,15 +235,17 @@ def cuboid(center, size, yaw, **kwargs):
     return np.concatenate(faces)
 
 
-def random_room(seed, width=256, height=256):
+def random_room(seed, width=256, height=256, triangles=None):
     """Training scene for the learned denoiser (not a benchmark workload):
     an open room of random size and wall colours lit by a ceiling quad
     light (random size, height and power, half the time under a diffuse
     shade, sometimes with a second small light), two to seven objects
     (faceted or smooth displaced spheres, boxes; a quarter of them glossy),
-    a random camera inside the room, depth 3 to 6. Returns the triangles,
-    camera, settings and the environment (None: the sky gradient, else a
-    constant radiance)."""
+    a random camera inside the room, depth 3 to 6. With `triangles` given,
+    the spheres share that budget (20 f^2 triangles each; at least one
+    object is a sphere), so the room has about that many triangles.
+    Returns the triangles, camera, settings and the environment (None: the
+    sky gradient, else a constant radiance)."""
     rng = np.random.Generator(np.random.PCG64(seed))
     hx, top, hz = rng.uniform(1.5, 4.0), rng.uniform(2.2, 4.5), rng.uniform(1.5, 4.0)
     colors = rng.uniform(0.08, 0.9, (5, 3))
@@ -260,15 +262,25 @@ def random_room(seed, width=256, height=256):
         lx, lz = rng.uniform(-hx + q, hx - q), rng.uniform(-hz + q, hz - q)
         parts.append(box_quad((lx - q, top - 0.01, lz - q), (2 * q, 0, 0), (0, 0, 2 * q), emission=emission,
                               mesh=21))
-    for k in range(int(rng.integers(2, 8))):
+    objects = int(rng.integers(2, 8))
+    kinds = rng.random(objects) < 0.6  # True: a sphere
+    if triangles is not None and not kinds.any():
+        kinds[0] = True
+    shares = None
+    if triangles is not None:
+        boxes = int((~kinds).sum())
+        budget = max(triangles - sum(len(p) for p in parts) - 12 * boxes, 20 * int(kinds.sum()))
+        shares = iter(rng.dirichlet(np.ones(int(kinds.sum()))) * budget)
+    for k in range(objects):
         size = rng.uniform(0.2, 0.35 * min(hx, hz, top))
         center = (rng.uniform(-hx + size, hx - size), rng.uniform(size, top - size), rng.uniform(-hz + size, hz - size))
         material = dict(color=rng.uniform(0.05, 0.95, 3), mesh=30 + k)
         if rng.random() < 0.25:
             material.update(smoothness=float(rng.uniform(0.6, 1.0)), specular_probability=float(rng.uniform(0.1, 0.6)),
                             specular_color=rng.uniform(0.6, 1.0, 3))
-        if rng.random() < 0.6:
-            v0, v1, v2, normals = geodesic_sphere(int(rng.integers(3, 40)), size, center, rng.uniform(0, 0.1), rng,
+        if kinds[k]:
+            f = int(rng.integers(3, 40)) if shares is None else max(1, int(round(math.sqrt(next(shares) / 20.0))))
+            v0, v1, v2, normals = geodesic_sphere(f, size, center, rng.uniform(0, 0.1), rng,
                                                   smooth=bool(rng.random() < 0.5))
             parts.append(records(v0, v1, v2, normals=normals if rng.random() < 0.7 else None, **material))
         else:

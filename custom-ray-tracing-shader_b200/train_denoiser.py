@@ -1,21 +1,23 @@
 """Trains the learned denoiser (the RtxUnet* entry points) on images that
 this library renders.
 
-Data: for every random room (scenes.random_room), a high-sample render is the
-target (linear radiance, the colour AOV of RtxReadAovs) and renders with few
-paths per pixel and other sampler seeds are the inputs (all ten AOVs). The
-images are cut into square crops; the network trains with Adam on random
-crops with random flips and an L1 loss on log(1 + radiance). Held-out rooms
-report PSNR on 8-bit display values (exposure tonemap and sRGB, as RtRender
-displays) for the input, the guided filter and the network.
-
-Defaults follow the training configuration of the denoiser: 200 rooms,
-4,800 crops of 128x128 (six inputs of 4 to 32 paths per pixel per room),
-1024-path targets, Adam at lr 1e-3 (cosine decay), 20K steps at batch 32.
+Data (the denoiser-training configuration): 200 seeded random rooms
+(scenes.random_room) whose triangle counts are drawn log-uniformly from 5K to
+500K; each is rendered at 384x384 once with 1024 paths per pixel (the
+target: linear radiance, the colour AOV of RtxReadAovs) and three times with
+4 paths per pixel and other sampler seeds (the inputs: all ten AOVs, 4-spp
+radiance, albedo, normal, linear depth). Every image is cut into nine
+128x128 crops, and 25 crops per room are kept: 5,000 crops. The network
+trains with Adam at lr 1e-3 (cosine decay) for 20K steps at batch 32 on
+random crops with random flips and an L1 loss on log(1 + radiance).
+Held-out rooms (other seeds) report PSNR of the display values (exposure
+tonemap and sRGB, as RtRender displays) for the input, the guided filter and
+the network at 4 and 8 paths per pixel.
 
 Usage:
-  python train_denoiser.py [--scenes 200] [--holdout 12] [--size 256]
-      [--target-spp 1024] [--steps 20000] [--out weights/denoiser_unet.bin]
+  python train_denoiser.py [--scenes 200] [--crops 5000] [--holdout 12]
+      [--size 384] [--input-spp 4] [--target-spp 1024] [--steps 20000]
+      [--out weights/denoiser_unet.bin]
 """
 import argparse
 import json
@@ -33,7 +35,15 @@ if str(HERE) not in sys.path:
 import scenes  # noqa: E402
 from native_api import DENOISER_WEIGHTS, Session, Settings, Unet, load_library  # noqa: E402
 
-INPUT_SPP = (4, 4, 8, 8, 16, 32)
+TRIANGLES = (5_000, 500_000)  # per room, log-uniform
+INPUTS_PER_ROOM = 3            # 4-spp renders per room (other sampler seeds)
+
+
+def training_plan(scenes_count, seed=1):
+    """(room seed, triangle budget) of every training room."""
+    rng = np.random.default_rng(seed)
+    lo, hi = np.log(TRIANGLES[0]), np.log(TRIANGLES[1])
+    return [(10_000 + i, int(round(np.exp(rng.uniform(lo, hi))))) for i in range(scenes_count)]
 
 
 def display(radiance, exposure):
@@ -57,9 +67,9 @@ def accumulate(session, camera, settings, spp, per_pass):
     assert session.sample_count() == spp
 
 
-def render_room(lib, seed, size, target_spp, input_spps):
+def render_room(lib, seed, size, target_spp, input_spps, triangles=50_000):
     """(inputs [k][size][size][10], target [size][size][3], exposure, guided filter displays)."""
-    tris, cam, st, env = scenes.random_room(seed, size, size)
+    tris, cam, st, env = scenes.random_room(seed, size, size, triangles=triangles)
     s = Session(lib)
     try:
         s.initialize(tris, size, size)
@@ -91,11 +101,12 @@ def crops(images, crop):
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split('\n\n')[0])
     ap.add_argument('--scenes', type=int, default=200, help='training rooms')
+    ap.add_argument('--crops', type=int, default=5000, help='training crops in all (an equal share per room)')
     ap.add_argument('--holdout', type=int, default=12, help='validation rooms (other seeds)')
-    ap.add_argument('--size', type=int, default=256, help='render resolution (square)')
+    ap.add_argument('--size', type=int, default=384, help='render resolution (square)')
     ap.add_argument('--crop', type=int, default=128)
+    ap.add_argument('--input-spp', type=int, default=4)
     ap.add_argument('--target-spp', type=int, default=1024)
-    ap.add_argument('--inputs-per-room', type=int, default=6)
     ap.add_argument('--steps', type=int, default=20000)
     ap.add_argument('--batch', type=int, default=32)
     ap.add_argument('--lr', type=float, default=1e-3)
@@ -104,21 +115,23 @@ def main(argv=None):
     ap.add_argument('--log', default=None, help='write a JSON summary here')
     args = ap.parse_args(argv)
     assert args.size % args.crop == 0 and args.crop % 16 == 0
+    per_room = -(-args.crops // args.scenes)
+    assert per_room <= INPUTS_PER_ROOM * (args.size // args.crop) ** 2
     lib = load_library()
-    rng = np.random.default_rng(args.seed)
 
     t0 = time.perf_counter()
-    train_in, train_t = [], []
-    for i in range(args.scenes):
-        spps = rng.choice(INPUT_SPP, args.inputs_per_room, replace=False)
-        inputs, target, _, _ = render_room(lib, 10_000 + i, args.size, args.target_spp, spps)
-        train_in.append(crops(inputs, args.crop))
-        train_t.append(crops(np.repeat(target[None], len(inputs), 0), args.crop))
-    train_in, train_t = np.concatenate(train_in), np.concatenate(train_t)
-    val = [render_room(lib, 900_000 + i, args.size, args.target_spp, (8, 16)) for i in range(args.holdout)]
+    train_in, train_t, budgets = [], [], []
+    for seed, budget in training_plan(args.scenes, args.seed):
+        inputs, target, _, _ = render_room(lib, seed, args.size, args.target_spp,
+                                           (args.input_spp,) * INPUTS_PER_ROOM, budget)
+        train_in.append(crops(inputs, args.crop)[:per_room])
+        train_t.append(crops(np.repeat(target[None], len(inputs), 0), args.crop)[:per_room])
+        budgets.append(budget)
+    train_in, train_t = np.concatenate(train_in)[:args.crops], np.concatenate(train_t)[:args.crops]
+    val = [render_room(lib, 900_000 + i, args.size, args.target_spp, (4, 8)) for i in range(args.holdout)]
     data_s = time.perf_counter() - t0
-    print(f'data: {len(train_in)} crops of {args.crop}^2 from {args.scenes} rooms, '
-          f'{args.holdout} held out, {data_s:.1f} s', flush=True)
+    print(f'data: {len(train_in)} crops of {args.crop}^2 from {args.scenes} rooms of '
+          f'{min(budgets)}-{max(budgets)} triangles, {args.holdout} held out, {data_s:.1f} s', flush=True)
 
     net = Unet(lib, seed=args.seed)
     t1 = time.perf_counter()
@@ -135,14 +148,16 @@ def main(argv=None):
     report = []
     for inputs, target, exposure, filtered in val:
         ref = display(target, exposure)
-        for k, spp in enumerate((8, 16)):
+        for k, spp in enumerate((4, 8)):
             out = net.infer(inputs[k])
             report.append({'spp': spp, 'input_db': psnr(display(inputs[k][..., 0:3], exposure), ref),
                            'filter_db': psnr(filtered[k], ref), 'unet_db': psnr(display(out, exposure), ref)})
-    summary = {'crops': len(train_in), 'crop': args.crop, 'rooms': args.scenes, 'target_spp': args.target_spp,
+    summary = {'crops': len(train_in), 'crop': args.crop, 'rooms': args.scenes,
+               'room_triangles': [min(budgets), max(budgets)], 'input_spp': args.input_spp,
+               'target_spp': args.target_spp, 'render_size': args.size,
                'steps': args.steps, 'batch': args.batch, 'lr': args.lr, 'data_seconds': data_s,
                'train_seconds': train_s, 'ms_per_step': 1e3 * train_s / max(args.steps, 1), 'loss': history}
-    for spp in (8, 16):
+    for spp in (4, 8):
         rows = [r for r in report if r['spp'] == spp]
         summary[f'holdout_{spp}spp'] = {key: float(np.mean([r[key] for r in rows]))
                                         for key in ('input_db', 'filter_db', 'unet_db')}

@@ -61,3 +61,29 @@ def test_end_to_end_equal_quality():
     tris, cam, st, w, h = scenes.end_to_end_room()
     assert len(tris) == 1997134 and (w, h) == (1920, 1080) and st.maxBounces == 5
     assert (tris['emission'] > 0).sum() == 2
+
+
+def test_denoiser_training_set():
+    """The learned denoiser's training configuration: 200 seeded rooms of 5K
+    to 500K triangles (log-uniform), 5,000 crops of 128x128, 4-spp inputs
+    with the ten AOV channels, 1024-spp targets, batch 32, 20K steps, Adam
+    at lr 1e-3."""
+    import inspect
+    import train_denoiser as td
+    plan = td.training_plan(200)
+    budgets = np.array([b for _, b in plan])
+    assert len(plan) == 200 and len({s for s, _ in plan}) == 200
+    assert budgets.min() >= 5_000 and budgets.max() <= 500_000
+    logs = np.log(budgets)
+    assert abs(np.exp(logs.mean()) / 50_000 - 1) < 0.35          # geometric mean of a log-uniform [5K, 500K]
+    assert budgets.min() < 8_000 and budgets.max() > 300_000
+    src = inspect.getsource(td.main)
+    for flag, value in (("'--scenes'", '200'), ("'--crops'", '5000'), ("'--crop'", '128'), ("'--input-spp'", '4'),
+                        ("'--target-spp'", '1024'), ("'--steps'", '20000'), ("'--batch'", '32'), ("'--lr'", '1e-3')):
+        line = next(l for l in src.splitlines() if flag in l)
+        assert f'default={value}' in line, (flag, line)
+    assert td.INPUTS_PER_ROOM * (384 // 128) ** 2 * 200 >= 5000
+    for seed, budget in (plan[0], plan[int(np.argmax(budgets))], plan[int(np.argmin(budgets))]):
+        tris, cam, st, env = scenes.random_room(seed, 384, 384, triangles=budget)
+        assert abs(len(tris) / budget - 1) < 0.25, (seed, budget, len(tris))
+        assert 3 <= st.maxBounces <= 6
