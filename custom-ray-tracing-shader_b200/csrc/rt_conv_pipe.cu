@@ -61,6 +61,8 @@ constexpr uint32_t kHeader = 1024;       // barriers and flags
 
 struct PipeArgs {
     int n, h, w, cin, cout, lowChannels;
+    int coutTotal;  // output channels of the layer; a block computes cout of them, from (block % nSplits) * cout
+    int nSplits;
     int tilesPerRow, stripRows, strips, units, ring;
     uint32_t weightBytes, slotBytes, lowSlotBytes, accCols, tmemCols;
     const float* bias;
@@ -197,15 +199,15 @@ __device__ __forceinline__ Unit unitOf(const PipeArgs& a, int u) {
 }
 
 template <int COUT>
-__device__ __forceinline__ void epilogueStore(const PipeArgs& a, const uint32_t (&acc)[COUT], size_t pix) {
+__device__ __forceinline__ void epilogueStore(const PipeArgs& a, const uint32_t (&acc)[COUT], size_t pix, int nBase) {
     float v[COUT];
 #pragma unroll
     for (int j = 0; j < COUT; j++) {
-        const float s = __uint_as_float(acc[j]) + (a.bias ? __ldg(a.bias + j) : 0.0f);
+        const float s = __uint_as_float(acc[j]) + (a.bias ? __ldg(a.bias + nBase + j) : 0.0f);
         v[j] = a.relu ? fmaxf(s, 0.0f) : s;
     }
     if (a.outF) {
-        float4* o = reinterpret_cast<float4*>(a.outF + pix * COUT);
+        float4* o = reinterpret_cast<float4*>(a.outF + pix * a.coutTotal + nBase);
 #pragma unroll
         for (int q = 0; q < COUT / 4; q++) {
             float4 x = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
@@ -216,7 +218,7 @@ __device__ __forceinline__ void epilogueStore(const PipeArgs& a, const uint32_t 
             o[q] = x;
         }
     } else {
-        uint4* o = reinterpret_cast<uint4*>(a.outB + pix * COUT);
+        uint4* o = reinterpret_cast<uint4*>(a.outB + pix * a.coutTotal + nBase);
 #pragma unroll
         for (int q = 0; q < COUT / 8; q++) {
             uint32_t words[4];
@@ -246,6 +248,10 @@ __global__ void __launch_bounds__(kThreads) convPipeKernel(const __grid_constant
     const int G = a.cin / 8, Glow = a.lowChannels / 8, Gin = G - Glow;
     const int R = a.ring;
     const uint64_t limit = a.waitLimitNs;
+    // The block's slice of output channels and its units (every nSplits-th
+    // block shares a slice; the grid is a multiple of nSplits).
+    const int nBase = (int)(blockIdx.x % (unsigned)a.nSplits) * COUT;
+    const int firstUnit = (int)(blockIdx.x / (unsigned)a.nSplits), unitStride = (int)(gridDim.x / (unsigned)a.nSplits);
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < R; s++) {
@@ -284,7 +290,7 @@ __global__ void __launch_bounds__(kThreads) convPipeKernel(const __grid_constant
             barExpectTx(wb, a.weightBytes);
             for (int t = 0; t < 9; t++)
                 for (int g = 0; g < G; g++)
-                    tmaLoad3(wAddr + (uint32_t)((t * G + g) * COUT * 16), &wMap, g * 8, 0, a.reverseTaps ? 8 - t : t,
+                    tmaLoad3(wAddr + (uint32_t)((t * G + g) * COUT * 16), &wMap, g * 8, nBase, a.reverseTaps ? 8 - t : t,
                              wb);
         }
         // Rows are numbered in issue order q; row q sits in slot q % R, its
@@ -310,7 +316,7 @@ __global__ void __launch_bounds__(kThreads) convPipeKernel(const __grid_constant
             if (lane == 0) barArrive(base + Header::full + 8 * (int)(e % R));
             return true;
         };
-        for (int u = blockIdx.x; u < a.units && ok; u += gridDim.x) {
+        for (int u = firstUnit; u < a.units && ok; u += unitStride) {
             const Unit U = unitOf(a, u);
             for (int r = U.y0 - 1; r <= U.y1 && ok; r++) {
                 const int s = (int)(q % R);
@@ -377,7 +383,7 @@ __global__ void __launch_bounds__(kThreads) convPipeKernel(const __grid_constant
             if (ok) ok = waitPhase(base + Header::weights, 0u, abortFlag, limit);
             long long q = 0, tile = 0;
             const uint32_t kStepA = (2u * kPlane) >> 4, kStepB = (2u * COUT * 16u) >> 4;
-            for (int u = blockIdx.x; u < a.units && ok; u += gridDim.x) {
+            for (int u = firstUnit; u < a.units && ok; u += unitStride) {
                 const Unit U = unitOf(a, u);
                 const long long q0 = q;  // row U.y0 - 1
                 for (int y = U.y0; y < U.y1 && ok; y++, tile++) {
@@ -428,7 +434,7 @@ __global__ void __launch_bounds__(kThreads) convPipeKernel(const __grid_constant
         const int quarter = warp & 3;
         long long tile = 0;
         bool ok = true;
-        for (int u = blockIdx.x; u < a.units && ok; u += gridDim.x) {
+        for (int u = firstUnit; u < a.units && ok; u += unitStride) {
             const Unit U = unitOf(a, u);
             for (int y = U.y0; y < U.y1; y++, tile++) {
                 const int b = (int)(tile & 1);
@@ -448,7 +454,7 @@ __global__ void __launch_bounds__(kThreads) convPipeKernel(const __grid_constant
                 __syncwarp();
                 if (lane == 0) barArrive(base + Header::accEmpty + 8 * b);
                 const int x = U.x0 + quarter * 32 + lane;
-                if (x < a.w) epilogueStore<COUT>(a, acc, ((size_t)U.img * a.h + y) * a.w + x);
+                if (x < a.w) epilogueStore<COUT>(a, acc, ((size_t)U.img * a.h + y) * a.w + x, nBase);
             }
         }
     }
@@ -518,21 +524,34 @@ uint32_t convPipeSmemBytes(int cin, int cout, int lowChannels, int ring) {
     return kHeader + weights + (uint32_t)ring * slot + 2u * lowSlot;
 }
 
+namespace {
+bool knownCout(int c) { return c == 16 || c == 32 || c == 48 || c == 64 || c == 80 || c == 96; }
+// Output-channel slices per layer: the fewest (1, 2, 3, 4, 6) whose slice is
+// a supported width and whose weights fit beside a ring of kMinRing rows;
+// 0 when none does.
+int pickSplits(int cin, int cout, int lowChannels) {
+    for (int s : {1, 2, 3, 4, 6})
+        if (cout % s == 0 && knownCout(cout / s) &&
+            convPipeSmemBytes(cin, cout / s, lowChannels, kMinRing) <= 227u * 1024u)
+            return s;
+    return 0;
+}
+}  // namespace
+
 bool convPipeSupported(int cin, int cout, int lowChannels) {
-    static const int couts[] = {16, 32, 48, 64, 80, 96};
-    bool known = false;
-    for (int c : couts) known = known || c == cout;
-    return known && cin >= 16 && cin % 16 == 0 && lowChannels % 16 == 0 && lowChannels < cin &&
-           convPipeSmemBytes(cin, cout, lowChannels, kMinRing) <= 227u * 1024u;
+    return cin >= 16 && cin % 16 == 0 && lowChannels % 16 == 0 && lowChannels < cin &&
+           pickSplits(cin, cout, lowChannels) > 0;
 }
 
 cudaError_t convPipe(const bf16* in, const bf16* low, int lowChannels, int n, int h, int w, int cin,
-                     const bf16* weights, bool reverseTaps, const float* bias, int cout, bf16* outB, float* outF,
+                     const bf16* weights, bool reverseTaps, const float* bias, int coutTotal, bf16* outB, float* outF,
                      bool relu, bool accumulate, int* errorFlag, cudaStream_t stream, const ConvPipeTest* test) {
     if (!low) lowChannels = 0;
-    if (n < 1 || h < 1 || w < 1 || !convPipeSupported(cin, cout, lowChannels) || (!outB && !outF) || !errorFlag ||
-        (lowChannels && (h % 2 || w % 2)))
+    if (n < 1 || h < 1 || w < 1 || !convPipeSupported(cin, coutTotal, lowChannels) || (!outB && !outF) ||
+        !errorFlag || (lowChannels && (h % 2 || w % 2)))
         return cudaErrorNotSupported;
+    const int nSplits = pickSplits(cin, coutTotal, lowChannels);
+    const int cout = coutTotal / nSplits;  // output channels per block
     const int cinIn = cin - lowChannels;
     CUtensorMap inMap{}, lowMap{}, wMap{};
     {
@@ -551,13 +570,15 @@ cudaError_t convPipe(const bf16* in, const bf16* low, int lowChannels, int n, in
         lowMap = inMap;
     }
     {
-        const uint64_t dims[3] = {(uint64_t)cin, (uint64_t)cout, 9};
-        const uint64_t strides[2] = {(uint64_t)cin * 2, (uint64_t)cout * cin * 2};
+        // [9][coutTotal][cin]; a block loads the rows of its slice.
+        const uint64_t dims[3] = {(uint64_t)cin, (uint64_t)coutTotal, 9};
+        const uint64_t strides[2] = {(uint64_t)cin * 2, (uint64_t)coutTotal * cin * 2};
         const uint32_t box[3] = {8, (uint32_t)cout, 1};
         if (!makeMap(&wMap, weights, 3, dims, strides, box)) return cudaErrorNotSupported;
     }
     PipeArgs a{};
     a.n = n; a.h = h; a.w = w; a.cin = cin; a.cout = cout; a.lowChannels = lowChannels;
+    a.coutTotal = coutTotal; a.nSplits = nSplits;
     a.tilesPerRow = (w + kM - 1) / kM;
     a.weightBytes = 9u * (uint32_t)cin * (uint32_t)cout * 2u;
     a.slotBytes = ((uint32_t)(cin / 8) * kPlane + 127u) & ~127u;
@@ -585,15 +606,16 @@ cudaError_t convPipe(const bf16* in, const bf16* low, int lowChannels, int n, in
     const uint32_t smemBytes = convPipeSmemBytes(cin, cout, lowChannels, a.ring);
     if (smemBytes > 227u * 1024u) return cudaErrorNotSupported;
     // Strips: long enough to reuse rows (each strip stages 2 extra rows),
-    // short enough to give every block about two units.
+    // short enough to give every block about two units; every slice of
+    // output channels walks all units.
     const long long columns = (long long)n * a.tilesPerRow;
-    const long long blocks = (long long)sms * perSm;
-    long long rows = std::max(1ll, columns * h / (2 * blocks));
+    const long long blocks = std::max<long long>(nSplits, (long long)sms * perSm / nSplits * nSplits);
+    long long rows = std::max(1ll, columns * h * nSplits / (2 * blocks));
     a.stripRows = (int)std::max(4ll, std::min<long long>(32, rows));
     if (test && test->stripRows > 0) a.stripRows = test->stripRows;
     a.strips = (h + a.stripRows - 1) / a.stripRows;
     a.units = (int)(columns * a.strips);
-    const int grid = (int)std::min<long long>(a.units, blocks);
+    const int grid = (int)std::min<long long>((long long)a.units * nSplits, blocks);
     switch (cout) {
         case 16: return launchPipe<16>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
         case 32: return launchPipe<32>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
