@@ -584,12 +584,11 @@ int RtDenoise(void* p, unsigned char* output, int outputBytes, float* millisecon
     }
     if ((e = cudaEventRecord(s->start, s->stream)) != cudaSuccess) { fail(s, e); return 0; }
     if (s->denoiser) {
-        // Learned denoiser: AOVs -> U-Net -> display, all on the session stream.
-        float* aov = reinterpret_cast<float*>(s->dDenoise);
-        float* radiance = aov + 10 * count;
-        std::string why;
-        if ((e = launchAovs(s->dSum, s->dDepth, s->samples, (int)count, aov, s->stream)) != cudaSuccess) { fail(s, e); return 0; }
-        if ((e = s->denoiser->net.inferDevice(aov, s->height, s->width, radiance, s->stream, why)) != cudaSuccess) { fail(s, e, why.empty() ? nullptr : why.c_str()); return 0; }
+        // Learned denoiser: running sums -> U-Net (AOVs formed in its input
+        // kernel, as RtxReadAovs forms them) -> display, on the session stream.
+        float* radiance = reinterpret_cast<float*>(s->dDenoise) + 10 * count;
+        if ((e = s->denoiser->net.inferFromSums(reinterpret_cast<const float*>(s->dSum), s->dDepth, s->samples,
+                                                s->height, s->width, radiance, s->stream)) != cudaSuccess) { fail(s, e); return 0; }
         if ((e = launchPresentRadiance(s->dSum, radiance, (int)count, s->lastSettings.exposure, s->dPixels, s->stream)) != cudaSuccess) { fail(s, e); return 0; }
         s->denoisedOffset = 10 * count;
         s->denoisedStride = 3;

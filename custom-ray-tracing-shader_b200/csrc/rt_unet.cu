@@ -18,6 +18,7 @@
 #include <cstring>
 #include <random>
 
+#include "rt_common.cuh"
 #include "rt_conv_tc.cuh"
 #include "rt_unet.cuh"
 
@@ -289,6 +290,59 @@ __global__ void adamKernel(float* p, const float* g, float* m, float* v, size_t 
     p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
 }
 // Network output (log space, padded frame) to linear radiance (w x h x 3).
+// Network input straight from the running sums: the AOVs of RtxReadAovs
+// (sum / samples, normalised normal, distance / samples), then the input
+// transform of inputKernel, for every pixel of the padded frame (beyond w x h
+// the edge pixels repeat).
+__global__ void sumsInputKernel(const float* sums, const float* depthSums, unsigned samples, int h, int w, int H,
+                                int W, bf16* x0) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)H * W) return;
+    const int X = (int)(i % W), Y = (int)(i / W);
+    const size_t src = (size_t)min(Y, h - 1) * w + min(X, w - 1);
+    const float* a = sums + src * 10;
+    const float inv = 1.0f / (float)samples;
+    const float3 c = scale(v3(a[0], a[1], a[2]), inv), al = scale(v3(a[3], a[4], a[5]), inv);
+    const float3 nr = normalize(v3(a[6], a[7], a[8]));
+    const float depth = depthSums[src] * inv;
+    float v[kInputPadded] = {};
+    v[0] = log1pf(fmaxf(c.x, 0.0f)); v[1] = log1pf(fmaxf(c.y, 0.0f)); v[2] = log1pf(fmaxf(c.z, 0.0f));
+    v[3] = al.x; v[4] = al.y; v[5] = al.z;
+    v[6] = nr.x; v[7] = nr.y; v[8] = nr.z;
+    v[9] = log1pf(fmaxf(depth, 0.0f));
+    uint4 packed[2];
+    uint32_t* words = reinterpret_cast<uint32_t*>(packed);
+#pragma unroll
+    for (int j = 0; j < kInputPadded / 2; j++) {
+        __nv_bfloat162 pair = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+        words[j] = *reinterpret_cast<uint32_t*>(&pair);
+    }
+    uint4* o = reinterpret_cast<uint4*>(x0 + (size_t)i * kInputPadded);
+    o[0] = packed[0];
+    o[1] = packed[1];
+}
+// Output layer and crop in one pass: the 1x1 convolution of outForwardKernel
+// (same summation order) for the pixels inside w x h, then expm1 and the
+// clamp of outputKernel.
+__global__ void outputFusedKernel(const bf16* d, int H, int W, int h, int w, int C, const float* wt, const float* b,
+                                  float* out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= w * h) return;
+    const int x = i % w, y = i / w;
+    const long long p = (long long)y * W + x;
+    float s[kOutChannels] = {b[0], b[1], b[2]};
+    for (int c8 = 0; c8 < C; c8 += 8) {
+        uint4 q = *reinterpret_cast<const uint4*>(d + p * C + c8);
+        const bf16* e = reinterpret_cast<const bf16*>(&q);
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            float v = __bfloat162float(e[j]);
+            for (int k = 0; k < kOutChannels; k++) s[k] += v * wt[(c8 + j) * kOutChannels + k];
+        }
+    }
+    for (int k = 0; k < kOutChannels; k++) out[(size_t)i * 3 + k] = fmaxf(expm1f(s[k]), 0.0f);
+}
+
 __global__ void outputKernel(const float* pred, int H, int W, int h, int w, float* out) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= w * h) return;
@@ -492,7 +546,7 @@ cudaError_t Unet::ensure(int n, int h, int w, bool training) {
     return cudaSuccess;
 }
 
-cudaError_t Unet::forward(cudaStream_t s, bool training) {
+cudaError_t Unet::forward(cudaStream_t s, bool training, bool outputLayer) {
     Activations& A = *act_;
     const int n = A.n;
     cudaError_t e;
@@ -531,6 +585,7 @@ cudaError_t Unet::forward(cudaStream_t s, bool training) {
             if (e != cudaSuccess) return e;
         }
     }
+    if (!outputLayer) return cudaGetLastError();
     const UnetLayer& O = layers_[18];
     long long pixels = (long long)n * A.H * A.W;
     outForwardKernel<<<blocksFor(pixels, 128), 128, 0, s>>>(A.a[17], pixels, O.cin, master_ + O.wOffset, master_ + O.bOffset, A.pred);
@@ -662,6 +717,20 @@ cudaError_t Unet::train(const float* aovs, const float* targets, int count, int 
     if (e == cudaSuccess) e = checkConvolutions(error);
     cudaFree(dA); cudaFree(dT); cudaFree(dLosses);
     return e;
+}
+
+cudaError_t Unet::inferFromSums(const float* sums, const float* depthSums, unsigned samples, int h, int w,
+                                float* radiance, cudaStream_t s) {
+    cudaError_t e = ensure(1, h, w, false);
+    if (e != cudaSuccess) return e;
+    Activations& A = *act_;
+    sumsInputKernel<<<blocksFor((long long)A.H * A.W, 256), 256, 0, s>>>(sums, depthSums, samples, h, w, A.H, A.W, A.x0);
+    if ((e = forward(s, false, false)) != cudaSuccess) return e;
+    const UnetLayer& O = layers_[18];
+    outputFusedKernel<<<blocksFor((long long)w * h, 256), 256, 0, s>>>(A.a[17], A.H, A.W, h, w, O.cin,
+                                                                      master_ + O.wOffset, master_ + O.bOffset,
+                                                                      radiance);
+    return cudaGetLastError();
 }
 
 cudaError_t Unet::inferDevice(const float* aovs, int h, int w, float* radiance, cudaStream_t s, std::string&) {

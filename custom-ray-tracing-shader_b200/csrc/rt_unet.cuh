@@ -46,6 +46,13 @@ public:
     // Inference from device AOV input (w x h x 10 FP32) to device linear
     // radiance (w x h x 3 FP32); any w, h (padded internally to 16).
     cudaError_t inferDevice(const float* aovs, int h, int w, float* radiance, cudaStream_t stream, std::string& error);
+    // The same inference straight from a session's running sums (10 four-
+    // byte fields per pixel: radiance, albedo and normal sums, coverage) and
+    // first-hit distance sums after `samples` paths per pixel: the AOVs are
+    // formed inside the input kernel with the expressions of RtxReadAovs, and
+    // the output layer writes the cropped radiance directly.
+    cudaError_t inferFromSums(const float* sums, const float* depthSums, unsigned samples, int h, int w,
+                              float* radiance, cudaStream_t stream);
     // Checkpoint file: parameters, and the Adam state when optimizerState.
     cudaError_t save(const char* path, bool optimizerState, std::string& error) const;
     // After the work has finished: an error if a tensor-core convolution gave
@@ -56,7 +63,7 @@ public:
 private:
     struct Activations;
     cudaError_t ensure(int n, int h, int w, bool training);
-    cudaError_t forward(cudaStream_t stream, bool training);
+    cudaError_t forward(cudaStream_t stream, bool training, bool outputLayer = true);
     cudaError_t backward(cudaStream_t stream);
     cudaError_t syncWeights(cudaStream_t stream);
 
