@@ -428,8 +428,13 @@ int deviceSms() {
 }  // namespace
 
 static std::atomic<int> g_convPath{0};
+static std::atomic<long long> g_pipeLaunches{0}, g_singleLaunches{0};
 void setConvPath(int mode) { g_convPath.store(mode); }
 int convPath() { return g_convPath.load(); }
+void convLaunchCounts(long long* pipe, long long* single) {
+    if (pipe) *pipe = g_pipeLaunches.load();
+    if (single) *single = g_singleLaunches.load();
+}
 
 cudaError_t convTc(const bf16* in, const bf16* low, int lowChannels, int n, int h, int w, int cin,
                    const bf16* weights, bool reverseTaps, const float* bias, int cout, bf16* outB, float* outF,
@@ -439,8 +444,12 @@ cudaError_t convTc(const bf16* in, const bf16* low, int lowChannels, int n, int 
     if (g_convPath.load() == 0 && convPipeSupported(cin, cout, low ? lowChannels : 0)) {
         cudaError_t e = convPipe(in, low, lowChannels, n, h, w, cin, weights, reverseTaps, bias, cout, outB, outF,
                                  relu, accumulate, errorFlag, stream);
-        if (e != cudaErrorNotSupported) return e;
+        if (e != cudaErrorNotSupported) {
+            g_pipeLaunches++;
+            return e;
+        }
     }
+    g_singleLaunches++;
     if (n < 1 || h < 1 || w < 1 || cin < 16 || cin % 16 || cout < 16 || cout % 16 || cout > 256 ||
         (!outB && !outF) || !errorFlag || (low && (lowChannels < 16 || lowChannels % 16 || lowChannels >= cin ||
                                                    h % 2 || w % 2)))

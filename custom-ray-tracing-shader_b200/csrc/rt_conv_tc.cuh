@@ -54,6 +54,8 @@ cudaError_t convTc(const __nv_bfloat16* in, const __nv_bfloat16* low, int lowCha
 // applies, 1 always the kernel above (process-wide; for comparisons).
 void setConvPath(int mode);
 int convPath();
+// Convolutions run so far by the pipelined and by the single-role kernel.
+void convLaunchCounts(long long* pipe, long long* single);
 
 // Test hooks of the pipelined form (convPipe): zero values keep the defaults.
 struct ConvPipeTest {

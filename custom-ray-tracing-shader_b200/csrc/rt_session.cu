@@ -912,6 +912,11 @@ int RtxSetConvPath(int mode) {
 
 int RtxDebugConvWaitProbe(void) { return rt::convPipeWaitProbe(); }
 
+int RtxConvLaunchCounts(long long* pipelined, long long* singleRole) {
+    rt::convLaunchCounts(pipelined, singleRole);
+    return 1;
+}
+
 int RtxDebugFailAllocation(int n) {
     if (n < 0) return 0;
     rt::g_failAllocationIn.store(n);

@@ -107,7 +107,7 @@ EXPORTS = ('RtCreate', 'RtDestroy', 'RtShutdown', 'RtInitialize', 'RtRender', 'R
            'RtAccumulationVersion', 'RtSampleCount', 'RtEmbreeBuildMilliseconds', 'RtCpuThreadCount',
            'RtBvhInfo', 'RtLastError', 'RtxQueryRays', 'RtxSobolSamples', 'RtxExportBvh', 'RtxBvhStatsGet',
            'RtxReadAccumulation', 'RtxRenderStatsGet', 'RtxRenderDevice', 'RtxSetIntegrator', 'RtxSetTuning',
-           'RtxDebugFailAllocation', 'RtxSetConvPath', 'RtxDebugConvWaitProbe',
+           'RtxDebugFailAllocation', 'RtxSetConvPath', 'RtxDebugConvWaitProbe', 'RtxConvLaunchCounts',
            'RtxQueryRaysStatic', 'RtxSetEnvironment', 'RtxUnetCreate', 'RtxUnetDestroy', 'RtxUnetParamCount',
            'RtxUnetLastError', 'RtxUnetGetParams', 'RtxUnetSetParams', 'RtxUnetLossGrad', 'RtxUnetTrain',
            'RtxUnetInfer', 'RtxUnetSave', 'RtxUnetLoad', 'RtxSetDenoiser', 'RtxReadAovs', 'RtxReadDenoised',
@@ -151,6 +151,7 @@ def load_library(path=None):
     lib.RtxDebugFailAllocation.argtypes = [c.c_int]
     lib.RtxSetConvPath.argtypes = [c.c_int]
     lib.RtxDebugConvWaitProbe.argtypes = []
+    lib.RtxConvLaunchCounts.argtypes = [c.c_void_p, c.c_void_p]
     lib.RtxQueryRaysStatic.argtypes = [vp, c.c_void_p, c.c_int, c.c_int, c.c_void_p]
     lib.RtxSetEnvironment.argtypes = [vp, c.c_int, c.c_float, c.c_float, c.c_float]
     lib.RtxUnetCreate.restype = vp

@@ -228,6 +228,10 @@ int RtxSetTuning(void* session, int key, int value);
  * kernel wherever its shared memory allows, 1 the single-role kernel for
  * every layer. Process-wide; results agree to BF16 rounding. */
 int RtxSetConvPath(int mode);
+/* Convolutions launched so far in this process by the warp-specialised
+ * kernel and by the single-role kernel (either pointer may be null); no
+ * counterpart in the reference. */
+int RtxConvLaunchCounts(long long* pipelined, long long* singleRole);
 /* Failure path of the warp-specialised convolution, no counterpart in the
  * reference: one launch whose wait on a barrier that nothing completes runs
  * out (2 ms limit) must report it through its error flag and free its

@@ -280,8 +280,20 @@ def test_conv_kernels_agree(lib, net):
     (RtxSetConvPath(1)) give the same inference and training gradients to
     BF16 rounding: at image sizes with partial 128-pixel column tiles, the
     concatenated decoder inputs read in place, and tiny deep levels."""
+    import ctypes as c
     rng = np.random.default_rng(12)
+
+    def counts():
+        pipe, single = c.c_longlong(), c.c_longlong()
+        lib.RtxConvLaunchCounts(c.byref(pipe), c.byref(single))
+        return pipe.value, single.value
     try:
+        before = counts()
+        aovs, _ = synthetic(rng, 1, 64, 256)
+        net.infer(aovs[0])
+        after = counts()
+        # 18 layers: the pipelined kernel takes all but the widest (224 -> 96, 128 -> 128 and 96 -> 128 at level 4).
+        assert after[0] - before[0] >= 14 and (after[0] - before[0]) + (after[1] - before[1]) == 18, (before, after)
         for h, w in ((64, 256), (72, 136), (37, 23)):
             aovs, _ = synthetic(rng, 1, h, w)
             assert lib.RtxSetConvPath(1)
