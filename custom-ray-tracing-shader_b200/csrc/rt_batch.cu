@@ -134,7 +134,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) batchExtendKernel(const u
                                                            const BatchScene* scenes, unsigned long long* counter,
                                                            int* errorFlag, int refill) {
     BatchExtendIO io{B.queue[q], B.pathA, B.pathB, B.hits, views, scenes};
-    persistentTrace<false>(io, B.counts[q], wide, packed, &B.counts[3], counter, errorFlag, 0, refill);
+    persistentTrace<false>(io, B.counts[q], wide, packed, &B.counts[3], counter, errorFlag, kStackCapacity, refill);
 }
 
 // Appends to a queue with one atomic per warp.
@@ -223,7 +223,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) batchShadowKernel(const u
                                                            WavefrontBuffers B, unsigned long long* counter,
                                                            int* errorFlag, int refill) {
     BatchShadowIO io{B.shadowRay, B.shadowDir, B.shadowContrib, B.radiance};
-    persistentTrace<true>(io, B.counts[2], wide, packed, &B.counts[4], counter, errorFlag, 0, refill);
+    persistentTrace<true>(io, B.counts[2], wide, packed, &B.counts[4], counter, errorFlag, kStackCapacity, refill);
 }
 
 __global__ void batchResetQueuesKernel(WavefrontBuffers B, int q) {

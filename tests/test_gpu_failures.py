@@ -45,6 +45,23 @@ def small_scene():
     return tris, cam, st, w, h
 
 
+def camera_rays(cam, count, seed=9):
+    """Rays from the camera towards random points of the box's interior,
+    which reach the sphere's deep subtrees like the camera rays of a pass."""
+    from native_api import QUERY_DTYPE
+    rng = np.random.Generator(np.random.PCG64(seed))
+    o = np.array([cam.origin.x, cam.origin.y, cam.origin.z])
+    target = rng.uniform((-0.9, 0.1, -0.9), (0.9, 1.9, 0.9), (count, 3))
+    d = target - o
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    q = np.zeros(count, QUERY_DTYPE)
+    for k, ax in enumerate('xyz'):
+        q['origin'][ax] = o[k]
+        q['direction'][ax] = d[:, k]
+    q['limit'] = np.float32(1e30)
+    return q
+
+
 def reference_pass(lib, tris, cam, st, w, h):
     with Session(lib) as s:
         s.initialize(tris, w, h)
@@ -64,9 +81,8 @@ def test_stack_overflow_is_reported_and_recoverable(lib, session, integrator):
     assert session.sample_count() == 0
     with pytest.raises(NativeError, match='stack overflow'):
         session.render_device(cam, st)
-    rng = np.random.Generator(np.random.PCG64(9))
     with pytest.raises(NativeError, match='stack overflow'):
-        session.query(scenes.random_rays(rng, 4000))
+        session.query(camera_rays(cam, 4000))
     with pytest.raises(NativeError, match='stack overflow'):
         session.render(cam, st, backend=0)  # the host backend shares the traversal
     for bad in (0, 49):
