@@ -57,6 +57,7 @@ constexpr uint32_t kLowPlane = (kLowHalo * 16 + 127) / 128 * 128;  // 1,152
 constexpr int kThreads = 192;
 constexpr int kMinRing = 3;  // the rows a tile reads; 4 and more let the producer run ahead
 constexpr int kMaxRing = 8;
+constexpr int kMaxAcc = 8;   // tensor-memory accumulators per block (tiles between the issuer and the epilogue)
 constexpr uint32_t kHeader = 1024;       // barriers and flags
 
 struct PipeArgs {
@@ -72,6 +73,13 @@ struct PipeArgs {
     int* errorFlag;
     unsigned long long waitLimitNs;
     int probe;  // 1: the issuer first waits on a barrier nothing completes (tests the abort path)
+    int nAcc;   // accumulators in tensor memory (2..kMaxAcc)
+    // Optional wait statistics (test hook), nanoseconds summed over blocks:
+    // [0] producer waiting for a free slot, [1] producer waiting for a low
+    // row, [2] issuer waiting for rows, [3] issuer waiting for a drained
+    // accumulator, [4] epilogue waiting for a full accumulator (per warp),
+    // [5] block lifetime.
+    unsigned long long* stats;
 };
 
 // Shared-memory header: barrier offsets (8 bytes each).
@@ -79,13 +87,13 @@ struct Header {
     static constexpr uint32_t full = 0;                    // kMaxRing
     static constexpr uint32_t empty = 8 * kMaxRing;        // kMaxRing
     static constexpr uint32_t lowFull = 16 * kMaxRing;     // kMaxRing
-    static constexpr uint32_t accFull = 24 * kMaxRing;     // 2
-    static constexpr uint32_t accEmpty = 24 * kMaxRing + 16;
-    static constexpr uint32_t weights = 24 * kMaxRing + 32;
-    static constexpr uint32_t probe = 24 * kMaxRing + 40;
-    static constexpr uint32_t drain = 24 * kMaxRing + 48;
-    static constexpr uint32_t tmemSlot = 24 * kMaxRing + 56;
-    static constexpr uint32_t abort = 24 * kMaxRing + 60;
+    static constexpr uint32_t accFull = 24 * kMaxRing;     // kMaxAcc
+    static constexpr uint32_t accEmpty = 24 * kMaxRing + 8 * kMaxAcc;
+    static constexpr uint32_t weights = 24 * kMaxRing + 16 * kMaxAcc;
+    static constexpr uint32_t probe = weights + 8;
+    static constexpr uint32_t drain = weights + 16;
+    static constexpr uint32_t tmemSlot = weights + 24;
+    static constexpr uint32_t abort = weights + 28;
 };
 static_assert(Header::abort + 4 <= kHeader, "header size");
 
@@ -245,6 +253,7 @@ __global__ void __launch_bounds__(kThreads) convPipeKernel(const __grid_constant
     const uint32_t lowAddr = ringAddr + (uint32_t)a.ring * a.slotBytes;  // 2 staging rows of the low input
     unsigned char* lowPtr = smem + (lowAddr - base);
     unsigned char* ringPtr = smem + (ringAddr - base);
+    const uint64_t blockStart = a.stats ? nowNs() : 0;
     const int G = a.cin / 8, Glow = a.lowChannels / 8, Gin = G - Glow;
     const int R = a.ring;
     const uint64_t limit = a.waitLimitNs;
@@ -259,7 +268,7 @@ __global__ void __launch_bounds__(kThreads) convPipeKernel(const __grid_constant
             barInit(base + Header::empty + 8 * s, 1);
         }
         for (int s = 0; s < 2; s++) barInit(base + Header::lowFull + 8 * s, 1);
-        for (int b = 0; b < 2; b++) {
+        for (int b = 0; b < a.nAcc; b++) {
             barInit(base + Header::accFull + 8 * b, 1);
             barInit(base + Header::accEmpty + 8 * b, 4);
         }
@@ -299,10 +308,13 @@ __global__ void __launch_bounds__(kThreads) convPipeKernel(const __grid_constant
         // two staging buffers), and before the producer would block on a
         // slot: a slot may be waiting for exactly that expansion.
         long long q = 0, expanded = 0;
+        uint64_t waitSlotNs = 0, waitLowNs = 0;
         bool ok = true;
         auto expand = [&](long long e) -> bool {
+            const uint64_t t1 = a.stats ? nowNs() : 0;
             if (!waitPhaseWarp(base + Header::lowFull + 8 * (int)(e & 1), (uint32_t)((e >> 1) & 1), abortFlag, limit))
                 return false;
+            if (a.stats) waitLowNs += nowNs() - t1;
             const uint4* src = reinterpret_cast<const uint4*>(lowPtr + (size_t)(e & 1) * a.lowSlotBytes);
             uint4* dst = reinterpret_cast<uint4*>(ringPtr + (size_t)(e % R) * a.slotBytes);
             // Staged pixel p is input x0 - 1 + p, whose low-resolution pixel
@@ -328,7 +340,11 @@ __global__ void __launch_bounds__(kThreads) convPipeKernel(const __grid_constant
                         expanded++;
                     }
                 }
-                if (!waitPhaseWarp(emptyBar, emptyParity, abortFlag, limit)) { ok = false; break; }
+                {
+                    const uint64_t t1 = a.stats ? nowNs() : 0;
+                    if (!waitPhaseWarp(emptyBar, emptyParity, abortFlag, limit)) { ok = false; break; }
+                    if (a.stats) waitSlotNs += nowNs() - t1;
+                }
                 if (lane == 0) {
                     const uint32_t fb = base + Header::full + 8 * s;
                     const uint32_t slot = ringAddr + (uint32_t)s * a.slotBytes;
@@ -372,6 +388,7 @@ __global__ void __launch_bounds__(kThreads) convPipeKernel(const __grid_constant
                 if (Glow && e >= expanded) barArrive(base + Header::full + 8 * (int)(e % R));
                 pollPhase(base + Header::full + 8 * (int)(e % R), (uint32_t)((e / R) & 1), limit);
             }
+            if (a.stats) { atomicAdd(a.stats + 0, waitSlotNs); atomicAdd(a.stats + 1, waitLowNs); }
         }
         __syncwarp();
     } else if (warp == 1) {
@@ -382,16 +399,25 @@ __global__ void __launch_bounds__(kThreads) convPipeKernel(const __grid_constant
             if (a.probe) ok = waitPhase(base + Header::probe, 0u, abortFlag, limit);
             if (ok) ok = waitPhase(base + Header::weights, 0u, abortFlag, limit);
             long long q = 0, tile = 0;
+            uint64_t waitRowNs = 0, waitAccNs = 0;
             const uint32_t kStepA = (2u * kPlane) >> 4, kStepB = (2u * COUT * 16u) >> 4;
             for (int u = firstUnit; u < a.units && ok; u += unitStride) {
                 const Unit U = unitOf(a, u);
                 const long long q0 = q;  // row U.y0 - 1
                 for (int y = U.y0; y < U.y1 && ok; y++, tile++) {
                     const long long qr = q0 + (y - U.y0);  // row y - 1
-                    for (long long e = (y == U.y0 ? qr : qr + 2); e <= qr + 2 && ok; e++)
-                        ok = waitPhase(base + Header::full + 8 * (int)(e % R), (uint32_t)((e / R) & 1), abortFlag, limit);
-                    const int b = (int)(tile & 1);
-                    if (ok) ok = waitPhase(base + Header::accEmpty + 8 * b, (uint32_t)(((tile >> 1) & 1) ^ 1), abortFlag, limit);
+                    {
+                        const uint64_t t1 = a.stats ? nowNs() : 0;
+                        for (long long e = (y == U.y0 ? qr : qr + 2); e <= qr + 2 && ok; e++)
+                            ok = waitPhase(base + Header::full + 8 * (int)(e % R), (uint32_t)((e / R) & 1), abortFlag, limit);
+                        if (a.stats) waitRowNs += nowNs() - t1;
+                    }
+                    const int b = (int)(tile % a.nAcc);
+                    if (ok) {
+                        const uint64_t t1 = a.stats ? nowNs() : 0;
+                        ok = waitPhase(base + Header::accEmpty + 8 * b, (uint32_t)(((tile / a.nAcc) & 1) ^ 1), abortFlag, limit);
+                        if (a.stats) waitAccNs += nowNs() - t1;
+                    }
                     if (!ok) break;
                     tcFenceAfter();
                     const uint32_t acc = tmem + (uint32_t)b * a.accCols;
@@ -419,26 +445,30 @@ __global__ void __launch_bounds__(kThreads) convPipeKernel(const __grid_constant
                 // accumulators) before the block's shared memory goes away.
                 for (long long e = q > R ? q - R : 0; e < q; e++)
                     pollPhase(base + Header::empty + 8 * (int)(e % R), (uint32_t)((e / R) & 1), limit);
-                for (long long t = tile > 2 ? tile - 2 : 0; t < tile; t++)
-                    pollPhase(base + Header::accFull + 8 * (int)(t & 1), (uint32_t)((t >> 1) & 1), limit);
+                for (long long t = tile > a.nAcc ? tile - a.nAcc : 0; t < tile; t++)
+                    pollPhase(base + Header::accFull + 8 * (int)(t % a.nAcc), (uint32_t)((t / a.nAcc) & 1), limit);
             } else {
                 *abortFlag = 1;
                 // Wait (bounded) for every MMA issued so far.
                 commit(base + Header::drain);
                 pollPhase(base + Header::drain, 0u, limit);
             }
+            if (a.stats) { atomicAdd(a.stats + 2, waitRowNs); atomicAdd(a.stats + 3, waitAccNs); }
         }
         __syncwarp();
     } else {
         // ---- epilogue: warps 2-5, lanes 32 * (warp % 4) ... of the accumulator ----
         const int quarter = warp & 3;
         long long tile = 0;
+        uint64_t waitNs = 0;
         bool ok = true;
         for (int u = firstUnit; u < a.units && ok; u += unitStride) {
             const Unit U = unitOf(a, u);
             for (int y = U.y0; y < U.y1; y++, tile++) {
-                const int b = (int)(tile & 1);
-                if (!waitPhaseWarp(base + Header::accFull + 8 * b, (uint32_t)((tile >> 1) & 1), abortFlag, limit)) { ok = false; break; }
+                const int b = (int)(tile % a.nAcc);
+                const uint64_t t1 = a.stats ? nowNs() : 0;
+                if (!waitPhaseWarp(base + Header::accFull + 8 * b, (uint32_t)((tile / a.nAcc) & 1), abortFlag, limit)) { ok = false; break; }
+                if (a.stats) waitNs += nowNs() - t1;
                 tcFenceAfter();
                 uint32_t acc[COUT];
                 const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)b * a.accCols;
@@ -457,10 +487,12 @@ __global__ void __launch_bounds__(kThreads) convPipeKernel(const __grid_constant
                 if (x < a.w) epilogueStore<COUT>(a, acc, ((size_t)U.img * a.h + y) * a.w + x, nBase);
             }
         }
+        if (a.stats && lane == 0) atomicAdd(a.stats + 4, waitNs);
     }
     tcFenceBefore();
     __syncthreads();
     if (threadIdx.x == 0 && *abortFlag) atomicExch(a.errorFlag, 1);
+    if (threadIdx.x == 0 && a.stats) atomicAdd(a.stats + 5, nowNs() - blockStart);
     if (warp == 1) {
         tcFenceAfter();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(a.tmemCols)
@@ -585,7 +617,11 @@ cudaError_t convPipe(const bf16* in, const bf16* low, int lowChannels, int n, in
     a.lowSlotBytes = ((uint32_t)(lowChannels / 8) * kLowPlane + 127u) & ~127u;
     a.accCols = 32;
     while (a.accCols < (uint32_t)cout) a.accCols <<= 1;
-    a.tmemCols = 2 * a.accCols;
+    a.nAcc = test && test->nAcc >= 2 && test->nAcc <= kMaxAcc ? test->nAcc : 2;
+    a.tmemCols = 32;
+    while (a.tmemCols < (uint32_t)a.nAcc * a.accCols) a.tmemCols <<= 1;
+    if (a.tmemCols > 512) return cudaErrorNotSupported;
+    a.stats = test ? test->stats : nullptr;
     a.bias = bias; a.outB = outB; a.outF = outF;
     a.relu = relu ? 1 : 0; a.accumulate = accumulate ? 1 : 0; a.reverseTaps = reverseTaps ? 1 : 0;
     a.errorFlag = errorFlag;

@@ -63,6 +63,8 @@ struct ConvPipeTest {
     int probe;                       // 1: the MMA issuer first waits on a barrier nothing completes
     int ring;                        // ring rows (4..8)
     int stripRows;                   // rows per strip
+    int nAcc;                        // tensor-memory accumulators (2..8)
+    unsigned long long* stats;       // device array of 6 wait/lifetime sums in ns (see rt_conv_pipe.cu)
 };
 
 // The same convolution as convTc, warp-specialised and fed by TMA (input
