@@ -292,15 +292,8 @@ __global__ void __launch_bounds__(kBinBlock) binKernel(const int* order, const i
     }
 }
 
-__device__ void splitTask(const Task T, int t, const BinAcc* taskBins, Split* splits, BinNode* nodes, int* counters,
-                          int* nextCount, Task* nextTasks, int nodeCapacity, int taskCapacity, int leafSize);
-
-// A task of at most kSmallTask primitives: binned by one warp in its private
-// shared-memory bins, then split by lane 0 from those bins (they never go
-// to global memory).
 __device__ void binSmallTask(const int* order, const float4* cent, const float4* plo, const float4* phi,
-                             const Task T, int t, BinAcc* my, int lane, Split* splits, BinNode* nodes, int* counters,
-                             int* nextCount, Task* nextTasks, int nodeCapacity, int taskCapacity, int leafSize) {
+                             const Task T, int t, BinAcc* bins, BinAcc* my, int lane) {
     if (T.count > kSmallTask) return;
     for (int i = lane; i < 3 * kBins; i += 32) {
         BinAcc& b = my[i];
@@ -323,46 +316,39 @@ __device__ void binSmallTask(const int* order, const float4* cent, const float4*
         }
     }
     __syncwarp();
-    if (lane == 0) splitTask(T, t, my, splits, nodes, counters, nextCount, nextTasks, nodeCapacity, taskCapacity, leafSize);
+    for (int i = lane; i < 3 * kBins; i += 32) bins[(size_t)t * 3 * kBins + i] = my[i];
     __syncwarp();
 }
 
 // One warp per small task: warp-private bins in shared memory (atomics only
-// within the warp), so these bins need no clearing and no global atomics,
-// and the task is split right there. Bins hold a count and minima/maxima, so
-// the order of accumulation does not change them.
-__global__ void __launch_bounds__(256, 4) binSmallKernel(const int* order, const float4* cent, const float4* plo,
+// within the warp), written out with plain stores, so these bins need no
+// clearing and no global atomics. Bins hold a count and minima/maxima, so the
+// order of accumulation does not change them.
+__global__ void __launch_bounds__(256) binSmallKernel(const int* order, const float4* cent, const float4* plo,
                                                       const float4* phi, const Task* tasks, const int* taskCount,
-                                                      Split* splits, BinNode* nodes, int* counters, int* nextCount,
-                                                      Task* nextTasks, int nodeCapacity, int taskCapacity,
-                                                      int leafSize) {
+                                                      BinAcc* bins) {
     __shared__ BinAcc sb[8][3 * kBins];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nTasks = taskCount[0];
     for (int t = blockIdx.x * 8 + warp; t < nTasks; t += gridDim.x * 8)
-        binSmallTask(order, cent, plo, phi, tasks[t], t, sb[warp], lane, splits, nodes, counters, nextCount, nextTasks,
-                     nodeCapacity, taskCapacity, leafSize);
+        binSmallTask(order, cent, plo, phi, tasks[t], t, bins, sb[warp], lane);
 }
 
 // One thread per open task: the reference's SAH sweep, then node records.
 // taskCount: this level's counts; nextCount: the next level's (open tasks,
 // tasks above kSmallTask); levelStart: receives the node count once this
 // level's nodes are allocated (the first node of the next depth).
-// Tasks above kSmallTask only (binSmallKernel splits the others).
+__device__ void splitTask(const Task T, int t, const BinAcc* bins, Split* splits, BinNode* nodes, int* counters,
+                          int* nextCount, Task* nextTasks, int nodeCapacity, int taskCapacity, int leafSize);
 __global__ void splitKernel(const Task* tasks, const int* taskCount, const BinAcc* bins, Split* splits, BinNode* nodes,
                             int* counters /*0 nodes,2 max depth,3 error*/, int* nextCount, Task* nextTasks,
                             int nodeCapacity, int taskCapacity, int leafSize) {
-    if (!taskCount[1]) return;
     const int nTasks = taskCount[0];
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nTasks; t += gridDim.x * blockDim.x) {
-        const Task T = tasks[t];
-        if (T.count <= kSmallTask) continue;
-        splitTask(T, t, &bins[(size_t)t * 3 * kBins], splits, nodes, counters, nextCount, nextTasks, nodeCapacity,
-                  taskCapacity, leafSize);
-    }
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nTasks; t += gridDim.x * blockDim.x)
+        splitTask(tasks[t], t, bins, splits, nodes, counters, nextCount, nextTasks, nodeCapacity, taskCapacity,
+                  leafSize);
 }
-// taskBins: the task's 3 x kBins bins.
-__device__ void splitTask(const Task T, int t, const BinAcc* taskBins, Split* splits, BinNode* nodes, int* counters,
+__device__ void splitTask(const Task T, int t, const BinAcc* bins, Split* splits, BinNode* nodes, int* counters,
                           int* nextCount, Task* nextTasks, int nodeCapacity, int taskCapacity, int leafSize) {
     atomicMax(&counters[2], T.depth);
     int bestAxis = -1, bestBin = -1;
@@ -372,7 +358,7 @@ __device__ void splitTask(const Task T, int t, const BinAcc* taskBins, Split* sp
         for (int a = 0; a < 3; a++) {
             float extent = T.chi[a] - T.clo[a];
             if (extent <= 1e-12f) continue;
-            const BinAcc* B = &taskBins[a * kBins];
+            const BinAcc* B = &bins[((size_t)t * 3 + a) * kBins];
             float sufLo[kBins][3], sufHi[kBins][3];
             int sufN[kBins];
             float accLo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, accHi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
@@ -407,7 +393,7 @@ __device__ void splitTask(const Task T, int t, const BinAcc* taskBins, Split* sp
         for (int k = 0; k < 3; k++) { C[side].lo[k] = C[side].clo[k] = FLT_MAX; C[side].hi[k] = C[side].chi[k] = -FLT_MAX; }
         C[side].count = 0;
     }
-    const BinAcc* B = &taskBins[bestAxis * kBins];
+    const BinAcc* B = &bins[((size_t)t * 3 + bestAxis) * kBins];
     for (int b = 0; b < kBins; b++) {
         if (!B[b].count) continue;
         Task& c = C[b <= bestBin ? 0 : 1];
@@ -754,9 +740,7 @@ cudaError_t buildBvh(const SceneTri* tris, int triCount, cudaStream_t stream, Bu
                 clearBinsKernel<<<clearBlocks, 256, 0, stream>>>(bins, tc, tasks);
                 binKernel<<<blocksFor(n, kBinBlock * kBinPer), kBinBlock, 0, stream>>>(out.order, posTask, cent, out.primLo,
                                                                                         out.primHi, tasks, n, bins, tc);
-                binSmallKernel<<<perTaskBlocks, 256, 0, stream>>>(out.order, cent, out.primLo, out.primHi, tasks, tc,
-                                                                  splits, rawNodes, counters, nc, tasksB, nodeCapacity,
-                                                                  taskCapacity, leafSize);
+                binSmallKernel<<<perTaskBlocks, 256, 0, stream>>>(out.order, cent, out.primLo, out.primHi, tasks, tc, bins);
                 splitKernel<<<splitBlocks, 128, 0, stream>>>(tasks, tc, bins, splits, rawNodes, counters, nc, tasksB,
                                                              nodeCapacity, taskCapacity, leafSize);
                 recordLevelKernel<<<1, 1, 0, stream>>>(counters, levelStartDev + level + 2);
