@@ -242,6 +242,58 @@ __device__ __forceinline__ void accumulateBin(BinAcc* dst, float4 lo, float4 hi,
     atomicMaxFloat(&dst->chi[0], c.x); atomicMaxFloat(&dst->chi[1], c.y); atomicMaxFloat(&dst->chi[2], c.z);
 }
 
+// Floats as integers of the same order (-0 below +0, as the atomics above
+// order them), so warp reductions can use the integer min/max instructions.
+__device__ __forceinline__ int orderedKey(float f) {
+    const int i = __float_as_int(f);
+    return i >= 0 ? i : i ^ 0x7FFFFFFF;
+}
+__device__ __forceinline__ float keyFloat(int k) { return __int_as_float(k >= 0 ? k : k ^ 0x7FFFFFFF); }
+
+// accumulateBin for a whole warp (every lane calls it; dst null: no
+// primitive). Spatially coherent primitives put most of a warp's lanes into
+// one bin, where per-lane atomics would serialise on one address: the lanes
+// of the first two destinations are reduced with warp instructions and
+// their leaders add the results; the lanes left over use per-lane atomics.
+// Counts and minima/maxima do not depend on the order of accumulation.
+__device__ void warpAccumulate(BinAcc* dst, float4 lo, float4 hi, float4 c) {
+    const unsigned full = 0xFFFFFFFFu;
+    const int lane = threadIdx.x & 31;
+    unsigned pending = __ballot_sync(full, dst != nullptr);
+    for (int round = 0; round < 2 && pending; round++) {
+        const int leader = __ffs(pending) - 1;
+        BinAcc* first = reinterpret_cast<BinAcc*>(__shfl_sync(full, reinterpret_cast<unsigned long long>(dst), leader));
+        const bool mine = dst != nullptr && dst == first;
+        const unsigned group = __ballot_sync(full, mine);
+        const int kMin = 0x7FFFFFFF, kMax = (int)0x80000000;
+        const int l0 = __reduce_min_sync(full, mine ? orderedKey(lo.x) : kMin);
+        const int l1 = __reduce_min_sync(full, mine ? orderedKey(lo.y) : kMin);
+        const int l2 = __reduce_min_sync(full, mine ? orderedKey(lo.z) : kMin);
+        const int h0 = __reduce_max_sync(full, mine ? orderedKey(hi.x) : kMax);
+        const int h1 = __reduce_max_sync(full, mine ? orderedKey(hi.y) : kMax);
+        const int h2 = __reduce_max_sync(full, mine ? orderedKey(hi.z) : kMax);
+        const int c0 = __reduce_min_sync(full, mine ? orderedKey(c.x) : kMin);
+        const int c1 = __reduce_min_sync(full, mine ? orderedKey(c.y) : kMin);
+        const int c2 = __reduce_min_sync(full, mine ? orderedKey(c.z) : kMin);
+        const int d0 = __reduce_max_sync(full, mine ? orderedKey(c.x) : kMax);
+        const int d1 = __reduce_max_sync(full, mine ? orderedKey(c.y) : kMax);
+        const int d2 = __reduce_max_sync(full, mine ? orderedKey(c.z) : kMax);
+        if (lane == leader) {
+            atomicAdd(&first->count, (unsigned)__popc(group));
+            atomicMinFloat(&first->lo[0], keyFloat(l0)); atomicMinFloat(&first->lo[1], keyFloat(l1));
+            atomicMinFloat(&first->lo[2], keyFloat(l2));
+            atomicMaxFloat(&first->hi[0], keyFloat(h0)); atomicMaxFloat(&first->hi[1], keyFloat(h1));
+            atomicMaxFloat(&first->hi[2], keyFloat(h2));
+            atomicMinFloat(&first->clo[0], keyFloat(c0)); atomicMinFloat(&first->clo[1], keyFloat(c1));
+            atomicMinFloat(&first->clo[2], keyFloat(c2));
+            atomicMaxFloat(&first->chi[0], keyFloat(d0)); atomicMaxFloat(&first->chi[1], keyFloat(d1));
+            atomicMaxFloat(&first->chi[2], keyFloat(d2));
+        }
+        pending &= ~group;
+    }
+    if ((pending >> lane) & 1u) accumulateBin(dst, lo, hi, c);
+}
+
 // Bins every primitive of every open task. The task owning the first position
 // of a block's chunk is aggregated in shared memory; others go to global bins.
 __global__ void __launch_bounds__(kBinBlock) binKernel(const int* order, const int* posTask, const float4* cent,
@@ -259,23 +311,31 @@ __global__ void __launch_bounds__(kBinBlock) binKernel(const int* order, const i
     }
     __syncthreads();
     int st = sTask;
+    // Every lane walks all kBinPer positions (warpAccumulate needs the whole
+    // warp); positions past the end or of finished or small tasks add nothing.
     for (int k = 0; k < kBinPer; k++) {
-        int j = base + k * kBinBlock + threadIdx.x;
-        if (j >= nPos) break;
-        int t = posTask[j];
-        if (t < 0) continue;
-        const Task& T = tasks[t];
-        if (T.count <= kSmallTask) continue;  // binned by binSmallKernel
-        int prim = order[j];
-        float4 c = cent[prim], lo = plo[prim], hi = phi[prim];
+        const int j = base + k * kBinBlock + threadIdx.x;
+        const int t = j < nPos ? posTask[j] : -1;
+        const Task* T = t >= 0 ? &tasks[t] : nullptr;
+        const bool valid = T && T->count > kSmallTask;  // small tasks: binned by binSmallKernel
+        float4 c = make_float4(0, 0, 0, 0), lo = c, hi = c;
+        if (valid) {
+            const int prim = order[j];
+            c = cent[prim]; lo = plo[prim]; hi = phi[prim];
+        }
+        if (!__any_sync(0xFFFFFFFFu, valid)) continue;
         for (int a = 0; a < 3; a++) {
-            float extent = T.chi[a] - T.clo[a];
-            if (extent <= 1e-12f) continue;
-            float s = kBins / extent;
-            float ca = a == 0 ? c.x : (a == 1 ? c.y : c.z);
-            int b = binOf(ca, T.clo[a], s);
-            BinAcc* dst = t == st ? &sb[a * kBins + b] : &bins[((size_t)t * 3 + a) * kBins + b];
-            accumulateBin(dst, lo, hi, c);
+            BinAcc* dst = nullptr;
+            if (valid) {
+                const float extent = T->chi[a] - T->clo[a];
+                if (extent > 1e-12f) {
+                    const float s = kBins / extent;
+                    const float ca = a == 0 ? c.x : (a == 1 ? c.y : c.z);
+                    const int b = binOf(ca, T->clo[a], s);
+                    dst = t == st ? &sb[a * kBins + b] : &bins[((size_t)t * 3 + a) * kBins + b];
+                }
+            }
+            warpAccumulate(dst, lo, hi, c);
         }
     }
     __syncthreads();
@@ -306,6 +366,8 @@ __device__ void binSmallTask(const int* order, const float4* cent, const float4*
         float extent = T.chi[a] - T.clo[a];
         scale[a] = extent <= 1e-12f ? 0.0f : kBins / extent;
     }
+    // Per-lane atomics: small tasks are deep in the tree, where a warp's
+    // primitives spread over the bins (warpAccumulate measured slower here).
     for (int j = T.first + lane; j < T.first + T.count; j += 32) {
         const int prim = order[j];
         const float4 c = cent[prim], lo = plo[prim], hi = phi[prim];
@@ -335,26 +397,23 @@ __global__ void __launch_bounds__(256) binSmallKernel(const int* order, const fl
 }
 
 // One thread per open task: the reference's SAH sweep, then node records.
+// The counters every task updates (maximum depth, node and task allocation)
+// are aggregated per warp first: one atomic per warp instead of one per
+// task on a single address, which serialised the deep levels (hundreds of
+// thousands of tasks). Node and task numbers within a level are assigned in
+// lane order instead of atomic order; nodes are renumbered to the
+// reference's order after the build, and tasks carry their own ranges.
 // taskCount: this level's counts; nextCount: the next level's (open tasks,
-// tasks above kSmallTask); levelStart: receives the node count once this
-// level's nodes are allocated (the first node of the next depth).
-__device__ void splitTask(const Task T, int t, const BinAcc* bins, Split* splits, BinNode* nodes, int* counters,
-                          int* nextCount, Task* nextTasks, int nodeCapacity, int taskCapacity, int leafSize);
-__global__ void splitKernel(const Task* tasks, const int* taskCount, const BinAcc* bins, Split* splits, BinNode* nodes,
-                            int* counters /*0 nodes,2 max depth,3 error*/, int* nextCount, Task* nextTasks,
-                            int nodeCapacity, int taskCapacity, int leafSize) {
-    const int nTasks = taskCount[0];
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nTasks; t += gridDim.x * blockDim.x)
-        splitTask(tasks[t], t, bins, splits, nodes, counters, nextCount, nextTasks, nodeCapacity, taskCapacity,
-                  leafSize);
-}
-__device__ void splitTask(const Task T, int t, const BinAcc* bins, Split* splits, BinNode* nodes, int* counters,
-                          int* nextCount, Task* nextTasks, int nodeCapacity, int taskCapacity, int leafSize) {
-    atomicMax(&counters[2], T.depth);
+// tasks above kSmallTask); counters: 0 nodes, 2 maximum depth, 3 error.
+__device__ void splitTask(bool have, const Task& T, int t, const BinAcc* bins, Split* splits, BinNode* nodes,
+                          int* counters, int* nextCount, Task* nextTasks, int nodeCapacity, int taskCapacity,
+                          int leafSize) {
+    const unsigned full = 0xFFFFFFFFu;
+    const int lane = threadIdx.x & 31;
     int bestAxis = -1, bestBin = -1;
-    float nodeArea = halfArea(T.lo, T.hi);
-    float bestCost = nodeArea * T.count;
-    if (T.count > leafSize && T.depth != kBinaryMaxDepth) {
+    if (have && T.count > leafSize && T.depth != kBinaryMaxDepth) {
+        const float nodeArea = halfArea(T.lo, T.hi);
+        float bestCost = nodeArea * T.count;
         for (int a = 0; a < 3; a++) {
             float extent = T.chi[a] - T.clo[a];
             if (extent <= 1e-12f) continue;
@@ -380,49 +439,89 @@ __device__ void splitTask(const Task T, int t, const BinAcc* bins, Split* splits
             }
         }
     }
+    const bool split = bestAxis >= 0;
+    // Children's boxes, centroid boxes and counts are unions over the bins.
+    Task C[2];
+    bool open[2] = {false, false};
+    if (split) {
+        for (int side = 0; side < 2; side++) {
+            for (int k = 0; k < 3; k++) { C[side].lo[k] = C[side].clo[k] = FLT_MAX; C[side].hi[k] = C[side].chi[k] = -FLT_MAX; }
+            C[side].count = 0;
+        }
+        const BinAcc* B = &bins[((size_t)t * 3 + bestAxis) * kBins];
+        for (int b = 0; b < kBins; b++) {
+            if (!B[b].count) continue;
+            Task& c = C[b <= bestBin ? 0 : 1];
+            growBox(c.lo, c.hi, B[b].lo, B[b].hi);
+            growBox(c.clo, c.chi, B[b].clo, B[b].chi);
+            c.count += (int)B[b].count;
+        }
+        for (int side = 0; side < 2; side++) {
+            C[side].depth = T.depth + 1;
+            open[side] = !(C[side].count <= leafSize || C[side].depth == kBinaryMaxDepth);
+        }
+    }
+    // Maximum depth: a task's own, its children's when it splits.
+    const int depth = __reduce_max_sync(full, have ? T.depth + (split ? 1 : 0) : -1);
+    if (lane == 0 && depth >= 0) atomicMax(&counters[2], depth);
+    // Two nodes per split task.
+    const unsigned splitMask = __ballot_sync(full, split);
+    const unsigned below = (1u << lane) - 1u;
+    int childBase = 0;
+    if (lane == 0 && splitMask) childBase = atomicAdd(&counters[0], 2 * __popc(splitMask));
+    childBase = __shfl_sync(full, childBase, 0);
+    // Next-level tasks: the open children, side 0 before side 1.
+    const unsigned open0 = __ballot_sync(full, open[0]), open1 = __ballot_sync(full, open[1]);
+    const unsigned big0 = __ballot_sync(full, open[0] && C[0].count > kSmallTask);
+    const unsigned big1 = __ballot_sync(full, open[1] && C[1].count > kSmallTask);
+    int taskBase = 0;
+    if (lane == 0 && (open0 | open1)) taskBase = atomicAdd(&nextCount[0], __popc(open0) + __popc(open1));
+    if (lane == 0 && (big0 | big1)) atomicAdd(&nextCount[1], __popc(big0) + __popc(big1));
+    taskBase = __shfl_sync(full, taskBase, 0);
+    if (!have) return;
+
     Split S;
     S.axis = bestAxis; S.bin = bestBin; S.leftCount = 0; S.childTask[0] = S.childTask[1] = -1;
-    if (bestAxis < 0) {
+    if (!split) {
         nodes[T.node] = BinNode{v3(T.lo[0], T.lo[1], T.lo[2]), T.first, v3(T.hi[0], T.hi[1], T.hi[2]), T.count};
         splits[t] = S;
         return;
     }
-    // Children's boxes, centroid boxes and counts are unions over the bins.
-    Task C[2];
-    for (int side = 0; side < 2; side++) {
-        for (int k = 0; k < 3; k++) { C[side].lo[k] = C[side].clo[k] = FLT_MAX; C[side].hi[k] = C[side].chi[k] = -FLT_MAX; }
-        C[side].count = 0;
-    }
-    const BinAcc* B = &bins[((size_t)t * 3 + bestAxis) * kBins];
-    for (int b = 0; b < kBins; b++) {
-        if (!B[b].count) continue;
-        Task& c = C[b <= bestBin ? 0 : 1];
-        growBox(c.lo, c.hi, B[b].lo, B[b].hi);
-        growBox(c.clo, c.chi, B[b].clo, B[b].chi);
-        c.count += (int)B[b].count;
-    }
-    int child = atomicAdd(&counters[0], 2);
+    const int child = childBase + 2 * __popc(splitMask & below);
     if (child + 2 > nodeCapacity) { atomicExch(&counters[3], 1); splits[t] = Split{-1, -1, 0, {-1, -1}}; return; }
     nodes[T.node] = BinNode{v3(T.lo[0], T.lo[1], T.lo[2]), child, v3(T.hi[0], T.hi[1], T.hi[2]), 0};
     C[0].first = T.first;
     C[1].first = T.first + C[0].count;
     S.leftCount = C[0].count;
+    int k = taskBase + __popc(open0 & below) + __popc(open1 & below);
     for (int side = 0; side < 2; side++) {
         Task& c = C[side];
         c.node = child + side;
-        c.depth = T.depth + 1;
-        atomicMax(&counters[2], c.depth);
-        if (c.count <= leafSize || c.depth == kBinaryMaxDepth) {
+        if (!open[side]) {
             nodes[c.node] = BinNode{v3(c.lo[0], c.lo[1], c.lo[2]), c.first, v3(c.hi[0], c.hi[1], c.hi[2]), c.count};
-        } else {
-            int k = atomicAdd(&nextCount[0], 1);
-            if (k >= taskCapacity) { atomicExch(&counters[3], 2); continue; }
-            if (c.count > kSmallTask) atomicAdd(&nextCount[1], 1);
-            nextTasks[k] = c;
-            S.childTask[side] = k;
+            continue;
         }
+        if (k >= taskCapacity) { atomicExch(&counters[3], 2); k++; continue; }
+        nextTasks[k] = c;
+        S.childTask[side] = k;
+        k++;
     }
     splits[t] = S;
+}
+__global__ void splitKernel(const Task* tasks, const int* taskCount, const BinAcc* bins, Split* splits, BinNode* nodes,
+                            int* counters, int* nextCount, Task* nextTasks, int nodeCapacity, int taskCapacity,
+                            int leafSize) {
+    const int nTasks = taskCount[0];
+    // Whole warps walk the tasks (splitTask uses warp collectives).
+    for (int base = blockIdx.x * blockDim.x; base < nTasks; base += gridDim.x * blockDim.x) {
+        const int t = base + (int)threadIdx.x;
+        const bool have = t < nTasks;
+        Task T;
+        if (have) T = tasks[t];
+        else T.count = 0, T.depth = 0;
+        splitTask(have, T, t, bins, splits, nodes, counters, nextCount, nextTasks, nodeCapacity, taskCapacity,
+                  leafSize);
+    }
 }
 
 __global__ void flagKernel(const int* order, const int* posTask, const float4* cent, const Task* tasks,
@@ -571,10 +670,40 @@ __global__ void collapseKernel(const BinNode* bn, const int* order, const float4
                                const SceneTri* tris, const Job* jobs, const int* jobCount, Job* nextJobs,
                                int* nextCount, WideNode* wide, float4* packed, int* counters, int wideCapacity,
                                int jobCapacity, int triCapacity, int group, int width, const int* primTri) {
+    // Whole warps walk the jobs: each plans its node, then the warp's wide
+    // children, packed triangles and next-level jobs are allocated with one
+    // atomic each (in lane order) instead of one per job on a single address.
     const int nJobs = *jobCount;
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nJobs; j += gridDim.x * blockDim.x)
-        collapseJob(jobs[j], bn, order, plo, phi, tris, nextJobs, wide, packed, counters, wideCapacity, jobCapacity,
-                    triCapacity, group, width, primTri, nextCount);
+    const unsigned full = 0xFFFFFFFFu;
+    const int lane = threadIdx.x & 31;
+    for (int base = blockIdx.x * blockDim.x; base < nJobs; base += gridDim.x * blockDim.x) {
+        const int j = base + (int)threadIdx.x;
+        const bool have = j < nJobs;
+        CollapsePlan P;
+        int ni = 0, nt = 0;
+        if (have) {
+            planCollapse(jobs[j], bn, order, plo, phi, group, width, primTri, P);
+            ni = P.nInterior;
+            nt = P.nTris;
+        }
+        int si = ni, st = nt;  // inclusive prefix sums over the warp
+        for (int off = 1; off < 32; off <<= 1) {
+            const int a = __shfl_up_sync(full, si, off), b = __shfl_up_sync(full, st, off);
+            if (lane >= off) { si += a; st += b; }
+        }
+        const int ti = __shfl_sync(full, si, 31), tt = __shfl_sync(full, st, 31);
+        int childBase = 0, triBase = 0, jobBase = 0;
+        if (lane == 0) {
+            if (ti) { childBase = atomicAdd(&counters[0], ti); jobBase = atomicAdd(nextCount, ti); }
+            if (tt) triBase = atomicAdd(&counters[1], tt);
+        }
+        childBase = __shfl_sync(full, childBase, 0);
+        triBase = __shfl_sync(full, triBase, 0);
+        jobBase = __shfl_sync(full, jobBase, 0);
+        if (have)
+            emitCollapse(P, childBase + si - ni, triBase + st - nt, jobBase + si - ni, tris, nextJobs, wide, packed,
+                         counters, wideCapacity, jobCapacity, triCapacity);
+    }
 }
 
 inline int blocksFor(long long n, int block) { return (int)((n + block - 1) / block); }

@@ -49,21 +49,27 @@ RT_HD int slotsOf(const BinNode& n, int group, int width) {
     return n.count <= width * group ? (n.count + group - 1) / group : 1;
 }
 
-// Builds wide node J.wide for one job: chooses up to eight children, assigns
-// slots, quantises child boxes, packs leaf triangles and emits jobs for the
-// interior children. counters: [0] wide nodes, [1] packed triangles,
-// [2] next-level jobs, [3] error code. Host and device (atomics through
-// portableAdd), so the collapse can be checked on the CPU. width (4 or 8):
-// most children per node; the node format keeps eight slots either way.
-// primTri: the triangle of each primitive when primitives are triangle pieces
-// (null: primitive p is triangle p). nextCount, when set, counts the
-// next-level jobs in place of counters[2].
-RT_HD void collapseJob(Job J, const BinNode* bn, const int* order, const float4* plo, const float4* phi,
-                       const SceneTri* tris, Job* nextJobs, WideNode* wide, float4* packed, int* counters,
-                       int wideCapacity, int jobCapacity, int triCapacity, int group, int width = 8,
-                       const int* primTri = nullptr, int* nextCount = nullptr) {
-    if (J.kind == 0 && bn[J.node].count > 0) { J.kind = 1; J.first = bn[J.node].first; J.count = bn[J.node].count; }
+// A job's wide node before its storage is allocated: the children, their
+// slots and boxes, and the triangles of each triangle group.
+struct CollapsePlan {
     Kid kids[8];
+    int nk, wide;
+    int slotKid[8];
+    int groupTris[8][3], groupCount[8];
+    int nInterior, nTris;  // wide children (= next-level jobs) and packed triangles
+    float nlo[3], nhi[3];
+};
+
+// Chooses up to eight children of job J's wide node, their boxes and slots,
+// and the triangles of its triangle groups. width (4 or 8): most children
+// per node; the node format keeps eight slots either way. primTri: the
+// triangle of each primitive when primitives are triangle pieces (null:
+// primitive p is triangle p).
+RT_HD void planCollapse(Job J, const BinNode* bn, const int* order, const float4* plo, const float4* phi, int group,
+                        int width, const int* primTri, CollapsePlan& P) {
+    if (J.kind == 0 && bn[J.node].count > 0) { J.kind = 1; J.first = bn[J.node].first; J.count = bn[J.node].count; }
+    P.wide = J.wide;
+    Kid* kids = P.kids;
     int nk = 0;
     if (J.kind == 0) {
         int cand[8], nc = 2;
@@ -139,7 +145,8 @@ RT_HD void collapseJob(Job J, const BinNode* bn, const int* order, const float4*
     }
     // Slot assignment: slot s holds the kid met first by rays whose direction
     // signs are s (bit 2 = x negative, bit 1 = y, bit 0 = z).
-    int slotKid[8] = {-1, -1, -1, -1, -1, -1, -1, -1};
+    int* slotKid = P.slotKid;
+    for (int s = 0; s < 8; s++) slotKid[s] = -1;
     {
         float cn[3], ck[8][3];
         for (int a = 0; a < 3; a++) cn[a] = 0.5f * (nlo[a] + nhi[a]);
@@ -165,7 +172,8 @@ RT_HD void collapseJob(Job J, const BinNode* bn, const int* order, const float4*
     }
     // Triangles of each triangle group, once each: pieces of one triangle in
     // the same group would only repeat its test (the group's box covers them).
-    int groupTris[8][3], groupCount[8];
+    int (*groupTris)[3] = P.groupTris;
+    int* groupCount = P.groupCount;
     int nInterior = 0, nTris = 0;
     for (int k = 0; k < nk; k++) {
         groupCount[k] = 0;
@@ -179,9 +187,26 @@ RT_HD void collapseJob(Job J, const BinNode* bn, const int* order, const float4*
         }
         nTris += groupCount[k];
     }
-    int childBase = nInterior ? portableAdd(&counters[0], nInterior) : 0;
-    int triBase = nTris ? portableAdd(&counters[1], nTris) : 0;
-    if (childBase + nInterior > wideCapacity || triBase + nTris > triCapacity) { portableSet(&counters[3], 3); return; }
+    P.nk = nk;
+    P.nInterior = nInterior;
+    P.nTris = nTris;
+    for (int a = 0; a < 3; a++) { P.nlo[a] = nlo[a]; P.nhi[a] = nhi[a]; }
+}
+
+// Writes a planned wide node whose storage has been allocated: wide children
+// from childBase, packed triangles from triBase, next-level jobs from
+// jobBase (nInterior of each). counters[3] receives an error code when an
+// allocation passes its capacity.
+RT_HD void emitCollapse(const CollapsePlan& P, int childBase, int triBase, int jobBase, const SceneTri* tris,
+                        Job* nextJobs, WideNode* wide, float4* packed, int* counters, int wideCapacity,
+                        int jobCapacity, int triCapacity) {
+    const Kid* kids = P.kids;
+    const int* slotKid = P.slotKid;
+    const int (*groupTris)[3] = P.groupTris;
+    const int* groupCount = P.groupCount;
+    const float* nlo = P.nlo;
+    const float* nhi = P.nhi;
+    if (childBase + P.nInterior > wideCapacity || triBase + P.nTris > triCapacity) { portableSet(&counters[3], 3); return; }
     WideNode W;
     W.px = nlo[0]; W.py = nlo[1]; W.pz = nlo[2];
     float sc[3];
@@ -233,13 +258,32 @@ RT_HD void collapseJob(Job J, const BinNode* bn, const int* order, const float4*
         } else {
             W.meta[s] = (unsigned char)(0x20u | (24u + (unsigned)s));
             W.imask |= (unsigned char)(1u << s);
-            int q = portableAdd(nextCount ? nextCount : &counters[2], 1);
-            if (q >= jobCapacity) { portableSet(&counters[3], 4); continue; }
+            const int q = jobBase + interiorSeen;
+            if (q >= jobCapacity) { portableSet(&counters[3], 4); interiorSeen++; continue; }
             nextJobs[q] = Job{K.kind == 0 ? 0 : 1, K.node, K.first, K.count, childBase + interiorSeen};
             interiorSeen++;
         }
     }
-    wide[J.wide] = W;
+    wide[P.wide] = W;
+}
+
+// Builds wide node J.wide for one job: planCollapse, then allocation of its
+// wide children, packed triangles and next-level jobs, then emitCollapse.
+// counters: [0] wide nodes, [1] packed triangles, [2] next-level jobs,
+// [3] error code. Host and device (atomics through portableAdd), so the
+// collapse can be checked on the CPU. nextCount, when set, counts the
+// next-level jobs in place of counters[2].
+RT_HD void collapseJob(Job J, const BinNode* bn, const int* order, const float4* plo, const float4* phi,
+                       const SceneTri* tris, Job* nextJobs, WideNode* wide, float4* packed, int* counters,
+                       int wideCapacity, int jobCapacity, int triCapacity, int group, int width = 8,
+                       const int* primTri = nullptr, int* nextCount = nullptr) {
+    CollapsePlan P;
+    planCollapse(J, bn, order, plo, phi, group, width, primTri, P);
+    const int childBase = P.nInterior ? portableAdd(&counters[0], P.nInterior) : 0;
+    const int triBase = P.nTris ? portableAdd(&counters[1], P.nTris) : 0;
+    const int jobBase = P.nInterior ? portableAdd(nextCount ? nextCount : &counters[2], P.nInterior) : 0;
+    emitCollapse(P, childBase, triBase, jobBase, tris, nextJobs, wide, packed, counters, wideCapacity, jobCapacity,
+                 triCapacity);
 }
 
 }  // namespace rt

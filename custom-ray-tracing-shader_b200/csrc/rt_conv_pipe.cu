@@ -21,6 +21,10 @@
 //              taps x cin/16 tcgen05.mma into one of two accumulators; a
 //              commit tells the epilogue the accumulator is full and another
 //              frees the ring slot of the row no later tile reads.
+//              The A operand stays in shared memory: with A in tensor
+//              memory (tcgen05.cp of each row's three shifted copies) an
+//              MMA of 128 x N x 16 measured ~85 SM cycles against ~42 from
+//              shared memory.
 //   warps 2-5  epilogue: tcgen05.ld of the accumulator (warp w reads lanes
 //              32 (w % 4) ...), which is then handed back to the issuer,
 //              bias, ReLU and the store (BF16, or FP32 added to or written).
@@ -307,10 +311,10 @@ __global__ void __launch_bounds__(kThreads) convPipeKernel(const __grid_constant
         // A row is expanded at most one row behind the last one issued (the
         // two staging buffers), and before the producer would block on a
         // slot: a slot may be waiting for exactly that expansion.
-        long long q = 0, expanded = 0;
+        int q = 0, expanded = 0;
         uint64_t waitSlotNs = 0, waitLowNs = 0;
         bool ok = true;
-        auto expand = [&](long long e) -> bool {
+        auto expand = [&](int e) -> bool {
             const uint64_t t1 = a.stats ? nowNs() : 0;
             if (!waitPhaseWarp(base + Header::lowFull + 8 * (int)(e & 1), (uint32_t)((e >> 1) & 1), abortFlag, limit))
                 return false;
@@ -331,7 +335,7 @@ __global__ void __launch_bounds__(kThreads) convPipeKernel(const __grid_constant
         for (int u = firstUnit; u < a.units && ok; u += unitStride) {
             const Unit U = unitOf(a, u);
             for (int r = U.y0 - 1; r <= U.y1 && ok; r++) {
-                const int s = (int)(q % R);
+                const int s = q % R;
                 const uint32_t emptyBar = base + Header::empty + 8 * s, emptyParity = (uint32_t)(((q / R) & 1) ^ 1);
                 if (Glow && expanded < q) {
                     const bool freeNow = __shfl_sync(0xFFFFFFFFu, lane == 0 ? (barTestWait(emptyBar, emptyParity) ? 1 : 0) : 0, 0) != 0;
@@ -382,9 +386,9 @@ __global__ void __launch_bounds__(kThreads) convPipeKernel(const __grid_constant
         if (!ok) *abortFlag = 1;
         if (lane == 0) {
             pollPhase(base + Header::weights, 0u, limit);
-            for (long long e = q > 2 ? q - 2 : 0; e < q && Glow; e++)
+            for (int e = q > 2 ? q - 2 : 0; e < q && Glow; e++)
                 pollPhase(base + Header::lowFull + 8 * (int)(e & 1), (uint32_t)((e >> 1) & 1), limit);
-            for (long long e = q > R ? q - R : 0; e < q; e++) {
+            for (int e = q > R ? q - R : 0; e < q; e++) {
                 if (Glow && e >= expanded) barArrive(base + Header::full + 8 * (int)(e % R));
                 pollPhase(base + Header::full + 8 * (int)(e % R), (uint32_t)((e / R) & 1), limit);
             }
@@ -393,60 +397,84 @@ __global__ void __launch_bounds__(kThreads) convPipeKernel(const __grid_constant
         __syncwarp();
     } else if (warp == 1) {
         // ---- MMA issuer ----
+        // The issue rate of one thread bounds the tensor pipe here (an MMA of
+        // 128 x COUT x 16 takes ~42 SM cycles; a single issuer that computes
+        // descriptors with divisions per MMA issues one per ~100), so the
+        // loop keeps ring positions as running 32-bit counters, makes the
+        // three row descriptors once per tile and steps descriptors by
+        // constants.
         bool ok = true;
         if (lane == 0) {
             const uint32_t idesc = ummaInstrDescBf16(kM, COUT);
             if (a.probe) ok = waitPhase(base + Header::probe, 0u, abortFlag, limit);
             if (ok) ok = waitPhase(base + Header::weights, 0u, abortFlag, limit);
-            long long q = 0, tile = 0;
             uint64_t waitRowNs = 0, waitAccNs = 0;
             const uint32_t kStepA = (2u * kPlane) >> 4, kStepB = (2u * COUT * 16u) >> 4;
+            const uint32_t tapStepB = ((uint32_t)G * COUT * 16u) >> 4;
+            const uint64_t wDesc = ummaSmemDesc(wAddr, COUT * 16u, 128u);
+            const int G2 = G / 2;
+            int rows = 0, tiles = 0;           // rows waited for, tiles issued
+            int waitSlot = 0, relSlot = 0;     // next row to wait for / to release
+            uint32_t waitParity = 0;
+            int accB = 0;
+            uint32_t accParity = 0;
+            auto nextRow = [&](int& slot) -> bool {
+                const uint64_t t1 = a.stats ? nowNs() : 0;
+                slot = waitSlot;
+                const bool got = waitPhase(base + Header::full + 8 * waitSlot, waitParity, abortFlag, limit);
+                if (a.stats) waitRowNs += nowNs() - t1;
+                if (++waitSlot == R) { waitSlot = 0; waitParity ^= 1u; }
+                rows++;
+                return got;
+            };
+            auto release = [&]() {
+                commit(base + Header::empty + 8 * relSlot);
+                if (++relSlot == R) relSlot = 0;
+            };
             for (int u = firstUnit; u < a.units && ok; u += unitStride) {
                 const Unit U = unitOf(a, u);
-                const long long q0 = q;  // row U.y0 - 1
-                for (int y = U.y0; y < U.y1 && ok; y++, tile++) {
-                    const long long qr = q0 + (y - U.y0);  // row y - 1
+                int s0 = 0, s1 = 0, s2 = 0;  // slots of rows y - 1, y, y + 1
+                ok = nextRow(s0) && nextRow(s1);
+                for (int y = U.y0; y < U.y1 && ok; y++) {
+                    if (!nextRow(s2)) { ok = false; break; }
                     {
                         const uint64_t t1 = a.stats ? nowNs() : 0;
-                        for (long long e = (y == U.y0 ? qr : qr + 2); e <= qr + 2 && ok; e++)
-                            ok = waitPhase(base + Header::full + 8 * (int)(e % R), (uint32_t)((e / R) & 1), abortFlag, limit);
-                        if (a.stats) waitRowNs += nowNs() - t1;
-                    }
-                    const int b = (int)(tile % a.nAcc);
-                    if (ok) {
-                        const uint64_t t1 = a.stats ? nowNs() : 0;
-                        ok = waitPhase(base + Header::accEmpty + 8 * b, (uint32_t)(((tile / a.nAcc) & 1) ^ 1), abortFlag, limit);
+                        ok = waitPhase(base + Header::accEmpty + 8 * accB, accParity ^ 1u, abortFlag, limit);
                         if (a.stats) waitAccNs += nowNs() - t1;
                     }
                     if (!ok) break;
                     tcFenceAfter();
-                    const uint32_t acc = tmem + (uint32_t)b * a.accCols;
+                    const uint32_t acc = tmem + (uint32_t)accB * a.accCols;
+                    const uint64_t rowDesc[3] = {ummaSmemDesc(ringAddr + (uint32_t)s0 * a.slotBytes, kPlane, 128u),
+                                                 ummaSmemDesc(ringAddr + (uint32_t)s1 * a.slotBytes, kPlane, 128u),
+                                                 ummaSmemDesc(ringAddr + (uint32_t)s2 * a.slotBytes, kPlane, 128u)};
+#pragma unroll
                     for (int t = 0; t < 9; t++) {
-                        const int dy = t / 3, dx = t % 3;
-                        const uint32_t slot = ringAddr + (uint32_t)((qr + dy) % R) * a.slotBytes;
-                        uint64_t aDesc = ummaSmemDesc(slot + (uint32_t)dx * 16u, kPlane, 128u);
-                        uint64_t bDesc = ummaSmemDesc(wAddr + (uint32_t)(t * G * COUT * 16), COUT * 16u, 128u);
-                        for (int k = 0; k < G / 2; k++, aDesc += kStepA, bDesc += kStepB)
+                        // dx pixels = dx * 16 bytes = dx descriptor units.
+                        uint64_t aDesc = rowDesc[t / 3] + (uint64_t)(t % 3);
+                        uint64_t bDesc = wDesc + (uint64_t)t * tapStepB;
+                        for (int k = 0; k < G2; k++, aDesc += kStepA, bDesc += kStepB)
                             mma(acc, aDesc, bDesc, idesc, (t > 0 || k > 0) ? 1u : 0u);
                     }
-                    commit(base + Header::accFull + 8 * b);
-                    commit(base + Header::empty + 8 * (int)(qr % R));  // row y - 1: no later tile reads it
+                    commit(base + Header::accFull + 8 * accB);
+                    release();  // row y - 1: no later tile reads it
+                    s0 = s1;
+                    s1 = s2;
+                    tiles++;
+                    if (++accB == a.nAcc) { accB = 0; accParity ^= 1u; }
                 }
                 if (!ok) break;
-                // Rows y1 - 1 and y1 of the strip are read by no later tile.
-                const long long last = q0 + (U.y1 - U.y0);
-                commit(base + Header::empty + 8 * (int)(last % R));
-                commit(base + Header::empty + 8 * (int)((last + 1) % R));
-                q = last + 2;
+                release();  // rows y1 - 1 and y1 of the strip: no later tile reads them
+                release();
             }
             if (ok) {
                 // The commits' arrivals land after the MMAs complete: wait for
-                // the last ones (the rows released last, the last two
+                // the last ones (the rows released last, the last
                 // accumulators) before the block's shared memory goes away.
-                for (long long e = q > R ? q - R : 0; e < q; e++)
-                    pollPhase(base + Header::empty + 8 * (int)(e % R), (uint32_t)((e / R) & 1), limit);
-                for (long long t = tile > a.nAcc ? tile - a.nAcc : 0; t < tile; t++)
-                    pollPhase(base + Header::accFull + 8 * (int)(t % a.nAcc), (uint32_t)((t / a.nAcc) & 1), limit);
+                for (int e = rows > R ? rows - R : 0; e < rows; e++)
+                    pollPhase(base + Header::empty + 8 * (e % R), (uint32_t)((e / R) & 1), limit);
+                for (int t = tiles > a.nAcc ? tiles - a.nAcc : 0; t < tiles; t++)
+                    pollPhase(base + Header::accFull + 8 * (t % a.nAcc), (uint32_t)((t / a.nAcc) & 1), limit);
             } else {
                 *abortFlag = 1;
                 // Wait (bounded) for every MMA issued so far.
@@ -459,15 +487,15 @@ __global__ void __launch_bounds__(kThreads) convPipeKernel(const __grid_constant
     } else {
         // ---- epilogue: warps 2-5, lanes 32 * (warp % 4) ... of the accumulator ----
         const int quarter = warp & 3;
-        long long tile = 0;
+        int b = 0;
+        uint32_t parity = 0;
         uint64_t waitNs = 0;
         bool ok = true;
         for (int u = firstUnit; u < a.units && ok; u += unitStride) {
             const Unit U = unitOf(a, u);
-            for (int y = U.y0; y < U.y1; y++, tile++) {
-                const int b = (int)(tile % a.nAcc);
+            for (int y = U.y0; y < U.y1; y++, b = b + 1 == a.nAcc ? 0 : b + 1, parity ^= b == 0 ? 1u : 0u) {
                 const uint64_t t1 = a.stats ? nowNs() : 0;
-                if (!waitPhaseWarp(base + Header::accFull + 8 * b, (uint32_t)((tile / a.nAcc) & 1), abortFlag, limit)) { ok = false; break; }
+                if (!waitPhaseWarp(base + Header::accFull + 8 * b, parity, abortFlag, limit)) { ok = false; break; }
                 if (a.stats) waitNs += nowNs() - t1;
                 tcFenceAfter();
                 uint32_t acc[COUT];
