@@ -60,7 +60,7 @@ constexpr uint32_t kPlane = (kHalo * 16 + 127) / 128 * 128;        // 2,176
 constexpr uint32_t kLowPlane = (kLowHalo * 16 + 127) / 128 * 128;  // 1,152
 constexpr int kThreads = 192;
 constexpr int kMinRing = 3;  // the rows a tile reads; 4 and more let the producer run ahead
-constexpr int kMaxRing = 8;
+constexpr int kMaxRing = 16;
 constexpr int kMaxAcc = 8;   // tensor-memory accumulators per block (tiles between the issuer and the epilogue)
 constexpr uint32_t kHeader = 1024;       // barriers and flags
 
@@ -98,8 +98,9 @@ struct Header {
     static constexpr uint32_t drain = weights + 16;
     static constexpr uint32_t tmemSlot = weights + 24;
     static constexpr uint32_t abort = weights + 28;
+    static constexpr uint32_t bias = 576;                  // the block's output channels' biases (<= 96 floats)
 };
-static_assert(Header::abort + 4 <= kHeader, "header size");
+static_assert(Header::abort + 4 <= Header::bias && Header::bias + 96 * 4 <= kHeader, "header size");
 
 __device__ __forceinline__ uint32_t smemAddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ uint64_t nowNs() {
@@ -202,6 +203,44 @@ __device__ __forceinline__ void tmemLoad16(uint32_t taddr, uint32_t (&r)[16]) {
 }
 __device__ __forceinline__ void tmemWaitLoads() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
 
+// One tile's 9 taps x G2 MMAs (K steps of 16 channels), every descriptor a
+// compile-time offset from the three row descriptors and the weights'. The
+// K count must be a compile-time constant: with a runtime inner loop one
+// thread issued an MMA per ~155 SM cycles, fully unrolled per ~60 (the tensor
+// pipe itself takes ~42 per 128 x N x 16 with N <= 64).
+template <int COUT, int G2>
+__device__ __forceinline__ void issueTile(uint32_t acc, const uint64_t (&rowDesc)[3], uint64_t wDesc, uint32_t idesc) {
+#pragma unroll
+    for (int t = 0; t < 9; t++) {
+#pragma unroll
+        for (int k = 0; k < G2; k++) {
+            const uint64_t aDesc = rowDesc[t / 3] + (uint64_t)(t % 3) + (uint64_t)k * ((2u * kPlane) >> 4);
+            const uint64_t bDesc = wDesc + (uint64_t)(((t * 2 * G2 + 2 * k) * COUT * 16) >> 4);
+            mma(acc, aDesc, bDesc, idesc, (t > 0 || k > 0) ? 1u : 0u);
+        }
+    }
+}
+template <int COUT>
+__device__ __forceinline__ void issueTileG(int G2, uint32_t acc, const uint64_t (&rowDesc)[3], uint64_t wDesc,
+                                           uint32_t idesc) {
+    switch (G2) {
+        case 1: issueTile<COUT, 1>(acc, rowDesc, wDesc, idesc); break;
+        case 2: issueTile<COUT, 2>(acc, rowDesc, wDesc, idesc); break;
+        case 3: issueTile<COUT, 3>(acc, rowDesc, wDesc, idesc); break;
+        case 4: issueTile<COUT, 4>(acc, rowDesc, wDesc, idesc); break;
+        case 5: issueTile<COUT, 5>(acc, rowDesc, wDesc, idesc); break;
+        case 6: issueTile<COUT, 6>(acc, rowDesc, wDesc, idesc); break;
+        case 7: issueTile<COUT, 7>(acc, rowDesc, wDesc, idesc); break;
+        case 8: issueTile<COUT, 8>(acc, rowDesc, wDesc, idesc); break;
+        case 9: issueTile<COUT, 9>(acc, rowDesc, wDesc, idesc); break;
+        case 10: issueTile<COUT, 10>(acc, rowDesc, wDesc, idesc); break;
+        case 11: issueTile<COUT, 11>(acc, rowDesc, wDesc, idesc); break;
+        case 12: issueTile<COUT, 12>(acc, rowDesc, wDesc, idesc); break;
+        case 13: issueTile<COUT, 13>(acc, rowDesc, wDesc, idesc); break;
+        default: issueTile<COUT, 14>(acc, rowDesc, wDesc, idesc); break;  // cin <= 224 (convPipeSupported)
+    }
+}
+
 // Unit u: image, column tile and strip of rows [y0, y1).
 struct Unit { int img, x0, y0, y1; };
 __device__ __forceinline__ Unit unitOf(const PipeArgs& a, int u) {
@@ -211,11 +250,12 @@ __device__ __forceinline__ Unit unitOf(const PipeArgs& a, int u) {
 }
 
 template <int COUT>
-__device__ __forceinline__ void epilogueStore(const PipeArgs& a, const uint32_t (&acc)[COUT], size_t pix, int nBase) {
+__device__ __forceinline__ void epilogueStore(const PipeArgs& a, const uint32_t (&acc)[COUT], size_t pix, int nBase,
+                                              const float* bias) {
     float v[COUT];
 #pragma unroll
     for (int j = 0; j < COUT; j++) {
-        const float s = __uint_as_float(acc[j]) + (a.bias ? __ldg(a.bias + nBase + j) : 0.0f);
+        const float s = __uint_as_float(acc[j]) + bias[j];  // shared memory: one broadcast read
         v[j] = a.relu ? fmaxf(s, 0.0f) : s;
     }
     if (a.outF) {
@@ -245,7 +285,7 @@ __device__ __forceinline__ void epilogueStore(const PipeArgs& a, const uint32_t 
 }
 
 template <int COUT>
-__global__ void __launch_bounds__(kThreads) convPipeKernel(const __grid_constant__ CUtensorMap inMap,
+__global__ void __launch_bounds__(kThreads, COUT <= 48 ? 4 : 2) convPipeKernel(const __grid_constant__ CUtensorMap inMap,
                                                           const __grid_constant__ CUtensorMap lowMap,
                                                           const __grid_constant__ CUtensorMap wMap, PipeArgs a) {
     extern __shared__ __align__(1024) unsigned char smem[];
@@ -282,6 +322,8 @@ __global__ void __launch_bounds__(kThreads) convPipeKernel(const __grid_constant
         *abortFlag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
+    float* sBias = reinterpret_cast<float*>(smem + Header::bias);
+    if (threadIdx.x < COUT) sBias[threadIdx.x] = a.bias ? a.bias[nBase + threadIdx.x] : 0.0f;
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(base + Header::tmemSlot),
                      "r"(a.tmemCols)
@@ -409,8 +451,6 @@ __global__ void __launch_bounds__(kThreads) convPipeKernel(const __grid_constant
             if (a.probe) ok = waitPhase(base + Header::probe, 0u, abortFlag, limit);
             if (ok) ok = waitPhase(base + Header::weights, 0u, abortFlag, limit);
             uint64_t waitRowNs = 0, waitAccNs = 0;
-            const uint32_t kStepA = (2u * kPlane) >> 4, kStepB = (2u * COUT * 16u) >> 4;
-            const uint32_t tapStepB = ((uint32_t)G * COUT * 16u) >> 4;
             const uint64_t wDesc = ummaSmemDesc(wAddr, COUT * 16u, 128u);
             const int G2 = G / 2;
             int rows = 0, tiles = 0;           // rows waited for, tiles issued
@@ -448,14 +488,7 @@ __global__ void __launch_bounds__(kThreads) convPipeKernel(const __grid_constant
                     const uint64_t rowDesc[3] = {ummaSmemDesc(ringAddr + (uint32_t)s0 * a.slotBytes, kPlane, 128u),
                                                  ummaSmemDesc(ringAddr + (uint32_t)s1 * a.slotBytes, kPlane, 128u),
                                                  ummaSmemDesc(ringAddr + (uint32_t)s2 * a.slotBytes, kPlane, 128u)};
-#pragma unroll
-                    for (int t = 0; t < 9; t++) {
-                        // dx pixels = dx * 16 bytes = dx descriptor units.
-                        uint64_t aDesc = rowDesc[t / 3] + (uint64_t)(t % 3);
-                        uint64_t bDesc = wDesc + (uint64_t)t * tapStepB;
-                        for (int k = 0; k < G2; k++, aDesc += kStepA, bDesc += kStepB)
-                            mma(acc, aDesc, bDesc, idesc, (t > 0 || k > 0) ? 1u : 0u);
-                    }
+                    issueTileG<COUT>(G2, acc, rowDesc, wDesc, idesc);
                     commit(base + Header::accFull + 8 * accB);
                     release();  // row y - 1: no later tile reads it
                     s0 = s1;
@@ -512,7 +545,7 @@ __global__ void __launch_bounds__(kThreads) convPipeKernel(const __grid_constant
                 __syncwarp();
                 if (lane == 0) barArrive(base + Header::accEmpty + 8 * b);
                 const int x = U.x0 + quarter * 32 + lane;
-                if (x < a.w) epilogueStore<COUT>(a, acc, ((size_t)U.img * a.h + y) * a.w + x, nBase);
+                if (x < a.w) epilogueStore<COUT>(a, acc, ((size_t)U.img * a.h + y) * a.w + x, nBase, sBias);
             }
         }
         if (a.stats && lane == 0) atomicAdd(a.stats + 4, waitNs);
@@ -599,8 +632,14 @@ int pickSplits(int cin, int cout, int lowChannels) {
 }  // namespace
 
 bool convPipeSupported(int cin, int cout, int lowChannels) {
-    return cin >= 16 && cin % 16 == 0 && lowChannels % 16 == 0 && lowChannels < cin &&
+    return cin >= 16 && cin <= 224 && cin % 16 == 0 && lowChannels % 16 == 0 && lowChannels < cin &&
            pickSplits(cin, cout, lowChannels) > 0;
+}
+
+bool convPipePreferred(int cin, int cout, int lowChannels) {
+    if (!convPipeSupported(cin, cout, lowChannels)) return false;
+    const int s = pickSplits(cin, cout, lowChannels);
+    return convPipeSmemBytes(cin, cout / s, lowChannels, 4) <= 227u * 1024u;
 }
 
 cudaError_t convPipe(const bf16* in, const bf16* low, int lowChannels, int n, int h, int w, int cin,
@@ -663,6 +702,7 @@ cudaError_t convPipe(const bf16* in, const bf16* low, int lowChannels, int n, in
     a.ring = convPipeSmemBytes(cin, cout, lowChannels, 4) <= 227u * 1024u ? 4 : kMinRing;
     int perSm = (int)(smemPerSm / (convPipeSmemBytes(cin, cout, lowChannels, a.ring) + 1024u));
     perSm = std::max(1, std::min({perSm, (int)(512u / a.tmemCols), 2048 / kThreads}));
+    if (test && test->blocksPerSm > 0 && test->blocksPerSm < perSm) perSm = test->blocksPerSm;
     while (a.ring < kMaxRing && (uint32_t)perSm * (convPipeSmemBytes(cin, cout, lowChannels, a.ring + 1) + 1024u) <= smemPerSm &&
            convPipeSmemBytes(cin, cout, lowChannels, a.ring + 1) <= 227u * 1024u)
         a.ring++;

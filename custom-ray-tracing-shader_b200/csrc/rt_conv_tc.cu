@@ -441,7 +441,7 @@ cudaError_t convTc(const bf16* in, const bf16* low, int lowChannels, int n, int 
                    bool relu, bool accumulate, int* errorFlag, cudaStream_t stream) {
     // The warp-specialised TMA form where its shared memory allows (see
     // rt_conv_pipe.cu); this kernel for the layers with the largest weights.
-    if (g_convPath.load() == 0 && convPipeSupported(cin, cout, low ? lowChannels : 0)) {
+    if (g_convPath.load() == 0 && convPipePreferred(cin, cout, low ? lowChannels : 0)) {
         cudaError_t e = convPipe(in, low, lowChannels, n, h, w, cin, weights, reverseTaps, bias, cout, outB, outF,
                                  relu, accumulate, errorFlag, stream);
         if (e != cudaErrorNotSupported) {

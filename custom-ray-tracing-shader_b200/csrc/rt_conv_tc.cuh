@@ -61,18 +61,25 @@ void convLaunchCounts(long long* pipe, long long* single);
 struct ConvPipeTest {
     unsigned long long waitLimitNs;  // bound of every wait (default one second)
     int probe;                       // 1: the MMA issuer first waits on a barrier nothing completes
-    int ring;                        // ring rows (4..8)
+    int ring;                        // ring rows (3..16)
     int stripRows;                   // rows per strip
     int nAcc;                        // tensor-memory accumulators (2..8)
     unsigned long long* stats;       // device array of 6 wait/lifetime sums in ns (see rt_conv_pipe.cu)
+    int blocksPerSm;                 // fewer blocks per SM than shared memory allows (each then gets a longer ring)
 };
 
 // The same convolution as convTc, warp-specialised and fed by TMA (input
 // rows in a ring of shared-memory slots, weights resident): for Cout in {16,
-// 32, 48, 64, 80, 96} when the weights and a ring of 4 rows fit in shared
+// 32, 48, 64, 80, 96} when the weights and a ring of 3 rows fit in shared
 // memory. Returns cudaErrorNotSupported (before any launch) for other
 // shapes. Same arguments as convTc, plus optional test hooks.
 bool convPipeSupported(int cin, int cout, int lowChannels);
+// Whether convTc hands the layer to convPipe (path 0): when a ring of at
+// least 4 rows fits beside the weights. With only the three rows a tile
+// reads, the producer cannot run ahead of the MMAs and the single-role
+// kernel is faster (1080p decoder layers 112->48 and 160->64: 287 and 368 us
+// pipelined against 207 and 210 us).
+bool convPipePreferred(int cin, int cout, int lowChannels);
 uint32_t convPipeSmemBytes(int cin, int cout, int lowChannels, int ring);
 cudaError_t convPipe(const __nv_bfloat16* in, const __nv_bfloat16* low, int lowChannels, int n, int h, int w, int cin,
                      const __nv_bfloat16* weights, bool reverseTaps, const float* bias, int cout,

@@ -218,23 +218,39 @@ __global__ void __launch_bounds__(kThreads) wgradTcKernel(const __grid_constant_
         if (lane == 0) {
             bool ok = true;
             const uint32_t idesc = idescMnMajor(kM, a.nDim);
+            // Stage and phase as running counters; descriptors as compile-
+            // time offsets from two per-stage bases (a single issuing
+            // thread that computes descriptors per MMA issues several
+            // times slower than the tensor pipe runs).
             long long k = 0;
+            int st = 0;
+            uint32_t parity = 0;
             for (long long s = seg0; s < seg1 && ok; s++, k++) {
-                const int st = (int)(k % S);
-                ok = waitPhase(base + Header::full + 8 * st, (uint32_t)((k / S) & 1), abortFlag, limit);
+                ok = waitPhase(base + Header::full + 8 * st, parity, abortFlag, limit);
                 if (!ok) break;
                 tcFenceAfter();
                 const uint32_t xs = stage0 + (uint32_t)st * a.stageBytes, ds = xs + a.xBytes;
-                for (int dx = 0; dx < 3; dx++) {
-                    const uint32_t acc = tmem + (uint32_t)dx * a.accCols;
-                    for (int kk = 0; kk < kM / 16; kk++) {
-                        // 16 pixels per MMA: 2 core-matrix groups of 8 along K (LBO = 128 bytes).
-                        const uint64_t xd = ummaSmemDesc(xs + (uint32_t)dx * 16u + (uint32_t)kk * 256u, 128u, kXPlane);
-                        const uint64_t dd = ummaSmemDesc(ds + (uint32_t)kk * 256u, 128u, kDPlane);
-                        mma(acc, a.mIsX ? xd : dd, a.mIsX ? dd : xd, idesc, (k > 0 || kk > 0) ? 1u : 0u);
-                    }
+                // 16 pixels per MMA: 2 core-matrix groups of 8 along K (LBO = 128 bytes),
+                // next 16 pixels 256 bytes on; tap dx one pixel (16 bytes) on.
+                const uint64_t xBase = ummaSmemDesc(xs, 128u, kXPlane), dBase = ummaSmemDesc(ds, 128u, kDPlane);
+                const uint32_t first = k > 0 ? 1u : 0u;
+                if (a.mIsX) {
+#pragma unroll
+                    for (int dx = 0; dx < 3; dx++)
+#pragma unroll
+                        for (int kk = 0; kk < kM / 16; kk++)
+                            mma(tmem + (uint32_t)dx * a.accCols, xBase + (uint64_t)(dx + 16 * kk), dBase + (uint64_t)(16 * kk),
+                                idesc, (first || kk > 0) ? 1u : 0u);
+                } else {
+#pragma unroll
+                    for (int dx = 0; dx < 3; dx++)
+#pragma unroll
+                        for (int kk = 0; kk < kM / 16; kk++)
+                            mma(tmem + (uint32_t)dx * a.accCols, dBase + (uint64_t)(16 * kk), xBase + (uint64_t)(dx + 16 * kk),
+                                idesc, (first || kk > 0) ? 1u : 0u);
                 }
                 commit(base + Header::empty + 8 * st);
+                if (++st == S) { st = 0; parity ^= 1u; }
             }
             if (ok) {
                 commit(base + Header::done);
