@@ -84,6 +84,9 @@ def parse():
                    help='skip timing U-Net training steps (batch 32 of 128x128 crops; 1 GPU runs it by default)')
     p.add_argument('--train-steps', type=int, default=20, help='timed training steps')
     p.add_argument('--train-step-only', action='store_true', help='only time U-Net training steps (for profiling)')
+    p.add_argument('--build-only', action='store_true',
+                   help='only the BVH builds of the workload at RtInitialize (for profiling): a warm-up build, then '
+                        '--steps timed builds')
     p.set_defaults(quality=True, batch=True, denoiser=True, train_step=True)
     return p.parse_args()
 
@@ -744,6 +747,25 @@ def l2_flusher():
     return (lambda: None), 'inputs larger than L2 (1.0M triangles: 116 MB records + 48 MB packed + 8.5 MB nodes)'
 
 
+def build_only_run(lib, args):
+    """The workload's BVH builds alone: RtInitialize of the workload scene
+    after a warm-up build, `--steps` times, with the build report of the
+    fastest (the traced tree; the reference's own tree is built on the
+    first RtxBvhStatsGet, after the traced tree's time is taken)."""
+    from native_api import Session
+    tris, _, _, w, h = workload(args)
+    peak, peak_kind = measured_peaks()
+    reports = []
+    for k in range(max(args.steps, 1) + 1):
+        with Session(lib) as s:
+            t0 = time.perf_counter()
+            s.initialize(tris, 64, 64)
+            wall = (time.perf_counter() - t0) * 1e3
+            if k > 0:
+                reports.append(build_report(tris, s.bvh_stats(), wall, peak, peak_kind))
+    return min(reports, key=lambda r: r['traced_tree']['ms'])
+
+
 def run_ours(args, rank, local_rank, world):
     import numpy as np
     from native_api import Session, load_library
@@ -1019,6 +1041,9 @@ def main():
     elif args.train_step_only:
         from native_api import load_library
         result = train_step_run(load_library(), args) if rank == 0 else None
+    elif args.build_only:
+        from native_api import load_library
+        result = build_only_run(load_library(), args) if rank == 0 else None
     elif args.impl == 'reference':
         result = run_reference(args, rank, world)
     else:

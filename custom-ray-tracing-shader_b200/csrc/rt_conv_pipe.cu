@@ -25,9 +25,17 @@
 //              memory (tcgen05.cp of each row's three shifted copies) an
 //              MMA of 128 x N x 16 measured ~85 SM cycles against ~42 from
 //              shared memory.
-//   warps 2-5  epilogue: tcgen05.ld of the accumulator (warp w reads lanes
-//              32 (w % 4) ...), which is then handed back to the issuer,
+//   warps 2-5  epilogue: tcgen05.ld of the accumulator (warp w of the block
+//              reads lanes 32 (w % 4) ...), which is then handed back to the issuer,
 //              bias, ReLU and the store (BF16, or FP32 added to or written).
+// A block runs one such pipeline, or two (12 warps, each pipeline with its
+// own ring, barriers and accumulators) where only one block fits per SM: a
+// single MMA issuer per SM issues at about half the tensor pipe's rate. The
+// two take every other unit of the block and share one copy of the weights.
+// (Splitting a concatenated input's channels between the two pipelines, the
+// low planes on one and the skip planes on the other with the epilogue
+// adding both accumulators, measured 352 against 364 us on the 80->32 layer
+// at 1080p and was dropped.)
 // Hand-offs are mbarriers only: full/empty per ring slot, full/empty per
 // accumulator, one for the weights. Every wait is bounded by %globaltimer;
 // a wait that runs out sets the block's abort flag and the error flag, every
@@ -58,11 +66,14 @@ constexpr int kLowHalo = kM / 2 + 2;     // low-resolution pixels per staged row
 // boundary.
 constexpr uint32_t kPlane = (kHalo * 16 + 127) / 128 * 128;        // 2,176
 constexpr uint32_t kLowPlane = (kLowHalo * 16 + 127) / 128 * 128;  // 1,152
-constexpr int kThreads = 192;
+constexpr int kPipeThreads = 192;  // warps of one pipeline: producer, MMA issuer, 4 epilogue warps
+constexpr int kMaxPipes = 2;
 constexpr int kMinRing = 3;  // the rows a tile reads; 4 and more let the producer run ahead
 constexpr int kMaxRing = 16;
 constexpr int kMaxAcc = 8;   // tensor-memory accumulators per block (tiles between the issuer and the epilogue)
-constexpr uint32_t kHeader = 1024;       // barriers and flags
+constexpr int kLowBufs = 4;  // staging rows of the low-resolution input (loads in flight ahead of the expansion)
+constexpr uint32_t kPipeHeader = 512;    // barriers of one pipeline
+constexpr uint32_t kHeader = 1536;       // barriers of kMaxPipes pipelines, shared barriers and flags, biases
 
 struct PipeArgs {
     int n, h, w, cin, cout, lowChannels;
@@ -70,6 +81,7 @@ struct PipeArgs {
     int nSplits;
     int tilesPerRow, stripRows, strips, units, ring;
     uint32_t weightBytes, slotBytes, lowSlotBytes, accCols, tmemCols;
+    uint32_t pipeBytes;  // shared memory of one pipeline: its ring and low-resolution staging rows
     const float* bias;
     bf16* outB;
     float* outF;
@@ -86,21 +98,24 @@ struct PipeArgs {
     unsigned long long* stats;
 };
 
-// Shared-memory header: barrier offsets (8 bytes each).
+// Shared-memory header. Barriers of pipeline p (8 bytes each) at
+// p * kPipeHeader + full, empty, ...; then the block's shared barriers and
+// flags, and the biases of its output channels.
 struct Header {
     static constexpr uint32_t full = 0;                    // kMaxRing
     static constexpr uint32_t empty = 8 * kMaxRing;        // kMaxRing
-    static constexpr uint32_t lowFull = 16 * kMaxRing;     // kMaxRing
-    static constexpr uint32_t accFull = 24 * kMaxRing;     // kMaxAcc
-    static constexpr uint32_t accEmpty = 24 * kMaxRing + 8 * kMaxAcc;
-    static constexpr uint32_t weights = 24 * kMaxRing + 16 * kMaxAcc;
+    static constexpr uint32_t lowFull = 16 * kMaxRing;     // kLowBufs
+    static constexpr uint32_t accFull = lowFull + 8 * kLowBufs;  // kMaxAcc
+    static constexpr uint32_t accEmpty = accFull + 8 * kMaxAcc;
+    static constexpr uint32_t drain = accEmpty + 8 * kMaxAcc;
+    static constexpr uint32_t weightsFull = drain + 8;     // this pipeline's weights (loaded by its producer)
+    static constexpr uint32_t weights = kMaxPipes * kPipeHeader;
     static constexpr uint32_t probe = weights + 8;
-    static constexpr uint32_t drain = weights + 16;
-    static constexpr uint32_t tmemSlot = weights + 24;
-    static constexpr uint32_t abort = weights + 28;
-    static constexpr uint32_t bias = 576;                  // the block's output channels' biases (<= 96 floats)
+    static constexpr uint32_t tmemSlot = weights + 16;
+    static constexpr uint32_t abort = weights + 20;
+    static constexpr uint32_t bias = weights + 64;         // the block's output channels' biases (<= 96 floats)
 };
-static_assert(Header::abort + 4 <= Header::bias && Header::bias + 96 * 4 <= kHeader, "header size");
+static_assert(Header::weightsFull + 8 <= kPipeHeader && Header::bias + 96 * 4 <= kHeader, "header size");
 
 __device__ __forceinline__ uint32_t smemAddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ uint64_t nowNs() {
@@ -284,47 +299,60 @@ __device__ __forceinline__ void epilogueStore(const PipeArgs& a, const uint32_t 
     }
 }
 
-template <int COUT>
-__global__ void __launch_bounds__(kThreads, COUT <= 48 ? 4 : 2) convPipeKernel(const __grid_constant__ CUtensorMap inMap,
-                                                          const __grid_constant__ CUtensorMap lowMap,
-                                                          const __grid_constant__ CUtensorMap wMap, PipeArgs a) {
+// PIPES independent pipelines per block (each its own warps, ring, barriers
+// and accumulators, every PIPES-th of the block's units), sharing the
+// weights: two pipelines give a layer whose weights leave room for one block
+// per SM two MMA issuers.
+template <int COUT, int PIPES>
+__global__ void __launch_bounds__(kPipeThreads * PIPES, PIPES > 1 ? 1 : (COUT <= 48 ? 4 : 2))
+    convPipeKernel(const __grid_constant__ CUtensorMap inMap, const __grid_constant__ CUtensorMap lowMap,
+                   const __grid_constant__ CUtensorMap wMap, PipeArgs a) {
     extern __shared__ __align__(1024) unsigned char smem[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31;
+    const int pipe = (int)(threadIdx.x >> 5) / 6, warp = (int)(threadIdx.x >> 5) % 6;  // warp: role within the pipeline
     const uint32_t base = smemAddr(smem);
+    const uint32_t pb = base + (uint32_t)pipe * kPipeHeader;  // this pipeline's barriers
     volatile int* abortFlag = reinterpret_cast<volatile int*>(smem + Header::abort);
     const uint32_t wAddr = base + kHeader;
-    const uint32_t ringAddr = wAddr + a.weightBytes;
-    const uint32_t lowAddr = ringAddr + (uint32_t)a.ring * a.slotBytes;  // 2 staging rows of the low input
+    const uint32_t slotBytes = a.slotBytes;
+    const uint32_t ringAddr = wAddr + a.weightBytes + (uint32_t)pipe * a.pipeBytes;
+    const uint32_t lowAddr = ringAddr + (uint32_t)a.ring * slotBytes;  // kLowBufs staging rows of the low input
     unsigned char* lowPtr = smem + (lowAddr - base);
     unsigned char* ringPtr = smem + (ringAddr - base);
     const uint64_t blockStart = a.stats ? nowNs() : 0;
+    // Planes of 8 channels: the low (upsampled) ones first in a slot, then
+    // the full-resolution ones.
     const int G = a.cin / 8, Glow = a.lowChannels / 8, Gin = G - Glow;
     const int R = a.ring;
     const uint64_t limit = a.waitLimitNs;
     // The block's slice of output channels and its units (every nSplits-th
     // block shares a slice; the grid is a multiple of nSplits).
     const int nBase = (int)(blockIdx.x % (unsigned)a.nSplits) * COUT;
-    const int firstUnit = (int)(blockIdx.x / (unsigned)a.nSplits), unitStride = (int)(gridDim.x / (unsigned)a.nSplits);
+    const int firstUnit = (int)(blockIdx.x / (unsigned)a.nSplits) + pipe * (int)(gridDim.x / (unsigned)a.nSplits);
+    const int unitStride = PIPES * (int)(gridDim.x / (unsigned)a.nSplits);
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < R; s++) {
-            barInit(base + Header::full + 8 * s, Glow ? 2 : 1);
-            barInit(base + Header::empty + 8 * s, 1);
+        for (int p = 0; p < PIPES; p++) {
+            const uint32_t b0 = base + (uint32_t)p * kPipeHeader;
+            for (int s = 0; s < R; s++) {
+                barInit(b0 + Header::full + 8 * s, Glow ? 2 : 1);
+                barInit(b0 + Header::empty + 8 * s, 1);
+            }
+            for (int s = 0; s < kLowBufs; s++) barInit(b0 + Header::lowFull + 8 * s, 1);
+            for (int b = 0; b < a.nAcc; b++) {
+                barInit(b0 + Header::accFull + 8 * b, 1);
+                barInit(b0 + Header::accEmpty + 8 * b, 4);
+            }
+            barInit(b0 + Header::drain, 1);
+            barInit(b0 + Header::weightsFull, 1);
         }
-        for (int s = 0; s < 2; s++) barInit(base + Header::lowFull + 8 * s, 1);
-        for (int b = 0; b < a.nAcc; b++) {
-            barInit(base + Header::accFull + 8 * b, 1);
-            barInit(base + Header::accEmpty + 8 * b, 4);
-        }
-        barInit(base + Header::weights, 1);
         barInit(base + Header::probe, 1);
-        barInit(base + Header::drain, 1);
         *abortFlag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
     float* sBias = reinterpret_cast<float*>(smem + Header::bias);
     if (threadIdx.x < COUT) sBias[threadIdx.x] = a.bias ? a.bias[nBase + threadIdx.x] : 0.0f;
-    if (warp == 1) {
+    if (threadIdx.x >> 5 == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(base + Header::tmemSlot),
                      "r"(a.tmemCols)
                      : "memory");
@@ -333,7 +361,9 @@ __global__ void __launch_bounds__(kThreads, COUT <= 48 ? 4 : 2) convPipeKernel(c
     tcFenceBefore();
     __syncthreads();
     tcFenceAfter();
-    const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(smem + Header::tmemSlot);
+    // This pipeline's accumulators.
+    const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(smem + Header::tmemSlot) +
+                          (uint32_t)pipe * (uint32_t)a.nAcc * a.accCols;
 
     if (warp == 0) {
         // ---- producer ----
@@ -341,50 +371,67 @@ __global__ void __launch_bounds__(kThreads, COUT <= 48 ? 4 : 2) convPipeKernel(c
             asm volatile("prefetch.tensormap [%0];\n" ::"l"(&inMap) : "memory");
             if (Glow) asm volatile("prefetch.tensormap [%0];\n" ::"l"(&lowMap) : "memory");
             asm volatile("prefetch.tensormap [%0];\n" ::"l"(&wMap) : "memory");
-            const uint32_t wb = base + Header::weights;
-            barExpectTx(wb, a.weightBytes);
-            for (int t = 0; t < 9; t++)
-                for (int g = 0; g < G; g++)
-                    tmaLoad3(wAddr + (uint32_t)((t * G + g) * COUT * 16), &wMap, g * 8, nBase, a.reverseTaps ? 8 - t : t,
-                             wb);
+            // The weights, tap-major ([tap][plane][cout][8]), once per block
+            // (pipeline 0's producer; both pipelines read them).
+            const uint32_t wb = pb + Header::weightsFull;
+            if (pipe == 0) {
+                barExpectTx(wb, a.weightBytes);
+                for (int t = 0; t < 9; t++)
+                    for (int g = 0; g < G; g++)
+                        tmaLoad3(wAddr + (uint32_t)((t * G + g) * COUT * 16), &wMap, g * 8, nBase,
+                                 a.reverseTaps ? 8 - t : t, wb);
+            }
         }
         // Rows are numbered in issue order q; row q sits in slot q % R, its
-        // low-resolution part (concatenated input) in staging buffer q % 2.
-        // A row is expanded at most one row behind the last one issued (the
-        // two staging buffers), and before the producer would block on a
-        // slot: a slot may be waiting for exactly that expansion.
+        // low-resolution part (concatenated input) in staging buffer
+        // q % kLowBufs until the warp expands it into the slot. Rows whose
+        // low part has landed are expanded as the producer goes (a test, not
+        // a wait), so the loads of later rows are not held up by one row's
+        // latency; a staging buffer is expanded before it is loaded again,
+        // and every issued row is expanded before the producer blocks on a
+        // slot (the issuer may be waiting for exactly those rows).
         int q = 0, expanded = 0;
         uint64_t waitSlotNs = 0, waitLowNs = 0;
         bool ok = true;
-        auto expand = [&](int e) -> bool {
+        auto lowLanded = [&](int e) -> bool {
+            const uint32_t bar = pb + Header::lowFull + 8 * (e % kLowBufs), parity = (uint32_t)((e / kLowBufs) & 1);
+            return __shfl_sync(0xFFFFFFFFu, lane == 0 ? (barTestWait(bar, parity) ? 1 : 0) : 0, 0) != 0;
+        };
+        auto expand = [&](int& e) -> bool {  // expands row e and advances e
             const uint64_t t1 = a.stats ? nowNs() : 0;
-            if (!waitPhaseWarp(base + Header::lowFull + 8 * (int)(e & 1), (uint32_t)((e >> 1) & 1), abortFlag, limit))
+            if (!waitPhaseWarp(pb + Header::lowFull + 8 * (e % kLowBufs), (uint32_t)((e / kLowBufs) & 1), abortFlag, limit))
                 return false;
             if (a.stats) waitLowNs += nowNs() - t1;
-            const uint4* src = reinterpret_cast<const uint4*>(lowPtr + (size_t)(e & 1) * a.lowSlotBytes);
-            uint4* dst = reinterpret_cast<uint4*>(ringPtr + (size_t)(e % R) * a.slotBytes);
+            const uint4* src = reinterpret_cast<const uint4*>(lowPtr + (size_t)(e % kLowBufs) * a.lowSlotBytes);
+            uint4* dst = reinterpret_cast<uint4*>(ringPtr + (size_t)(e % R) * slotBytes);
             // Staged pixel p is input x0 - 1 + p, whose low-resolution pixel
             // floor((x0 - 1 + p) / 2) is staged at (p + 1) / 2 (x0 even).
-            for (int v = lane; v < Glow * kHalo; v += 32) {
-                const int g = v / kHalo, p = v % kHalo;
-                dst[g * (kPlane / 16) + p] = src[g * (kLowPlane / 16) + (p + 1) / 2];
+            for (int g = 0; g < Glow; g++) {
+                const uint4* srcPlane = src + g * (kLowPlane / 16);
+                uint4* dstPlane = dst + g * (kPlane / 16);
+#pragma unroll
+                for (int k = 0; k < (kHalo + 31) / 32; k++) {
+                    const int p = lane + 32 * k;
+                    if (p < kHalo) dstPlane[p] = srcPlane[(p + 1) / 2];
+                }
             }
             asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
             __syncwarp();
-            if (lane == 0) barArrive(base + Header::full + 8 * (int)(e % R));
+            if (lane == 0) barArrive(pb + Header::full + 8 * (e % R));
+            e++;
             return true;
         };
         for (int u = firstUnit; u < a.units && ok; u += unitStride) {
             const Unit U = unitOf(a, u);
             for (int r = U.y0 - 1; r <= U.y1 && ok; r++) {
                 const int s = q % R;
-                const uint32_t emptyBar = base + Header::empty + 8 * s, emptyParity = (uint32_t)(((q / R) & 1) ^ 1);
-                if (Glow && expanded < q) {
+                const uint32_t emptyBar = pb + Header::empty + 8 * s, emptyParity = (uint32_t)(((q / R) & 1) ^ 1);
+                if (Glow) {
+                    while (ok && expanded < q && lowLanded(expanded)) ok = expand(expanded);
+                    while (ok && expanded <= q - kLowBufs) ok = expand(expanded);  // this row's staging buffer
                     const bool freeNow = __shfl_sync(0xFFFFFFFFu, lane == 0 ? (barTestWait(emptyBar, emptyParity) ? 1 : 0) : 0, 0) != 0;
-                    if (!freeNow) {
-                        if (!expand(expanded)) { ok = false; break; }
-                        expanded++;
-                    }
+                    while (ok && !freeNow && expanded < q) ok = expand(expanded);
+                    if (!ok) break;
                 }
                 {
                     const uint64_t t1 = a.stats ? nowNs() : 0;
@@ -392,14 +439,14 @@ __global__ void __launch_bounds__(kThreads, COUT <= 48 ? 4 : 2) convPipeKernel(c
                     if (a.stats) waitSlotNs += nowNs() - t1;
                 }
                 if (lane == 0) {
-                    const uint32_t fb = base + Header::full + 8 * s;
-                    const uint32_t slot = ringAddr + (uint32_t)s * a.slotBytes;
+                    const uint32_t fb = pb + Header::full + 8 * s;
+                    const uint32_t slot = ringAddr + (uint32_t)s * slotBytes;
                     barExpectTx(fb, (uint32_t)Gin * kHalo * 16u);  // the boxes' bytes (planes are padded)
                     for (int g = 0; g < Gin; g++)
                         tmaLoad4(slot + (uint32_t)(Glow + g) * kPlane, &inMap, g * 8, U.x0 - 1, r, U.img, fb);
                     if (Glow) {
-                        const uint32_t lb = base + Header::lowFull + 8 * (int)(q & 1);
-                        const uint32_t ls = lowAddr + (uint32_t)(q & 1) * a.lowSlotBytes;
+                        const uint32_t lb = pb + Header::lowFull + 8 * (q % kLowBufs);
+                        const uint32_t ls = lowAddr + (uint32_t)(q % kLowBufs) * a.lowSlotBytes;
                         barExpectTx(lb, (uint32_t)Glow * kLowHalo * 16u);
                         for (int g = 0; g < Glow; g++)
                             tmaLoad4(ls + (uint32_t)g * kLowPlane, &lowMap, g * 8, U.x0 / 2 - 1, r >> 1, U.img, lb);
@@ -407,32 +454,23 @@ __global__ void __launch_bounds__(kThreads, COUT <= 48 ? 4 : 2) convPipeKernel(c
                 }
                 __syncwarp();
                 q++;
-                // Keep at most one row unexpanded (its staging buffer is
-                // the one the next row does not use).
-                if (Glow && expanded < q - 1) {
-                    if (!expand(expanded)) { ok = false; break; }
-                    expanded++;
-                }
             }
         }
-        while (ok && Glow && expanded < q) {
-            ok = expand(expanded);
-            if (ok) expanded++;
-        }
+        while (ok && Glow && expanded < q) ok = expand(expanded);
         // Every load issued must land before the block exits, also when the
         // issuer gave up before reading them: poll the phases of the weights,
-        // the two staging buffers and the last R slots (each the latest
+        // the staging buffers and the last R slots (each the latest
         // phase of its barrier, so the parities are unambiguous). After a
         // failure, rows not expanded get their second arrival first so
         // their slot's phase can complete.
         if (!ok) *abortFlag = 1;
         if (lane == 0) {
-            pollPhase(base + Header::weights, 0u, limit);
-            for (int e = q > 2 ? q - 2 : 0; e < q && Glow; e++)
-                pollPhase(base + Header::lowFull + 8 * (int)(e & 1), (uint32_t)((e >> 1) & 1), limit);
+            if (pipe == 0) pollPhase(pb + Header::weightsFull, 0u, limit);
+            for (int e = q > kLowBufs ? q - kLowBufs : 0; e < q && Glow; e++)
+                pollPhase(pb + Header::lowFull + 8 * (e % kLowBufs), (uint32_t)((e / kLowBufs) & 1), limit);
             for (int e = q > R ? q - R : 0; e < q; e++) {
-                if (Glow && e >= expanded) barArrive(base + Header::full + 8 * (int)(e % R));
-                pollPhase(base + Header::full + 8 * (int)(e % R), (uint32_t)((e / R) & 1), limit);
+                if (Glow && e >= expanded) barArrive(pb + Header::full + 8 * (int)(e % R));
+                pollPhase(pb + Header::full + 8 * (int)(e % R), (uint32_t)((e / R) & 1), limit);
             }
             if (a.stats) { atomicAdd(a.stats + 0, waitSlotNs); atomicAdd(a.stats + 1, waitLowNs); }
         }
@@ -449,7 +487,8 @@ __global__ void __launch_bounds__(kThreads, COUT <= 48 ? 4 : 2) convPipeKernel(c
         if (lane == 0) {
             const uint32_t idesc = ummaInstrDescBf16(kM, COUT);
             if (a.probe) ok = waitPhase(base + Header::probe, 0u, abortFlag, limit);
-            if (ok) ok = waitPhase(base + Header::weights, 0u, abortFlag, limit);
+            if (ok)
+                ok = waitPhase(base + Header::weightsFull, 0u, abortFlag, limit);  // pipeline 0's barrier
             uint64_t waitRowNs = 0, waitAccNs = 0;
             const uint64_t wDesc = ummaSmemDesc(wAddr, COUT * 16u, 128u);
             const int G2 = G / 2;
@@ -461,14 +500,14 @@ __global__ void __launch_bounds__(kThreads, COUT <= 48 ? 4 : 2) convPipeKernel(c
             auto nextRow = [&](int& slot) -> bool {
                 const uint64_t t1 = a.stats ? nowNs() : 0;
                 slot = waitSlot;
-                const bool got = waitPhase(base + Header::full + 8 * waitSlot, waitParity, abortFlag, limit);
+                const bool got = waitPhase(pb + Header::full + 8 * waitSlot, waitParity, abortFlag, limit);
                 if (a.stats) waitRowNs += nowNs() - t1;
                 if (++waitSlot == R) { waitSlot = 0; waitParity ^= 1u; }
                 rows++;
                 return got;
             };
             auto release = [&]() {
-                commit(base + Header::empty + 8 * relSlot);
+                commit(pb + Header::empty + 8 * relSlot);
                 if (++relSlot == R) relSlot = 0;
             };
             for (int u = firstUnit; u < a.units && ok; u += unitStride) {
@@ -479,17 +518,17 @@ __global__ void __launch_bounds__(kThreads, COUT <= 48 ? 4 : 2) convPipeKernel(c
                     if (!nextRow(s2)) { ok = false; break; }
                     {
                         const uint64_t t1 = a.stats ? nowNs() : 0;
-                        ok = waitPhase(base + Header::accEmpty + 8 * accB, accParity ^ 1u, abortFlag, limit);
+                        ok = waitPhase(pb + Header::accEmpty + 8 * accB, accParity ^ 1u, abortFlag, limit);
                         if (a.stats) waitAccNs += nowNs() - t1;
                     }
                     if (!ok) break;
                     tcFenceAfter();
                     const uint32_t acc = tmem + (uint32_t)accB * a.accCols;
-                    const uint64_t rowDesc[3] = {ummaSmemDesc(ringAddr + (uint32_t)s0 * a.slotBytes, kPlane, 128u),
-                                                 ummaSmemDesc(ringAddr + (uint32_t)s1 * a.slotBytes, kPlane, 128u),
-                                                 ummaSmemDesc(ringAddr + (uint32_t)s2 * a.slotBytes, kPlane, 128u)};
+                    const uint64_t rowDesc[3] = {ummaSmemDesc(ringAddr + (uint32_t)s0 * slotBytes, kPlane, 128u),
+                                                 ummaSmemDesc(ringAddr + (uint32_t)s1 * slotBytes, kPlane, 128u),
+                                                 ummaSmemDesc(ringAddr + (uint32_t)s2 * slotBytes, kPlane, 128u)};
                     issueTileG<COUT>(G2, acc, rowDesc, wDesc, idesc);
-                    commit(base + Header::accFull + 8 * accB);
+                    commit(pb + Header::accFull + 8 * accB);
                     release();  // row y - 1: no later tile reads it
                     s0 = s1;
                     s1 = s2;
@@ -505,21 +544,24 @@ __global__ void __launch_bounds__(kThreads, COUT <= 48 ? 4 : 2) convPipeKernel(c
                 // the last ones (the rows released last, the last
                 // accumulators) before the block's shared memory goes away.
                 for (int e = rows > R ? rows - R : 0; e < rows; e++)
-                    pollPhase(base + Header::empty + 8 * (e % R), (uint32_t)((e / R) & 1), limit);
+                    pollPhase(pb + Header::empty + 8 * (e % R), (uint32_t)((e / R) & 1), limit);
                 for (int t = tiles > a.nAcc ? tiles - a.nAcc : 0; t < tiles; t++)
-                    pollPhase(base + Header::accFull + 8 * (t % a.nAcc), (uint32_t)((t / a.nAcc) & 1), limit);
+                    pollPhase(pb + Header::accFull + 8 * (t % a.nAcc), (uint32_t)((t / a.nAcc) & 1), limit);
             } else {
                 *abortFlag = 1;
                 // Wait (bounded) for every MMA issued so far.
-                commit(base + Header::drain);
-                pollPhase(base + Header::drain, 0u, limit);
+                commit(pb + Header::drain);
+                pollPhase(pb + Header::drain, 0u, limit);
             }
             if (a.stats) { atomicAdd(a.stats + 2, waitRowNs); atomicAdd(a.stats + 3, waitAccNs); }
         }
         __syncwarp();
     } else {
         // ---- epilogue: warps 2-5, lanes 32 * (warp % 4) ... of the accumulator ----
-        const int quarter = warp & 3;
+        // A warp may read only tensor-memory lanes 32 * (its warp index in
+        // the block mod 4) ...: warps 2-5 of pipeline 0 and 8-11 of
+        // pipeline 1 each cover the four quarters once.
+        const int quarter = (int)(threadIdx.x >> 5) & 3;
         int b = 0;
         uint32_t parity = 0;
         uint64_t waitNs = 0;
@@ -528,22 +570,22 @@ __global__ void __launch_bounds__(kThreads, COUT <= 48 ? 4 : 2) convPipeKernel(c
             const Unit U = unitOf(a, u);
             for (int y = U.y0; y < U.y1; y++, b = b + 1 == a.nAcc ? 0 : b + 1, parity ^= b == 0 ? 1u : 0u) {
                 const uint64_t t1 = a.stats ? nowNs() : 0;
-                if (!waitPhaseWarp(base + Header::accFull + 8 * b, parity, abortFlag, limit)) { ok = false; break; }
+                if (!waitPhaseWarp(pb + Header::accFull + 8 * b, parity, abortFlag, limit)) { ok = false; break; }
                 if (a.stats) waitNs += nowNs() - t1;
                 tcFenceAfter();
                 uint32_t acc[COUT];
-                const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)b * a.accCols;
+                const uint32_t lanes = (uint32_t)(quarter * 32) << 16;
 #pragma unroll
                 for (int c = 0; c < COUT / 16; c++) {
                     uint32_t r[16];
-                    tmemLoad16(taddr + (uint32_t)(16 * c), r);
+                    tmemLoad16(tmem + lanes + (uint32_t)b * a.accCols + (uint32_t)(16 * c), r);
 #pragma unroll
                     for (int j = 0; j < 16; j++) acc[16 * c + j] = r[j];
                 }
                 tmemWaitLoads();
                 tcFenceBefore();
                 __syncwarp();
-                if (lane == 0) barArrive(base + Header::accEmpty + 8 * b);
+                if (lane == 0) barArrive(pb + Header::accEmpty + 8 * b);
                 const int x = U.x0 + quarter * 32 + lane;
                 if (x < a.w) epilogueStore<COUT>(a, acc, ((size_t)U.img * a.h + y) * a.w + x, nBase, sBias);
             }
@@ -554,7 +596,7 @@ __global__ void __launch_bounds__(kThreads, COUT <= 48 ? 4 : 2) convPipeKernel(c
     __syncthreads();
     if (threadIdx.x == 0 && *abortFlag) atomicExch(a.errorFlag, 1);
     if (threadIdx.x == 0 && a.stats) atomicAdd(a.stats + 5, nowNs() - blockStart);
-    if (warp == 1) {
+    if (threadIdx.x >> 5 == 1) {
         tcFenceAfter();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(a.tmemCols)
                      : "memory");
@@ -594,27 +636,27 @@ int deviceSmCount() {
     return sms > 0 ? sms : 1;
 }
 
-template <int COUT>
+template <int COUT, int PIPES>
 cudaError_t launchPipe(const CUtensorMap& inMap, const CUtensorMap& lowMap, const CUtensorMap& wMap,
                        const PipeArgs& a, int grid, uint32_t smemBytes, cudaStream_t stream) {
     static bool configured = false;
     if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(convPipeKernel<COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaError_t e = cudaFuncSetAttribute(convPipeKernel<COUT, PIPES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              227 * 1024);
         if (e != cudaSuccess) return e;
         configured = true;
     }
-    convPipeKernel<COUT><<<grid, kThreads, smemBytes, stream>>>(inMap, lowMap, wMap, a);
+    convPipeKernel<COUT, PIPES><<<grid, kPipeThreads * PIPES, smemBytes, stream>>>(inMap, lowMap, wMap, a);
     return cudaGetLastError();
 }
 
 }  // namespace
 
-uint32_t convPipeSmemBytes(int cin, int cout, int lowChannels, int ring) {
+uint32_t convPipeSmemBytes(int cin, int cout, int lowChannels, int ring, int pipes) {
     const uint32_t weights = 9u * (uint32_t)cin * (uint32_t)cout * 2u;
     const uint32_t slot = ((uint32_t)(cin / 8) * kPlane + 127u) & ~127u;
     const uint32_t lowSlot = ((uint32_t)(lowChannels / 8) * kLowPlane + 127u) & ~127u;
-    return kHeader + weights + (uint32_t)ring * slot + 2u * lowSlot;
+    return kHeader + weights + (uint32_t)pipes * ((uint32_t)ring * slot + (uint32_t)kLowBufs * lowSlot);
 }
 
 namespace {
@@ -625,7 +667,7 @@ bool knownCout(int c) { return c == 16 || c == 32 || c == 48 || c == 64 || c == 
 int pickSplits(int cin, int cout, int lowChannels) {
     for (int s : {1, 2, 3, 4, 6})
         if (cout % s == 0 && knownCout(cout / s) &&
-            convPipeSmemBytes(cin, cout / s, lowChannels, kMinRing) <= 227u * 1024u)
+            convPipeSmemBytes(cin, cout / s, lowChannels, kMinRing, 1) <= 227u * 1024u)
             return s;
     return 0;
 }
@@ -639,7 +681,7 @@ bool convPipeSupported(int cin, int cout, int lowChannels) {
 bool convPipePreferred(int cin, int cout, int lowChannels) {
     if (!convPipeSupported(cin, cout, lowChannels)) return false;
     const int s = pickSplits(cin, cout, lowChannels);
-    return convPipeSmemBytes(cin, cout / s, lowChannels, 4) <= 227u * 1024u;
+    return convPipeSmemBytes(cin, cout / s, lowChannels, 4, 1) <= 227u * 1024u;
 }
 
 cudaError_t convPipe(const bf16* in, const bf16* low, int lowChannels, int n, int h, int w, int cin,
@@ -685,8 +727,12 @@ cudaError_t convPipe(const bf16* in, const bf16* low, int lowChannels, int n, in
     a.accCols = 32;
     while (a.accCols < (uint32_t)cout) a.accCols <<= 1;
     a.nAcc = test && test->nAcc >= 2 && test->nAcc <= kMaxAcc ? test->nAcc : 2;
-    a.tmemCols = 32;
-    while (a.tmemCols < (uint32_t)a.nAcc * a.accCols) a.tmemCols <<= 1;
+    auto tmemColumns = [&](int pipes) {
+        uint32_t c = 32;
+        while (c < (uint32_t)pipes * (uint32_t)a.nAcc * a.accCols) c <<= 1;
+        return c;
+    };
+    a.tmemCols = tmemColumns(1);
     if (a.tmemCols > 512) return cudaErrorNotSupported;
     a.stats = test ? test->stats : nullptr;
     a.bias = bias; a.outB = outB; a.outF = outF;
@@ -695,38 +741,59 @@ cudaError_t convPipe(const bf16* in, const bf16* low, int lowChannels, int n, in
     a.waitLimitNs = test && test->waitLimitNs ? test->waitLimitNs : 1000000000ull;
     a.probe = test && test->probe ? 1 : 0;
     // Blocks per SM from shared and tensor memory at a ring of 4 rows (3
-    // where 4 do not fit); then the largest ring (up to 8 rows) that keeps
-    // that many blocks per SM.
+    // where 4 do not fit); then the largest ring (up to kMaxRing rows) that
+    // keeps that many blocks per SM. Where one block fits per SM (one MMA
+    // issuer per SM issues at about half the tensor pipe's rate), a block
+    // runs two pipelines on alternate units, sharing the weights, when two
+    // rings of 4 rows fit.
     const int sms = deviceSmCount();
-    const uint32_t smemPerSm = 228u * 1024u;
-    a.ring = convPipeSmemBytes(cin, cout, lowChannels, 4) <= 227u * 1024u ? 4 : kMinRing;
-    int perSm = (int)(smemPerSm / (convPipeSmemBytes(cin, cout, lowChannels, a.ring) + 1024u));
-    perSm = std::max(1, std::min({perSm, (int)(512u / a.tmemCols), 2048 / kThreads}));
+    const uint32_t smemPerSm = 228u * 1024u, smemMax = 227u * 1024u;
+    a.ring = convPipeSmemBytes(cin, cout, lowChannels, 4, 1) <= smemMax ? 4 : kMinRing;
+    int perSm = (int)(smemPerSm / (convPipeSmemBytes(cin, cout, lowChannels, a.ring, 1) + 1024u));
+    perSm = std::max(1, std::min({perSm, (int)(512u / a.tmemCols), 2048 / kPipeThreads}));
     if (test && test->blocksPerSm > 0 && test->blocksPerSm < perSm) perSm = test->blocksPerSm;
-    while (a.ring < kMaxRing && (uint32_t)perSm * (convPipeSmemBytes(cin, cout, lowChannels, a.ring + 1) + 1024u) <= smemPerSm &&
-           convPipeSmemBytes(cin, cout, lowChannels, a.ring + 1) <= 227u * 1024u)
+    const int force = test ? test->pipes : 0;  // 1 or 2 pipelines
+    const bool twoFit = convPipeSmemBytes(cin, cout, lowChannels, 4, 2) <= smemMax && tmemColumns(2) <= 512u;
+    if (force == 2 && !twoFit) return cudaErrorNotSupported;
+    int pipes = 1;
+    if (force == 2 || (force == 0 && perSm == 1 && twoFit)) {
+        pipes = 2;
+        perSm = 1;
+        a.ring = 4;
+        a.tmemCols = tmemColumns(2);
+    }
+    while (a.ring < kMaxRing &&
+           (uint32_t)perSm * (convPipeSmemBytes(cin, cout, lowChannels, a.ring + 1, pipes) + 1024u) <= smemPerSm &&
+           convPipeSmemBytes(cin, cout, lowChannels, a.ring + 1, pipes) <= smemMax)
         a.ring++;
     if (test && test->ring >= kMinRing && test->ring <= kMaxRing) a.ring = test->ring;
-    const uint32_t smemBytes = convPipeSmemBytes(cin, cout, lowChannels, a.ring);
-    if (smemBytes > 227u * 1024u) return cudaErrorNotSupported;
+    const uint32_t smemBytes = convPipeSmemBytes(cin, cout, lowChannels, a.ring, pipes);
+    if (smemBytes > smemMax) return cudaErrorNotSupported;
+    a.pipeBytes = (uint32_t)a.ring * a.slotBytes + (uint32_t)kLowBufs * a.lowSlotBytes;
     // Strips: long enough to reuse rows (each strip stages 2 extra rows),
     // short enough to give every block about two units; every slice of
     // output channels walks all units.
     const long long columns = (long long)n * a.tilesPerRow;
     const long long blocks = std::max<long long>(nSplits, (long long)sms * perSm / nSplits * nSplits);
-    long long rows = std::max(1ll, columns * h * nSplits / (2 * blocks));
+    long long rows = std::max(1ll, columns * h * nSplits / (2 * blocks * pipes));
     a.stripRows = (int)std::max(4ll, std::min<long long>(32, rows));
     if (test && test->stripRows > 0) a.stripRows = test->stripRows;
     a.strips = (h + a.stripRows - 1) / a.stripRows;
     a.units = (int)(columns * a.strips);
     const int grid = (int)std::min<long long>((long long)a.units * nSplits, blocks);
     switch (cout) {
-        case 16: return launchPipe<16>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
-        case 32: return launchPipe<32>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
-        case 48: return launchPipe<48>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
-        case 64: return launchPipe<64>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
-        case 80: return launchPipe<80>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
-        case 96: return launchPipe<96>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
+        case 16: return pipes == 2 ? launchPipe<16, 2>(inMap, lowMap, wMap, a, grid, smemBytes, stream)
+                           : launchPipe<16, 1>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
+        case 32: return pipes == 2 ? launchPipe<32, 2>(inMap, lowMap, wMap, a, grid, smemBytes, stream)
+                           : launchPipe<32, 1>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
+        case 48: return pipes == 2 ? launchPipe<48, 2>(inMap, lowMap, wMap, a, grid, smemBytes, stream)
+                           : launchPipe<48, 1>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
+        case 64: return pipes == 2 ? launchPipe<64, 2>(inMap, lowMap, wMap, a, grid, smemBytes, stream)
+                           : launchPipe<64, 1>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
+        case 80: return pipes == 2 ? launchPipe<80, 2>(inMap, lowMap, wMap, a, grid, smemBytes, stream)
+                           : launchPipe<80, 1>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
+        case 96: return pipes == 2 ? launchPipe<96, 2>(inMap, lowMap, wMap, a, grid, smemBytes, stream)
+                           : launchPipe<96, 1>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
         default: return cudaErrorNotSupported;
     }
 }
