@@ -128,6 +128,40 @@ __device__ __forceinline__ void mmaCommit(uint32_t bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar)
                  : "memory");
 }
+// The 9 taps x K MMAs of a tile (or of one channel chunk of it), K a
+// compile-time constant: one thread issuing from a loop with a runtime trip
+// count issued an MMA per ~155 SM cycles, fully unrolled per ~60 (the
+// tensor pipe itself takes ~42 per 128 x N x 16 with N <= 64). aTap[t] is
+// tap t's A offset and every step a 16-byte-unit offset from the bases.
+template <int K>
+__device__ __forceinline__ void issueTaps(uint32_t acc, uint64_t aBase, const uint32_t (&aTap)[9], uint32_t kStepA,
+                                          uint64_t bBase, uint32_t tapStepB, uint32_t kStepB, uint32_t idesc,
+                                          bool accumulateFirst) {
+#pragma unroll
+    for (int t = 0; t < 9; t++)
+#pragma unroll
+        for (int k = 0; k < K; k++)
+            mmaBf16(acc, aBase + aTap[t] + (uint64_t)k * kStepA, bBase + (uint64_t)t * tapStepB + (uint64_t)k * kStepB,
+                    idesc, (accumulateFirst || t > 0 || k > 0) ? 1u : 0u);
+}
+__device__ __forceinline__ void issueTapsK(int k, uint32_t acc, uint64_t aBase, const uint32_t (&aTap)[9],
+                                           uint32_t kStepA, uint64_t bBase, uint32_t tapStepB, uint32_t kStepB,
+                                           uint32_t idesc, bool accumulateFirst) {
+#define RT_ISSUE_CASE(K) \
+    case K: issueTaps<K>(acc, aBase, aTap, kStepA, bBase, tapStepB, kStepB, idesc, accumulateFirst); return;
+    switch (k) {
+        RT_ISSUE_CASE(1) RT_ISSUE_CASE(2) RT_ISSUE_CASE(3) RT_ISSUE_CASE(4) RT_ISSUE_CASE(5) RT_ISSUE_CASE(6)
+        RT_ISSUE_CASE(7) RT_ISSUE_CASE(8) RT_ISSUE_CASE(9) RT_ISSUE_CASE(10) RT_ISSUE_CASE(11) RT_ISSUE_CASE(12)
+        RT_ISSUE_CASE(13) RT_ISSUE_CASE(14)
+        default: break;
+    }
+#undef RT_ISSUE_CASE
+    // Wider chunks (cin above 224 held whole): the loop form.
+    for (int t = 0; t < 9; t++)
+        for (int j = 0; j < k; j++)
+            mmaBf16(acc, aBase + aTap[t] + (uint64_t)j * kStepA, bBase + (uint64_t)t * tapStepB + (uint64_t)j * kStepB,
+                    idesc, (accumulateFirst || t > 0 || j > 0) ? 1u : 0u);
+}
 __device__ __forceinline__ void tmemLoad16(uint32_t taddr, uint32_t (&r)[16]) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
@@ -139,7 +173,7 @@ __device__ __forceinline__ void tmemLoad16(uint32_t taddr, uint32_t (&r)[16]) {
 }
 
 template <int DRAIN, int ISSUER>
-__global__ void __launch_bounds__(WarpLayout<DRAIN, ISSUER>::kThreads, 1) convTcKernel(ConvTcArgs a) {
+__global__ void __launch_bounds__(WarpLayout<DRAIN, ISSUER>::kThreads, DRAIN == 4 ? 4 : 2) convTcKernel(ConvTcArgs a) {
     using Layout = WarpLayout<DRAIN, ISSUER>;
     constexpr int kThreads = Layout::kThreads, kIssuer = Layout::kIssuer, kDrainWarps = Layout::kDrainWarps;
     extern __shared__ __align__(1024) unsigned char smem[];
@@ -322,14 +356,11 @@ __global__ void __launch_bounds__(WarpLayout<DRAIN, ISSUER>::kThreads, 1) convTc
                         const uint64_t aBase = ummaSmemDesc(smemAddress(hbuf), ringPlane, 128u);
                         const uint64_t bBase = ummaSmemDesc(smemAddress(wbuf), (uint32_t)a.cout * 16u, 128u);
                         const uint32_t acc = tmem + (uint32_t)(y & 1) * a.accCols;
-                        const uint32_t kStepA = 2u * 4u * kHaloW, kStepB = 2u * (uint32_t)a.cout;
-                        for (int t = 0; t < 9; t++) {
-                            const int dy = t / 3, dx = t % 3, slot = (y + dy - 1) & 3;
-                            uint64_t aDesc = aBase + (uint32_t)(slot * kHaloW + dx);
-                            uint64_t bDesc = bBase + (uint32_t)(t * groups) * (uint32_t)a.cout;
-                            for (int k = 0; k < a.kc / 16; k++, aDesc += kStepA, bDesc += kStepB)
-                                mmaBf16(acc, aDesc, bDesc, idesc, (t > 0 || k > 0) ? 1u : 0u);
-                        }
+                        uint32_t aTap[9];
+                        for (int t = 0; t < 9; t++)
+                            aTap[t] = (uint32_t)(((y + t / 3 - 1) & 3) * kHaloW + t % 3);
+                        issueTapsK(a.kc / 16, acc, aBase, aTap, 2u * 4u * kHaloW, bBase, (uint32_t)(groups * a.cout),
+                                   2u * (uint32_t)a.cout, idesc, false);
                         mmaCommit((y & 1) ? bar1 : bar0);
                     }
                 }
@@ -384,14 +415,10 @@ __global__ void __launch_bounds__(WarpLayout<DRAIN, ISSUER>::kThreads, 1) convTc
                 const uint64_t bBase = ummaSmemDesc(
                     smemAddress(a.resident ? wbuf + (size_t)c * stageW : wbuf + (size_t)stage * stageW),
                     (uint32_t)a.cout * 16u, 128u);
-                const uint32_t kStepA = 2u * 3u * kHaloW, kStepB = 2u * (uint32_t)a.cout;
-                for (int t = 0; t < 9; t++) {
-                    const int dy = t / 3, dx = t % 3;
-                    uint64_t aDesc = aBase + (uint32_t)(dy * kHaloW + dx);
-                    uint64_t bDesc = bBase + (uint32_t)(t * groups) * (uint32_t)a.cout;
-                    for (int k = 0; k < a.kc / 16; k++, aDesc += kStepA, bDesc += kStepB)
-                        mmaBf16(tmem, aDesc, bDesc, idesc, (c > 0 || t > 0 || k > 0) ? 1u : 0u);
-                }
+                uint32_t aTap[9];
+                for (int t = 0; t < 9; t++) aTap[t] = (uint32_t)((t / 3) * kHaloW + t % 3);
+                issueTapsK(a.kc / 16, tmem, aBase, aTap, 2u * 3u * kHaloW, bBase, (uint32_t)(groups * a.cout),
+                           2u * (uint32_t)a.cout, idesc, c > 0);
                 mmaCommit(stage ? bar1 : bar0);
             }
             pending[stage] = true;
