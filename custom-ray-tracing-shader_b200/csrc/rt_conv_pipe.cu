@@ -28,14 +28,10 @@
 //   warps 2-5  epilogue: tcgen05.ld of the accumulator (warp w of the block
 //              reads lanes 32 (w % 4) ...), which is then handed back to the issuer,
 //              bias, ReLU and the store (BF16, or FP32 added to or written).
-// A block runs one such pipeline, or two (12 warps, each pipeline with its
-// own ring, barriers and accumulators) where only one block fits per SM: a
-// single MMA issuer per SM issues at about half the tensor pipe's rate. The
-// two take every other unit of the block and share one copy of the weights.
-// (Splitting a concatenated input's channels between the two pipelines, the
-// low planes on one and the skip planes on the other with the epilogue
-// adding both accumulators, measured 352 against 364 us on the 80->32 layer
-// at 1080p and was dropped.)
+//   warp 6     a second MMA issuer where only one block fits per SM (a single
+//              issuing thread per SM issues at about half the tensor pipe's
+//              rate): the two issue alternate tiles from the same ring, each
+//              into its own accumulators, and both release every row.
 // Hand-offs are mbarriers only: full/empty per ring slot, full/empty per
 // accumulator, one for the weights. Every wait is bounded by %globaltimer;
 // a wait that runs out sets the block's abort flag and the error flag, every
@@ -67,13 +63,12 @@ constexpr int kLowHalo = kM / 2 + 2;     // low-resolution pixels per staged row
 constexpr uint32_t kPlane = (kHalo * 16 + 127) / 128 * 128;        // 2,176
 constexpr uint32_t kLowPlane = (kLowHalo * 16 + 127) / 128 * 128;  // 1,152
 constexpr int kPipeThreads = 192;  // warps of one pipeline: producer, MMA issuer, 4 epilogue warps
-constexpr int kMaxPipes = 2;
 constexpr int kMinRing = 3;  // the rows a tile reads; 4 and more let the producer run ahead
 constexpr int kMaxRing = 16;
 constexpr int kMaxAcc = 8;   // tensor-memory accumulators per block (tiles between the issuer and the epilogue)
 constexpr int kLowBufs = 4;  // staging rows of the low-resolution input (loads in flight ahead of the expansion)
-constexpr uint32_t kPipeHeader = 512;    // barriers of one pipeline
-constexpr uint32_t kHeader = 1536;       // barriers of kMaxPipes pipelines, shared barriers and flags, biases
+constexpr uint32_t kPipeHeader = 512;    // mbarriers (the rest of the header: flags and biases)
+constexpr uint32_t kHeader = 1024;       // barriers, flags and biases
 
 struct PipeArgs {
     int n, h, w, cin, cout, lowChannels;
@@ -81,7 +76,6 @@ struct PipeArgs {
     int nSplits;
     int tilesPerRow, stripRows, strips, units, ring;
     uint32_t weightBytes, slotBytes, lowSlotBytes, accCols, tmemCols;
-    uint32_t pipeBytes;  // shared memory of one pipeline: its ring and low-resolution staging rows
     const float* bias;
     bf16* outB;
     float* outF;
@@ -98,9 +92,8 @@ struct PipeArgs {
     unsigned long long* stats;
 };
 
-// Shared-memory header. Barriers of pipeline p (8 bytes each) at
-// p * kPipeHeader + full, empty, ...; then the block's shared barriers and
-// flags, and the biases of its output channels.
+// Shared-memory header: mbarriers (8 bytes each) at full, empty, ...; then
+// flags and the biases of the block's output channels.
 struct Header {
     static constexpr uint32_t full = 0;                    // kMaxRing
     static constexpr uint32_t empty = 8 * kMaxRing;        // kMaxRing
@@ -108,8 +101,8 @@ struct Header {
     static constexpr uint32_t accFull = lowFull + 8 * kLowBufs;  // kMaxAcc
     static constexpr uint32_t accEmpty = accFull + 8 * kMaxAcc;
     static constexpr uint32_t drain = accEmpty + 8 * kMaxAcc;
-    static constexpr uint32_t weightsFull = drain + 8;     // this pipeline's weights (loaded by its producer)
-    static constexpr uint32_t weights = kMaxPipes * kPipeHeader;
+    static constexpr uint32_t weightsFull = drain + 8;     // the weights (loaded once per block)
+    static constexpr uint32_t weights = kPipeHeader;
     static constexpr uint32_t probe = weights + 8;
     static constexpr uint32_t tmemSlot = weights + 16;
     static constexpr uint32_t abort = weights + 20;
@@ -299,23 +292,25 @@ __device__ __forceinline__ void epilogueStore(const PipeArgs& a, const uint32_t 
     }
 }
 
-// PIPES independent pipelines per block (each its own warps, ring, barriers
-// and accumulators, every PIPES-th of the block's units), sharing the
-// weights: two pipelines give a layer whose weights leave room for one block
-// per SM two MMA issuers.
-template <int COUT, int PIPES>
-__global__ void __launch_bounds__(kPipeThreads * PIPES, PIPES > 1 ? 1 : (COUT <= 48 ? 4 : 2))
+// ISS MMA issuers (warp 1, and warp 6 when ISS = 2) share the ring: issuer i
+// issues the block's tiles t with t % ISS = i into its own accumulators, and
+// every issuer releases every row (a slot's empty barrier counts ISS
+// arrivals). Two issuers give a layer that fits one block per SM two issuing
+// threads without a second ring.
+template <int COUT, int ISS>
+__global__ void __launch_bounds__(kPipeThreads + 32 * (ISS - 1), ISS > 1 ? 1 : (COUT <= 48 ? 4 : 2))
     convPipeKernel(const __grid_constant__ CUtensorMap inMap, const __grid_constant__ CUtensorMap lowMap,
                    const __grid_constant__ CUtensorMap wMap, PipeArgs a) {
     extern __shared__ __align__(1024) unsigned char smem[];
     const int lane = threadIdx.x & 31;
-    const int pipe = (int)(threadIdx.x >> 5) / 6, warp = (int)(threadIdx.x >> 5) % 6;  // warp: role within the pipeline
+    const int me = (int)(threadIdx.x >> 5) == 6 ? 1 : 0;          // issuer index (warp 6 is the second issuer)
+    const int warp = me ? 1 : (int)(threadIdx.x >> 5);            // role: 0 producer, 1 issuer, 2-5 epilogue
     const uint32_t base = smemAddr(smem);
-    const uint32_t pb = base + (uint32_t)pipe * kPipeHeader;  // this pipeline's barriers
+    const uint32_t pb = base;  // barriers
     volatile int* abortFlag = reinterpret_cast<volatile int*>(smem + Header::abort);
     const uint32_t wAddr = base + kHeader;
     const uint32_t slotBytes = a.slotBytes;
-    const uint32_t ringAddr = wAddr + a.weightBytes + (uint32_t)pipe * a.pipeBytes;
+    const uint32_t ringAddr = wAddr + a.weightBytes;
     const uint32_t lowAddr = ringAddr + (uint32_t)a.ring * slotBytes;  // kLowBufs staging rows of the low input
     unsigned char* lowPtr = smem + (lowAddr - base);
     unsigned char* ringPtr = smem + (ringAddr - base);
@@ -328,24 +323,21 @@ __global__ void __launch_bounds__(kPipeThreads * PIPES, PIPES > 1 ? 1 : (COUT <=
     // The block's slice of output channels and its units (every nSplits-th
     // block shares a slice; the grid is a multiple of nSplits).
     const int nBase = (int)(blockIdx.x % (unsigned)a.nSplits) * COUT;
-    const int firstUnit = (int)(blockIdx.x / (unsigned)a.nSplits) + pipe * (int)(gridDim.x / (unsigned)a.nSplits);
-    const int unitStride = PIPES * (int)(gridDim.x / (unsigned)a.nSplits);
+    const int firstUnit = (int)(blockIdx.x / (unsigned)a.nSplits);
+    const int unitStride = (int)(gridDim.x / (unsigned)a.nSplits);
 
     if (threadIdx.x == 0) {
-        for (int p = 0; p < PIPES; p++) {
-            const uint32_t b0 = base + (uint32_t)p * kPipeHeader;
-            for (int s = 0; s < R; s++) {
-                barInit(b0 + Header::full + 8 * s, Glow ? 2 : 1);
-                barInit(b0 + Header::empty + 8 * s, 1);
-            }
-            for (int s = 0; s < kLowBufs; s++) barInit(b0 + Header::lowFull + 8 * s, 1);
-            for (int b = 0; b < a.nAcc; b++) {
-                barInit(b0 + Header::accFull + 8 * b, 1);
-                barInit(b0 + Header::accEmpty + 8 * b, 4);
-            }
-            barInit(b0 + Header::drain, 1);
-            barInit(b0 + Header::weightsFull, 1);
+        for (int s = 0; s < R; s++) {
+            barInit(pb + Header::full + 8 * s, Glow ? 2 : 1);
+            barInit(pb + Header::empty + 8 * s, ISS);
         }
+        for (int s = 0; s < kLowBufs; s++) barInit(pb + Header::lowFull + 8 * s, 1);
+        for (int b = 0; b < ISS * a.nAcc; b++) {  // issuer i's accumulator b at i * nAcc + b
+            barInit(pb + Header::accFull + 8 * b, 1);
+            barInit(pb + Header::accEmpty + 8 * b, 4);
+        }
+        barInit(pb + Header::drain, ISS);
+        barInit(pb + Header::weightsFull, 1);
         barInit(base + Header::probe, 1);
         *abortFlag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
@@ -361,9 +353,7 @@ __global__ void __launch_bounds__(kPipeThreads * PIPES, PIPES > 1 ? 1 : (COUT <=
     tcFenceBefore();
     __syncthreads();
     tcFenceAfter();
-    // This pipeline's accumulators.
-    const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(smem + Header::tmemSlot) +
-                          (uint32_t)pipe * (uint32_t)a.nAcc * a.accCols;
+    const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(smem + Header::tmemSlot);
 
     if (warp == 0) {
         // ---- producer ----
@@ -371,10 +361,9 @@ __global__ void __launch_bounds__(kPipeThreads * PIPES, PIPES > 1 ? 1 : (COUT <=
             asm volatile("prefetch.tensormap [%0];\n" ::"l"(&inMap) : "memory");
             if (Glow) asm volatile("prefetch.tensormap [%0];\n" ::"l"(&lowMap) : "memory");
             asm volatile("prefetch.tensormap [%0];\n" ::"l"(&wMap) : "memory");
-            // The weights, tap-major ([tap][plane][cout][8]), once per block
-            // (pipeline 0's producer; both pipelines read them).
+            // The weights, tap-major ([tap][plane][cout][8]), once per block.
             const uint32_t wb = pb + Header::weightsFull;
-            if (pipe == 0) {
+            {
                 barExpectTx(wb, a.weightBytes);
                 for (int t = 0; t < 9; t++)
                     for (int g = 0; g < G; g++)
@@ -465,7 +454,7 @@ __global__ void __launch_bounds__(kPipeThreads * PIPES, PIPES > 1 ? 1 : (COUT <=
         // their slot's phase can complete.
         if (!ok) *abortFlag = 1;
         if (lane == 0) {
-            if (pipe == 0) pollPhase(pb + Header::weightsFull, 0u, limit);
+            pollPhase(pb + Header::weightsFull, 0u, limit);
             for (int e = q > kLowBufs ? q - kLowBufs : 0; e < q && Glow; e++)
                 pollPhase(pb + Header::lowFull + 8 * (e % kLowBufs), (uint32_t)((e / kLowBufs) & 1), limit);
             for (int e = q > R ? q - R : 0; e < q; e++) {
@@ -488,15 +477,16 @@ __global__ void __launch_bounds__(kPipeThreads * PIPES, PIPES > 1 ? 1 : (COUT <=
             const uint32_t idesc = ummaInstrDescBf16(kM, COUT);
             if (a.probe) ok = waitPhase(base + Header::probe, 0u, abortFlag, limit);
             if (ok)
-                ok = waitPhase(base + Header::weightsFull, 0u, abortFlag, limit);  // pipeline 0's barrier
+                ok = waitPhase(pb + Header::weightsFull, 0u, abortFlag, limit);
             uint64_t waitRowNs = 0, waitAccNs = 0;
             const uint64_t wDesc = ummaSmemDesc(wAddr, COUT * 16u, 128u);
             const int G2 = G / 2;
-            int rows = 0, tiles = 0;           // rows waited for, tiles issued
-            int waitSlot = 0, relSlot = 0;     // next row to wait for / to release
+            int rows = 0, tiles = 0, mine = 0;  // rows waited for, the block's tiles, this issuer's tiles
+            int waitSlot = 0, relSlot = 0;      // next row to wait for / to release
             uint32_t waitParity = 0;
-            int accB = 0;
+            int accB = 0;                       // this issuer's next accumulator (of nAcc)
             uint32_t accParity = 0;
+            const int accBase = me * a.nAcc;
             auto nextRow = [&](int& slot) -> bool {
                 const uint64_t t1 = a.stats ? nowNs() : 0;
                 slot = waitSlot;
@@ -514,26 +504,28 @@ __global__ void __launch_bounds__(kPipeThreads * PIPES, PIPES > 1 ? 1 : (COUT <=
                 const Unit U = unitOf(a, u);
                 int s0 = 0, s1 = 0, s2 = 0;  // slots of rows y - 1, y, y + 1
                 ok = nextRow(s0) && nextRow(s1);
-                for (int y = U.y0; y < U.y1 && ok; y++) {
+                for (int y = U.y0; y < U.y1 && ok; y++, tiles++) {
                     if (!nextRow(s2)) { ok = false; break; }
-                    {
-                        const uint64_t t1 = a.stats ? nowNs() : 0;
-                        ok = waitPhase(pb + Header::accEmpty + 8 * accB, accParity ^ 1u, abortFlag, limit);
-                        if (a.stats) waitAccNs += nowNs() - t1;
+                    if (tiles % ISS == me) {
+                        {
+                            const uint64_t t1 = a.stats ? nowNs() : 0;
+                            ok = waitPhase(pb + Header::accEmpty + 8 * (accBase + accB), accParity ^ 1u, abortFlag, limit);
+                            if (a.stats) waitAccNs += nowNs() - t1;
+                        }
+                        if (!ok) break;
+                        tcFenceAfter();
+                        const uint32_t acc = tmem + (uint32_t)(accBase + accB) * a.accCols;
+                        const uint64_t rowDesc[3] = {ummaSmemDesc(ringAddr + (uint32_t)s0 * slotBytes, kPlane, 128u),
+                                                     ummaSmemDesc(ringAddr + (uint32_t)s1 * slotBytes, kPlane, 128u),
+                                                     ummaSmemDesc(ringAddr + (uint32_t)s2 * slotBytes, kPlane, 128u)};
+                        issueTileG<COUT>(G2, acc, rowDesc, wDesc, idesc);
+                        commit(pb + Header::accFull + 8 * (accBase + accB));
+                        mine++;
+                        if (++accB == a.nAcc) { accB = 0; accParity ^= 1u; }
                     }
-                    if (!ok) break;
-                    tcFenceAfter();
-                    const uint32_t acc = tmem + (uint32_t)accB * a.accCols;
-                    const uint64_t rowDesc[3] = {ummaSmemDesc(ringAddr + (uint32_t)s0 * slotBytes, kPlane, 128u),
-                                                 ummaSmemDesc(ringAddr + (uint32_t)s1 * slotBytes, kPlane, 128u),
-                                                 ummaSmemDesc(ringAddr + (uint32_t)s2 * slotBytes, kPlane, 128u)};
-                    issueTileG<COUT>(G2, acc, rowDesc, wDesc, idesc);
-                    commit(pb + Header::accFull + 8 * accB);
-                    release();  // row y - 1: no later tile reads it
+                    release();  // row y - 1: no later tile reads it (this issuer's arrival)
                     s0 = s1;
                     s1 = s2;
-                    tiles++;
-                    if (++accB == a.nAcc) { accB = 0; accParity ^= 1u; }
                 }
                 if (!ok) break;
                 release();  // rows y1 - 1 and y1 of the strip: no later tile reads them
@@ -545,8 +537,8 @@ __global__ void __launch_bounds__(kPipeThreads * PIPES, PIPES > 1 ? 1 : (COUT <=
                 // accumulators) before the block's shared memory goes away.
                 for (int e = rows > R ? rows - R : 0; e < rows; e++)
                     pollPhase(pb + Header::empty + 8 * (e % R), (uint32_t)((e / R) & 1), limit);
-                for (int t = tiles > a.nAcc ? tiles - a.nAcc : 0; t < tiles; t++)
-                    pollPhase(pb + Header::accFull + 8 * (t % a.nAcc), (uint32_t)((t / a.nAcc) & 1), limit);
+                for (int t = mine > a.nAcc ? mine - a.nAcc : 0; t < mine; t++)
+                    pollPhase(pb + Header::accFull + 8 * (accBase + t % a.nAcc), (uint32_t)((t / a.nAcc) & 1), limit);
             } else {
                 *abortFlag = 1;
                 // Wait (bounded) for every MMA issued so far.
@@ -562,13 +554,18 @@ __global__ void __launch_bounds__(kPipeThreads * PIPES, PIPES > 1 ? 1 : (COUT <=
         // the block mod 4) ...: warps 2-5 of pipeline 0 and 8-11 of
         // pipeline 1 each cover the four quarters once.
         const int quarter = (int)(threadIdx.x >> 5) & 3;
-        int b = 0;
-        uint32_t parity = 0;
+        int bOf[ISS] = {};             // per issuer: next accumulator and its phase
+        uint32_t parityOf[ISS] = {};
+        int tile = 0;
         uint64_t waitNs = 0;
         bool ok = true;
         for (int u = firstUnit; u < a.units && ok; u += unitStride) {
             const Unit U = unitOf(a, u);
-            for (int y = U.y0; y < U.y1; y++, b = b + 1 == a.nAcc ? 0 : b + 1, parity ^= b == 0 ? 1u : 0u) {
+            for (int y = U.y0; y < U.y1; y++, tile++) {
+                const int i = tile % ISS;
+                const int b = i * a.nAcc + bOf[i];
+                const uint32_t parity = parityOf[i];
+                if (++bOf[i] == a.nAcc) { bOf[i] = 0; parityOf[i] ^= 1u; }
                 const uint64_t t1 = a.stats ? nowNs() : 0;
                 if (!waitPhaseWarp(pb + Header::accFull + 8 * b, parity, abortFlag, limit)) { ok = false; break; }
                 if (a.stats) waitNs += nowNs() - t1;
@@ -636,27 +633,27 @@ int deviceSmCount() {
     return sms > 0 ? sms : 1;
 }
 
-template <int COUT, int PIPES>
+template <int COUT, int ISS>
 cudaError_t launchPipe(const CUtensorMap& inMap, const CUtensorMap& lowMap, const CUtensorMap& wMap,
                        const PipeArgs& a, int grid, uint32_t smemBytes, cudaStream_t stream) {
     static bool configured = false;
     if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(convPipeKernel<COUT, PIPES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaError_t e = cudaFuncSetAttribute(convPipeKernel<COUT, ISS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              227 * 1024);
         if (e != cudaSuccess) return e;
         configured = true;
     }
-    convPipeKernel<COUT, PIPES><<<grid, kPipeThreads * PIPES, smemBytes, stream>>>(inMap, lowMap, wMap, a);
+    convPipeKernel<COUT, ISS><<<grid, kPipeThreads + 32 * (ISS - 1), smemBytes, stream>>>(inMap, lowMap, wMap, a);
     return cudaGetLastError();
 }
 
 }  // namespace
 
-uint32_t convPipeSmemBytes(int cin, int cout, int lowChannels, int ring, int pipes) {
+uint32_t convPipeSmemBytes(int cin, int cout, int lowChannels, int ring) {
     const uint32_t weights = 9u * (uint32_t)cin * (uint32_t)cout * 2u;
     const uint32_t slot = ((uint32_t)(cin / 8) * kPlane + 127u) & ~127u;
     const uint32_t lowSlot = ((uint32_t)(lowChannels / 8) * kLowPlane + 127u) & ~127u;
-    return kHeader + weights + (uint32_t)pipes * ((uint32_t)ring * slot + (uint32_t)kLowBufs * lowSlot);
+    return kHeader + weights + (uint32_t)ring * slot + (uint32_t)kLowBufs * lowSlot;
 }
 
 namespace {
@@ -667,7 +664,7 @@ bool knownCout(int c) { return c == 16 || c == 32 || c == 48 || c == 64 || c == 
 int pickSplits(int cin, int cout, int lowChannels) {
     for (int s : {1, 2, 3, 4, 6})
         if (cout % s == 0 && knownCout(cout / s) &&
-            convPipeSmemBytes(cin, cout / s, lowChannels, kMinRing, 1) <= 227u * 1024u)
+            convPipeSmemBytes(cin, cout / s, lowChannels, kMinRing) <= 227u * 1024u)
             return s;
     return 0;
 }
@@ -681,7 +678,7 @@ bool convPipeSupported(int cin, int cout, int lowChannels) {
 bool convPipePreferred(int cin, int cout, int lowChannels) {
     if (!convPipeSupported(cin, cout, lowChannels)) return false;
     const int s = pickSplits(cin, cout, lowChannels);
-    return convPipeSmemBytes(cin, cout / s, lowChannels, 4, 1) <= 227u * 1024u;
+    return convPipeSmemBytes(cin, cout / s, lowChannels, 4) <= 227u * 1024u;
 }
 
 cudaError_t convPipe(const bf16* in, const bf16* low, int lowChannels, int n, int h, int w, int cin,
@@ -727,9 +724,9 @@ cudaError_t convPipe(const bf16* in, const bf16* low, int lowChannels, int n, in
     a.accCols = 32;
     while (a.accCols < (uint32_t)cout) a.accCols <<= 1;
     a.nAcc = test && test->nAcc >= 2 && test->nAcc <= kMaxAcc ? test->nAcc : 2;
-    auto tmemColumns = [&](int pipes) {
+    auto tmemColumns = [&](int issuers) {
         uint32_t c = 32;
-        while (c < (uint32_t)pipes * (uint32_t)a.nAcc * a.accCols) c <<= 1;
+        while (c < (uint32_t)issuers * (uint32_t)a.nAcc * a.accCols) c <<= 1;
         return c;
     };
     a.tmemCols = tmemColumns(1);
@@ -743,57 +740,50 @@ cudaError_t convPipe(const bf16* in, const bf16* low, int lowChannels, int n, in
     // Blocks per SM from shared and tensor memory at a ring of 4 rows (3
     // where 4 do not fit); then the largest ring (up to kMaxRing rows) that
     // keeps that many blocks per SM. Where one block fits per SM (one MMA
-    // issuer per SM issues at about half the tensor pipe's rate), a block
-    // runs two pipelines on alternate units, sharing the weights, when two
-    // rings of 4 rows fit.
+    // issuer per SM issues at about half the tensor pipe's rate), the block
+    // runs two issuers on the same ring.
     const int sms = deviceSmCount();
     const uint32_t smemPerSm = 228u * 1024u, smemMax = 227u * 1024u;
-    a.ring = convPipeSmemBytes(cin, cout, lowChannels, 4, 1) <= smemMax ? 4 : kMinRing;
-    int perSm = (int)(smemPerSm / (convPipeSmemBytes(cin, cout, lowChannels, a.ring, 1) + 1024u));
+    a.ring = convPipeSmemBytes(cin, cout, lowChannels, 4) <= smemMax ? 4 : kMinRing;
+    int perSm = (int)(smemPerSm / (convPipeSmemBytes(cin, cout, lowChannels, a.ring) + 1024u));
     perSm = std::max(1, std::min({perSm, (int)(512u / a.tmemCols), 2048 / kPipeThreads}));
     if (test && test->blocksPerSm > 0 && test->blocksPerSm < perSm) perSm = test->blocksPerSm;
-    const int force = test ? test->pipes : 0;  // 1 or 2 pipelines
-    const bool twoFit = convPipeSmemBytes(cin, cout, lowChannels, 4, 2) <= smemMax && tmemColumns(2) <= 512u;
+    const int force = test ? test->issuers : 0;  // 1 or 2 issuers
+    const bool twoFit = tmemColumns(2) <= 512u && 2 * a.nAcc <= kMaxAcc;
     if (force == 2 && !twoFit) return cudaErrorNotSupported;
-    int pipes = 1;
-    if (force == 2 || (force == 0 && perSm == 1 && twoFit)) {
-        pipes = 2;
-        perSm = 1;
-        a.ring = 4;
-        a.tmemCols = tmemColumns(2);
-    }
+    const int issuers = (force == 2 || (force == 0 && perSm == 1 && twoFit)) ? 2 : 1;
+    a.tmemCols = tmemColumns(issuers);
     while (a.ring < kMaxRing &&
-           (uint32_t)perSm * (convPipeSmemBytes(cin, cout, lowChannels, a.ring + 1, pipes) + 1024u) <= smemPerSm &&
-           convPipeSmemBytes(cin, cout, lowChannels, a.ring + 1, pipes) <= smemMax)
+           (uint32_t)perSm * (convPipeSmemBytes(cin, cout, lowChannels, a.ring + 1) + 1024u) <= smemPerSm &&
+           convPipeSmemBytes(cin, cout, lowChannels, a.ring + 1) <= smemMax)
         a.ring++;
     if (test && test->ring >= kMinRing && test->ring <= kMaxRing) a.ring = test->ring;
-    const uint32_t smemBytes = convPipeSmemBytes(cin, cout, lowChannels, a.ring, pipes);
+    const uint32_t smemBytes = convPipeSmemBytes(cin, cout, lowChannels, a.ring);
     if (smemBytes > smemMax) return cudaErrorNotSupported;
-    a.pipeBytes = (uint32_t)a.ring * a.slotBytes + (uint32_t)kLowBufs * a.lowSlotBytes;
     // Strips: long enough to reuse rows (each strip stages 2 extra rows),
     // short enough to give every block about two units; every slice of
     // output channels walks all units.
     const long long columns = (long long)n * a.tilesPerRow;
     const long long blocks = std::max<long long>(nSplits, (long long)sms * perSm / nSplits * nSplits);
-    long long rows = std::max(1ll, columns * h * nSplits / (2 * blocks * pipes));
+    long long rows = std::max(1ll, columns * h * nSplits / (2 * blocks));
     a.stripRows = (int)std::max(4ll, std::min<long long>(32, rows));
     if (test && test->stripRows > 0) a.stripRows = test->stripRows;
     a.strips = (h + a.stripRows - 1) / a.stripRows;
     a.units = (int)(columns * a.strips);
     const int grid = (int)std::min<long long>((long long)a.units * nSplits, blocks);
     switch (cout) {
-        case 16: return pipes == 2 ? launchPipe<16, 2>(inMap, lowMap, wMap, a, grid, smemBytes, stream)
-                           : launchPipe<16, 1>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
-        case 32: return pipes == 2 ? launchPipe<32, 2>(inMap, lowMap, wMap, a, grid, smemBytes, stream)
-                           : launchPipe<32, 1>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
-        case 48: return pipes == 2 ? launchPipe<48, 2>(inMap, lowMap, wMap, a, grid, smemBytes, stream)
-                           : launchPipe<48, 1>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
-        case 64: return pipes == 2 ? launchPipe<64, 2>(inMap, lowMap, wMap, a, grid, smemBytes, stream)
-                           : launchPipe<64, 1>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
-        case 80: return pipes == 2 ? launchPipe<80, 2>(inMap, lowMap, wMap, a, grid, smemBytes, stream)
-                           : launchPipe<80, 1>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
-        case 96: return pipes == 2 ? launchPipe<96, 2>(inMap, lowMap, wMap, a, grid, smemBytes, stream)
-                           : launchPipe<96, 1>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
+        case 16: return issuers == 2 ? launchPipe<16, 2>(inMap, lowMap, wMap, a, grid, smemBytes, stream)
+                             : launchPipe<16, 1>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
+        case 32: return issuers == 2 ? launchPipe<32, 2>(inMap, lowMap, wMap, a, grid, smemBytes, stream)
+                             : launchPipe<32, 1>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
+        case 48: return issuers == 2 ? launchPipe<48, 2>(inMap, lowMap, wMap, a, grid, smemBytes, stream)
+                             : launchPipe<48, 1>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
+        case 64: return issuers == 2 ? launchPipe<64, 2>(inMap, lowMap, wMap, a, grid, smemBytes, stream)
+                             : launchPipe<64, 1>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
+        case 80: return issuers == 2 ? launchPipe<80, 2>(inMap, lowMap, wMap, a, grid, smemBytes, stream)
+                             : launchPipe<80, 1>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
+        case 96: return issuers == 2 ? launchPipe<96, 2>(inMap, lowMap, wMap, a, grid, smemBytes, stream)
+                             : launchPipe<96, 1>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
         default: return cudaErrorNotSupported;
     }
 }

@@ -66,7 +66,7 @@ struct ConvPipeTest {
     int nAcc;                        // tensor-memory accumulators (2..8)
     unsigned long long* stats;       // device array of 6 wait/lifetime sums in ns (see rt_conv_pipe.cu)
     int blocksPerSm;                 // fewer blocks per SM than shared memory allows (each then gets a longer ring)
-    int pipes;                       // pipelines per block: 0 chosen per layer, 1, or 2 (on alternate units)
+    int issuers;                     // MMA issuers per block: 0 chosen per layer, 1, or 2 (sharing the ring)
 };
 
 // The same convolution as convTc, warp-specialised and fed by TMA (input
@@ -81,7 +81,7 @@ bool convPipeSupported(int cin, int cout, int lowChannels);
 // kernel is faster (1080p decoder layers 112->48 and 160->64: 287 and 368 us
 // pipelined against 207 and 210 us).
 bool convPipePreferred(int cin, int cout, int lowChannels);
-uint32_t convPipeSmemBytes(int cin, int cout, int lowChannels, int ring, int pipes = 1);
+uint32_t convPipeSmemBytes(int cin, int cout, int lowChannels, int ring);
 cudaError_t convPipe(const __nv_bfloat16* in, const __nv_bfloat16* low, int lowChannels, int n, int h, int w, int cin,
                      const __nv_bfloat16* weights, bool reverseTaps, const float* bias, int cout,
                      __nv_bfloat16* outB, float* outF, bool relu, bool accumulate, int* errorFlag,
