@@ -20,6 +20,10 @@ Line fields beyond the common contract:
   build         GPU BVH build (binned SAH + wide collapse), Mtris/s
   reference_cuda  the reference's own CUDA renderer built for sm_100a, same
                 scene and settings, when oracle/_ref is present
+  config1       the small configuration (5,132-triangle Cornell box,
+                256x256, 64 paths per pixel as 4 passes of 16, depth 4):
+                this library's device time, and the reference's CPU loop on
+                one core (its backend 0) over a bounded row sample
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 For N > 1 run under torch.distributed.run; each rank renders its own copy of
@@ -277,6 +281,67 @@ def cpu_baseline(tris, cam, settings, w, h, budget_s):
                   f'{rays} rays in {elapsed:.2f} s',
         'seconds': elapsed, 'rays': rays,
     }
+
+
+def guarded(fn, *args):
+    """An auxiliary measurement that must not cost the bench line."""
+    try:
+        return fn(*args)
+    except Exception as e:  # reported in the line instead
+        return {'error': f'{type(e).__name__}: {e}'}
+
+
+def config1_run(lib, budget_s=6.0):
+    """Config 1 (scenes.cornell_sphere: 256x256, 64 paths per pixel as 4
+    passes of 16, depth 4) on the GPU through the session, and the
+    reference's CPU render loop on one thread (its backend 0,
+    Native/renderer.cu:405-416) over evenly spaced rows of one 16-path pass,
+    sized to about budget_s seconds. Rays of the CPU sample are counted by
+    the oracle on the same rows (identical paths)."""
+    import scenes
+    from native_api import Session
+    from oracle_api import Oracle, Reference, reference_available
+    tris, cam, st, w, h = scenes.cornell_sphere()
+    st.raysPerPixel = 16
+    with Session(lib) as s:
+        s.initialize(tris, w, h)
+        s.render_device(cam, st)  # warm-up pass
+        s.lib.RtReset(s.handle)
+        ms, rays = 0.0, 0
+        for _ in range(4):
+            ms += s.render_device(cam, st)
+            stats = s.render_stats()
+            rays += int(stats['primaryRays'] + stats['secondaryRays'] + stats['shadowRays'])
+        assert s.sample_count() == 64
+    kind = 'reference' if reference_available() else 'port'
+    impl = Reference() if kind == 'reference' else Oracle()
+    sc = impl.scene(tris)
+    t0 = time.perf_counter()
+    impl.render(sc, cam, st, w, h, rows=(h // 2, h // 2 + 1), threads=1)
+    per_row = max(time.perf_counter() - t0, 1e-4)
+    stride = max(1, h // int(max(1, min(h, budget_s / per_row))))
+    rows = sample_rows(h, stride)
+    t0 = time.perf_counter()
+    for y in rows:
+        impl.render(sc, cam, st, w, h, rows=(y, y + 1), threads=1)
+    elapsed = time.perf_counter() - t0
+    sc.close()
+    o = Oracle()
+    osc = o.scene(tris)
+    cpu_rays = 0
+    for y in rows:
+        _, _, counts = o.render(osc, cam, st, w, h, rows=(y, y + 1))
+        cpu_rays += int(counts[0] + counts[1] + counts[2])
+    osc.close()
+    cpu_rate = cpu_rays / elapsed / 1e6
+    gpu_rate = rays / ms / 1e3
+    return {'workload': 'cornell_sphere 5,132 triangles, 256x256, 64 spp (4 passes of 16), depth 4',
+            'gpu': {'device_ms': ms, 'mrays_per_s': gpu_rate, 'rays': rays},
+            'cpu_single_core': {'value': cpu_rate, 'unit': METRIC, 'cores': 1, 'kind': kind,
+                                'sample': f'{len(rows)} of {h} rows (every {stride}th) x {w} px x 16 spp, '
+                                          f'{cpu_rays} rays in {elapsed:.2f} s',
+                                'estimated_full_config_s': rays / (cpu_rate * 1e6) if cpu_rate > 0 else None},
+            'speedup_vs_single_core': gpu_rate / cpu_rate if cpu_rate > 0 else None}
 
 
 def reference_cuda(tris, cam, settings, w, h, rays_per_step, first_pass, steps=3):
@@ -967,6 +1032,7 @@ def run_ours(args, rank, local_rank, world):
             'wall_ms_per_step': wall * 1e3 / args.steps,
             'build': build_report(tris, bvh, init_wall_ms, peak, peak_kind),
             'reference_cuda': ref_cuda,
+            'config1': guarded(config1_run, lib) if (not args.no_cpu_baseline and world == 1) else None,
             'time_to_35db': quality_run(lib, args) if (args.quality and world == 1) else None,
             'batch': batch_run(lib, args) if (args.batch and world == 1) else None,
             'denoiser': denoiser_run(lib, args) if (args.denoiser and world == 1) else None,
