@@ -84,6 +84,10 @@ struct PipeArgs {
     unsigned long long waitLimitNs;
     int probe;  // 1: the issuer first waits on a barrier nothing completes (tests the abort path)
     int nAcc;   // accumulators in tensor memory (2..kMaxAcc)
+    // Optional addend of the upsampled half of a decoder convolution, at half
+    // resolution: 4 blocks of coutTotal channels per low pixel, block
+    // (y % 2) * 2 + x % 2 for output pixel (x, y); added before bias and ReLU.
+    const bf16* upAdd;
     // Optional wait statistics (test hook), nanoseconds summed over blocks:
     // [0] producer waiting for a free slot, [1] producer waiting for a low
     // row, [2] issuer waiting for rows, [3] issuer waiting for a drained
@@ -258,14 +262,30 @@ __device__ __forceinline__ Unit unitOf(const PipeArgs& a, int u) {
 }
 
 template <int COUT>
-__device__ __forceinline__ void epilogueStore(const PipeArgs& a, const uint32_t (&acc)[COUT], size_t pix, int nBase,
-                                              const float* bias) {
+__device__ __forceinline__ void epilogueStore(const PipeArgs& a, const uint32_t (&acc)[COUT], int img, int y, int x,
+                                              int nBase, const float* bias) {
+    const size_t pix = ((size_t)img * a.h + y) * a.w + x;
     float v[COUT];
 #pragma unroll
-    for (int j = 0; j < COUT; j++) {
-        const float s = __uint_as_float(acc[j]) + bias[j];  // shared memory: one broadcast read
-        v[j] = a.relu ? fmaxf(s, 0.0f) : s;
+    for (int j = 0; j < COUT; j++) v[j] = __uint_as_float(acc[j]) + bias[j];  // bias: one broadcast read from shared memory
+    if (a.upAdd) {
+        const size_t low = ((size_t)img * (a.h / 2) + y / 2) * (a.w / 2) + x / 2;
+        const uint4* u = reinterpret_cast<const uint4*>(a.upAdd + low * 4 * a.coutTotal +
+                                                        (size_t)((y & 1) * 2 + (x & 1)) * a.coutTotal + nBase);
+#pragma unroll
+        for (int q = 0; q < COUT / 8; q++) {
+            const uint4 word = __ldg(u + q);
+            const __nv_bfloat162* pairs = reinterpret_cast<const __nv_bfloat162*>(&word);
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const float2 f = __bfloat1622float2(pairs[j]);
+                v[8 * q + 2 * j] += f.x;
+                v[8 * q + 2 * j + 1] += f.y;
+            }
+        }
     }
+#pragma unroll
+    for (int j = 0; j < COUT; j++) v[j] = a.relu ? fmaxf(v[j], 0.0f) : v[j];
     if (a.outF) {
         float4* o = reinterpret_cast<float4*>(a.outF + pix * a.coutTotal + nBase);
 #pragma unroll
@@ -584,7 +604,7 @@ __global__ void __launch_bounds__(kPipeThreads + 32 * (ISS - 1), ISS > 1 ? 1 : (
                 __syncwarp();
                 if (lane == 0) barArrive(pb + Header::accEmpty + 8 * b);
                 const int x = U.x0 + quarter * 32 + lane;
-                if (x < a.w) epilogueStore<COUT>(a, acc, ((size_t)U.img * a.h + y) * a.w + x, nBase, sBias);
+                if (x < a.w) epilogueStore<COUT>(a, acc, U.img, y, x, nBase, sBias);
             }
         }
         if (a.stats && lane == 0) atomicAdd(a.stats + 4, waitNs);
@@ -683,10 +703,11 @@ bool convPipePreferred(int cin, int cout, int lowChannels) {
 
 cudaError_t convPipe(const bf16* in, const bf16* low, int lowChannels, int n, int h, int w, int cin,
                      const bf16* weights, bool reverseTaps, const float* bias, int coutTotal, bf16* outB, float* outF,
-                     bool relu, bool accumulate, int* errorFlag, cudaStream_t stream, const ConvPipeTest* test) {
+                     bool relu, bool accumulate, int* errorFlag, cudaStream_t stream, const ConvPipeTest* test,
+                     const bf16* upAddend) {
     if (!low) lowChannels = 0;
     if (n < 1 || h < 1 || w < 1 || !convPipeSupported(cin, coutTotal, lowChannels) || (!outB && !outF) ||
-        !errorFlag || (lowChannels && (h % 2 || w % 2)))
+        !errorFlag || (lowChannels && (h % 2 || w % 2)) || (upAddend && (h % 2 || w % 2 || lowChannels)))
         return cudaErrorNotSupported;
     const int nSplits = pickSplits(cin, coutTotal, lowChannels);
     const int cout = coutTotal / nSplits;  // output channels per block
@@ -732,7 +753,7 @@ cudaError_t convPipe(const bf16* in, const bf16* low, int lowChannels, int n, in
     a.tmemCols = tmemColumns(1);
     if (a.tmemCols > 512) return cudaErrorNotSupported;
     a.stats = test ? test->stats : nullptr;
-    a.bias = bias; a.outB = outB; a.outF = outF;
+    a.bias = bias; a.outB = outB; a.outF = outF; a.upAdd = upAddend;
     a.relu = relu ? 1 : 0; a.accumulate = accumulate ? 1 : 0; a.reverseTaps = reverseTaps ? 1 : 0;
     a.errorFlag = errorFlag;
     a.waitLimitNs = test && test->waitLimitNs ? test->waitLimitNs : 1000000000ull;

@@ -463,9 +463,64 @@ void convLaunchCounts(long long* pipe, long long* single) {
     if (single) *single = g_singleLaunches.load();
 }
 
+namespace {
+// Low-resolution tap (a, b) of output parity (py, px) collects the full taps
+// (dy, dx) with floor((py + dy - 1) / 2) = a - 1 and floor((px + dx - 1) / 2)
+// = b - 1: nearest upsampling maps upsampled pixel 2i + t to low pixel i.
+__global__ void combineUpsampledWeightsKernel(const bf16* w, int cout, int cin, int lowChannels, bf16* lowW,
+                                              bf16* skipW) {
+    const int skipC = cin - lowChannels;
+    const long long nLow = 9ll * 4 * cout * lowChannels, nSkip = 9ll * cout * skipC;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nLow + nSkip;
+         i += (long long)gridDim.x * blockDim.x) {
+        if (i < nLow) {
+            const int ci = (int)(i % lowChannels);
+            const int row = (int)((i / lowChannels) % (4 * cout));
+            const int tap = (int)(i / lowChannels / (4 * cout));
+            const int blk = row / cout, c = row % cout, py = blk >> 1, px = blk & 1;
+            const int a = tap / 3, b = tap % 3;
+            float sum = 0.0f;
+            for (int dy = 0; dy < 3; dy++) {
+                if (((py + dy + 1) >> 1) != a) continue;  // floor((py + dy - 1) / 2) + 1
+                for (int dx = 0; dx < 3; dx++) {
+                    if (((px + dx + 1) >> 1) != b) continue;
+                    sum += __bfloat162float(w[((size_t)(dy * 3 + dx) * cout + c) * cin + ci]);
+                }
+            }
+            lowW[i] = __float2bfloat16(sum);
+        } else {
+            const long long j = i - nLow;
+            const int ci = (int)(j % skipC);
+            const int c = (int)((j / skipC) % cout);
+            const int tap = (int)(j / skipC / cout);
+            skipW[j] = w[((size_t)tap * cout + c) * cin + lowChannels + ci];
+        }
+    }
+}
+}  // namespace
+
+cudaError_t combineUpsampledWeights(const bf16* weights, int cout, int cin, int lowChannels, bf16* lowWeights,
+                                    bf16* skipWeights, cudaStream_t stream) {
+    if (!weights || !lowWeights || !skipWeights || lowChannels <= 0 || lowChannels >= cin) return cudaErrorInvalidValue;
+    combineUpsampledWeightsKernel<<<296, 256, 0, stream>>>(weights, cout, cin, lowChannels, lowWeights, skipWeights);
+    return cudaGetLastError();
+}
+
+bool upsampledSplitSupported(int cin, int cout, int lowChannels) {
+    return lowChannels > 0 && lowChannels < cin && convPipePreferred(lowChannels, 4 * cout, 0) &&
+           convPipePreferred(cin - lowChannels, cout, 0);
+}
+
 cudaError_t convTc(const bf16* in, const bf16* low, int lowChannels, int n, int h, int w, int cin,
                    const bf16* weights, bool reverseTaps, const float* bias, int cout, bf16* outB, float* outF,
-                   bool relu, bool accumulate, int* errorFlag, cudaStream_t stream) {
+                   bool relu, bool accumulate, int* errorFlag, cudaStream_t stream, const bf16* upAddend) {
+    if (upAddend) {  // the second pass of the two-pass decoder form: pipelined kernel only
+        if (low || !convPipePreferred(cin, cout, 0)) return cudaErrorNotSupported;
+        cudaError_t e = convPipe(in, nullptr, 0, n, h, w, cin, weights, reverseTaps, bias, cout, outB, outF, relu,
+                                 accumulate, errorFlag, stream, nullptr, upAddend);
+        if (e == cudaSuccess) g_pipeLaunches++;
+        return e;
+    }
     // The warp-specialised TMA form where its shared memory allows (see
     // rt_conv_pipe.cu); this kernel for the layers with the largest weights.
     if (g_convPath.load() == 0 && convPipePreferred(cin, cout, low ? lowChannels : 0)) {

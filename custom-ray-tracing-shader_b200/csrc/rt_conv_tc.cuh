@@ -46,9 +46,28 @@ __host__ __device__ constexpr uint64_t ummaSmemDesc(uint32_t address, uint32_t l
 // With `low` set, the input is the concatenation [upsample2(low), in] read
 // in place: channels [0, lowChannels) from low (h/2 x w/2, nearest) and the
 // rest from `in` (cin - lowChannels channels per pixel); h and w even.
+// upAddend (optional, pipelined form only): the upsampled half of a decoder
+// convolution computed at half resolution (see combineUpsampledWeights),
+// 4 blocks of cout channels per low pixel, added before bias and ReLU.
 cudaError_t convTc(const __nv_bfloat16* in, const __nv_bfloat16* low, int lowChannels, int n, int h, int w, int cin,
                    const __nv_bfloat16* weights, bool reverseTaps, const float* bias, int cout, __nv_bfloat16* outB,
-                   float* outF, bool relu, bool accumulate, int* errorFlag, cudaStream_t stream);
+                   float* outF, bool relu, bool accumulate, int* errorFlag, cudaStream_t stream,
+                   const __nv_bfloat16* upAddend = nullptr);
+
+// A decoder convolution over [upsample2(low), skip] as two convolutions:
+// the low half at low resolution with 4 blocks of cout output channels, one
+// per output-pixel parity (py, px) (nearest upsampling makes each output
+// pixel's 3x3 window over the upsampled image a 3x3 window over the low
+// image with some taps merged), and the skip half at full resolution, whose
+// epilogue adds the first's block (see convTc's upAddend). This writes the
+// low half's weights [tap'][4 * cout][lowChannels] (tap' over the low
+// image's 3x3 window, block (py, px) = sum of the full taps that land
+// there) and the skip half's [tap][cout][cin - lowChannels], both BF16 (the
+// sums in FP32), from the forward weights [tap][cout][cin].
+cudaError_t combineUpsampledWeights(const __nv_bfloat16* weights, int cout, int cin, int lowChannels,
+                                    __nv_bfloat16* lowWeights, __nv_bfloat16* skipWeights, cudaStream_t stream);
+// Whether the two-pass form runs on the pipelined kernel for this layer.
+bool upsampledSplitSupported(int cin, int cout, int lowChannels);
 
 // Which kernel convTc runs: 0 (default) the pipelined form wherever it
 // applies, 1 always the kernel above (process-wide; for comparisons).
@@ -85,7 +104,8 @@ uint32_t convPipeSmemBytes(int cin, int cout, int lowChannels, int ring);
 cudaError_t convPipe(const __nv_bfloat16* in, const __nv_bfloat16* low, int lowChannels, int n, int h, int w, int cin,
                      const __nv_bfloat16* weights, bool reverseTaps, const float* bias, int cout,
                      __nv_bfloat16* outB, float* outF, bool relu, bool accumulate, int* errorFlag,
-                     cudaStream_t stream, const ConvPipeTest* test = nullptr);
+                     cudaStream_t stream, const ConvPipeTest* test = nullptr,
+                     const __nv_bfloat16* upAddend = nullptr);
 
 // Weight gradient on tcgen05 (rt_wgrad_tc.cu): dw[tap][ci][co] += sum_p
 // x[p + off(tap)][ci] dy[p][co] over NHWC BF16 x (cin channels) and dy (cout

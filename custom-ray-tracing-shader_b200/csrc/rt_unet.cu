@@ -385,6 +385,12 @@ struct Unet::Activations {
     bf16* a[18] = {};        // outputs of the 18 3x3 layers
     bf16* pool[4] = {};      // pooled encoder outputs (levels 1..4 inputs)
     bf16* cat[4] = {};       // decoder inputs: concat(upsample(lower), skip) at levels 3..0
+    // Two-pass form of the decoders' first convolutions (inference): the
+    // upsampled half at half resolution (4 parity blocks of cout channels)
+    // and each layer's combined weights (low half, skip half).
+    bf16* upHalf = nullptr;
+    bf16* upWeights[4] = {};
+    bf16* skipWeights[4] = {};
     float* pred = nullptr;   // network output, log space
     float* target = nullptr; // log-space target
     float* dPred = nullptr;
@@ -529,11 +535,20 @@ cudaError_t Unet::ensure(int n, int h, int w, bool training) {
         if ((e = A.make(A.pool[l - 1], px(l) * kWidths[l - 1])) != cudaSuccess) return e;
         if (training && (e = A.make(A.dPool[l - 1], px(l) * kWidths[l - 1])) != cudaSuccess) return e;
     }
+    size_t upHalf = 0;
     for (int j = 0; j < 4; j++) {  // decoder level 3 - j
         int level = 3 - j;
+        const UnetLayer& L = layers_[10 + 2 * j];
+        const int Cl = layers_[9 + 2 * j].cout;
+        if (upsampledSplitSupported(L.cin, L.cout, Cl)) {
+            upHalf = std::max(upHalf, px(level) * L.cout);  // (H / 2) x (W / 2) x 4 cout
+            if ((e = A.make(A.upWeights[j], (size_t)9 * 4 * L.cout * Cl)) != cudaSuccess) return e;
+            if ((e = A.make(A.skipWeights[j], (size_t)9 * L.cout * (L.cin - Cl))) != cudaSuccess) return e;
+        }
         if (training && (e = A.make(A.cat[j], px(level) * layers_[10 + 2 * j].cin)) != cudaSuccess) return e;
         if (training && (e = A.make(A.dCat[j], px(level) * layers_[10 + 2 * j].cin)) != cudaSuccess) return e;
     }
+    if (upHalf && (e = A.make(A.upHalf, upHalf)) != cudaSuccess) return e;
     if ((e = A.make(A.pred, px(0) * kOutChannels)) != cudaSuccess) return e;
     if (training) {
         if ((e = A.make(A.target, px(0) * kOutChannels)) != cudaSuccess) return e;
@@ -576,6 +591,16 @@ cudaError_t Unet::forward(cudaStream_t s, bool training, bool outputLayer) {
                 // The weight gradient reads the concatenated input: keep it.
                 upConcatKernel<<<blocksFor((long long)n * H * W * (Cl + Cs), 256), 256, 0, s>>>(low, Cl, skip, Cs, n, H, W, A.cat[j]);
                 e = convTc(A.cat[j], nullptr, 0, n, H, W, L.cin, wT_ + L.wOffset, false, master_ + L.bOffset, L.cout, A.a[k], nullptr, true, false, convError_, s);
+            } else if (r == 0 && A.upWeights[j] && convPath() == 0) {
+                // Inference, two passes: the upsampled half at half
+                // resolution (4 parity blocks), then the skip half adding it.
+                e = combineUpsampledWeights(wT_ + L.wOffset, L.cout, L.cin, Cl, A.upWeights[j], A.skipWeights[j], s);
+                if (e == cudaSuccess)
+                    e = convTc(low, nullptr, 0, n, H / 2, W / 2, Cl, A.upWeights[j], false, nullptr, 4 * L.cout, A.upHalf,
+                               nullptr, false, false, convError_, s);
+                if (e == cudaSuccess)
+                    e = convTc(skip, nullptr, 0, n, H, W, Cs, A.skipWeights[j], false, master_ + L.bOffset, L.cout, A.a[k],
+                               nullptr, true, false, convError_, s, A.upHalf);
             } else if (r == 0) {
                 // Inference: the convolution reads [upsample(low), skip] in place.
                 e = convTc(skip, low, Cl, n, H, W, L.cin, wT_ + L.wOffset, false, master_ + L.bOffset, L.cout, A.a[k], nullptr, true, false, convError_, s);
