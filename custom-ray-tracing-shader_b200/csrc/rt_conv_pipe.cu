@@ -261,21 +261,28 @@ __device__ __forceinline__ Unit unitOf(const PipeArgs& a, int u) {
     return Unit{img, xt * kM, y0, min(a.h, y0 + a.stripRows)};
 }
 
+// The upsampled-half addend of output pixel (x, y) (see PipeArgs::upAdd),
+// loaded before the epilogue waits for its accumulator so the load's latency
+// overlaps the wait.
+template <int COUT>
+__device__ __forceinline__ void loadUpAddend(const PipeArgs& a, int img, int y, int x, int nBase, uint4 (&u)[COUT / 8]) {
+    const size_t low = ((size_t)img * (a.h / 2) + y / 2) * (a.w / 2) + x / 2;
+    const uint4* src = reinterpret_cast<const uint4*>(a.upAdd + low * 4 * a.coutTotal +
+                                                      (size_t)((y & 1) * 2 + (x & 1)) * a.coutTotal + nBase);
+#pragma unroll
+    for (int q = 0; q < COUT / 8; q++) u[q] = __ldg(src + q);
+}
 template <int COUT>
 __device__ __forceinline__ void epilogueStore(const PipeArgs& a, const uint32_t (&acc)[COUT], int img, int y, int x,
-                                              int nBase, const float* bias) {
+                                              int nBase, const float* bias, const uint4 (&up)[COUT / 8]) {
     const size_t pix = ((size_t)img * a.h + y) * a.w + x;
     float v[COUT];
 #pragma unroll
     for (int j = 0; j < COUT; j++) v[j] = __uint_as_float(acc[j]) + bias[j];  // bias: one broadcast read from shared memory
     if (a.upAdd) {
-        const size_t low = ((size_t)img * (a.h / 2) + y / 2) * (a.w / 2) + x / 2;
-        const uint4* u = reinterpret_cast<const uint4*>(a.upAdd + low * 4 * a.coutTotal +
-                                                        (size_t)((y & 1) * 2 + (x & 1)) * a.coutTotal + nBase);
 #pragma unroll
         for (int q = 0; q < COUT / 8; q++) {
-            const uint4 word = __ldg(u + q);
-            const __nv_bfloat162* pairs = reinterpret_cast<const __nv_bfloat162*>(&word);
+            const __nv_bfloat162* pairs = reinterpret_cast<const __nv_bfloat162*>(&up[q]);
 #pragma unroll
             for (int j = 0; j < 4; j++) {
                 const float2 f = __bfloat1622float2(pairs[j]);
@@ -586,6 +593,9 @@ __global__ void __launch_bounds__(kPipeThreads + 32 * (ISS - 1), ISS > 1 ? 1 : (
                 const int b = i * a.nAcc + bOf[i];
                 const uint32_t parity = parityOf[i];
                 if (++bOf[i] == a.nAcc) { bOf[i] = 0; parityOf[i] ^= 1u; }
+                const int x = U.x0 + quarter * 32 + lane;
+                uint4 up[COUT / 8];
+                if (a.upAdd && x < a.w) loadUpAddend<COUT>(a, U.img, y, x, nBase, up);
                 const uint64_t t1 = a.stats ? nowNs() : 0;
                 if (!waitPhaseWarp(pb + Header::accFull + 8 * b, parity, abortFlag, limit)) { ok = false; break; }
                 if (a.stats) waitNs += nowNs() - t1;
@@ -603,8 +613,7 @@ __global__ void __launch_bounds__(kPipeThreads + 32 * (ISS - 1), ISS > 1 ? 1 : (
                 tcFenceBefore();
                 __syncwarp();
                 if (lane == 0) barArrive(pb + Header::accEmpty + 8 * b);
-                const int x = U.x0 + quarter * 32 + lane;
-                if (x < a.w) epilogueStore<COUT>(a, acc, U.img, y, x, nBase, sBias);
+                if (x < a.w) epilogueStore<COUT>(a, acc, U.img, y, x, nBase, sBias, up);
             }
         }
         if (a.stats && lane == 0) atomicAdd(a.stats + 4, waitNs);
