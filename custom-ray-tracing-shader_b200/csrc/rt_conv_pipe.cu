@@ -68,7 +68,7 @@ constexpr int kMaxRing = 16;
 constexpr int kMaxAcc = 8;   // tensor-memory accumulators per block (tiles between the issuer and the epilogue)
 constexpr int kLowBufs = 4;  // staging rows of the low-resolution input (loads in flight ahead of the expansion)
 constexpr uint32_t kPipeHeader = 512;    // mbarriers (the rest of the header: flags and biases)
-constexpr uint32_t kHeader = 1024;       // barriers, flags and biases
+constexpr uint32_t kHeader = 2048;       // barriers, flags and biases
 
 struct PipeArgs {
     int n, h, w, cin, cout, lowChannels;
@@ -110,9 +110,9 @@ struct Header {
     static constexpr uint32_t probe = weights + 8;
     static constexpr uint32_t tmemSlot = weights + 16;
     static constexpr uint32_t abort = weights + 20;
-    static constexpr uint32_t bias = weights + 64;         // the block's output channels' biases (<= 96 floats)
+    static constexpr uint32_t bias = weights + 64;         // the block's output channels' biases (<= 128 floats)
 };
-static_assert(Header::weightsFull + 8 <= kPipeHeader && Header::bias + 96 * 4 <= kHeader, "header size");
+static_assert(Header::weightsFull + 8 <= kPipeHeader && Header::bias + 128 * 4 <= kHeader, "header size");
 
 __device__ __forceinline__ uint32_t smemAddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ uint64_t nowNs() {
@@ -263,26 +263,29 @@ __device__ __forceinline__ Unit unitOf(const PipeArgs& a, int u) {
 
 // The upsampled-half addend of output pixel (x, y) (see PipeArgs::upAdd),
 // loaded before the epilogue waits for its accumulator so the load's latency
-// overlaps the wait.
+// overlaps the wait (COUT <= 96; wider layers take no addend).
+__host__ __device__ constexpr int upWords(int cout) { return cout <= 96 ? cout / 8 : 1; }
 template <int COUT>
-__device__ __forceinline__ void loadUpAddend(const PipeArgs& a, int img, int y, int x, int nBase, uint4 (&u)[COUT / 8]) {
+__device__ __forceinline__ void loadUpAddend(const PipeArgs& a, int img, int y, int x, int nBase,
+                                             uint4 (&u)[upWords(COUT)]) {
     const size_t low = ((size_t)img * (a.h / 2) + y / 2) * (a.w / 2) + x / 2;
     const uint4* src = reinterpret_cast<const uint4*>(a.upAdd + low * 4 * a.coutTotal +
                                                       (size_t)((y & 1) * 2 + (x & 1)) * a.coutTotal + nBase);
 #pragma unroll
-    for (int q = 0; q < COUT / 8; q++) u[q] = __ldg(src + q);
+    for (int q = 0; q < upWords(COUT); q++) u[q] = __ldg(src + q);
 }
+// Bias, the addend, ReLU and the store of 16 output channels (c0 .. c0 + 15
+// of the block's COUT) of one pixel, from 16 accumulator columns.
 template <int COUT>
-__device__ __forceinline__ void epilogueStore(const PipeArgs& a, const uint32_t (&acc)[COUT], int img, int y, int x,
-                                              int nBase, const float* bias, const uint4 (&up)[COUT / 8]) {
-    const size_t pix = ((size_t)img * a.h + y) * a.w + x;
-    float v[COUT];
+__device__ __forceinline__ void epilogueStore16(const PipeArgs& a, const uint32_t (&acc)[16], size_t pix, int c0,
+                                                int nBase, const float* bias, const uint4 (&up)[upWords(COUT)]) {
+    float v[16];
 #pragma unroll
-    for (int j = 0; j < COUT; j++) v[j] = __uint_as_float(acc[j]) + bias[j];  // bias: one broadcast read from shared memory
-    if (a.upAdd) {
+    for (int j = 0; j < 16; j++) v[j] = __uint_as_float(acc[j]) + bias[c0 + j];  // bias: broadcast from shared memory
+    if (COUT <= 96 && a.upAdd) {
 #pragma unroll
-        for (int q = 0; q < COUT / 8; q++) {
-            const __nv_bfloat162* pairs = reinterpret_cast<const __nv_bfloat162*>(&up[q]);
+        for (int q = 0; q < 2; q++) {
+            const __nv_bfloat162* pairs = reinterpret_cast<const __nv_bfloat162*>(&up[c0 / 8 + q]);
 #pragma unroll
             for (int j = 0; j < 4; j++) {
                 const float2 f = __bfloat1622float2(pairs[j]);
@@ -292,11 +295,11 @@ __device__ __forceinline__ void epilogueStore(const PipeArgs& a, const uint32_t 
         }
     }
 #pragma unroll
-    for (int j = 0; j < COUT; j++) v[j] = a.relu ? fmaxf(v[j], 0.0f) : v[j];
+    for (int j = 0; j < 16; j++) v[j] = a.relu ? fmaxf(v[j], 0.0f) : v[j];
     if (a.outF) {
-        float4* o = reinterpret_cast<float4*>(a.outF + pix * a.coutTotal + nBase);
+        float4* o = reinterpret_cast<float4*>(a.outF + pix * a.coutTotal + nBase + c0);
 #pragma unroll
-        for (int q = 0; q < COUT / 4; q++) {
+        for (int q = 0; q < 4; q++) {
             float4 x = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
             if (a.accumulate) {
                 const float4 old = o[q];
@@ -305,9 +308,9 @@ __device__ __forceinline__ void epilogueStore(const PipeArgs& a, const uint32_t 
             o[q] = x;
         }
     } else {
-        uint4* o = reinterpret_cast<uint4*>(a.outB + pix * a.coutTotal + nBase);
+        uint4* o = reinterpret_cast<uint4*>(a.outB + pix * a.coutTotal + nBase + c0);
 #pragma unroll
-        for (int q = 0; q < COUT / 8; q++) {
+        for (int q = 0; q < 2; q++) {
             uint32_t words[4];
 #pragma unroll
             for (int j = 0; j < 4; j++) {
@@ -370,7 +373,7 @@ __global__ void __launch_bounds__(kPipeThreads + 32 * (ISS - 1), ISS > 1 ? 1 : (
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
     float* sBias = reinterpret_cast<float*>(smem + Header::bias);
-    if (threadIdx.x < COUT) sBias[threadIdx.x] = a.bias ? a.bias[nBase + threadIdx.x] : 0.0f;
+    for (int c = threadIdx.x; c < COUT; c += blockDim.x) sBias[c] = a.bias ? a.bias[nBase + c] : 0.0f;
     if (threadIdx.x >> 5 == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(base + Header::tmemSlot),
                      "r"(a.tmemCols)
@@ -594,26 +597,25 @@ __global__ void __launch_bounds__(kPipeThreads + 32 * (ISS - 1), ISS > 1 ? 1 : (
                 const uint32_t parity = parityOf[i];
                 if (++bOf[i] == a.nAcc) { bOf[i] = 0; parityOf[i] ^= 1u; }
                 const int x = U.x0 + quarter * 32 + lane;
-                uint4 up[COUT / 8];
-                if (a.upAdd && x < a.w) loadUpAddend<COUT>(a, U.img, y, x, nBase, up);
+                uint4 up[upWords(COUT)];
+                if (COUT <= 96 && a.upAdd && x < a.w) loadUpAddend<COUT>(a, U.img, y, x, nBase, up);
                 const uint64_t t1 = a.stats ? nowNs() : 0;
                 if (!waitPhaseWarp(pb + Header::accFull + 8 * b, parity, abortFlag, limit)) { ok = false; break; }
                 if (a.stats) waitNs += nowNs() - t1;
                 tcFenceAfter();
-                uint32_t acc[COUT];
-                const uint32_t lanes = (uint32_t)(quarter * 32) << 16;
+                // 16 accumulator columns at a time: load, finish and store.
+                const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)b * a.accCols;
+                const size_t pix = ((size_t)U.img * a.h + y) * a.w + x;
 #pragma unroll
                 for (int c = 0; c < COUT / 16; c++) {
                     uint32_t r[16];
-                    tmemLoad16(tmem + lanes + (uint32_t)b * a.accCols + (uint32_t)(16 * c), r);
-#pragma unroll
-                    for (int j = 0; j < 16; j++) acc[16 * c + j] = r[j];
+                    tmemLoad16(taddr + (uint32_t)(16 * c), r);
+                    tmemWaitLoads();
+                    if (x < a.w) epilogueStore16<COUT>(a, r, pix, 16 * c, nBase, sBias, up);
                 }
-                tmemWaitLoads();
                 tcFenceBefore();
                 __syncwarp();
                 if (lane == 0) barArrive(pb + Header::accEmpty + 8 * b);
-                if (x < a.w) epilogueStore<COUT>(a, acc, U.img, y, x, nBase, sBias, up);
             }
         }
         if (a.stats && lane == 0) atomicAdd(a.stats + 4, waitNs);
@@ -686,7 +688,7 @@ uint32_t convPipeSmemBytes(int cin, int cout, int lowChannels, int ring) {
 }
 
 namespace {
-bool knownCout(int c) { return c == 16 || c == 32 || c == 48 || c == 64 || c == 80 || c == 96; }
+bool knownCout(int c) { return c == 16 || c == 32 || c == 48 || c == 64 || c == 80 || c == 96 || c == 128; }
 // Output-channel slices per layer: the fewest (1, 2, 3, 4, 6) whose slice is
 // a supported width and whose weights fit beside a ring of kMinRing rows;
 // 0 when none does.
@@ -716,7 +718,8 @@ cudaError_t convPipe(const bf16* in, const bf16* low, int lowChannels, int n, in
                      const bf16* upAddend) {
     if (!low) lowChannels = 0;
     if (n < 1 || h < 1 || w < 1 || !convPipeSupported(cin, coutTotal, lowChannels) || (!outB && !outF) ||
-        !errorFlag || (lowChannels && (h % 2 || w % 2)) || (upAddend && (h % 2 || w % 2 || lowChannels)))
+        !errorFlag || (lowChannels && (h % 2 || w % 2)) ||
+        (upAddend && (h % 2 || w % 2 || lowChannels || coutTotal > 96)))
         return cudaErrorNotSupported;
     const int nSplits = pickSplits(cin, coutTotal, lowChannels);
     const int cout = coutTotal / nSplits;  // output channels per block
@@ -814,6 +817,8 @@ cudaError_t convPipe(const bf16* in, const bf16* low, int lowChannels, int n, in
                              : launchPipe<80, 1>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
         case 96: return issuers == 2 ? launchPipe<96, 2>(inMap, lowMap, wMap, a, grid, smemBytes, stream)
                              : launchPipe<96, 1>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
+        case 128: return issuers == 2 ? launchPipe<128, 2>(inMap, lowMap, wMap, a, grid, smemBytes, stream)
+                              : launchPipe<128, 1>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
         default: return cudaErrorNotSupported;
     }
 }

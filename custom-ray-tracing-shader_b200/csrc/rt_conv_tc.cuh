@@ -90,7 +90,7 @@ struct ConvPipeTest {
 
 // The same convolution as convTc, warp-specialised and fed by TMA (input
 // rows in a ring of shared-memory slots, weights resident): for Cout in {16,
-// 32, 48, 64, 80, 96} when the weights and a ring of 3 rows fit in shared
+// 32, 48, 64, 80, 96, 128} when the weights and a ring of 3 rows fit in shared
 // memory. Returns cudaErrorNotSupported (before any launch) for other
 // shapes. Same arguments as convTc, plus optional test hooks.
 bool convPipeSupported(int cin, int cout, int lowChannels);
