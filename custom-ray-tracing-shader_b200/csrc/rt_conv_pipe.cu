@@ -88,6 +88,7 @@ struct PipeArgs {
     // resolution: 4 blocks of coutTotal channels per low pixel, block
     // (y % 2) * 2 + x % 2 for output pixel (x, y); added before bias and ReLU.
     const bf16* upAdd;
+    ConvHead head;  // head.out set: the fused 1x1 output head (see ConvHead); activations not stored
     // Optional wait statistics (test hook), nanoseconds summed over blocks:
     // [0] producer waiting for a free slot, [1] producer waiting for a low
     // row, [2] issuer waiting for rows, [3] issuer waiting for a drained
@@ -278,7 +279,8 @@ __device__ __forceinline__ void loadUpAddend(const PipeArgs& a, int img, int y, 
 // of the block's COUT) of one pixel, from 16 accumulator columns.
 template <int COUT>
 __device__ __forceinline__ void epilogueStore16(const PipeArgs& a, const uint32_t (&acc)[16], size_t pix, int c0,
-                                                int nBase, const float* bias, const uint4 (&up)[upWords(COUT)]) {
+                                                int nBase, const float* bias, const uint4 (&up)[upWords(COUT)],
+                                                float (&headSum)[3]) {
     float v[16];
 #pragma unroll
     for (int j = 0; j < 16; j++) v[j] = __uint_as_float(acc[j]) + bias[c0 + j];  // bias: broadcast from shared memory
@@ -296,6 +298,16 @@ __device__ __forceinline__ void epilogueStore16(const PipeArgs& a, const uint32_
     }
 #pragma unroll
     for (int j = 0; j < 16; j++) v[j] = a.relu ? fmaxf(v[j], 0.0f) : v[j];
+    if (a.head.out) {
+        // The head reads the activations as BF16, channel by channel.
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+            const float x = __bfloat162float(__float2bfloat16_rn(v[j]));
+#pragma unroll
+            for (int k = 0; k < 3; k++) headSum[k] += x * __ldg(a.head.wt + (nBase + c0 + j) * 3 + k);
+        }
+        return;
+    }
     if (a.outF) {
         float4* o = reinterpret_cast<float4*>(a.outF + pix * a.coutTotal + nBase + c0);
 #pragma unroll
@@ -606,12 +618,22 @@ __global__ void __launch_bounds__(kPipeThreads + 32 * (ISS - 1), ISS > 1 ? 1 : (
                 // 16 accumulator columns at a time: load, finish and store.
                 const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)b * a.accCols;
                 const size_t pix = ((size_t)U.img * a.h + y) * a.w + x;
+                float headSum[3] = {0.0f, 0.0f, 0.0f};
+                if (a.head.out) {
+#pragma unroll
+                    for (int k = 0; k < 3; k++) headSum[k] = __ldg(a.head.b + k);
+                }
 #pragma unroll
                 for (int c = 0; c < COUT / 16; c++) {
                     uint32_t r[16];
                     tmemLoad16(taddr + (uint32_t)(16 * c), r);
                     tmemWaitLoads();
-                    if (x < a.w) epilogueStore16<COUT>(a, r, pix, 16 * c, nBase, sBias, up);
+                    if (x < a.w) epilogueStore16<COUT>(a, r, pix, 16 * c, nBase, sBias, up, headSum);
+                }
+                if (a.head.out && x < a.head.w && y < a.head.h) {
+                    float* o = a.head.out + ((size_t)y * a.head.w + x) * 3;
+#pragma unroll
+                    for (int k = 0; k < 3; k++) o[k] = fmaxf(expm1f(headSum[k]), 0.0f);
                 }
                 tcFenceBefore();
                 __syncwarp();
@@ -715,13 +737,15 @@ bool convPipePreferred(int cin, int cout, int lowChannels) {
 cudaError_t convPipe(const bf16* in, const bf16* low, int lowChannels, int n, int h, int w, int cin,
                      const bf16* weights, bool reverseTaps, const float* bias, int coutTotal, bf16* outB, float* outF,
                      bool relu, bool accumulate, int* errorFlag, cudaStream_t stream, const ConvPipeTest* test,
-                     const bf16* upAddend) {
+                     const bf16* upAddend, const ConvHead* head) {
     if (!low) lowChannels = 0;
-    if (n < 1 || h < 1 || w < 1 || !convPipeSupported(cin, coutTotal, lowChannels) || (!outB && !outF) ||
+    if (n < 1 || h < 1 || w < 1 || !convPipeSupported(cin, coutTotal, lowChannels) || (!outB && !outF && !head) ||
+        (head && (!head->out || !head->wt || !head->b || n != 1 || head->h > h || head->w > w)) ||
         !errorFlag || (lowChannels && (h % 2 || w % 2)) ||
         (upAddend && (h % 2 || w % 2 || lowChannels || coutTotal > 96)))
         return cudaErrorNotSupported;
     const int nSplits = pickSplits(cin, coutTotal, lowChannels);
+    if (head && nSplits != 1) return cudaErrorNotSupported;  // the head sums over all output channels of a pixel
     const int cout = coutTotal / nSplits;  // output channels per block
     const int cinIn = cin - lowChannels;
     CUtensorMap inMap{}, lowMap{}, wMap{};
@@ -766,6 +790,7 @@ cudaError_t convPipe(const bf16* in, const bf16* low, int lowChannels, int n, in
     if (a.tmemCols > 512) return cudaErrorNotSupported;
     a.stats = test ? test->stats : nullptr;
     a.bias = bias; a.outB = outB; a.outF = outF; a.upAdd = upAddend;
+    if (head) a.head = *head;
     a.relu = relu ? 1 : 0; a.accumulate = accumulate ? 1 : 0; a.reverseTaps = reverseTaps ? 1 : 0;
     a.errorFlag = errorFlag;
     a.waitLimitNs = test && test->waitLimitNs ? test->waitLimitNs : 1000000000ull;

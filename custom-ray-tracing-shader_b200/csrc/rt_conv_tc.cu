@@ -513,11 +513,12 @@ bool upsampledSplitSupported(int cin, int cout, int lowChannels) {
 
 cudaError_t convTc(const bf16* in, const bf16* low, int lowChannels, int n, int h, int w, int cin,
                    const bf16* weights, bool reverseTaps, const float* bias, int cout, bf16* outB, float* outF,
-                   bool relu, bool accumulate, int* errorFlag, cudaStream_t stream, const bf16* upAddend) {
-    if (upAddend) {  // the second pass of the two-pass decoder form: pipelined kernel only
+                   bool relu, bool accumulate, int* errorFlag, cudaStream_t stream, const bf16* upAddend,
+                   const ConvHead* head) {
+    if (upAddend || head) {  // the two-pass decoder form's second pass, a fused head: pipelined kernel only
         if (low || !convPipePreferred(cin, cout, 0)) return cudaErrorNotSupported;
         cudaError_t e = convPipe(in, nullptr, 0, n, h, w, cin, weights, reverseTaps, bias, cout, outB, outF, relu,
-                                 accumulate, errorFlag, stream, nullptr, upAddend);
+                                 accumulate, errorFlag, stream, nullptr, upAddend, head);
         if (e == cudaSuccess) g_pipeLaunches++;
         return e;
     }

@@ -46,13 +46,25 @@ __host__ __device__ constexpr uint64_t ummaSmemDesc(uint32_t address, uint32_t l
 // With `low` set, the input is the concatenation [upsample2(low), in] read
 // in place: channels [0, lowChannels) from low (h/2 x w/2, nearest) and the
 // rest from `in` (cin - lowChannels channels per pixel); h and w even.
+// A 1x1 output head fused into a convolution's epilogue (pipelined form
+// only): for the output pixels inside crop (w x h, row stride w), out[pixel]
+// [k] = max(expm1(b[k] + sum_c bf16(act[c]) * wt[c * 3 + k]), 0) for k < 3,
+// summed over the channels in order as a separate 1x1 pass over the BF16
+// activations would; the convolution's own activations are not stored.
+struct ConvHead {
+    const float* wt;  // [cout][3]
+    const float* b;   // [3]
+    float* out;       // [h][w][3]
+    int h, w;
+};
+
 // upAddend (optional, pipelined form only): the upsampled half of a decoder
 // convolution computed at half resolution (see combineUpsampledWeights),
 // 4 blocks of cout channels per low pixel, added before bias and ReLU.
 cudaError_t convTc(const __nv_bfloat16* in, const __nv_bfloat16* low, int lowChannels, int n, int h, int w, int cin,
                    const __nv_bfloat16* weights, bool reverseTaps, const float* bias, int cout, __nv_bfloat16* outB,
                    float* outF, bool relu, bool accumulate, int* errorFlag, cudaStream_t stream,
-                   const __nv_bfloat16* upAddend = nullptr);
+                   const __nv_bfloat16* upAddend = nullptr, const ConvHead* head = nullptr);
 
 // A decoder convolution over [upsample2(low), skip] as two convolutions:
 // the low half at low resolution with 4 blocks of cout output channels, one
@@ -105,7 +117,7 @@ cudaError_t convPipe(const __nv_bfloat16* in, const __nv_bfloat16* low, int lowC
                      const __nv_bfloat16* weights, bool reverseTaps, const float* bias, int cout,
                      __nv_bfloat16* outB, float* outF, bool relu, bool accumulate, int* errorFlag,
                      cudaStream_t stream, const ConvPipeTest* test = nullptr,
-                     const __nv_bfloat16* upAddend = nullptr);
+                     const __nv_bfloat16* upAddend = nullptr, const ConvHead* head = nullptr);
 
 // Weight gradient on tcgen05 (rt_wgrad_tc.cu): dw[tap][ci][co] += sum_p
 // x[p + off(tap)][ci] dy[p][co] over NHWC BF16 x (cin channels) and dy (cout

@@ -561,7 +561,8 @@ cudaError_t Unet::ensure(int n, int h, int w, bool training) {
     return cudaSuccess;
 }
 
-cudaError_t Unet::forward(cudaStream_t s, bool training, bool outputLayer) {
+cudaError_t Unet::forward(cudaStream_t s, bool training, bool outputLayer, const ConvHead* head, bool* headDone) {
+    if (headDone) *headDone = false;
     Activations& A = *act_;
     const int n = A.n;
     cudaError_t e;
@@ -604,6 +605,14 @@ cudaError_t Unet::forward(cudaStream_t s, bool training, bool outputLayer) {
             } else if (r == 0) {
                 // Inference: the convolution reads [upsample(low), skip] in place.
                 e = convTc(skip, low, Cl, n, H, W, L.cin, wT_ + L.wOffset, false, master_ + L.bOffset, L.cout, A.a[k], nullptr, true, false, convError_, s);
+            } else if (k == 17 && head && !training && convPath() == 0 && convPipePreferred(L.cin, L.cout, 0)) {
+                // The last convolution with the output head in its epilogue.
+                e = convTc(A.a[k - 1], nullptr, 0, n, H, W, L.cin, wT_ + L.wOffset, false, master_ + L.bOffset, L.cout,
+                           nullptr, nullptr, true, false, convError_, s, nullptr, head);
+                if (e == cudaSuccess && headDone) *headDone = true;
+                if (e == cudaErrorNotSupported)
+                    e = convTc(A.a[k - 1], nullptr, 0, n, H, W, L.cin, wT_ + L.wOffset, false, master_ + L.bOffset,
+                               L.cout, A.a[k], nullptr, true, false, convError_, s);
             } else {
                 e = convTc(A.a[k - 1], nullptr, 0, n, H, W, L.cin, wT_ + L.wOffset, false, master_ + L.bOffset, L.cout, A.a[k], nullptr, true, false, convError_, s);
             }
@@ -750,11 +759,14 @@ cudaError_t Unet::inferFromSums(const float* sums, const float* depthSums, unsig
     if (e != cudaSuccess) return e;
     Activations& A = *act_;
     sumsInputKernel<<<blocksFor((long long)A.H * A.W, 256), 256, 0, s>>>(sums, depthSums, samples, h, w, A.H, A.W, A.x0);
-    if ((e = forward(s, false, false)) != cudaSuccess) return e;
     const UnetLayer& O = layers_[18];
-    outputFusedKernel<<<blocksFor((long long)w * h, 256), 256, 0, s>>>(A.a[17], A.H, A.W, h, w, O.cin,
-                                                                      master_ + O.wOffset, master_ + O.bOffset,
-                                                                      radiance);
+    const ConvHead head{master_ + O.wOffset, master_ + O.bOffset, radiance, h, w};
+    bool fused = false;
+    if ((e = forward(s, false, false, &head, &fused)) != cudaSuccess) return e;
+    if (!fused)
+        outputFusedKernel<<<blocksFor((long long)w * h, 256), 256, 0, s>>>(A.a[17], A.H, A.W, h, w, O.cin,
+                                                                          master_ + O.wOffset, master_ + O.bOffset,
+                                                                          radiance);
     return cudaGetLastError();
 }
 

@@ -15,6 +15,8 @@
 #include <string>
 #include <vector>
 
+#include "rt_conv_tc.cuh"
+
 namespace rt {
 
 struct UnetLayer {
@@ -63,7 +65,10 @@ public:
 private:
     struct Activations;
     cudaError_t ensure(int n, int h, int w, bool training);
-    cudaError_t forward(cudaStream_t stream, bool training, bool outputLayer = true);
+    // head (inference): the output head to fuse into the last convolution;
+    // *headDone tells whether it was (else A.a[17] holds that layer's output).
+    cudaError_t forward(cudaStream_t stream, bool training, bool outputLayer = true, const ConvHead* head = nullptr,
+                        bool* headDone = nullptr);
     cudaError_t backward(cudaStream_t stream);
     cudaError_t syncWeights(cudaStream_t stream);
 
