@@ -225,8 +225,10 @@ int RtxSetTuning(void* session, int key, int value);
 
 /* Which tensor-core convolution kernel the learned denoiser runs, no
  * counterpart in the reference: 0 (default) the warp-specialised TMA-fed
- * kernel wherever its shared memory allows, 1 the single-role kernel for
- * every layer. Process-wide; results agree to BF16 rounding. */
+ * kernel wherever its shared memory allows (inference then also runs the
+ * decoders' concatenated layers as two passes and fuses the output head
+ * into the last layer), 1 the single-role kernel for every layer, one pass
+ * each. Process-wide; results agree to BF16 rounding. */
 int RtxSetConvPath(int mode);
 /* Convolutions launched so far in this process by the warp-specialised
  * kernel and by the single-role kernel (either pointer may be null); no
