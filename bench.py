@@ -624,6 +624,11 @@ def batch_run(lib, args):
         graph = frames(1)
         launches = frames(0)
         tuned = b.stats()
+        # One persistent launch per frame over a (view, tile) queue, the
+        # reference's launch shape (RTX_BATCH_PERSISTENT).
+        b.set_tuning(persistent=1)
+        persistent = frames(1)
+        b.set_tuning(persistent=0)
     finally:
         b.close()
     # Per-view launches: every view alone through the single-view device path.
@@ -651,7 +656,8 @@ def batch_run(lib, args):
         'build_ms': built['buildMs'], 'build_mtris_per_s': built['triangles'] / built['buildMs'] / 1e3,
         'generate_s': gen_s, 'autotune_s': tune_s, 'autotune': tried,
         'tuned': {k: tuned[k] for k in ('block', 'capacity', 'refill', 'width', 'pieces', 'lanes')},
-        'batched_graph': graph, 'batched_launches': launches, 'per_view_launches': per_view,
+        'batched_graph': graph, 'batched_launches': launches, 'persistent_launch': persistent,
+        'per_view_launches': per_view,
         'speedup_vs_per_view': per_view['frame_ms'] / graph['frame_ms'],
         'same_rays': graph['rays_per_frame'] == per_view_rays,
     }

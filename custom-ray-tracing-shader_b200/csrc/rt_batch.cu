@@ -256,6 +256,56 @@ __global__ void batchAdvanceKernel(unsigned* sample, int rpp) {
     if (blockIdx.x == 0 && threadIdx.x == 0) *sample += (unsigned)rpp;
 }
 
+// ---- one persistent launch per frame (RTX_BATCH_PERSISTENT) ----
+// Resident blocks pull tiles of 16 x 8 pixels from one queue over every
+// view of every scene (tiles[v] .. tiles[v + 1] - 1 are view v's, in rows;
+// tiles[viewCount + 1] is the queue's cursor) and trace each pixel's paths
+// with the reference's launch shape (renderPixel, one thread per pixel, the
+// whole traversal stack in shared memory), starting at the view's scene's
+// root in the arena.
+constexpr int kBatchTileX = 16, kBatchTileY = 8, kBatchMegaBlock = kBatchTileX * kBatchTileY;
+__global__ void __launch_bounds__(kBatchMegaBlock) batchMegaKernel(BatchFrame F, unsigned* tiles) {
+    extern __shared__ uint2 smemStack[];
+    __shared__ unsigned tile;
+    uint2* stack = smemStack + threadIdx.x;
+    const unsigned total = tiles[F.viewCount];
+    const unsigned sample0 = *F.sample;
+    unsigned nPrimary = 0, nSecondary = 0, nShadow = 0;
+    int overflow = 0;
+    for (;;) {
+        if (threadIdx.x == 0) tile = atomicAdd(&tiles[F.viewCount + 1], 1u);
+        __syncthreads();
+        const unsigned t = tile;
+        __syncthreads();
+        if (t >= total) break;
+        int lo = 0, hi = F.viewCount - 1;  // the view v with tiles[v] <= t < tiles[v + 1]
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (tiles[mid] <= t) lo = mid; else hi = mid - 1;
+        }
+        const BatchView V = F.views[lo];
+        const BatchScene& S = F.scenes[V.scene];
+        const unsigned local = t - tiles[lo], tilesX = (unsigned)(V.w + kBatchTileX - 1) / kBatchTileX;
+        const int x = (int)(local % tilesX) * kBatchTileX + (int)threadIdx.x % kBatchTileX;
+        const int y = (int)(local / tilesX) * kBatchTileY + (int)threadIdx.x / kBatchTileX;
+        if (x < V.w && y < V.h) {
+            SceneView sv = S.view;
+            sv.root = S.root;
+            renderPixel(sv, V.cam, F.set, x, y, V.w, V.h, sample0, F.passXor, F.seedHash, F.sums + V.pixelStart,
+                        F.depthSums + V.pixelStart, F.pixels + V.pixelStart, stack, kBatchMegaBlock, &overflow,
+                        nPrimary, nSecondary, nShadow);
+        }
+    }
+    const unsigned sa = __reduce_add_sync(0xFFFFFFFFu, nPrimary), sb = __reduce_add_sync(0xFFFFFFFFu, nSecondary),
+                   sc = __reduce_add_sync(0xFFFFFFFFu, nShadow);
+    if ((threadIdx.x & 31) == 0) {
+        if (sa) atomicAdd(&F.counters[0], (unsigned long long)sa);
+        if (sb) atomicAdd(&F.counters[1], (unsigned long long)sb);
+        if (sc) atomicAdd(&F.counters[2], (unsigned long long)sc);
+    }
+    if (overflow) atomicExch(F.errorFlag, 1);
+}
+
 // Arena copies: indices of scene k move by its node / triangle offsets.
 __global__ void rebaseNodesKernel(uint4* nodes, int count, unsigned nodeBase, unsigned triBase) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -378,6 +428,8 @@ struct Batch {
     int lanesReady = 1;
     // Tuning.
     int block = 128, capacity = 0, refill = 24, width = 8, useGraph = 1, pieces = 3, leaf = 2, lanes = 2;
+    int persistent = 0;             // RTX_BATCH_PERSISTENT: one persistent launch per frame
+    unsigned* dTiles = nullptr;     // [views + 2]: tile prefix per view, then the frame's tile cursor
     int environmentMode = 0;
     float3 environment = make_float3(0.0f, 0.0f, 0.0f);
     // Frame state.
@@ -411,10 +463,10 @@ void freeArena(Batch* b) {
 }
 
 void freeViews(Batch* b) {
-    void* owned[] = {b->dViews, b->dSum, b->dDepth, b->dPixels};
+    void* owned[] = {b->dViews, b->dSum, b->dDepth, b->dPixels, b->dTiles};
     for (void* p : owned)
         if (p) cudaFree(p);
-    b->dViews = nullptr; b->dSum = nullptr; b->dDepth = nullptr; b->dPixels = nullptr;
+    b->dViews = nullptr; b->dSum = nullptr; b->dDepth = nullptr; b->dPixels = nullptr; b->dTiles = nullptr;
     b->viewsReady = false;
     dropGraph(b);
 }
@@ -528,18 +580,26 @@ bool ensureViews(Batch* b) {
     if (b->viewsReady) return true;
     freeViews(b);
     std::vector<BatchView> table;
+    std::vector<unsigned> tiles(1, 0u);
     size_t pixels = 0;
     for (BatchViewData& V : b->views) {
         V.pixelStart = (unsigned)pixels;
         table.push_back(BatchView{V.cam, V.w, V.h, V.scene, V.pixelStart});
         pixels += (size_t)V.w * V.h;
+        tiles.push_back(tiles.back() + (unsigned)(((V.w + kBatchTileX - 1) / kBatchTileX) *
+                                                  ((V.h + kBatchTileY - 1) / kBatchTileY)));
     }
+    tiles.push_back(0u);  // the cursor
     if (pixels > 0x7FFFFFFFull) { b->error = "batch has more than 2^31 pixels"; return false; }
     cudaError_t e;
     if ((e = rt::deviceAlloc(&b->dViews, sizeof(BatchView) * table.size())) != cudaSuccess) return failB(b, e);
     if ((e = rt::deviceAlloc(&b->dSum, sizeof(Accum) * pixels)) != cudaSuccess) return failB(b, e, "accumulation");
     if ((e = rt::deviceAlloc(&b->dDepth, sizeof(float) * pixels)) != cudaSuccess) return failB(b, e, "accumulation");
     if ((e = rt::deviceAlloc(&b->dPixels, sizeof(uchar4) * pixels)) != cudaSuccess) return failB(b, e, "accumulation");
+    if ((e = rt::deviceAlloc(&b->dTiles, sizeof(unsigned) * tiles.size())) != cudaSuccess) return failB(b, e);
+    if ((e = cudaMemcpyAsync(b->dTiles, tiles.data(), sizeof(unsigned) * tiles.size(), cudaMemcpyHostToDevice,
+                             b->stream)) != cudaSuccess)
+        return failB(b, e);
     if ((e = cudaMemcpyAsync(b->dViews, table.data(), sizeof(BatchView) * table.size(), cudaMemcpyHostToDevice,
                              b->stream)) != cudaSuccess)
         return failB(b, e);
@@ -622,6 +682,27 @@ cudaError_t enqueueFrame(Batch* b, const Settings& set, int* launches) {
     n++;
     BatchFrame F{b->dViews, (int)b->views.size(), b->dScenes, set, b->dPassXor, b->dSeedHash, b->dSample,
                  b->dSum, b->dDepth, b->dPixels, b->dCounters, b->dError};
+    if (b->persistent) {
+        // One launch traces the frame; the cursor restarts every frame.
+        const size_t smem = sizeof(uint2) * kStackCapacity * kBatchMegaBlock;
+        static bool configured = false;
+        if (!configured) {
+            if ((e = cudaFuncSetAttribute(batchMegaKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
+                cudaSuccess)
+                return e;
+            configured = true;
+        }
+        int perSm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, batchMegaKernel, kBatchMegaBlock, smem) != cudaSuccess ||
+            perSm < 1)
+            perSm = 1;
+        if ((e = cudaMemsetAsync(b->dTiles + b->views.size() + 1, 0, sizeof(unsigned), s)) != cudaSuccess) return e;
+        batchMegaKernel<<<deviceSms() * perSm, kBatchMegaBlock, smem, s>>>(F, b->dTiles);
+        batchAdvanceKernel<<<1, 32, 0, s>>>(b->dSample, set.raysPerPixel);
+        n += 2;
+        if (launches) *launches = n;
+        return cudaGetLastError();
+    }
     const int cap = b->wave.capacity;
     const int shadeBlocks = deviceSms() * (2048 / 256);
     if (nLanes > 1) {
@@ -918,6 +999,10 @@ int RtxBatchSetTuning(void* p, int key, int value) {
         case RTX_BATCH_LANES:
             if (value < 1 || value > kMaxLanes) break;
             if (value != b->lanes) { b->lanes = value; dropGraph(b); }
+            return 1;
+        case RTX_BATCH_PERSISTENT:
+            if (value != 0 && value != 1) break;
+            if (value != b->persistent) { b->persistent = value; dropGraph(b); }
             return 1;
         default:
             break;

@@ -179,11 +179,13 @@ struct TraversalCounters { unsigned nodes, tris; };
 // this library: their depth is checked against kStackCapacity).
 template <bool ANY>
 RT_HD Hit traverse(const uint4* nodes, const float4* tris, float3 o, float3 d, float limit, uint2* stack,
-                   int stackStride, int* overflow, TraversalCounters* counters, int stackLimit = kStackCapacity) {
+                   int stackStride, int* overflow, TraversalCounters* counters, int stackLimit = kStackCapacity,
+                   unsigned root = 0) {
     Hit hit{-1, limit, 0.0f, 0.0f};
     RaySetup r = setupRay(o, d);
-    // Virtual root group: one interior child (node 0) in the highest slot.
-    uint2 group = make_uint2(0u, 0x80000000u);
+    // Virtual root group: one interior child (the root node, 0 for a single
+    // scene, a scene's first node in a batch arena) in the highest slot.
+    uint2 group = make_uint2(root, 0x80000000u);
     uint2 triGroup = make_uint2(0u, 0u);
     int top = 0;
     unsigned nodeVisits = 0, triTests = 0;

@@ -73,6 +73,7 @@ struct SceneView {
     int environmentMode;     // 0: the reference's sky gradient x skyStrength; 1: constant radiance
     float3 environment;      // the constant radiance of mode 1
     int stackLimit = kStackCapacity;  // traversal stack entries before the overflow error
+    unsigned root = 0;                // root node of the scene's wide tree (its first node in a batch arena)
 };
 
 // ---- BRDF and sky (renderer.cu:181-196) ----
@@ -264,13 +265,13 @@ RT_HD void renderPixel(const SceneView& sc, const Camera& cam, const Settings& s
             rng.base = 4u + 8u * (unsigned)bounce;
             if (bounce == 0) nPrimary++; else nSecondary++;
             Hit hit = traverse<false>(sc.wide, sc.packed, st.origin, st.dir, 1e30f, stack, stackStride, overflow, nullptr,
-                                     sc.stackLimit);
+                                     sc.stackLimit, sc.root);
             ShadowRequest req;
             unsigned f = shadeBounce(sc, set, bounce, st, hit, rng, req);
             if (f & kShadow) {
                 nShadow++;
                 Hit sh = traverse<true>(sc.wide, sc.packed, req.origin, req.dir, req.limit, stack, stackStride, overflow,
-                                        nullptr, sc.stackLimit);
+                                        nullptr, sc.stackLimit, sc.root);
                 if (sh.index < 0) st.radiance = add(st.radiance, req.contribution);
             }
             if (!(f & kContinue)) break;

@@ -434,7 +434,7 @@ class Unet:
 class Batch:
     """Many views of many scenes rendered together (RtxBatch* entry points)."""
 
-    BLOCK, CAPACITY, REFILL, GRAPH, WIDTH, PIECES, LEAF, LANES = 1, 2, 3, 4, 5, 6, 7, 8
+    BLOCK, CAPACITY, REFILL, GRAPH, WIDTH, PIECES, LEAF, LANES, PERSISTENT = 1, 2, 3, 4, 5, 6, 7, 8, 9
 
     def __init__(self, lib=None):
         self.lib = lib or load_library()
@@ -502,10 +502,10 @@ class Batch:
         return out
 
     def set_tuning(self, block=None, capacity=None, refill=None, graph=None, width=None, pieces=None, leaf=None,
-                   lanes=None):
+                   lanes=None, persistent=None):
         for key, value in ((self.BLOCK, block), (self.CAPACITY, capacity), (self.REFILL, refill),
                            (self.GRAPH, graph), (self.WIDTH, width), (self.PIECES, pieces), (self.LEAF, leaf),
-                           (self.LANES, lanes)):
+                           (self.LANES, lanes), (self.PERSISTENT, persistent)):
             if value is not None:
                 self.check(self.lib.RtxBatchSetTuning(self.handle, key, int(value)))
 

@@ -327,6 +327,8 @@ int RtxReadDenoised(void* session, float* rgb, int count);
 #define RTX_BATCH_PIECES 6    /* most pieces per triangle of the traversal trees (1..8, default 3; see RTX_TUNE_PIECES) */
 #define RTX_BATCH_LEAF 7      /* leaf size of the traversal trees (1..8, default 2) */
 #define RTX_BATCH_LANES 8     /* waves in flight (1..4, default 2; see RTX_TUNE_LANES) */
+#define RTX_BATCH_PERSISTENT 9 /* 1: one persistent launch per frame pulling 16x8 tiles of every view from one
+                                  queue, a thread per pixel tracing its whole paths; 0 (default): waves */
 typedef struct RtxBatchTune {
     int block, capacity, refill, width;
     float frameMs;  /* device time of one frame of one path per pixel */

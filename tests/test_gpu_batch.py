@@ -106,6 +106,8 @@ def make_batch(lib, scene_list, views):
     {'lanes': 3, 'capacity': 3000, 'graph': 0},
     {'lanes': 3, 'capacity': 10000},       # waves cross sample rows as well as views
     {'lanes': 1, 'capacity': 20000},
+    {'persistent': 1},                     # one persistent launch per frame over a (view, tile) queue
+    {'persistent': 1, 'graph': 0},
 ])
 def test_batch_equals_single_view_renders(lib, reference, tuning):
     scene_list, views, expect = reference
@@ -178,7 +180,8 @@ def test_batch_errors(lib):
         b.add_view(k, cam, 16, 16)
         with pytest.raises(Exception, match='render first'):
             b.image(0)
-        for key, value in (('block', 96), ('capacity', 10), ('refill', 0), ('graph', 2), ('width', 6), ('lanes', 5)):
+        for key, value in (('block', 96), ('capacity', 10), ('refill', 0), ('graph', 2), ('width', 6), ('lanes', 5),
+                           ('persistent', 2)):
             with pytest.raises(Exception, match='out of range'):
                 b.set_tuning(**{key: value})
         bad = Settings(4, 1.0, 0.0, 1.0, 0.5, 42, 17)
