@@ -82,8 +82,9 @@ def parse():
                    help="waves in flight, 1..4 (RTX_TUNE_LANES; default: the library default)")
     p.add_argument('--denoiser-only', action='store_true',
                    help='only time learned-denoiser inference at 1920x1080 (a small case for profiling)')
-    p.add_argument('--conv-path', type=int, choices=(0, 1), default=0,
-                   help='convolution kernel of the denoiser (RtxSetConvPath): 0 pipelined where it fits, 1 single-role')
+    p.add_argument('--conv-path', type=int, choices=(0, 1, 2), default=0,
+                   help='convolution kernel of the denoiser (RtxSetConvPath): 0 pipelined where it fits, '
+                        '1 single-role, 2 pipelined with tap-by-tap issue only')
     p.add_argument('--no-train-step', dest='train_step', action='store_false',
                    help='skip timing U-Net training steps (batch 32 of 128x128 crops; 1 GPU runs it by default)')
     p.add_argument('--train-steps', type=int, default=20, help='timed training steps')

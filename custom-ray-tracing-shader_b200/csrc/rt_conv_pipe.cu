@@ -24,7 +24,12 @@
 //              The A operand stays in shared memory: with A in tensor
 //              memory (tcgen05.cp of each row's three shifted copies) an
 //              MMA of 128 x N x 16 measured ~85 SM cycles against ~42 from
-//              shared memory.
+//              shared memory. Unsplit 32-channel layers use the stacked-row
+//              issue instead (see Seg): per input row and column tap one MMA
+//              over the three kernel rows' weights side by side into the
+//              accumulator blocks of three output rows, so a row is read
+//              by 3 cin/16 MMAs of N = 96 instead of 9 cin/16 of N = 32, and
+//              its slot is freed as soon as they complete.
 //   warps 2-5  epilogue: tcgen05.ld of the accumulator (warp w of the block
 //              reads lanes 32 (w % 4) ...), which is then handed back to the issuer,
 //              bias, ReLU and the store (BF16, or FP32 added to or written).
@@ -254,6 +259,56 @@ __device__ __forceinline__ void issueTileG(int G2, uint32_t acc, const uint64_t 
     }
 }
 
+// The stacked-row form: an input row r feeds output rows r + 1, r and r - 1
+// through the kernel rows dy = 0, 1, 2, so one MMA per column tap dx and K
+// step multiplies the row (A, read once) by the three kernel rows' weights
+// side by side along N (B: [dy = 2 | dy = 1 | dy = 0] x COUT, N = 3 COUT)
+// into three consecutive accumulator blocks (output rows r - 1, r, r + 1) of
+// a ring of blocks in tensor memory. Where that range wraps around the ring,
+// or at a strip's first and last rows, the MMA covers fewer blocks (Seg: the
+// first block's column, the B offset of its kernel row in descriptor units,
+// the instruction descriptor for its width and the accumulate flag). An
+// output row's first MMA (input row r + 1's dy = 0, dx = 0, first K step)
+// starts its block from zero: that step issues the fresh block apart.
+// Each output row thus receives the taps in the order t = 3 dy + dx with the
+// K steps inner, the tap-per-tile form's order.
+struct Seg { uint32_t d, b, id, acc; };
+template <int COUT, int G2>
+__device__ __forceinline__ void issueRowStacked(const Seg (&first)[3], int nFirst, const Seg (&rest)[2], int nRest,
+                                                uint64_t aDesc, uint64_t wDesc) {
+#pragma unroll
+    for (int dx = 0; dx < 3; dx++) {
+#pragma unroll
+        for (int k = 0; k < G2; k++) {
+            const uint64_t ad = aDesc + (uint64_t)dx + (uint64_t)k * ((2u * kPlane) >> 4);
+            // Weights: per (dx, plane g) a region of 3 COUT rows of 16 bytes.
+            const uint64_t bd = wDesc + (uint64_t)(((dx * 2 * G2 + 2 * k) * 3 * COUT * 16) >> 4);
+            if (dx == 0 && k == 0) {
+#pragma unroll
+                for (int s = 0; s < 3; s++)
+                    if (s < nFirst) mma(first[s].d, ad, bd + first[s].b, first[s].id, first[s].acc);
+            } else {
+                mma(rest[0].d, ad, bd + rest[0].b, rest[0].id, 1u);
+                if (nRest > 1) mma(rest[1].d, ad, bd + rest[1].b, rest[1].id, 1u);
+            }
+        }
+    }
+}
+template <int COUT>
+__device__ __forceinline__ void issueRowStackedG(int G2, const Seg (&first)[3], int nFirst, const Seg (&rest)[2],
+                                                 int nRest, uint64_t aDesc, uint64_t wDesc) {
+    switch (G2) {
+        case 1: issueRowStacked<COUT, 1>(first, nFirst, rest, nRest, aDesc, wDesc); break;
+        case 2: issueRowStacked<COUT, 2>(first, nFirst, rest, nRest, aDesc, wDesc); break;
+        case 3: issueRowStacked<COUT, 3>(first, nFirst, rest, nRest, aDesc, wDesc); break;
+        case 4: issueRowStacked<COUT, 4>(first, nFirst, rest, nRest, aDesc, wDesc); break;
+        case 5: issueRowStacked<COUT, 5>(first, nFirst, rest, nRest, aDesc, wDesc); break;
+        case 6: issueRowStacked<COUT, 6>(first, nFirst, rest, nRest, aDesc, wDesc); break;
+        case 7: issueRowStacked<COUT, 7>(first, nFirst, rest, nRest, aDesc, wDesc); break;
+        default: issueRowStacked<COUT, 8>(first, nFirst, rest, nRest, aDesc, wDesc); break;  // cin <= 128 (host check)
+    }
+}
+
 // Unit u: image, column tile and strip of rows [y0, y1).
 struct Unit { int img, x0, y0, y1; };
 __device__ __forceinline__ Unit unitOf(const PipeArgs& a, int u) {
@@ -339,7 +394,8 @@ __device__ __forceinline__ void epilogueStore16(const PipeArgs& a, const uint32_
 // every issuer releases every row (a slot's empty barrier counts ISS
 // arrivals). Two issuers give a layer that fits one block per SM two issuing
 // threads without a second ring.
-template <int COUT, int ISS>
+// STACK: the stacked-row issue (one issuer; a.nAcc blocks of COUT columns).
+template <int COUT, int ISS, bool STACK>
 __global__ void __launch_bounds__(kPipeThreads + 32 * (ISS - 1), ISS > 1 ? 1 : (COUT <= 48 ? 4 : 2))
     convPipeKernel(const __grid_constant__ CUtensorMap inMap, const __grid_constant__ CUtensorMap lowMap,
                    const __grid_constant__ CUtensorMap wMap, PipeArgs a) {
@@ -403,14 +459,17 @@ __global__ void __launch_bounds__(kPipeThreads + 32 * (ISS - 1), ISS > 1 ? 1 : (
             asm volatile("prefetch.tensormap [%0];\n" ::"l"(&inMap) : "memory");
             if (Glow) asm volatile("prefetch.tensormap [%0];\n" ::"l"(&lowMap) : "memory");
             asm volatile("prefetch.tensormap [%0];\n" ::"l"(&wMap) : "memory");
-            // The weights, tap-major ([tap][plane][cout][8]), once per block.
+            // The weights, once per block: tap-major ([tap][plane][cout][8]),
+            // or for the stacked form [dx][plane][2 - dy][cout][8].
             const uint32_t wb = pb + Header::weightsFull;
             {
                 barExpectTx(wb, a.weightBytes);
                 for (int t = 0; t < 9; t++)
-                    for (int g = 0; g < G; g++)
-                        tmaLoad3(wAddr + (uint32_t)((t * G + g) * COUT * 16), &wMap, g * 8, nBase,
+                    for (int g = 0; g < G; g++) {
+                        const int region = STACK ? ((t % 3) * G + g) * 3 + 2 - t / 3 : t * G + g;
+                        tmaLoad3(wAddr + (uint32_t)(region * COUT * 16), &wMap, g * 8, nBase,
                                  a.reverseTaps ? 8 - t : t, wb);
+                    }
             }
         }
         // Rows are numbered in issue order q; row q sits in slot q % R, its
@@ -542,6 +601,69 @@ __global__ void __launch_bounds__(kPipeThreads + 32 * (ISS - 1), ISS > 1 ? 1 : (
                 commit(pb + Header::empty + 8 * relSlot);
                 if (++relSlot == R) relSlot = 0;
             };
+            if constexpr (STACK) {
+                // Per input row i of a strip of S output rows (row y0 - 1 + i,
+                // i = 0 .. S + 1): output rows jLo .. jHi of the strip, whose
+                // blocks are (p0 + j) % NB; block p0 + i is fresh.
+                const int NB = a.nAcc;
+                const uint64_t wStack = ummaSmemDesc(wAddr, 3u * COUT * 16u, 128u);
+                const uint32_t id0 = ummaInstrDescBf16(kM, 0);  // plus (N / 8) << 17 for N = blocks x COUT
+                for (int u = firstUnit; u < a.units && ok; u += unitStride) {
+                    const Unit U = unitOf(a, u);
+                    const int S = U.y1 - U.y0;
+                    const int p0 = accB;
+                    for (int i = 0; i <= S + 1; i++) {
+                        int slot = 0;
+                        if (!nextRow(slot)) { ok = false; break; }
+                        const bool fresh = i < S;
+                        if (fresh) {
+                            const uint64_t t1 = a.stats ? nowNs() : 0;
+                            ok = waitPhase(pb + Header::accEmpty + 8 * accB, accParity ^ 1u, abortFlag, limit);
+                            if (a.stats) waitAccNs += nowNs() - t1;
+                            if (!ok) break;
+                            tcFenceAfter();
+                        }
+                        const int jLo = i > 2 ? i - 2 : 0, jHi = i < S - 1 ? i : S - 1;
+                        // Output rows lo .. hi as one segment, or two where the ring wraps.
+                        auto range = [&](int lo, int hi, uint32_t accFlag, Seg& s0, Seg& s1) -> int {
+                            const int p = (p0 + lo) % NB, len = hi - lo + 1, run = len < NB - p ? len : NB - p;
+                            s0 = Seg{tmem + (uint32_t)(p * COUT), (uint32_t)((lo - i + 2) * COUT),
+                                     id0 + ((uint32_t)(run * COUT / 8) << 17), accFlag};
+                            s1 = Seg{tmem, (uint32_t)((lo + run - i + 2) * COUT),
+                                     id0 + ((uint32_t)((len - run) * COUT / 8) << 17), accFlag};
+                            return run < len ? 2 : 1;
+                        };
+                        Seg first[3], rest[2];
+                        const int nRest = range(jLo, jHi, 1u, rest[0], rest[1]);
+                        int nFirst = nRest;
+                        first[0] = rest[0];
+                        first[1] = rest[1];
+                        if (fresh) {
+                            // The fresh block (output row i = jHi) apart, from zero.
+                            Seg fr, unused;
+                            range(jHi, jHi, 0u, fr, unused);
+                            if (jHi == jLo) {
+                                first[0] = fr;
+                                nFirst = 1;
+                            } else {
+                                nFirst = range(jLo, jHi - 1, 1u, first[0], first[1]) + 1;
+                                if (nFirst == 3) first[2] = fr;
+                                else first[1] = fr;
+                            }
+                        }
+                        const uint64_t aDesc = ummaSmemDesc(ringAddr + (uint32_t)slot * slotBytes, kPlane, 128u);
+                        issueRowStackedG<COUT>(G2, first, nFirst, rest, nRest, aDesc, wStack);
+                        release();  // row i: no later MMA reads it
+                        if (i >= 2) {  // output row i - 2 has all its taps
+                            commit(pb + Header::accFull + 8 * ((p0 + i - 2) % NB));
+                        }
+                        if (fresh) {
+                            mine++;
+                            if (++accB == NB) { accB = 0; accParity ^= 1u; }
+                        }
+                    }
+                }
+            } else
             for (int u = firstUnit; u < a.units && ok; u += unitStride) {
                 const Unit U = unitOf(a, u);
                 int s0 = 0, s1 = 0, s2 = 0;  // slots of rows y - 1, y, y + 1
@@ -686,17 +808,17 @@ int deviceSmCount() {
     return sms > 0 ? sms : 1;
 }
 
-template <int COUT, int ISS>
+template <int COUT, int ISS, bool STACK = false>
 cudaError_t launchPipe(const CUtensorMap& inMap, const CUtensorMap& lowMap, const CUtensorMap& wMap,
                        const PipeArgs& a, int grid, uint32_t smemBytes, cudaStream_t stream) {
     static bool configured = false;
     if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(convPipeKernel<COUT, ISS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaError_t e = cudaFuncSetAttribute(convPipeKernel<COUT, ISS, STACK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              227 * 1024);
         if (e != cudaSuccess) return e;
         configured = true;
     }
-    convPipeKernel<COUT, ISS><<<grid, kPipeThreads + 32 * (ISS - 1), smemBytes, stream>>>(inMap, lowMap, wMap, a);
+    convPipeKernel<COUT, ISS, STACK><<<grid, kPipeThreads + 32 * (ISS - 1), smemBytes, stream>>>(inMap, lowMap, wMap, a);
     return cudaGetLastError();
 }
 
@@ -809,8 +931,34 @@ cudaError_t convPipe(const bf16* in, const bf16* low, int lowChannels, int n, in
     const int force = test ? test->issuers : 0;  // 1 or 2 issuers
     const bool twoFit = tmemColumns(2) <= 512u && 2 * a.nAcc <= kMaxAcc;
     if (force == 2 && !twoFit) return cudaErrorNotSupported;
-    const int issuers = (force == 2 || (force == 0 && perSm == 1 && twoFit)) ? 2 : 1;
+    // The stacked-row form (Cout 32 or 64 per block, no concatenated input):
+    // one issuer, a ring of at least 4 accumulator blocks of cout columns.
+    const int stackMode = test ? test->stacked : (convStacking() ? 0 : 1);
+    const bool stackFits = !lowChannels && (cout == 32 || cout == 64) && cin <= 128 && force != 2;
+    // Measured per layer: the stacked form is faster for unsplit 32-channel
+    // layers (1080p 16 -> 32: 78.6 -> 74.2 us, 32 -> 32: 98.9 -> 94.0), slower
+    // for 64 output channels (64 -> 64 at 480x272: 31.4 -> 36.9) and for a
+    // 32-channel slice of a split layer (128 -> 128 at 120x68: 19.2 -> 23.0).
+    const bool stackDefault = cout == 32 && nSplits == 1;
+    if (stackMode == 2 && !stackFits) return cudaErrorNotSupported;
+    const bool stacked = stackFits && (stackMode == 2 || (stackMode == 0 && stackDefault));
+    const int issuers = !stacked && (force == 2 || (force == 0 && perSm == 1 && twoFit)) ? 2 : 1;
     a.tmemCols = tmemColumns(issuers);
+    if (stacked) {
+        auto colsFor = [](int per) {  // tensor-memory columns of a block at per blocks per SM
+            uint32_t c = 512;
+            while (c * (uint32_t)per > 512u) c >>= 1;
+            return c;
+        };
+        while (perSm > 1 && colsFor(perSm) < 4u * (uint32_t)cout) perSm--;
+        const uint32_t cols = colsFor(perSm);
+        int nb = std::min<int>(kMaxAcc, (int)(cols / (uint32_t)cout));
+        if (test && test->nAcc >= 3 && test->nAcc <= kMaxAcc && (uint32_t)test->nAcc * cout <= cols) nb = test->nAcc;
+        a.nAcc = nb;
+        a.accCols = (uint32_t)cout;
+        a.tmemCols = 32;
+        while (a.tmemCols < (uint32_t)(nb * cout)) a.tmemCols <<= 1;
+    }
     while (a.ring < kMaxRing &&
            (uint32_t)perSm * (convPipeSmemBytes(cin, cout, lowChannels, a.ring + 1) + 1024u) <= smemPerSm &&
            convPipeSmemBytes(cin, cout, lowChannels, a.ring + 1) <= smemMax)
@@ -818,13 +966,12 @@ cudaError_t convPipe(const bf16* in, const bf16* low, int lowChannels, int n, in
     if (test && test->ring >= kMinRing && test->ring <= kMaxRing) a.ring = test->ring;
     const uint32_t smemBytes = convPipeSmemBytes(cin, cout, lowChannels, a.ring);
     if (smemBytes > smemMax) return cudaErrorNotSupported;
-    // Strips: long enough to reuse rows (each strip stages 2 extra rows),
-    // short enough to give every block about two units; every slice of
-    // output channels walks all units.
+    // Strips: balanced over the blocks (balancedStripRows); units that do
+    // not divide evenly leave a last round on part of the GPU, strips too
+    // long leave blocks idle. Every slice of output channels walks all units.
     const long long columns = (long long)n * a.tilesPerRow;
     const long long blocks = std::max<long long>(nSplits, (long long)sms * perSm / nSplits * nSplits);
-    long long rows = std::max(1ll, columns * h * nSplits / (2 * blocks));
-    a.stripRows = (int)std::max(4ll, std::min<long long>(32, rows));
+    a.stripRows = balancedStripRows(columns * nSplits, h, blocks);
     if (test && test->stripRows > 0) a.stripRows = test->stripRows;
     a.strips = (h + a.stripRows - 1) / a.stripRows;
     a.units = (int)(columns * a.strips);
@@ -832,11 +979,13 @@ cudaError_t convPipe(const bf16* in, const bf16* low, int lowChannels, int n, in
     switch (cout) {
         case 16: return issuers == 2 ? launchPipe<16, 2>(inMap, lowMap, wMap, a, grid, smemBytes, stream)
                              : launchPipe<16, 1>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
-        case 32: return issuers == 2 ? launchPipe<32, 2>(inMap, lowMap, wMap, a, grid, smemBytes, stream)
+        case 32: return stacked ? launchPipe<32, 1, true>(inMap, lowMap, wMap, a, grid, smemBytes, stream)
+                       : issuers == 2 ? launchPipe<32, 2>(inMap, lowMap, wMap, a, grid, smemBytes, stream)
                              : launchPipe<32, 1>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
         case 48: return issuers == 2 ? launchPipe<48, 2>(inMap, lowMap, wMap, a, grid, smemBytes, stream)
                              : launchPipe<48, 1>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
-        case 64: return issuers == 2 ? launchPipe<64, 2>(inMap, lowMap, wMap, a, grid, smemBytes, stream)
+        case 64: return stacked ? launchPipe<64, 1, true>(inMap, lowMap, wMap, a, grid, smemBytes, stream)
+                       : issuers == 2 ? launchPipe<64, 2>(inMap, lowMap, wMap, a, grid, smemBytes, stream)
                              : launchPipe<64, 1>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
         case 80: return issuers == 2 ? launchPipe<80, 2>(inMap, lowMap, wMap, a, grid, smemBytes, stream)
                              : launchPipe<80, 1>(inMap, lowMap, wMap, a, grid, smemBytes, stream);

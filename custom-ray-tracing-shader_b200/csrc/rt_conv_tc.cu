@@ -458,6 +458,9 @@ static std::atomic<int> g_convPath{0};
 static std::atomic<long long> g_pipeLaunches{0}, g_singleLaunches{0};
 void setConvPath(int mode) { g_convPath.store(mode); }
 int convPath() { return g_convPath.load(); }
+static std::atomic<bool> g_convStacking{true};
+void setConvStacking(bool on) { g_convStacking.store(on); }
+bool convStacking() { return g_convStacking.load(); }
 void convLaunchCounts(long long* pipe, long long* single) {
     if (pipe) *pipe = g_pipeLaunches.load();
     if (single) *single = g_singleLaunches.load();
@@ -602,9 +605,7 @@ cudaError_t convTc(const bf16* in, const bf16* low, int lowChannels, int n, int 
     if (wide) perSm = std::min(perSm, 2048 / WarpLayout<8, 1>::kThreads);
     int units = a.tiles;
     if (a.ring) {
-        // Strips long enough to reuse rows, short enough for two units per block.
-        const long long rows = (long long)n * h * a.tilesPerRow;
-        a.stripRows = (int)std::max(1ll, std::min(32ll, rows / (2ll * deviceSms() * perSm)));
+        a.stripRows = balancedStripRows((long long)n * a.tilesPerRow, h, (long long)deviceSms() * perSm);
         units = n * a.tilesPerRow * ((h + a.stripRows - 1) / a.stripRows);
     }
     const int grid = std::min(units, deviceSms() * perSm);

@@ -83,8 +83,28 @@ bool upsampledSplitSupported(int cin, int cout, int lowChannels);
 
 // Which kernel convTc runs: 0 (default) the pipelined form wherever it
 // applies, 1 always the kernel above (process-wide; for comparisons).
+// Rows per strip for kernels whose blocks walk (image, column tile, strip)
+// units: the length (1-64 rows) that minimises the rows the busiest of
+// `blocks` blocks stages, ceil(units / blocks) strips of s + 2 rows each (a
+// strip stages one halo row above and below); the longest of equals.
+inline int balancedStripRows(long long columns, int h, long long blocks) {
+    int best = 1;
+    long long bestCost = -1;
+    for (int s = 1; s <= 64; s++) {
+        const long long units = columns * ((h + s - 1) / s);
+        const long long cost = (units + blocks - 1) / blocks * (s + 2);
+        if (bestCost < 0 || cost <= bestCost) { bestCost = cost; best = s; }
+        if (s >= h) break;
+    }
+    return best;
+}
+
 void setConvPath(int mode);
 int convPath();
+// Whether the pipelined kernel may use its stacked-row issue (default on;
+// off runs every layer tap per tile, for comparison: results are identical).
+void setConvStacking(bool on);
+bool convStacking();
 // Convolutions run so far by the pipelined and by the single-role kernel.
 void convLaunchCounts(long long* pipe, long long* single);
 
@@ -98,6 +118,7 @@ struct ConvPipeTest {
     unsigned long long* stats;       // device array of 6 wait/lifetime sums in ns (see rt_conv_pipe.cu)
     int blocksPerSm;                 // fewer blocks per SM than shared memory allows (each then gets a longer ring)
     int issuers;                     // MMA issuers per block: 0 chosen per layer, 1, or 2 (sharing the ring)
+    int stacked;                     // 0 chosen per layer, 1 tap-per-tile issue, 2 stacked-row issue
 };
 
 // The same convolution as convTc, warp-specialised and fed by TMA (input

@@ -320,6 +320,37 @@ def test_conv_kernels_agree(lib, net):
         lib.RtxSetConvPath(0)
 
 
+def test_stacked_row_issue_identical(lib, net):
+    """Unsplit 32-channel layers issue one MMA per input row and column tap
+    over the three kernel rows' weights side by side (accumulator blocks per
+    output row in a ring); RtxSetConvPath(2) issues every tap per output tile
+    instead. Each output row receives the taps in the same order either way,
+    so inference is bit-identical: at sizes whose strips end mid-image, with
+    a partial column tile, and with one-row strips. Training agrees to FP32
+    summation order (the loss and the bias and head gradients sum with
+    atomics, whose order varies from run to run)."""
+    rng = np.random.default_rng(21)
+    try:
+        for h, w in ((200, 300), (37, 130), (16, 16)):
+            aovs, _ = synthetic(rng, 1, h, w)
+            assert lib.RtxSetConvPath(2)
+            tap = net.infer(aovs[0])
+            assert lib.RtxSetConvPath(0)
+            stacked = net.infer(aovs[0])
+            assert np.array_equal(tap, stacked), (h, w)
+        aovs, target = synthetic(rng, 3, 48, 144)
+        lib.RtxSetConvPath(2)
+        loss_tap, grad_tap = net.loss_grad(aovs, target)
+        lib.RtxSetConvPath(0)
+        loss_stacked, grad_stacked = net.loss_grad(aovs, target)
+        assert abs(loss_tap - loss_stacked) <= 1e-6 * loss_tap
+        g, e = grad_stacked.astype(np.float64), grad_tap.astype(np.float64)
+        assert np.linalg.norm(g - e) <= 1e-5 * np.linalg.norm(e)
+        assert not lib.RtxSetConvPath(3)
+    finally:
+        lib.RtxSetConvPath(0)
+
+
 def test_conv_wait_limit_reports_and_recovers(lib):
     """A pipelined convolution whose tensor-core issuer waits on a barrier
     that nothing completes gives up after its (2 ms) limit, reports through
