@@ -75,6 +75,45 @@ constexpr int kLowBufs = 4;  // staging rows of the low-resolution input (loads 
 constexpr uint32_t kPipeHeader = 512;    // mbarriers (the rest of the header: flags and biases)
 constexpr uint32_t kHeader = 2048;       // barriers, flags and biases
 
+// Staged-row layouts. SW = 0: planes of 8 channels x 130 pixels x 16 bytes,
+// kPlane apart (no swizzle; one TMA box of 8 channels per plane). SW = 16,
+// 32 or 64: slabs of SW channels, one TMA box each with the 32-, 64- or
+// 128-byte swizzle, i.e. the K-major swizzled operand layout of that width
+// (pixel rows of 2 SW bytes, 8-row groups 16 SW bytes apart), each slab on a
+// 1024-byte boundary. A box of 8 channels moves 16 bytes per pixel; the TMA
+// unit moved a 1080p row set of 32 channels in 44 us that way, in 27 us as
+// 16-channel and 23 us as 32-channel swizzled boxes.
+__host__ __device__ constexpr uint32_t slabBytes(int sw) { return ((uint32_t)(kHalo * 2 * sw) + 1023u) & ~1023u; }
+// Descriptor units (16 bytes) from a staged row's start to the A operand of
+// pixel shift dx (the tap's column) and K step k (16 channels).
+template <int SW>
+__host__ __device__ constexpr uint32_t aOffset(int dx, int k) {
+    return SW == 0 ? (uint32_t)dx + (uint32_t)k * ((2u * kPlane) >> 4)
+                   : (uint32_t)dx * (uint32_t)(SW / 8) + (uint32_t)(k / (SW / 16)) * (slabBytes(SW) >> 4) +
+                         (uint32_t)(k % (SW / 16)) * 2u;
+}
+// The A descriptor of a staged row at `addr` (layout type in bits 61-63:
+// 6 = 32-byte, 4 = 64-byte, 2 = 128-byte swizzle).
+__host__ __device__ constexpr uint64_t rowDescriptor(uint32_t addr, int sw) {
+    return sw == 0 ? ummaSmemDesc(addr, kPlane, 128u)
+                   : ummaSmemDesc(addr, 16u, 16u * (uint32_t)sw) | ((uint64_t)(sw == 16 ? 6 : sw == 32 ? 4 : 2) << 61);
+}
+// Offset of the ring from the start of shared memory (its base is 1024-byte
+// aligned; the kernel checks): the header, the weights, and for slabs the pad
+// to a 1024-byte boundary.
+__host__ __device__ constexpr uint32_t ringOffset(uint32_t weightBytes, int sw) {
+    return sw ? (kHeader + weightBytes + 1023u) & ~1023u : kHeader + weightBytes;
+}
+// Staged row bytes of cin channels in layout sw.
+__host__ __device__ constexpr uint32_t rowBytes(int cin, int sw) {
+    return sw == 0 ? (((uint32_t)(cin / 8) * kPlane + 127u) & ~127u) : (uint32_t)(cin / sw) * slabBytes(sw);
+}
+// The layout of a layer's rows: the widest slab dividing cin, planes for
+// the concatenated input (its low half is expanded into the planes).
+__host__ __device__ constexpr int rowLayout(int cin, int lowChannels) {
+    return lowChannels ? 0 : cin % 64 == 0 ? 64 : cin % 32 == 0 ? 32 : 16;
+}
+
 struct PipeArgs {
     int n, h, w, cin, cout, lowChannels;
     int coutTotal;  // output channels of the layer; a block computes cout of them, from (block % nSplits) * cout
@@ -89,6 +128,7 @@ struct PipeArgs {
     unsigned long long waitLimitNs;
     int probe;  // 1: the issuer first waits on a barrier nothing completes (tests the abort path)
     int nAcc;   // accumulators in tensor memory (2..kMaxAcc)
+    int sw;     // staged-row layout (rowLayout)
     // Optional addend of the upsampled half of a decoder convolution, at half
     // resolution: 4 blocks of coutTotal channels per low pixel, block
     // (y % 2) * 2 + x % 2 for output pixel (x, y); added before bias and ReLU.
@@ -226,36 +266,46 @@ __device__ __forceinline__ void tmemWaitLoads() { asm volatile("tcgen05.wait::ld
 // K count must be a compile-time constant: with a runtime inner loop one
 // thread issued an MMA per ~155 SM cycles, fully unrolled per ~60 (the tensor
 // pipe itself takes ~42 per 128 x N x 16 with N <= 64).
-template <int COUT, int G2>
+template <int COUT, int G2, int SW>
 __device__ __forceinline__ void issueTile(uint32_t acc, const uint64_t (&rowDesc)[3], uint64_t wDesc, uint32_t idesc) {
 #pragma unroll
     for (int t = 0; t < 9; t++) {
 #pragma unroll
         for (int k = 0; k < G2; k++) {
-            const uint64_t aDesc = rowDesc[t / 3] + (uint64_t)(t % 3) + (uint64_t)k * ((2u * kPlane) >> 4);
+            const uint64_t aDesc = rowDesc[t / 3] + (uint64_t)aOffset<SW>(t % 3, k);
             const uint64_t bDesc = wDesc + (uint64_t)(((t * 2 * G2 + 2 * k) * COUT * 16) >> 4);
             mma(acc, aDesc, bDesc, idesc, (t > 0 || k > 0) ? 1u : 0u);
         }
     }
 }
-template <int COUT>
-__device__ __forceinline__ void issueTileG(int G2, uint32_t acc, const uint64_t (&rowDesc)[3], uint64_t wDesc,
+template <int COUT, int SW>
+__device__ __forceinline__ void issueTileK(int G2, uint32_t acc, const uint64_t (&rowDesc)[3], uint64_t wDesc,
                                            uint32_t idesc) {
     switch (G2) {
-        case 1: issueTile<COUT, 1>(acc, rowDesc, wDesc, idesc); break;
-        case 2: issueTile<COUT, 2>(acc, rowDesc, wDesc, idesc); break;
-        case 3: issueTile<COUT, 3>(acc, rowDesc, wDesc, idesc); break;
-        case 4: issueTile<COUT, 4>(acc, rowDesc, wDesc, idesc); break;
-        case 5: issueTile<COUT, 5>(acc, rowDesc, wDesc, idesc); break;
-        case 6: issueTile<COUT, 6>(acc, rowDesc, wDesc, idesc); break;
-        case 7: issueTile<COUT, 7>(acc, rowDesc, wDesc, idesc); break;
-        case 8: issueTile<COUT, 8>(acc, rowDesc, wDesc, idesc); break;
-        case 9: issueTile<COUT, 9>(acc, rowDesc, wDesc, idesc); break;
-        case 10: issueTile<COUT, 10>(acc, rowDesc, wDesc, idesc); break;
-        case 11: issueTile<COUT, 11>(acc, rowDesc, wDesc, idesc); break;
-        case 12: issueTile<COUT, 12>(acc, rowDesc, wDesc, idesc); break;
-        case 13: issueTile<COUT, 13>(acc, rowDesc, wDesc, idesc); break;
-        default: issueTile<COUT, 14>(acc, rowDesc, wDesc, idesc); break;  // cin <= 224 (convPipeSupported)
+        case 1: issueTile<COUT, 1, SW>(acc, rowDesc, wDesc, idesc); break;
+        case 2: issueTile<COUT, 2, SW>(acc, rowDesc, wDesc, idesc); break;
+        case 3: issueTile<COUT, 3, SW>(acc, rowDesc, wDesc, idesc); break;
+        case 4: issueTile<COUT, 4, SW>(acc, rowDesc, wDesc, idesc); break;
+        case 5: issueTile<COUT, 5, SW>(acc, rowDesc, wDesc, idesc); break;
+        case 6: issueTile<COUT, 6, SW>(acc, rowDesc, wDesc, idesc); break;
+        case 7: issueTile<COUT, 7, SW>(acc, rowDesc, wDesc, idesc); break;
+        case 8: issueTile<COUT, 8, SW>(acc, rowDesc, wDesc, idesc); break;
+        case 9: issueTile<COUT, 9, SW>(acc, rowDesc, wDesc, idesc); break;
+        case 10: issueTile<COUT, 10, SW>(acc, rowDesc, wDesc, idesc); break;
+        case 11: issueTile<COUT, 11, SW>(acc, rowDesc, wDesc, idesc); break;
+        case 12: issueTile<COUT, 12, SW>(acc, rowDesc, wDesc, idesc); break;
+        case 13: issueTile<COUT, 13, SW>(acc, rowDesc, wDesc, idesc); break;
+        default: issueTile<COUT, 14, SW>(acc, rowDesc, wDesc, idesc); break;  // cin <= 224 (convPipeSupported)
+    }
+}
+template <int COUT>
+__device__ __forceinline__ void issueTileG(int G2, int sw, uint32_t acc, const uint64_t (&rowDesc)[3], uint64_t wDesc,
+                                           uint32_t idesc) {
+    switch (sw) {
+        case 16: issueTileK<COUT, 16>(G2, acc, rowDesc, wDesc, idesc); break;
+        case 32: issueTileK<COUT, 32>(G2, acc, rowDesc, wDesc, idesc); break;
+        case 64: issueTileK<COUT, 64>(G2, acc, rowDesc, wDesc, idesc); break;
+        default: issueTileK<COUT, 0>(G2, acc, rowDesc, wDesc, idesc); break;
     }
 }
 
@@ -273,14 +323,14 @@ __device__ __forceinline__ void issueTileG(int G2, uint32_t acc, const uint64_t 
 // Each output row thus receives the taps in the order t = 3 dy + dx with the
 // K steps inner, the tap-per-tile form's order.
 struct Seg { uint32_t d, b, id, acc; };
-template <int COUT, int G2>
+template <int COUT, int G2, int SW>
 __device__ __forceinline__ void issueRowStacked(const Seg (&first)[3], int nFirst, const Seg (&rest)[2], int nRest,
                                                 uint64_t aDesc, uint64_t wDesc) {
 #pragma unroll
     for (int dx = 0; dx < 3; dx++) {
 #pragma unroll
         for (int k = 0; k < G2; k++) {
-            const uint64_t ad = aDesc + (uint64_t)dx + (uint64_t)k * ((2u * kPlane) >> 4);
+            const uint64_t ad = aDesc + (uint64_t)aOffset<SW>(dx, k);
             // Weights: per (dx, plane g) a region of 3 COUT rows of 16 bytes.
             const uint64_t bd = wDesc + (uint64_t)(((dx * 2 * G2 + 2 * k) * 3 * COUT * 16) >> 4);
             if (dx == 0 && k == 0) {
@@ -294,18 +344,28 @@ __device__ __forceinline__ void issueRowStacked(const Seg (&first)[3], int nFirs
         }
     }
 }
-template <int COUT>
-__device__ __forceinline__ void issueRowStackedG(int G2, const Seg (&first)[3], int nFirst, const Seg (&rest)[2],
+template <int COUT, int SW>
+__device__ __forceinline__ void issueRowStackedK(int G2, const Seg (&first)[3], int nFirst, const Seg (&rest)[2],
                                                  int nRest, uint64_t aDesc, uint64_t wDesc) {
     switch (G2) {
-        case 1: issueRowStacked<COUT, 1>(first, nFirst, rest, nRest, aDesc, wDesc); break;
-        case 2: issueRowStacked<COUT, 2>(first, nFirst, rest, nRest, aDesc, wDesc); break;
-        case 3: issueRowStacked<COUT, 3>(first, nFirst, rest, nRest, aDesc, wDesc); break;
-        case 4: issueRowStacked<COUT, 4>(first, nFirst, rest, nRest, aDesc, wDesc); break;
-        case 5: issueRowStacked<COUT, 5>(first, nFirst, rest, nRest, aDesc, wDesc); break;
-        case 6: issueRowStacked<COUT, 6>(first, nFirst, rest, nRest, aDesc, wDesc); break;
-        case 7: issueRowStacked<COUT, 7>(first, nFirst, rest, nRest, aDesc, wDesc); break;
-        default: issueRowStacked<COUT, 8>(first, nFirst, rest, nRest, aDesc, wDesc); break;  // cin <= 128 (host check)
+        case 1: issueRowStacked<COUT, 1, SW>(first, nFirst, rest, nRest, aDesc, wDesc); break;
+        case 2: issueRowStacked<COUT, 2, SW>(first, nFirst, rest, nRest, aDesc, wDesc); break;
+        case 3: issueRowStacked<COUT, 3, SW>(first, nFirst, rest, nRest, aDesc, wDesc); break;
+        case 4: issueRowStacked<COUT, 4, SW>(first, nFirst, rest, nRest, aDesc, wDesc); break;
+        case 5: issueRowStacked<COUT, 5, SW>(first, nFirst, rest, nRest, aDesc, wDesc); break;
+        case 6: issueRowStacked<COUT, 6, SW>(first, nFirst, rest, nRest, aDesc, wDesc); break;
+        case 7: issueRowStacked<COUT, 7, SW>(first, nFirst, rest, nRest, aDesc, wDesc); break;
+        default: issueRowStacked<COUT, 8, SW>(first, nFirst, rest, nRest, aDesc, wDesc); break;  // cin <= 128 (host check)
+    }
+}
+template <int COUT>
+__device__ __forceinline__ void issueRowStackedG(int G2, int sw, const Seg (&first)[3], int nFirst, const Seg (&rest)[2],
+                                                 int nRest, uint64_t aDesc, uint64_t wDesc) {
+    switch (sw) {
+        case 16: issueRowStackedK<COUT, 16>(G2, first, nFirst, rest, nRest, aDesc, wDesc); break;
+        case 32: issueRowStackedK<COUT, 32>(G2, first, nFirst, rest, nRest, aDesc, wDesc); break;
+        case 64: issueRowStackedK<COUT, 64>(G2, first, nFirst, rest, nRest, aDesc, wDesc); break;
+        default: issueRowStackedK<COUT, 0>(G2, first, nFirst, rest, nRest, aDesc, wDesc); break;
     }
 }
 
@@ -408,11 +468,15 @@ __global__ void __launch_bounds__(kPipeThreads + 32 * (ISS - 1), ISS > 1 ? 1 : (
     volatile int* abortFlag = reinterpret_cast<volatile int*>(smem + Header::abort);
     const uint32_t wAddr = base + kHeader;
     const uint32_t slotBytes = a.slotBytes;
-    const uint32_t ringAddr = wAddr + a.weightBytes;
+    const uint32_t ringAddr = base + ringOffset(a.weightBytes, a.sw);  // slabs: on 1024-byte boundaries
     const uint32_t lowAddr = ringAddr + (uint32_t)a.ring * slotBytes;  // kLowBufs staging rows of the low input
     unsigned char* lowPtr = smem + (lowAddr - base);
     unsigned char* ringPtr = smem + (ringAddr - base);
     const uint64_t blockStart = a.stats ? nowNs() : 0;
+    if (a.sw && (base & 1023u)) {  // swizzled slabs need a 1024-byte aligned base: report, touch nothing
+        if (threadIdx.x == 0) atomicExch(a.errorFlag, 1);
+        return;
+    }
     // Planes of 8 channels: the low (upsampled) ones first in a slot, then
     // the full-resolution ones.
     const int G = a.cin / 8, Glow = a.lowChannels / 8, Gin = G - Glow;
@@ -531,9 +595,14 @@ __global__ void __launch_bounds__(kPipeThreads + 32 * (ISS - 1), ISS > 1 ? 1 : (
                 if (lane == 0) {
                     const uint32_t fb = pb + Header::full + 8 * s;
                     const uint32_t slot = ringAddr + (uint32_t)s * slotBytes;
-                    barExpectTx(fb, (uint32_t)Gin * kHalo * 16u);  // the boxes' bytes (planes are padded)
-                    for (int g = 0; g < Gin; g++)
-                        tmaLoad4(slot + (uint32_t)(Glow + g) * kPlane, &inMap, g * 8, U.x0 - 1, r, U.img, fb);
+                    barExpectTx(fb, (uint32_t)Gin * kHalo * 16u);  // the boxes' bytes (planes and slabs are padded)
+                    if (a.sw) {
+                        for (int j = 0; j < a.cin / a.sw; j++)
+                            tmaLoad4(slot + (uint32_t)j * slabBytes(a.sw), &inMap, j * a.sw, U.x0 - 1, r, U.img, fb);
+                    } else {
+                        for (int g = 0; g < Gin; g++)
+                            tmaLoad4(slot + (uint32_t)(Glow + g) * kPlane, &inMap, g * 8, U.x0 - 1, r, U.img, fb);
+                    }
                     if (Glow) {
                         const uint32_t lb = pb + Header::lowFull + 8 * (q % kLowBufs);
                         const uint32_t ls = lowAddr + (uint32_t)(q % kLowBufs) * a.lowSlotBytes;
@@ -651,8 +720,8 @@ __global__ void __launch_bounds__(kPipeThreads + 32 * (ISS - 1), ISS > 1 ? 1 : (
                                 else first[1] = fr;
                             }
                         }
-                        const uint64_t aDesc = ummaSmemDesc(ringAddr + (uint32_t)slot * slotBytes, kPlane, 128u);
-                        issueRowStackedG<COUT>(G2, first, nFirst, rest, nRest, aDesc, wStack);
+                        const uint64_t aDesc = rowDescriptor(ringAddr + (uint32_t)slot * slotBytes, a.sw);
+                        issueRowStackedG<COUT>(G2, a.sw, first, nFirst, rest, nRest, aDesc, wStack);
                         release();  // row i: no later MMA reads it
                         if (i >= 2) {  // output row i - 2 has all its taps
                             commit(pb + Header::accFull + 8 * ((p0 + i - 2) % NB));
@@ -679,10 +748,10 @@ __global__ void __launch_bounds__(kPipeThreads + 32 * (ISS - 1), ISS > 1 ? 1 : (
                         if (!ok) break;
                         tcFenceAfter();
                         const uint32_t acc = tmem + (uint32_t)(accBase + accB) * a.accCols;
-                        const uint64_t rowDesc[3] = {ummaSmemDesc(ringAddr + (uint32_t)s0 * slotBytes, kPlane, 128u),
-                                                     ummaSmemDesc(ringAddr + (uint32_t)s1 * slotBytes, kPlane, 128u),
-                                                     ummaSmemDesc(ringAddr + (uint32_t)s2 * slotBytes, kPlane, 128u)};
-                        issueTileG<COUT>(G2, acc, rowDesc, wDesc, idesc);
+                        const uint64_t rowDesc[3] = {rowDescriptor(ringAddr + (uint32_t)s0 * slotBytes, a.sw),
+                                                     rowDescriptor(ringAddr + (uint32_t)s1 * slotBytes, a.sw),
+                                                     rowDescriptor(ringAddr + (uint32_t)s2 * slotBytes, a.sw)};
+                        issueTileG<COUT>(G2, a.sw, acc, rowDesc, wDesc, idesc);
                         commit(pb + Header::accFull + 8 * (accBase + accB));
                         mine++;
                         if (++accB == a.nAcc) { accB = 0; accParity ^= 1u; }
@@ -790,14 +859,19 @@ PFN_cuTensorMapEncodeTiled_v12000 encodeTiled() {
     return fn;
 }
 
-// Rank-4 or rank-3 BF16 tensor map, no swizzle, zero fill outside the tensor.
+// Rank-4 or rank-3 BF16 tensor map, zero fill outside the tensor; no swizzle,
+// or the swizzle of a slab of `sw` channels (rowLayout).
 bool makeMap(CUtensorMap* map, const void* ptr, int rank, const uint64_t* dims, const uint64_t* strides,
-             const uint32_t* box) {
+             const uint32_t* box, int sw = 0) {
     auto fn = encodeTiled();
     if (!fn) return false;
     uint32_t elem[4] = {1, 1, 1, 1};
+    const CUtensorMapSwizzle swizzle = sw == 16   ? CU_TENSOR_MAP_SWIZZLE_32B
+                                       : sw == 32 ? CU_TENSOR_MAP_SWIZZLE_64B
+                                       : sw == 64 ? CU_TENSOR_MAP_SWIZZLE_128B
+                                                  : CU_TENSOR_MAP_SWIZZLE_NONE;
     return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, (cuuint32_t)rank, const_cast<void*>(ptr), dims, strides, box,
-              elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              elem, CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
@@ -824,11 +898,18 @@ cudaError_t launchPipe(const CUtensorMap& inMap, const CUtensorMap& lowMap, cons
 
 }  // namespace
 
-uint32_t convPipeSmemBytes(int cin, int cout, int lowChannels, int ring) {
-    const uint32_t weights = 9u * (uint32_t)cin * (uint32_t)cout * 2u;
-    const uint32_t slot = ((uint32_t)(cin / 8) * kPlane + 127u) & ~127u;
+namespace {
+uint32_t pipeSmemBytes(int cin, int cout, int lowChannels, int ring, int sw) {
     const uint32_t lowSlot = ((uint32_t)(lowChannels / 8) * kLowPlane + 127u) & ~127u;
-    return kHeader + weights + (uint32_t)ring * slot + (uint32_t)kLowBufs * lowSlot;
+    return ringOffset(9u * (uint32_t)cin * (uint32_t)cout * 2u, sw) + (uint32_t)ring * rowBytes(cin, sw) +
+           (uint32_t)kLowBufs * lowSlot;
+}
+}  // namespace
+
+// Planes: the layer routing (convPipeSupported / convPipePreferred) does not
+// depend on whether the swizzled slabs fit (a layer falls back to planes).
+uint32_t convPipeSmemBytes(int cin, int cout, int lowChannels, int ring) {
+    return pipeSmemBytes(cin, cout, lowChannels, ring, 0);
 }
 
 namespace {
@@ -870,12 +951,17 @@ cudaError_t convPipe(const bf16* in, const bf16* low, int lowChannels, int n, in
     if (head && nSplits != 1) return cudaErrorNotSupported;  // the head sums over all output channels of a pixel
     const int cout = coutTotal / nSplits;  // output channels per block
     const int cinIn = cin - lowChannels;
+    // convPipeReference(): tap-per-tile issue over rows staged as planes, the
+    // form the stacked issue and the swizzled slabs are checked against.
+    const bool reference = convPipeReference();
+    int sw = (test ? test->planes != 0 : reference) ? 0 : rowLayout(cin, lowChannels);
+    if (sw && pipeSmemBytes(cin, cout, lowChannels, 4, sw) > 227u * 1024u) sw = 0;  // slabs need a ring of 4 rows
     CUtensorMap inMap{}, lowMap{}, wMap{};
     {
         const uint64_t dims[4] = {(uint64_t)cinIn, (uint64_t)w, (uint64_t)h, (uint64_t)n};
         const uint64_t strides[3] = {(uint64_t)cinIn * 2, (uint64_t)w * cinIn * 2, (uint64_t)h * w * cinIn * 2};
-        const uint32_t box[4] = {8, kHalo, 1, 1};
-        if (!makeMap(&inMap, in, 4, dims, strides, box)) return cudaErrorNotSupported;
+        const uint32_t box[4] = {(uint32_t)(sw ? sw : 8), kHalo, 1, 1};
+        if (!makeMap(&inMap, in, 4, dims, strides, box, sw)) return cudaErrorNotSupported;
     }
     if (lowChannels) {
         const uint64_t dims[4] = {(uint64_t)lowChannels, (uint64_t)(w / 2), (uint64_t)(h / 2), (uint64_t)n};
@@ -898,7 +984,8 @@ cudaError_t convPipe(const bf16* in, const bf16* low, int lowChannels, int n, in
     a.coutTotal = coutTotal; a.nSplits = nSplits;
     a.tilesPerRow = (w + kM - 1) / kM;
     a.weightBytes = 9u * (uint32_t)cin * (uint32_t)cout * 2u;
-    a.slotBytes = ((uint32_t)(cin / 8) * kPlane + 127u) & ~127u;
+    a.slotBytes = rowBytes(cin, sw);
+    a.sw = sw;
     a.lowSlotBytes = ((uint32_t)(lowChannels / 8) * kLowPlane + 127u) & ~127u;
     a.accCols = 32;
     while (a.accCols < (uint32_t)cout) a.accCols <<= 1;
@@ -924,8 +1011,8 @@ cudaError_t convPipe(const bf16* in, const bf16* low, int lowChannels, int n, in
     // runs two issuers on the same ring.
     const int sms = deviceSmCount();
     const uint32_t smemPerSm = 228u * 1024u, smemMax = 227u * 1024u;
-    a.ring = convPipeSmemBytes(cin, cout, lowChannels, 4) <= smemMax ? 4 : kMinRing;
-    int perSm = (int)(smemPerSm / (convPipeSmemBytes(cin, cout, lowChannels, a.ring) + 1024u));
+    a.ring = pipeSmemBytes(cin, cout, lowChannels, 4, sw) <= smemMax ? 4 : kMinRing;
+    int perSm = (int)(smemPerSm / (pipeSmemBytes(cin, cout, lowChannels, a.ring, sw) + 1024u));
     perSm = std::max(1, std::min({perSm, (int)(512u / a.tmemCols), 2048 / kPipeThreads}));
     if (test && test->blocksPerSm > 0 && test->blocksPerSm < perSm) perSm = test->blocksPerSm;
     const int force = test ? test->issuers : 0;  // 1 or 2 issuers
@@ -933,7 +1020,7 @@ cudaError_t convPipe(const bf16* in, const bf16* low, int lowChannels, int n, in
     if (force == 2 && !twoFit) return cudaErrorNotSupported;
     // The stacked-row form (Cout 32 or 64 per block, no concatenated input):
     // one issuer, a ring of at least 4 accumulator blocks of cout columns.
-    const int stackMode = test ? test->stacked : (convStacking() ? 0 : 1);
+    const int stackMode = test ? test->stacked : (reference ? 1 : 0);
     const bool stackFits = !lowChannels && (cout == 32 || cout == 64) && cin <= 128 && force != 2;
     // Measured per layer: the stacked form is faster for unsplit 32-channel
     // layers (1080p 16 -> 32: 78.6 -> 74.2 us, 32 -> 32: 98.9 -> 94.0), slower
@@ -960,11 +1047,11 @@ cudaError_t convPipe(const bf16* in, const bf16* low, int lowChannels, int n, in
         while (a.tmemCols < (uint32_t)(nb * cout)) a.tmemCols <<= 1;
     }
     while (a.ring < kMaxRing &&
-           (uint32_t)perSm * (convPipeSmemBytes(cin, cout, lowChannels, a.ring + 1) + 1024u) <= smemPerSm &&
-           convPipeSmemBytes(cin, cout, lowChannels, a.ring + 1) <= smemMax)
+           (uint32_t)perSm * (pipeSmemBytes(cin, cout, lowChannels, a.ring + 1, sw) + 1024u) <= smemPerSm &&
+           pipeSmemBytes(cin, cout, lowChannels, a.ring + 1, sw) <= smemMax)
         a.ring++;
     if (test && test->ring >= kMinRing && test->ring <= kMaxRing) a.ring = test->ring;
-    const uint32_t smemBytes = convPipeSmemBytes(cin, cout, lowChannels, a.ring);
+    const uint32_t smemBytes = pipeSmemBytes(cin, cout, lowChannels, a.ring, sw);
     if (smemBytes > smemMax) return cudaErrorNotSupported;
     // Strips: balanced over the blocks (balancedStripRows); units that do
     // not divide evenly leave a last round on part of the GPU, strips too

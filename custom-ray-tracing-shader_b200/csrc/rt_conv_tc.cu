@@ -458,9 +458,9 @@ static std::atomic<int> g_convPath{0};
 static std::atomic<long long> g_pipeLaunches{0}, g_singleLaunches{0};
 void setConvPath(int mode) { g_convPath.store(mode); }
 int convPath() { return g_convPath.load(); }
-static std::atomic<bool> g_convStacking{true};
-void setConvStacking(bool on) { g_convStacking.store(on); }
-bool convStacking() { return g_convStacking.load(); }
+static std::atomic<bool> g_convPipeReference{false};
+void setConvPipeReference(bool on) { g_convPipeReference.store(on); }
+bool convPipeReference() { return g_convPipeReference.load(); }
 void convLaunchCounts(long long* pipe, long long* single) {
     if (pipe) *pipe = g_pipeLaunches.load();
     if (single) *single = g_singleLaunches.load();

@@ -101,10 +101,12 @@ inline int balancedStripRows(long long columns, int h, long long blocks) {
 
 void setConvPath(int mode);
 int convPath();
-// Whether the pipelined kernel may use its stacked-row issue (default on;
-// off runs every layer tap per tile, for comparison: results are identical).
-void setConvStacking(bool on);
-bool convStacking();
+// The pipelined kernel's reference form (default off): every layer's MMAs
+// issued tap by tap per output tile over input rows staged as planes of 8
+// channels, instead of the stacked-row issue and swizzled slabs; results are
+// identical, for comparison.
+void setConvPipeReference(bool on);
+bool convPipeReference();
 // Convolutions run so far by the pipelined and by the single-role kernel.
 void convLaunchCounts(long long* pipe, long long* single);
 
@@ -119,6 +121,7 @@ struct ConvPipeTest {
     int blocksPerSm;                 // fewer blocks per SM than shared memory allows (each then gets a longer ring)
     int issuers;                     // MMA issuers per block: 0 chosen per layer, 1, or 2 (sharing the ring)
     int stacked;                     // 0 chosen per layer, 1 tap-per-tile issue, 2 stacked-row issue
+    int planes;                      // 1: input rows staged as planes of 8 channels (no swizzled slabs)
 };
 
 // The same convolution as convTc, warp-specialised and fed by TMA (input

@@ -907,7 +907,7 @@ int RtxSetEnvironment(void* p, int mode, float r, float g, float b) {
 int RtxSetConvPath(int mode) {
     if (mode < 0 || mode > 2) return 0;
     rt::setConvPath(mode == 1 ? 1 : 0);
-    rt::setConvStacking(mode == 0);
+    rt::setConvPipeReference(mode == 2);
     return 1;
 }
 

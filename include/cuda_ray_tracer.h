@@ -227,11 +227,13 @@ int RtxSetTuning(void* session, int key, int value);
  * counterpart in the reference: 0 (default) the warp-specialised TMA-fed
  * kernel wherever its shared memory allows (inference then also runs the
  * decoders' concatenated layers as two passes and fuses the output head
- * into the last layer; unsplit 32-channel layers issue one MMA per input row
- * and column tap over the three kernel rows' weights side by side), 1 the
+ * into the last layer; input rows are staged as swizzled slabs of 16-64
+ * channels, and unsplit 32-channel layers issue one MMA per input row and
+ * column tap over the three kernel rows' weights side by side), 1 the
  * single-role kernel for every layer, one pass each, 2 as 0 with every
- * layer's MMAs issued tap by tap per output tile. Process-wide; 0 and 2 give
- * identical results, 1 agrees with them to BF16 rounding. */
+ * layer's MMAs issued tap by tap per output tile over rows staged as planes
+ * of 8 channels. Process-wide; 0 and 2 give identical results, 1 agrees with
+ * them to BF16 rounding. */
 int RtxSetConvPath(int mode);
 /* Convolutions launched so far in this process by the warp-specialised
  * kernel and by the single-role kernel (either pointer may be null); no

@@ -321,14 +321,17 @@ def test_conv_kernels_agree(lib, net):
 
 
 def test_stacked_row_issue_identical(lib, net):
-    """Unsplit 32-channel layers issue one MMA per input row and column tap
-    over the three kernel rows' weights side by side (accumulator blocks per
-    output row in a ring); RtxSetConvPath(2) issues every tap per output tile
-    instead. Each output row receives the taps in the same order either way,
-    so inference is bit-identical: at sizes whose strips end mid-image, with
-    a partial column tile, and with one-row strips. Training agrees to FP32
-    summation order (the loss and the bias and head gradients sum with
-    atomics, whose order varies from run to run)."""
+    """The pipelined kernel's default form stages input rows as swizzled
+    slabs of 16-64 channels (one TMA box each) and, for unsplit 32-channel
+    layers, issues one MMA per input row and column tap over the three kernel
+    rows' weights side by side (accumulator blocks per output row in a ring);
+    RtxSetConvPath(2) stages rows as planes of 8 channels and issues every tap
+    per output tile. The MMAs see the same operands and each output row
+    receives the taps in the same order either way, so inference is
+    bit-identical: at sizes whose strips end mid-image, with a partial column
+    tile, and with one-row strips. Training agrees to FP32 summation order
+    (the loss and the bias and head gradients sum with atomics, whose order
+    varies from run to run)."""
     rng = np.random.default_rng(21)
     try:
         for h, w in ((200, 300), (37, 130), (16, 16)):
