@@ -68,6 +68,10 @@ constexpr int kLowHalo = kM / 2 + 2;     // low-resolution pixels per staged row
 constexpr uint32_t kPlane = (kHalo * 16 + 127) / 128 * 128;        // 2,176
 constexpr uint32_t kLowPlane = (kLowHalo * 16 + 127) / 128 * 128;  // 1,152
 constexpr int kPipeThreads = 192;  // warps of one pipeline: producer, MMA issuer, 4 epilogue warps
+// Threads of a block: the pipeline, a second issuer (warp 6) for ISS = 2,
+// and with EPI = 8 four more epilogue warps (7-10) that drain the second
+// half of each accumulator's columns.
+__host__ __device__ constexpr int pipeThreads(int iss, int epi) { return kPipeThreads + 32 * (iss - 1) + 32 * (epi - 4); }
 constexpr int kMinRing = 3;  // the rows a tile reads; 4 and more let the producer run ahead
 constexpr int kMaxRing = 16;
 constexpr int kMaxAcc = 8;   // tensor-memory accumulators per block (tiles between the issuer and the epilogue)
@@ -133,6 +137,8 @@ struct PipeArgs {
     // resolution: 4 blocks of coutTotal channels per low pixel, block
     // (y % 2) * 2 + x % 2 for output pixel (x, y); added before bias and ReLU.
     const bf16* upAdd;
+    long long upPixels;   // low pixels of upAdd (planes of 8 channels: see convTc)
+    long long outPixels;  // > 0: BF16 output as planes of 8 channels over this many pixels
     ConvHead head;  // head.out set: the fused 1x1 output head (see ConvHead); activations not stored
     // Optional wait statistics (test hook), nanoseconds summed over blocks:
     // [0] producer waiting for a free slot, [1] producer waiting for a low
@@ -379,16 +385,18 @@ __device__ __forceinline__ Unit unitOf(const PipeArgs& a, int u) {
 
 // The upsampled-half addend of output pixel (x, y) (see PipeArgs::upAdd),
 // loaded before the epilogue waits for its accumulator so the load's latency
-// overlaps the wait (COUT <= 96; wider layers take no addend).
-__host__ __device__ constexpr int upWords(int cout) { return cout <= 96 ? cout / 8 : 1; }
+// overlaps the wait (COUT <= 64; wider layers take no addend).
+__host__ __device__ constexpr int upWords(int cout) { return cout <= 64 ? cout / 8 : 1; }
 template <int COUT>
 __device__ __forceinline__ void loadUpAddend(const PipeArgs& a, int img, int y, int x, int nBase,
                                              uint4 (&u)[upWords(COUT)]) {
+    // Planes of 8 channels over the low pixels: block (y % 2) * 2 + x % 2's
+    // channels nBase ... are planes (block * coutTotal + nBase) / 8 + q.
     const size_t low = ((size_t)img * (a.h / 2) + y / 2) * (a.w / 2) + x / 2;
-    const uint4* src = reinterpret_cast<const uint4*>(a.upAdd + low * 4 * a.coutTotal +
-                                                      (size_t)((y & 1) * 2 + (x & 1)) * a.coutTotal + nBase);
+    const size_t plane0 = (size_t)(((y & 1) * 2 + (x & 1)) * a.coutTotal + nBase) / 8;
+    const uint4* src = reinterpret_cast<const uint4*>(a.upAdd);
 #pragma unroll
-    for (int q = 0; q < upWords(COUT); q++) u[q] = __ldg(src + q);
+    for (int q = 0; q < upWords(COUT); q++) u[q] = __ldg(src + (plane0 + q) * (size_t)a.upPixels + low);
 }
 // Bias, the addend, ReLU and the store of 16 output channels (c0 .. c0 + 15
 // of the block's COUT) of one pixel, from 16 accumulator columns.
@@ -399,7 +407,7 @@ __device__ __forceinline__ void epilogueStore16(const PipeArgs& a, const uint32_
     float v[16];
 #pragma unroll
     for (int j = 0; j < 16; j++) v[j] = __uint_as_float(acc[j]) + bias[c0 + j];  // bias: broadcast from shared memory
-    if (COUT <= 96 && a.upAdd) {
+    if (COUT <= 64 && a.upAdd) {
 #pragma unroll
         for (int q = 0; q < 2; q++) {
             const __nv_bfloat162* pairs = reinterpret_cast<const __nv_bfloat162*>(&up[c0 / 8 + q]);
@@ -435,7 +443,6 @@ __device__ __forceinline__ void epilogueStore16(const PipeArgs& a, const uint32_
             o[q] = x;
         }
     } else {
-        uint4* o = reinterpret_cast<uint4*>(a.outB + pix * a.coutTotal + nBase + c0);
 #pragma unroll
         for (int q = 0; q < 2; q++) {
             uint32_t words[4];
@@ -444,7 +451,9 @@ __device__ __forceinline__ void epilogueStore16(const PipeArgs& a, const uint32_
                 __nv_bfloat162 pair = __floats2bfloat162_rn(v[8 * q + 2 * j], v[8 * q + 2 * j + 1]);
                 words[j] = *reinterpret_cast<uint32_t*>(&pair);
             }
-            o[q] = make_uint4(words[0], words[1], words[2], words[3]);
+            uint4* o = a.outPixels ? reinterpret_cast<uint4*>(a.outB) + ((size_t)(nBase + c0) / 8 + q) * (size_t)a.outPixels + pix
+                                   : reinterpret_cast<uint4*>(a.outB + pix * a.coutTotal + nBase + c0) + q;
+            *o = make_uint4(words[0], words[1], words[2], words[3]);
         }
     }
 }
@@ -455,8 +464,8 @@ __device__ __forceinline__ void epilogueStore16(const PipeArgs& a, const uint32_
 // arrivals). Two issuers give a layer that fits one block per SM two issuing
 // threads without a second ring.
 // STACK: the stacked-row issue (one issuer; a.nAcc blocks of COUT columns).
-template <int COUT, int ISS, bool STACK>
-__global__ void __launch_bounds__(kPipeThreads + 32 * (ISS - 1), ISS > 1 ? 1 : (COUT <= 48 ? 4 : 2))
+template <int COUT, int ISS, bool STACK, int EPI>
+__global__ void __launch_bounds__(pipeThreads(ISS, EPI), ISS > 1 ? 1 : (COUT <= 48 ? 4 : 2))
     convPipeKernel(const __grid_constant__ CUtensorMap inMap, const __grid_constant__ CUtensorMap lowMap,
                    const __grid_constant__ CUtensorMap wMap, PipeArgs a) {
     extern __shared__ __align__(1024) unsigned char smem[];
@@ -496,7 +505,7 @@ __global__ void __launch_bounds__(kPipeThreads + 32 * (ISS - 1), ISS > 1 ? 1 : (
         for (int s = 0; s < kLowBufs; s++) barInit(pb + Header::lowFull + 8 * s, 1);
         for (int b = 0; b < ISS * a.nAcc; b++) {  // issuer i's accumulator b at i * nAcc + b
             barInit(pb + Header::accFull + 8 * b, 1);
-            barInit(pb + Header::accEmpty + 8 * b, 4);
+            barInit(pb + Header::accEmpty + 8 * b, EPI);
         }
         barInit(pb + Header::drain, ISS);
         barInit(pb + Header::weightsFull, 1);
@@ -782,11 +791,14 @@ __global__ void __launch_bounds__(kPipeThreads + 32 * (ISS - 1), ISS > 1 ? 1 : (
         }
         __syncwarp();
     } else {
-        // ---- epilogue: warps 2-5, lanes 32 * (warp % 4) ... of the accumulator ----
+        // ---- epilogue: warps 2-5 (and 7-10), lanes 32 * (warp % 4) ... ----
         // A warp may read only tensor-memory lanes 32 * (its warp index in
-        // the block mod 4) ...: warps 2-5 of pipeline 0 and 8-11 of
-        // pipeline 1 each cover the four quarters once.
+        // the block mod 4) ...: warps 2-5 cover the four quarters once, and
+        // with EPI = 8 warps 7-10 once more; each set then drains half of
+        // the accumulator's columns.
         const int quarter = (int)(threadIdx.x >> 5) & 3;
+        constexpr int kChunks = COUT / 16 / (EPI / 4);  // 16-column chunks per warp
+        const int chunk0 = EPI == 8 && (threadIdx.x >> 5) >= 7 ? kChunks : 0;
         int bOf[ISS] = {};             // per issuer: next accumulator and its phase
         uint32_t parityOf[ISS] = {};
         int tile = 0;
@@ -801,7 +813,7 @@ __global__ void __launch_bounds__(kPipeThreads + 32 * (ISS - 1), ISS > 1 ? 1 : (
                 if (++bOf[i] == a.nAcc) { bOf[i] = 0; parityOf[i] ^= 1u; }
                 const int x = U.x0 + quarter * 32 + lane;
                 uint4 up[upWords(COUT)];
-                if (COUT <= 96 && a.upAdd && x < a.w) loadUpAddend<COUT>(a, U.img, y, x, nBase, up);
+                if (COUT <= 64 && a.upAdd && x < a.w) loadUpAddend<COUT>(a, U.img, y, x, nBase, up);
                 const uint64_t t1 = a.stats ? nowNs() : 0;
                 if (!waitPhaseWarp(pb + Header::accFull + 8 * b, parity, abortFlag, limit)) { ok = false; break; }
                 if (a.stats) waitNs += nowNs() - t1;
@@ -815,7 +827,7 @@ __global__ void __launch_bounds__(kPipeThreads + 32 * (ISS - 1), ISS > 1 ? 1 : (
                     for (int k = 0; k < 3; k++) headSum[k] = __ldg(a.head.b + k);
                 }
 #pragma unroll
-                for (int c = 0; c < COUT / 16; c++) {
+                for (int c = chunk0; c < chunk0 + kChunks; c++) {
                     uint32_t r[16];
                     tmemLoad16(taddr + (uint32_t)(16 * c), r);
                     tmemWaitLoads();
@@ -882,17 +894,17 @@ int deviceSmCount() {
     return sms > 0 ? sms : 1;
 }
 
-template <int COUT, int ISS, bool STACK = false>
+template <int COUT, int ISS, bool STACK = false, int EPI = 4>
 cudaError_t launchPipe(const CUtensorMap& inMap, const CUtensorMap& lowMap, const CUtensorMap& wMap,
                        const PipeArgs& a, int grid, uint32_t smemBytes, cudaStream_t stream) {
     static bool configured = false;
     if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(convPipeKernel<COUT, ISS, STACK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaError_t e = cudaFuncSetAttribute(convPipeKernel<COUT, ISS, STACK, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              227 * 1024);
         if (e != cudaSuccess) return e;
         configured = true;
     }
-    convPipeKernel<COUT, ISS, STACK><<<grid, kPipeThreads + 32 * (ISS - 1), smemBytes, stream>>>(inMap, lowMap, wMap, a);
+    convPipeKernel<COUT, ISS, STACK, EPI><<<grid, pipeThreads(ISS, EPI), smemBytes, stream>>>(inMap, lowMap, wMap, a);
     return cudaGetLastError();
 }
 
@@ -940,12 +952,12 @@ bool convPipePreferred(int cin, int cout, int lowChannels) {
 cudaError_t convPipe(const bf16* in, const bf16* low, int lowChannels, int n, int h, int w, int cin,
                      const bf16* weights, bool reverseTaps, const float* bias, int coutTotal, bf16* outB, float* outF,
                      bool relu, bool accumulate, int* errorFlag, cudaStream_t stream, const ConvPipeTest* test,
-                     const bf16* upAddend, const ConvHead* head) {
+                     const bf16* upAddend, const ConvHead* head, bool planarOut) {
     if (!low) lowChannels = 0;
     if (n < 1 || h < 1 || w < 1 || !convPipeSupported(cin, coutTotal, lowChannels) || (!outB && !outF && !head) ||
         (head && (!head->out || !head->wt || !head->b || n != 1 || head->h > h || head->w > w)) ||
         !errorFlag || (lowChannels && (h % 2 || w % 2)) ||
-        (upAddend && (h % 2 || w % 2 || lowChannels || coutTotal > 96)))
+        (upAddend && (h % 2 || w % 2 || lowChannels || coutTotal > 64)) || (planarOut && (!outB || outF || head)))
         return cudaErrorNotSupported;
     const int nSplits = pickSplits(cin, coutTotal, lowChannels);
     if (head && nSplits != 1) return cudaErrorNotSupported;  // the head sums over all output channels of a pixel
@@ -999,6 +1011,8 @@ cudaError_t convPipe(const bf16* in, const bf16* low, int lowChannels, int n, in
     if (a.tmemCols > 512) return cudaErrorNotSupported;
     a.stats = test ? test->stats : nullptr;
     a.bias = bias; a.outB = outB; a.outF = outF; a.upAdd = upAddend;
+    a.outPixels = planarOut ? (long long)n * h * w : 0;
+    a.upPixels = (long long)n * (h / 2) * (w / 2);
     if (head) a.head = *head;
     a.relu = relu ? 1 : 0; a.accumulate = accumulate ? 1 : 0; a.reverseTaps = reverseTaps ? 1 : 0;
     a.errorFlag = errorFlag;
@@ -1063,6 +1077,10 @@ cudaError_t convPipe(const bf16* in, const bf16* low, int lowChannels, int n, in
     a.strips = (h + a.stripRows - 1) / a.stripRows;
     a.units = (int)(columns * a.strips);
     const int grid = (int)std::min<long long>((long long)a.units * nSplits, blocks);
+    // Eight epilogue warps where one block per SM drains wide accumulators
+    // (two issuers, 96 or 128 columns); the fused head needs a pixel's
+    // channels in one thread.
+    const bool wideEpilogue = issuers == 2 && cout >= 96 && !head && !(test && test->epilogueWarps == 4);
     switch (cout) {
         case 16: return issuers == 2 ? launchPipe<16, 2>(inMap, lowMap, wMap, a, grid, smemBytes, stream)
                              : launchPipe<16, 1>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
@@ -1076,9 +1094,11 @@ cudaError_t convPipe(const bf16* in, const bf16* low, int lowChannels, int n, in
                              : launchPipe<64, 1>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
         case 80: return issuers == 2 ? launchPipe<80, 2>(inMap, lowMap, wMap, a, grid, smemBytes, stream)
                              : launchPipe<80, 1>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
-        case 96: return issuers == 2 ? launchPipe<96, 2>(inMap, lowMap, wMap, a, grid, smemBytes, stream)
+        case 96: return issuers == 2 ? (wideEpilogue ? launchPipe<96, 2, false, 8>(inMap, lowMap, wMap, a, grid, smemBytes, stream)
+                                             : launchPipe<96, 2>(inMap, lowMap, wMap, a, grid, smemBytes, stream))
                              : launchPipe<96, 1>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
-        case 128: return issuers == 2 ? launchPipe<128, 2>(inMap, lowMap, wMap, a, grid, smemBytes, stream)
+        case 128: return issuers == 2 ? (wideEpilogue ? launchPipe<128, 2, false, 8>(inMap, lowMap, wMap, a, grid, smemBytes, stream)
+                                              : launchPipe<128, 2>(inMap, lowMap, wMap, a, grid, smemBytes, stream))
                               : launchPipe<128, 1>(inMap, lowMap, wMap, a, grid, smemBytes, stream);
         default: return cudaErrorNotSupported;
     }

@@ -510,18 +510,18 @@ cudaError_t combineUpsampledWeights(const bf16* weights, int cout, int cin, int 
 }
 
 bool upsampledSplitSupported(int cin, int cout, int lowChannels) {
-    return lowChannels > 0 && lowChannels < cin && convPipePreferred(lowChannels, 4 * cout, 0) &&
+    return lowChannels > 0 && lowChannels < cin && cout <= 64 && convPipePreferred(lowChannels, 4 * cout, 0) &&
            convPipePreferred(cin - lowChannels, cout, 0);
 }
 
 cudaError_t convTc(const bf16* in, const bf16* low, int lowChannels, int n, int h, int w, int cin,
                    const bf16* weights, bool reverseTaps, const float* bias, int cout, bf16* outB, float* outF,
                    bool relu, bool accumulate, int* errorFlag, cudaStream_t stream, const bf16* upAddend,
-                   const ConvHead* head) {
-    if (upAddend || head) {  // the two-pass decoder form's second pass, a fused head: pipelined kernel only
+                   const ConvHead* head, bool planarOut) {
+    if (upAddend || head || planarOut) {  // the two-pass decoder form, a fused head: pipelined kernel only
         if (low || !convPipePreferred(cin, cout, 0)) return cudaErrorNotSupported;
         cudaError_t e = convPipe(in, nullptr, 0, n, h, w, cin, weights, reverseTaps, bias, cout, outB, outF, relu,
-                                 accumulate, errorFlag, stream, nullptr, upAddend, head);
+                                 accumulate, errorFlag, stream, nullptr, upAddend, head, planarOut);
         if (e == cudaSuccess) g_pipeLaunches++;
         return e;
     }

@@ -60,11 +60,16 @@ struct ConvHead {
 
 // upAddend (optional, pipelined form only): the upsampled half of a decoder
 // convolution computed at half resolution (see combineUpsampledWeights),
-// 4 blocks of cout channels per low pixel, added before bias and ReLU.
+// 4 blocks of cout channels per low pixel, added before bias and ReLU; it is
+// stored as planes of 8 channels over the low pixels, element (low pixel q,
+// channel c of the 4 cout) at ((c / 8) * lowPixels + q) * 8 + c % 8, which
+// is what a convolution with planarOut (pipelined form only) writes: a warp's
+// 32 pixels then store 512 contiguous bytes per plane instead of 16 bytes per
+// pixel at the pixel stride.
 cudaError_t convTc(const __nv_bfloat16* in, const __nv_bfloat16* low, int lowChannels, int n, int h, int w, int cin,
                    const __nv_bfloat16* weights, bool reverseTaps, const float* bias, int cout, __nv_bfloat16* outB,
                    float* outF, bool relu, bool accumulate, int* errorFlag, cudaStream_t stream,
-                   const __nv_bfloat16* upAddend = nullptr, const ConvHead* head = nullptr);
+                   const __nv_bfloat16* upAddend = nullptr, const ConvHead* head = nullptr, bool planarOut = false);
 
 // A decoder convolution over [upsample2(low), skip] as two convolutions:
 // the low half at low resolution with 4 blocks of cout output channels, one
@@ -122,6 +127,7 @@ struct ConvPipeTest {
     int issuers;                     // MMA issuers per block: 0 chosen per layer, 1, or 2 (sharing the ring)
     int stacked;                     // 0 chosen per layer, 1 tap-per-tile issue, 2 stacked-row issue
     int planes;                      // 1: input rows staged as planes of 8 channels (no swizzled slabs)
+    int epilogueWarps;               // 4: no second set of epilogue warps (0 chosen per layer)
 };
 
 // The same convolution as convTc, warp-specialised and fed by TMA (input
@@ -141,7 +147,7 @@ cudaError_t convPipe(const __nv_bfloat16* in, const __nv_bfloat16* low, int lowC
                      const __nv_bfloat16* weights, bool reverseTaps, const float* bias, int cout,
                      __nv_bfloat16* outB, float* outF, bool relu, bool accumulate, int* errorFlag,
                      cudaStream_t stream, const ConvPipeTest* test = nullptr,
-                     const __nv_bfloat16* upAddend = nullptr, const ConvHead* head = nullptr);
+                     const __nv_bfloat16* upAddend = nullptr, const ConvHead* head = nullptr, bool planarOut = false);
 
 // Weight gradient on tcgen05 (rt_wgrad_tc.cu): dw[tap][ci][co] += sum_p
 // x[p + off(tap)][ci] dy[p][co] over NHWC BF16 x (cin channels) and dy (cout

@@ -598,7 +598,7 @@ cudaError_t Unet::forward(cudaStream_t s, bool training, bool outputLayer, const
                 e = combineUpsampledWeights(wT_ + L.wOffset, L.cout, L.cin, Cl, A.upWeights[j], A.skipWeights[j], s);
                 if (e == cudaSuccess)
                     e = convTc(low, nullptr, 0, n, H / 2, W / 2, Cl, A.upWeights[j], false, nullptr, 4 * L.cout, A.upHalf,
-                               nullptr, false, false, convError_, s);
+                               nullptr, false, false, convError_, s, nullptr, nullptr, true);
                 if (e == cudaSuccess)
                     e = convTc(skip, nullptr, 0, n, H, W, Cs, A.skipWeights[j], false, master_ + L.bOffset, L.cout, A.a[k],
                                nullptr, true, false, convError_, s, A.upHalf);
