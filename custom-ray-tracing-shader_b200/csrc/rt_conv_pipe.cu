@@ -144,7 +144,8 @@ struct PipeArgs {
     // [0] producer waiting for a free slot, [1] producer waiting for a low
     // row, [2] issuer waiting for rows, [3] issuer waiting for a drained
     // accumulator, [4] epilogue waiting for a full accumulator (per warp),
-    // [5] block lifetime.
+    // [5] block lifetime, [6] stacked issuer inside its MMA issue, [7]
+    // stacked issuer committing.
     unsigned long long* stats;
 };
 
@@ -163,8 +164,9 @@ struct Header {
     static constexpr uint32_t tmemSlot = weights + 16;
     static constexpr uint32_t abort = weights + 20;
     static constexpr uint32_t bias = weights + 64;         // the block's output channels' biases (<= 128 floats)
+    static constexpr uint32_t head = bias + 128 * 4;       // fused head: per channel {w0, w1, w2, 0} (<= 32 channels)
 };
-static_assert(Header::weightsFull + 8 <= kPipeHeader && Header::bias + 128 * 4 <= kHeader, "header size");
+static_assert(Header::weightsFull + 8 <= kPipeHeader && Header::head + 32 * 16 <= kHeader, "header size");
 
 __device__ __forceinline__ uint32_t smemAddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ uint64_t nowNs() {
@@ -403,7 +405,7 @@ __device__ __forceinline__ void loadUpAddend(const PipeArgs& a, int img, int y, 
 template <int COUT>
 __device__ __forceinline__ void epilogueStore16(const PipeArgs& a, const uint32_t (&acc)[16], size_t pix, int c0,
                                                 int nBase, const float* bias, const uint4 (&up)[upWords(COUT)],
-                                                float (&headSum)[3]) {
+                                                float (&headSum)[3], const float4* headW) {
     float v[16];
 #pragma unroll
     for (int j = 0; j < 16; j++) v[j] = __uint_as_float(acc[j]) + bias[c0 + j];  // bias: broadcast from shared memory
@@ -422,12 +424,15 @@ __device__ __forceinline__ void epilogueStore16(const PipeArgs& a, const uint32_
 #pragma unroll
     for (int j = 0; j < 16; j++) v[j] = a.relu ? fmaxf(v[j], 0.0f) : v[j];
     if (a.head.out) {
-        // The head reads the activations as BF16, channel by channel.
+        // The head reads the activations as BF16, channel by channel (its
+        // weights from shared memory, one 16-byte broadcast per channel).
 #pragma unroll
         for (int j = 0; j < 16; j++) {
             const float x = __bfloat162float(__float2bfloat16_rn(v[j]));
-#pragma unroll
-            for (int k = 0; k < 3; k++) headSum[k] += x * __ldg(a.head.wt + (nBase + c0 + j) * 3 + k);
+            const float4 wv = headW[c0 + j];
+            headSum[0] += x * wv.x;
+            headSum[1] += x * wv.y;
+            headSum[2] += x * wv.z;
         }
         return;
     }
@@ -515,6 +520,11 @@ __global__ void __launch_bounds__(pipeThreads(ISS, EPI), ISS > 1 ? 1 : (COUT <= 
     }
     float* sBias = reinterpret_cast<float*>(smem + Header::bias);
     for (int c = threadIdx.x; c < COUT; c += blockDim.x) sBias[c] = a.bias ? a.bias[nBase + c] : 0.0f;
+    const float4* sHead = reinterpret_cast<const float4*>(smem + Header::head);
+    if (a.head.out)
+        for (int c = threadIdx.x; c < COUT && c < 32; c += blockDim.x)
+            reinterpret_cast<float4*>(smem + Header::head)[c] =
+                make_float4(a.head.wt[c * 3], a.head.wt[c * 3 + 1], a.head.wt[c * 3 + 2], 0.0f);
     if (threadIdx.x >> 5 == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(base + Header::tmemSlot),
                      "r"(a.tmemCols)
@@ -657,7 +667,7 @@ __global__ void __launch_bounds__(pipeThreads(ISS, EPI), ISS > 1 ? 1 : (COUT <= 
             if (a.probe) ok = waitPhase(base + Header::probe, 0u, abortFlag, limit);
             if (ok)
                 ok = waitPhase(pb + Header::weightsFull, 0u, abortFlag, limit);
-            uint64_t waitRowNs = 0, waitAccNs = 0;
+            uint64_t waitRowNs = 0, waitAccNs = 0, issueNs = 0, commitNs = 0;
             const uint64_t wDesc = ummaSmemDesc(wAddr, COUT * 16u, 128u);
             const int G2 = G / 2;
             int rows = 0, tiles = 0, mine = 0;  // rows waited for, the block's tiles, this issuer's tiles
@@ -682,14 +692,15 @@ __global__ void __launch_bounds__(pipeThreads(ISS, EPI), ISS > 1 ? 1 : (COUT <= 
             if constexpr (STACK) {
                 // Per input row i of a strip of S output rows (row y0 - 1 + i,
                 // i = 0 .. S + 1): output rows jLo .. jHi of the strip, whose
-                // blocks are (p0 + j) % NB; block p0 + i is fresh.
+                // blocks are (p0 + j) % NB for the strip's first block p0 (kept as
+                // running counters); block p0 + i is fresh.
                 const int NB = a.nAcc;
                 const uint64_t wStack = ummaSmemDesc(wAddr, 3u * COUT * 16u, 128u);
                 const uint32_t id0 = ummaInstrDescBf16(kM, 0);  // plus (N / 8) << 17 for N = blocks x COUT
                 for (int u = firstUnit; u < a.units && ok; u += unitStride) {
                     const Unit U = unitOf(a, u);
                     const int S = U.y1 - U.y0;
-                    const int p0 = accB;
+                    int pLo = accB;  // block of output row jLo (running, no division)
                     for (int i = 0; i <= S + 1; i++) {
                         int slot = 0;
                         if (!nextRow(slot)) { ok = false; break; }
@@ -702,9 +713,9 @@ __global__ void __launch_bounds__(pipeThreads(ISS, EPI), ISS > 1 ? 1 : (COUT <= 
                             tcFenceAfter();
                         }
                         const int jLo = i > 2 ? i - 2 : 0, jHi = i < S - 1 ? i : S - 1;
-                        // Output rows lo .. hi as one segment, or two where the ring wraps.
-                        auto range = [&](int lo, int hi, uint32_t accFlag, Seg& s0, Seg& s1) -> int {
-                            const int p = (p0 + lo) % NB, len = hi - lo + 1, run = len < NB - p ? len : NB - p;
+                        // Output rows lo .. hi (lo's block p) as one segment, or two where the ring wraps.
+                        auto range = [&](int p, int lo, int hi, uint32_t accFlag, Seg& s0, Seg& s1) -> int {
+                            const int len = hi - lo + 1, run = len < NB - p ? len : NB - p;
                             s0 = Seg{tmem + (uint32_t)(p * COUT), (uint32_t)((lo - i + 2) * COUT),
                                      id0 + ((uint32_t)(run * COUT / 8) << 17), accFlag};
                             s1 = Seg{tmem, (uint32_t)((lo + run - i + 2) * COUT),
@@ -712,29 +723,33 @@ __global__ void __launch_bounds__(pipeThreads(ISS, EPI), ISS > 1 ? 1 : (COUT <= 
                             return run < len ? 2 : 1;
                         };
                         Seg first[3], rest[2];
-                        const int nRest = range(jLo, jHi, 1u, rest[0], rest[1]);
+                        const int nRest = range(pLo, jLo, jHi, 1u, rest[0], rest[1]);
                         int nFirst = nRest;
                         first[0] = rest[0];
                         first[1] = rest[1];
                         if (fresh) {
                             // The fresh block (output row i = jHi) apart, from zero.
                             Seg fr, unused;
-                            range(jHi, jHi, 0u, fr, unused);
+                            range(accB, jHi, jHi, 0u, fr, unused);  // jHi = i: the fresh block
                             if (jHi == jLo) {
                                 first[0] = fr;
                                 nFirst = 1;
                             } else {
-                                nFirst = range(jLo, jHi - 1, 1u, first[0], first[1]) + 1;
+                                nFirst = range(pLo, jLo, jHi - 1, 1u, first[0], first[1]) + 1;
                                 if (nFirst == 3) first[2] = fr;
                                 else first[1] = fr;
                             }
                         }
                         const uint64_t aDesc = rowDescriptor(ringAddr + (uint32_t)slot * slotBytes, a.sw);
+                        const uint64_t t2 = a.stats ? nowNs() : 0;
                         issueRowStackedG<COUT>(G2, a.sw, first, nFirst, rest, nRest, aDesc, wStack);
+                        const uint64_t t3 = a.stats ? nowNs() : 0;
                         release();  // row i: no later MMA reads it
-                        if (i >= 2) {  // output row i - 2 has all its taps
-                            commit(pb + Header::accFull + 8 * ((p0 + i - 2) % NB));
+                        if (i >= 2) {  // output row i - 2 = jLo has all its taps
+                            commit(pb + Header::accFull + 8 * pLo);
+                            pLo = pLo + 1 == NB ? 0 : pLo + 1;
                         }
+                        if (a.stats) { issueNs += t3 - t2; commitNs += nowNs() - t3; }
                         if (fresh) {
                             mine++;
                             if (++accB == NB) { accB = 0; accParity ^= 1u; }
@@ -787,7 +802,12 @@ __global__ void __launch_bounds__(pipeThreads(ISS, EPI), ISS > 1 ? 1 : (COUT <= 
                 commit(pb + Header::drain);
                 pollPhase(pb + Header::drain, 0u, limit);
             }
-            if (a.stats) { atomicAdd(a.stats + 2, waitRowNs); atomicAdd(a.stats + 3, waitAccNs); }
+            if (a.stats) {
+                atomicAdd(a.stats + 2, waitRowNs);
+                atomicAdd(a.stats + 3, waitAccNs);
+                atomicAdd(a.stats + 6, issueNs);
+                atomicAdd(a.stats + 7, commitNs);
+            }
         }
         __syncwarp();
     } else {
@@ -799,6 +819,10 @@ __global__ void __launch_bounds__(pipeThreads(ISS, EPI), ISS > 1 ? 1 : (COUT <= 
         const int quarter = (int)(threadIdx.x >> 5) & 3;
         constexpr int kChunks = COUT / 16 / (EPI / 4);  // 16-column chunks per warp
         const int chunk0 = EPI == 8 && (threadIdx.x >> 5) >= 7 ? kChunks : 0;
+        // Chunks loaded before one wait: all of them (up to 5, else a divisor)
+        // where registers allow (one or two blocks per SM), else one.
+        constexpr int kGroup = !(ISS == 2 || COUT >= 64) ? 1
+                               : kChunks <= 5 ? kChunks : kChunks % 4 == 0 ? 4 : kChunks % 3 == 0 ? 3 : 2;
         int bOf[ISS] = {};             // per issuer: next accumulator and its phase
         uint32_t parityOf[ISS] = {};
         int tile = 0;
@@ -826,12 +850,17 @@ __global__ void __launch_bounds__(pipeThreads(ISS, EPI), ISS > 1 ? 1 : (COUT <= 
 #pragma unroll
                     for (int k = 0; k < 3; k++) headSum[k] = __ldg(a.head.b + k);
                 }
+                // Up to kGroup chunks of 16 columns loaded before one wait,
+                // then finished and stored.
 #pragma unroll
-                for (int c = chunk0; c < chunk0 + kChunks; c++) {
-                    uint32_t r[16];
-                    tmemLoad16(taddr + (uint32_t)(16 * c), r);
+                for (int g = 0; g < kChunks; g += kGroup) {
+                    uint32_t r[kGroup][16];
+#pragma unroll
+                    for (int c = 0; c < kGroup; c++) tmemLoad16(taddr + (uint32_t)(16 * (chunk0 + g + c)), r[c]);
                     tmemWaitLoads();
-                    if (x < a.w) epilogueStore16<COUT>(a, r, pix, 16 * c, nBase, sBias, up, headSum);
+#pragma unroll
+                    for (int c = 0; c < kGroup; c++)
+                        if (x < a.w) epilogueStore16<COUT>(a, r[c], pix, 16 * (chunk0 + g + c), nBase, sBias, up, headSum, sHead);
                 }
                 if (a.head.out && x < a.head.w && y < a.head.h) {
                     float* o = a.head.out + ((size_t)y * a.head.w + x) * 3;
@@ -960,7 +989,7 @@ cudaError_t convPipe(const bf16* in, const bf16* low, int lowChannels, int n, in
         (upAddend && (h % 2 || w % 2 || lowChannels || coutTotal > 64)) || (planarOut && (!outB || outF || head)))
         return cudaErrorNotSupported;
     const int nSplits = pickSplits(cin, coutTotal, lowChannels);
-    if (head && nSplits != 1) return cudaErrorNotSupported;  // the head sums over all output channels of a pixel
+    if (head && (nSplits != 1 || coutTotal > 32)) return cudaErrorNotSupported;  // one pixel's channels in one thread
     const int cout = coutTotal / nSplits;  // output channels per block
     const int cinIn = cin - lowChannels;
     // convPipeReference(): tap-per-tile issue over rows staged as planes, the

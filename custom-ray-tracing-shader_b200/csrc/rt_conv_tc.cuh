@@ -86,8 +86,6 @@ cudaError_t combineUpsampledWeights(const __nv_bfloat16* weights, int cout, int 
 // Whether the two-pass form runs on the pipelined kernel for this layer.
 bool upsampledSplitSupported(int cin, int cout, int lowChannels);
 
-// Which kernel convTc runs: 0 (default) the pipelined form wherever it
-// applies, 1 always the kernel above (process-wide; for comparisons).
 // Rows per strip for kernels whose blocks walk (image, column tile, strip)
 // units: the length (1-64 rows) that minimises the rows the busiest of
 // `blocks` blocks stages, ceil(units / blocks) strips of s + 2 rows each (a
@@ -104,6 +102,8 @@ inline int balancedStripRows(long long columns, int h, long long blocks) {
     return best;
 }
 
+// Which kernel convTc runs: 0 (default) the pipelined form wherever it
+// applies, 1 always the kernel above (process-wide; for comparisons).
 void setConvPath(int mode);
 int convPath();
 // The pipelined kernel's reference form (default off): every layer's MMAs
