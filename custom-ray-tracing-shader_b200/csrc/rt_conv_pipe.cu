@@ -518,6 +518,18 @@ __global__ void __launch_bounds__(pipeThreads(ISS, EPI), ISS > 1 ? 1 : (COUT <= 
         *abortFlag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
+    if (threadIdx.x >> 5 == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(base + Header::tmemSlot),
+                     "r"(a.tmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+    }
+    // Programmatic dependent launch (the host launches with it): the next
+    // kernel in the stream may start its own setup now; this block waits for
+    // the previous kernel to complete before any read of global memory
+    // (input rows, weights, bias, addend, the accumulated output).
+    asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+    asm volatile("griddepcontrol.wait;\n" ::: "memory");
     float* sBias = reinterpret_cast<float*>(smem + Header::bias);
     for (int c = threadIdx.x; c < COUT; c += blockDim.x) sBias[c] = a.bias ? a.bias[nBase + c] : 0.0f;
     const float4* sHead = reinterpret_cast<const float4*>(smem + Header::head);
@@ -525,12 +537,6 @@ __global__ void __launch_bounds__(pipeThreads(ISS, EPI), ISS > 1 ? 1 : (COUT <= 
         for (int c = threadIdx.x; c < COUT && c < 32; c += blockDim.x)
             reinterpret_cast<float4*>(smem + Header::head)[c] =
                 make_float4(a.head.wt[c * 3], a.head.wt[c * 3 + 1], a.head.wt[c * 3 + 2], 0.0f);
-    if (threadIdx.x >> 5 == 1) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(base + Header::tmemSlot),
-                     "r"(a.tmemCols)
-                     : "memory");
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
-    }
     tcFenceBefore();
     __syncthreads();
     tcFenceAfter();
@@ -933,8 +939,20 @@ cudaError_t launchPipe(const CUtensorMap& inMap, const CUtensorMap& lowMap, cons
         if (e != cudaSuccess) return e;
         configured = true;
     }
-    convPipeKernel<COUT, ISS, STACK, EPI><<<grid, pipeThreads(ISS, EPI), smemBytes, stream>>>(inMap, lowMap, wMap, a);
-    return cudaGetLastError();
+    // Programmatic stream serialization: the kernel's setup may overlap the
+    // previous kernel's tail (it waits with griddepcontrol.wait before
+    // reading anything that kernel wrote).
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)pipeThreads(ISS, EPI));
+    cfg.dynamicSmemBytes = smemBytes;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, convPipeKernel<COUT, ISS, STACK, EPI>, inMap, lowMap, wMap, a);
 }
 
 }  // namespace
