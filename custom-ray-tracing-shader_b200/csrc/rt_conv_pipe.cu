@@ -517,6 +517,21 @@ __global__ void __launch_bounds__(pipeThreads(ISS, EPI), ISS > 1 ? 1 : (COUT <= 
         barInit(base + Header::probe, 1);
         *abortFlag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        // The weights, once per block, before the wait for the previous
+        // kernel below: no convolution's weights are written by the kernel
+        // launched just before it (they come from initialisation, the
+        // optimiser or the merge of the two-pass form, each launched without
+        // programmatic dependence, so complete before this kernel starts).
+        // Tap-major ([tap][plane][cout][8]), or for the stacked form
+        // [dx][plane][2 - dy][cout][8]. This thread is the producer's lane 0.
+        asm volatile("prefetch.tensormap [%0];\n" ::"l"(&wMap) : "memory");
+        const uint32_t wb = pb + Header::weightsFull;
+        barExpectTx(wb, a.weightBytes);
+        for (int t = 0; t < 9; t++)
+            for (int g = 0; g < G; g++) {
+                const int region = STACK ? ((t % 3) * G + g) * 3 + 2 - t / 3 : t * G + g;
+                tmaLoad3(wAddr + (uint32_t)(region * COUT * 16), &wMap, g * 8, nBase, a.reverseTaps ? 8 - t : t, wb);
+            }
     }
     if (threadIdx.x >> 5 == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(base + Header::tmemSlot),
@@ -526,8 +541,8 @@ __global__ void __launch_bounds__(pipeThreads(ISS, EPI), ISS > 1 ? 1 : (COUT <= 
     }
     // Programmatic dependent launch (the host launches with it): the next
     // kernel in the stream may start its own setup now; this block waits for
-    // the previous kernel to complete before any read of global memory
-    // (input rows, weights, bias, addend, the accumulated output).
+    // the previous kernel to complete before any other read of global memory
+    // (input rows, bias, addend, the accumulated output).
     asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
     asm volatile("griddepcontrol.wait;\n" ::: "memory");
     float* sBias = reinterpret_cast<float*>(smem + Header::bias);
@@ -547,19 +562,6 @@ __global__ void __launch_bounds__(pipeThreads(ISS, EPI), ISS > 1 ? 1 : (COUT <= 
         if (lane == 0) {
             asm volatile("prefetch.tensormap [%0];\n" ::"l"(&inMap) : "memory");
             if (Glow) asm volatile("prefetch.tensormap [%0];\n" ::"l"(&lowMap) : "memory");
-            asm volatile("prefetch.tensormap [%0];\n" ::"l"(&wMap) : "memory");
-            // The weights, once per block: tap-major ([tap][plane][cout][8]),
-            // or for the stacked form [dx][plane][2 - dy][cout][8].
-            const uint32_t wb = pb + Header::weightsFull;
-            {
-                barExpectTx(wb, a.weightBytes);
-                for (int t = 0; t < 9; t++)
-                    for (int g = 0; g < G; g++) {
-                        const int region = STACK ? ((t % 3) * G + g) * 3 + 2 - t / 3 : t * G + g;
-                        tmaLoad3(wAddr + (uint32_t)(region * COUT * 16), &wMap, g * 8, nBase,
-                                 a.reverseTaps ? 8 - t : t, wb);
-                    }
-            }
         }
         // Rows are numbered in issue order q; row q sits in slot q % R, its
         // low-resolution part (concatenated input) in staging buffer
